@@ -1,0 +1,300 @@
+"""Flat-terrain preparation of a prognostic solve (host side, numpy).
+
+Restates what GRAL computes before it calls ``PrognosticFlowfield.Calculate()`` on flat terrain:
+
+* the stretched vertical grid, ``GenerateVerticalGridFlat`` (ProgramFunctions.cs:27-77) with
+  ``HOKART[1] = DZK[1]`` (ProgramFunctions.cs:552), in float32 as the reference;
+* the surface index KKART from the building heights and KADVMAX (MicroscaleFlat.cs:56-197);
+* the prognostic sub-domain mask ADVDOM (ReadGeometryAndDomains.cs:321-347);
+* the reference point of the sub-domains (MicroscaleTerrainSearchRefPoint.cs:27-100);
+* the initial wind field, zero inside obstacles with the same face rules as
+  MicroscaleFlat.cs:83-185.  The vertical profile is a neutral log law scaled to a given speed at
+  10 m instead of GRAL's measured-profile power law; both the CUDA solver and the oracle start
+  from this same field.
+
+Synthetic inputs only: buildings, inflow and stability are seeded, there is no file IO.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+from .abi import FieldArrays, StaticArrays
+
+F32 = np.float32
+
+
+def vertical_grid_flat(dz1: float, stretch: float, top: float = 800.0,
+                       max_bound: int = 2048) -> Tuple[int, np.ndarray, np.ndarray]:
+    """DZK, HOKART of the flat-terrain grid; returns (NKK, dzk[NKK+2], hokart[NKK+2])."""
+    dzk = np.zeros(max_bound, dtype=F32)
+    hok = np.zeros(max_bound, dtype=F32)
+    dzk[1] = F32(dz1)
+    hok[1] = dzk[1]
+    s = F32(stretch)
+    nkk = 0
+    for i in range(2, max_bound):
+        dzk[i] = F32(dzk[i - 1] * s)
+        hok[i] = F32(hok[i - 1] + dzk[i])
+        if hok[i] >= top:
+            nkk = i
+            break
+    nkk = min(nkk, max_bound - 2)
+    return nkk, dzk[: nkk + 2].copy(), hok[: nkk + 2].copy()
+
+
+@dataclass
+class Building:
+    i0: int   # first 1-based cell index in x
+    i1: int   # last cell index in x (inclusive)
+    j0: int
+    j1: int
+    height: float
+
+
+@dataclass
+class Situation:
+    """One weather situation: inflow direction/speed/roughness and stability."""
+    direction_deg: float = 270.0   # meteorological: wind blowing FROM this direction
+    speed_10m: float = 3.0
+    z0: float = 0.2
+    ustar: float = 0.3
+    obukhov: float = 1000.0        # > 0 stable/neutral, < 0 unstable
+    potdtdz: float = 0.0
+
+
+@dataclass
+class Domain:
+    """Everything a solve needs except the per-situation fields."""
+    nii: int
+    njj: int
+    nkk: int
+    dxk: float
+    dyk: float
+    vert_cells_ff: int
+    kadvmax: int
+    ref: Tuple[int, int]
+    static: StaticArrays
+    buildings: List[Building] = field(default_factory=list)
+
+    @property
+    def cols(self) -> int:
+        return (self.nii + 2) * (self.njj + 2)
+
+    def params(self, situation: Optional[Situation] = None, *, model: int = 1, iterations: int = 100,
+               iter_min: Optional[int] = None, simd_width: int = 8, quantise: int = 1,
+               conv_cadence: int = 100, conv_threshold: float = 0.012, latitude: float = 47.0,
+               relax: float = 0.1, relaxp: float = 1.0, building_z0: float = 0.001) -> dict:
+        sit = situation or Situation()
+        cor = float(F32(2 * 7.29 * 0.00001 * math.sin(abs(latitude) * 3.1415 / 180)))
+        return dict(
+            nii=self.nii, njj=self.njj, nkk=self.nkk, kadvmax=self.kadvmax,
+            vert_cells_ff=self.vert_cells_ff, dxk=self.dxk, dyk=self.dyk,
+            turbulence_model=model, simd_width=simd_width,
+            iteration_steps_min=iterations if iter_min is None else iter_min,
+            iteration_steps_max=iterations, conv_cadence=conv_cadence,
+            conv_threshold=conv_threshold, relax=relax, relaxp=relaxp,
+            building_z0=building_z0, coriolis=cor, potdtdz=sit.potdtdz,
+            ref_i=self.ref[0], ref_j=self.ref[1], quantise=quantise, turb_init=0,
+            std_dev_v=1.0, std_dev_w=1.0, bd_lay_height=1000.0, v0_1=float(F32(2.0 * sit.ustar)))
+
+
+def rasterise(nii: int, njj: int, buildings: List[Building]) -> np.ndarray:
+    cutk = np.zeros((nii + 2, njj + 2), dtype=F32)
+    for b in buildings:
+        cutk[b.i0:b.i1 + 1, b.j0:b.j1 + 1] = np.maximum(cutk[b.i0:b.i1 + 1, b.j0:b.j1 + 1], F32(b.height))
+    return cutk
+
+
+def kkart_from_cutk(cutk: np.ndarray, dzk: np.ndarray, hokart: np.ndarray, nkk: int) -> np.ndarray:
+    """KKART = highest k whose cell centre HOKART[k-1] + DZK[k]/2 lies at or below CUTK
+    (MicroscaleFlat.cs:86-87, 168-176)."""
+    vertk = (hokart[0:nkk] + dzk[1:nkk + 1] * F32(0.5)).astype(F32)   # index k-1 -> level k
+    below = vertk[None, None, :] <= cutk[:, :, None]
+    kk = np.where(below.any(axis=2), nkk - np.argmax(below[:, :, ::-1], axis=2), 0)
+    return kk.astype(np.int16)
+
+
+def advdom_from_cutk(cutk: np.ndarray, nii: int, njj: int, dxk: float, dyk: float,
+                     factor: int = 15) -> np.ndarray:
+    """Prognostic sub-domains around every building cell (ReadGeometryAndDomains.cs:321-347)."""
+    adv = np.zeros_like(cutk, dtype=np.uint8)
+    ii, jj = np.nonzero(cutk[1:nii + 1, 1:njj + 1] > 0)
+    for i, j in zip(ii + 1, jj + 1):
+        h = cutk[i, j]
+        ip = int(F32(factor) * h / F32(dxk))
+        jp = int(F32(factor) * h / F32(dyk))
+        adv[max(1, i - ip):min(nii, i + ip) + 1, max(1, j - jp):min(njj, j + jp) + 1] = 1
+    return adv
+
+
+def search_reference_point(adv: np.ndarray) -> Tuple[int, int]:
+    """Spiral search from the border inwards (MicroscaleTerrainSearchRefPoint.cs:27-100)."""
+    xmax, ymax = adv.shape
+    searchmax = min(xmax, ymax) // 2
+    delta = 1
+    i = j = 1
+    found = False
+    while not found and delta < searchmax:
+        i = j = delta
+        while j < ymax - delta and not found:
+            if adv[i, j] == 1:
+                found = True
+            else:
+                j += 1
+        while i < xmax - delta and not found:
+            if adv[i, j] == 1:
+                found = True
+            else:
+                i += 1
+        while j > delta and not found:
+            if adv[i, j] == 1:
+                found = True
+            else:
+                j -= 1
+        while i > delta and not found:
+            if adv[i, j] == 1:
+                found = True
+            else:
+                i -= 1
+        delta += 1
+    if not found:
+        return (1, 1)
+    return (i, j)
+
+
+def make_domain(nii: int, njj: int, dxk: float, dz1: float, stretch: float, vert_cells_ff: int,
+                buildings: List[Building], *, dyk: Optional[float] = None, z0: float = 0.2,
+                ustar: float = 0.3, obukhov: float = 1000.0, subdomain_factor: int = 15,
+                veg: Optional[np.ndarray] = None, cov: Optional[np.ndarray] = None,
+                top: float = 800.0) -> Domain:
+    dyk = dxk if dyk is None else dyk
+    nkk, dzk, hok = vertical_grid_flat(dz1, stretch, top=top)
+    cutk = rasterise(nii, njj, buildings)
+    kkart = kkart_from_cutk(cutk, dzk, hok, nkk)
+    kmax_b = int(kkart[cutk > 0].max()) if (cutk > 0).any() else 1
+    kadvmax = min(nkk, max(1, kmax_b) + vert_cells_ff)
+    adv = advdom_from_cutk(cutk, nii, njj, dxk, dyk, subdomain_factor)
+    shape2 = (nii + 2, njj + 2)
+    st = StaticArrays(
+        kkart=kkart, advdom=adv, cutk=cutk,
+        cov=np.zeros(shape2, F32) if cov is None else cov.astype(F32),
+        z0=np.full(shape2, F32(z0)), z0_init=np.full(shape2, F32(z0)),
+        ob_init=np.full(shape2, F32(obukhov)), ust_init=np.full(shape2, F32(ustar)),
+        dzk=dzk, hokart=hok)
+    if veg is not None:
+        st.veg = np.ascontiguousarray(veg, dtype=F32)
+        st.veg_mask = (st.veg.max(axis=2) > 0).astype(np.uint8)
+    ref = search_reference_point(adv)
+    return Domain(nii, njj, nkk, dxk, dyk, vert_cells_ff, kadvmax, ref, st, buildings)
+
+
+def log_profile(z: np.ndarray, speed_10m: float, z0: float) -> np.ndarray:
+    return speed_10m * np.maximum(np.log(np.maximum(z, 1e-6) / z0), 0.0) / math.log(10.0 / z0)
+
+
+def initial_fields(dom: Domain, sit: Situation, model: int = 1) -> FieldArrays:
+    """Initial UK/VK/WK (and TURB/TDISS buffers) with the obstacle rules of MicroscaleFlat.cs."""
+    nii, njj, nkk = dom.nii, dom.njj, dom.nkk
+    st = dom.static
+    shape = (nii + 2, njj + 2, nkk + 2)
+    uk = np.zeros(shape, F32)
+    vk = np.zeros(shape, F32)
+    wk = np.zeros(shape, F32)
+    vertk = np.zeros(nkk + 2, F32)
+    vertk[1:nkk + 1] = st.hokart[0:nkk] + st.dzk[1:nkk + 1] * F32(0.5)
+    sp = log_profile(vertk.astype(np.float64), sit.speed_10m, sit.z0)
+    th = math.radians(sit.direction_deg)
+    u = (-sp * math.sin(th)).astype(F32)
+    v = (-sp * math.cos(th)).astype(F32)
+    u[0] = v[0] = 0
+    u[nkk + 1] = v[nkk + 1] = 0
+    cut = st.cutk
+    inside = vertk[None, None, :] <= cut[:, :, None]             # cell (i,j,k) inside an obstacle
+    inside[..., 0] = False
+    inside[..., nkk + 1] = False
+    uk[1:nii + 1, 1:njj + 1, :] = u
+    vk[1:nii + 1, 1:njj + 1, :] = v
+    # zero inside obstacles and on faces shared with an obstacle cell
+    uk[inside] = 0
+    vk[inside] = 0
+    uk[2:nii + 1][inside[1:nii]] = 0                              # west neighbour is an obstacle
+    vk[:, 2:njj + 1][inside[:, 1:njj]] = 0                        # south neighbour is an obstacle
+    uk[nii + 1, 1:njj + 1, :] = uk[nii, 1:njj + 1, :]
+    vk[1:nii + 1, njj + 1, :] = vk[1:nii + 1, njj, :]
+    uk[..., 0] = 0
+    vk[..., 0] = 0
+    turb = tdiss = None
+    if model != 1:
+        turb = np.zeros(shape, F32)
+        tdiss = np.zeros(shape, F32)
+    return FieldArrays(uk, vk, wk, turb, tdiss)
+
+
+# --------------------------------------------------------------------------------------------
+# Named workloads
+# --------------------------------------------------------------------------------------------
+
+def cube_domain(n: int = 100, dx: float = 2.0, dz1: float = 2.0, stretch: float = 1.01,
+                vert_cells_ff: int = 20, size_m: float = 20.0, height: float = 20.0,
+                **kw) -> Domain:
+    """One cube building at the domain centre (100x100x20 at 2 m, 20 m cube by default)."""
+    nb = int(round(size_m / dx))
+    c0 = n // 2 - nb // 2 + 1
+    b = Building(c0, c0 + nb - 1, c0, c0 + nb - 1, height)
+    return make_domain(n, n, dx, dz1, stretch, vert_cells_ff, [b], **kw)
+
+
+def random_buildings(nii: int, njj: int, dx: float, count: int, seed: int,
+                     foot_m: Tuple[float, float] = (10.0, 40.0),
+                     height_m: Tuple[float, float] = (10.0, 30.0), margin_cells: int = 6,
+                     gap_cells: int = 2) -> List[Building]:
+    """Non-overlapping rectangles by rejection sampling (seeded numpy PCG64)."""
+    rng = np.random.default_rng(seed)
+    occ = np.zeros((nii + 2, njj + 2), dtype=bool)
+    out: List[Building] = []
+    tries = 0
+    while len(out) < count and tries < 200000:
+        tries += 1
+        wx = int(round(rng.uniform(*foot_m) / dx))
+        wy = int(round(rng.uniform(*foot_m) / dx))
+        wx, wy = max(wx, 1), max(wy, 1)
+        i0 = int(rng.integers(1 + margin_cells, nii - margin_cells - wx + 1))
+        j0 = int(rng.integers(1 + margin_cells, njj - margin_cells - wy + 1))
+        a0, a1 = max(1, i0 - gap_cells), min(nii, i0 + wx - 1 + gap_cells)
+        b0, b1 = max(1, j0 - gap_cells), min(njj, j0 + wy - 1 + gap_cells)
+        if occ[a0:a1 + 1, b0:b1 + 1].any():
+            continue
+        occ[i0:i0 + wx, j0:j0 + wy] = True
+        h = float(F32(rng.uniform(*height_m)))
+        out.append(Building(i0, i0 + wx - 1, j0, j0 + wy - 1, h))
+    return out
+
+
+def city_domain(n: int = 400, dx: float = 2.0, dz1: float = 2.0, stretch: float = 1.05,
+                vert_cells_ff: int = 30, n_buildings: int = 64, seed: int = 2, **kw) -> Domain:
+    """Production-size grid: 400x400 cells at 2 m, 64 seeded buildings, 10-30 m tall."""
+    bl = random_buildings(n, n, dx, n_buildings, seed)
+    return make_domain(n, n, dx, dz1, stretch, vert_cells_ff, bl, **kw)
+
+
+def small_domain(nii: int = 16, njj: int = 14, seed: int = 0, n_buildings: int = 3,
+                 vert_cells_ff: int = 12, stretch: float = 1.05, dx: float = 2.0,
+                 with_veg: bool = False, **kw) -> Domain:
+    """Small seeded test grid with a few buildings of mixed heights (and optional vegetation)."""
+    rng = np.random.default_rng(1000 + seed)
+    bl = random_buildings(nii, njj, dx, n_buildings, seed, foot_m=(4.0, 8.0), height_m=(3.0, 16.0),
+                          margin_cells=3, gap_cells=1)
+    veg = cov = None
+    if with_veg:
+        nkk, _, _ = vertical_grid_flat(2.0, stretch)
+        veg = np.zeros((nii + 2, njj + 2, nkk + 2), F32)
+        cov = np.zeros((nii + 2, njj + 2), F32)
+        for _ in range(3):
+            i = int(rng.integers(3, nii - 2)); j = int(rng.integers(3, njj - 2))
+            veg[i - 1:i + 2, j - 1:j + 2, 1:6] = F32(rng.uniform(0.05, 0.5))
+            cov[i - 1:i + 2, j - 1:j + 2] = F32(rng.uniform(0.2, 0.9))
+    return make_domain(nii, njj, dx, 2.0, stretch, vert_cells_ff, bl, veg=veg, cov=cov, **kw)

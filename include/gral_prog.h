@@ -1,0 +1,156 @@
+/*
+ * gral_prog.h -- C ABI of the B200 prognostic microscale flow solver.
+ *
+ * Drop-in for GRAL's `PrognosticFlowfield.Calculate()` (PrognosticFlowfield.cs:32),
+ * which MicroscaleFlat.Calculate (MicroscaleFlat.cs:381) and MicroscaleTerrain.Calculate
+ * (MicroscaleTerrain.cs:847) call once per weather situation.  The reference method takes no
+ * arguments and works on `Program.*` statics; this ABI passes the same data explicitly:
+ *
+ *   gral_params  -- the scalars the reference reads from Program.* and from the control files
+ *                   (turbulence_model.txt, Integrationtime.txt, relaxation_factors.txt,
+ *                   building_roughness.txt, in.dat flags), PrognosticFlowfield.cs:147-291.
+ *   gral_static  -- per-grid arrays that do not change during a solve (KKART, ADVDOM, CUTK, COV,
+ *                   VEG, DZK, HOKART, roughness), ProgramDeclarations.cs:84-92, 456-484.
+ *   gral_fields  -- the wind (and k-eps) fields read and written by the solve: UK, VK, WK,
+ *                   TURB, TDISS, ProgramDeclarations.cs:432-440, 464-468.
+ *
+ * Host layout of every 3-D array: [NII+2][NJJ+2][NKK+2] float, k fastest, indices as in the
+ * reference (1-based i, j, k; UK on west faces, VK on south faces, WK on bottom faces), so a
+ * jagged `float[][][]` row of the reference maps to one contiguous run of NKK+2 floats.
+ * 2-D per-column arrays are [NII+2][NJJ+2], j fastest.
+ *
+ * All functions return GRAL_OK (0) or a negative GRAL_E* code; nothing aborts or throws across
+ * the ABI.  A context is used by one host thread at a time; calls are synchronous.  Signatures
+ * hold only pointers, integers, floats and POD structs (blittable for P/Invoke under
+ * DisableRuntimeMarshalling, GRAL.csproj:23).
+ */
+#ifndef GRAL_PROG_H
+#define GRAL_PROG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRAL_PROG_ABI_VERSION 1
+
+#define GRAL_OK 0
+#define GRAL_EINVAL (-1)     /* bad dimensions, pointers or parameters */
+#define GRAL_ENOMEM (-2)     /* device or host allocation failed / batch exceeds capacity */
+#define GRAL_ECUDA (-3)      /* CUDA runtime error (text via gral_prog_last_error) */
+#define GRAL_ETIMEDOUT (-4)  /* a bounded device-side wait gave up */
+#define GRAL_ENONFINITE (-5) /* non-finite value in the solved fields */
+#define GRAL_ENODEV (-6)     /* no usable CUDA device */
+#define GRAL_ESTATE (-7)     /* call out of order (e.g. store before load) */
+
+/* Solver scalars.  Defaults in brackets are the reference defaults. */
+typedef struct gral_params {
+    int32_t nii, njj, nkk;        /* Program.NII/NJJ/NKK */
+    int32_t kadvmax;              /* Program.KADVMAX (MicroscaleFlat.cs:196) */
+    int32_t vert_cells_ff;        /* Program.VertCellsFF (micro_vert_layers.txt) */
+    float dxk, dyk;               /* Program.DXK/DYK */
+    int32_t turbulence_model;     /* 0 no diffusion, 1 mixing length [1], 2 k-eps */
+    int32_t simd_width;           /* model-1 parity width: 8 = Vector<float> path [8] */
+    int32_t iteration_steps_min;  /* [100] Integrationtime.txt line 1 */
+    int32_t iteration_steps_max;  /* [500] Integrationtime.txt line 2 */
+    int32_t conv_cadence;         /* [100] convergence test every this many iterations */
+    double conv_threshold;        /* [0.012] DeltaMean / topwind^2 threshold */
+    float relax, relaxp;          /* [0.1, 1] relaxation_factors.txt */
+    float building_z0;            /* [0.001] building_roughness.txt */
+    float coriolis;               /* Program.CorolisParam */
+    float potdtdz;                /* Program.PotdTdz (k-eps buoyancy) */
+    int32_t ref_i, ref_j;         /* Program.SubDomainRefPos */
+    int32_t quantise;             /* [1] Frund rounding as the reference; 0 switches it off */
+    int32_t turb_init;            /* model != 1: 0 = initialise TURB/TDISS as the reference's
+                                     default meteo branch (PrognosticFlowfield.cs:410-510);
+                                     1 = take TURB/TDISS from gral_fields as given */
+    float std_dev_v, std_dev_w;   /* Program.StdDeviationV/W [1, 1] */
+    float bd_lay_height;          /* Program.BdLayHeight */
+    float v0_1;                   /* Program.V0[1] (sigma_v used by the TURB initialisation) */
+} gral_params;
+
+/* Per-grid inputs; shared by all situations of a batch. */
+typedef struct gral_static {
+    const int16_t *kkart;     /* Program.KKART   [NII+2][NJJ+2] */
+    const uint8_t *advdom;    /* Program.ADVDOM  [NII+2][NJJ+2] (prognostic sub-domain mask) */
+    const float *cutk;        /* Program.CUTK    [NII+2][NJJ+2] (building height above ground) */
+    const float *cov;         /* Program.COV     [NII+2][NJJ+2] (vegetation cover) */
+    const float *z0;          /* roughness the momentum/TKE wall laws look up per column
+                                 (Z0Gramm[IUstern][JUstern] or Z0Gral[i][j]) [NII+2][NJJ+2] */
+    const float *z0_init;     /* roughness of the TURB initialisation per column (model != 1) */
+    const float *ob_init;     /* Obukhov length of the TURB initialisation per column */
+    const float *ust_init;    /* friction velocity of the TURB initialisation per column */
+    const float *veg;         /* Program.VEG [NII+2][NJJ+2][NKK+2], or NULL */
+    const uint8_t *veg_mask;  /* 1 where Program.VEG[i][j] is not null; NULL = no vegetation */
+    const float *dzk;         /* Program.DZK    [NKK+2] */
+    const float *hokart;      /* Program.HOKART [NKK+2] */
+} gral_static;
+
+/* Per-situation fields, read and written in place. */
+typedef struct gral_fields {
+    float *uk, *vk, *wk;      /* [NII+2][NJJ+2][NKK+2] */
+    float *turb, *tdiss;      /* same layout; required when turbulence_model != 1, else NULL */
+} gral_fields;
+
+#define GRAL_MAX_HISTORY 64
+
+typedef struct gral_stats {
+    int32_t iterations;          /* SIMPLE iterations executed */
+    int32_t iteration_loops;     /* value of IterationLoops printed by the reference at exit */
+    int32_t converged;           /* 1 if the cadence test stopped the loop */
+    int32_t convergence_problem; /* DeltaFinish > DeltaFirst (PrognosticFlowfield.cs:1187) */
+    double delta_first, delta_finish;
+    int32_t n_history;
+    double delta_history[GRAL_MAX_HISTORY];   /* _delta at each cadence test */
+    int32_t uk_unrealistic, vk_unrealistic, wk_unrealistic;  /* PrognosticFlowfield.cs:1193 */
+    double geschw_max;           /* GESCHW_MAX */
+    float topwind, dtime;
+    double frund;
+    float last_delta_umax;
+    float *trace_delta_umax;     /* optional, caller-owned: DeltaUMax per iteration */
+    int32_t trace_capacity;
+    double ms_total, ms_upload, ms_iterate, ms_download;
+} gral_stats;
+
+typedef struct gral_ctx gral_ctx;
+
+/* Library version (GRAL_PROG_ABI_VERSION). */
+int gral_prog_version(void);
+
+/* Create a context for grids up to nii x njj x nkk and up to max_batch situations solved
+ * together.  Replaces the reference's lazy allocation of UKS/VKS/WKS/DPMNEW
+ * (PrognosticFlowfield.cs:45-103). */
+int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax,
+                     int32_t max_batch, gral_ctx **out);
+
+/* One situation: PrognosticFlowfield.Calculate() (PrognosticFlowfield.cs:32-1245).  Reads
+ * `fields`, runs the SIMPLE loop to convergence or iteration_steps_max, writes the fields back.
+ * `stats` may be NULL. */
+int gral_prog_solve(gral_ctx *ctx, const gral_params *p, const gral_static *s,
+                    gral_fields *f, gral_stats *stats);
+
+/* n situations on the same grid, each with its own params and fields, solved together with a
+ * per-situation convergence mask.  p, f and stats are arrays of length n (stats may be NULL). */
+int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s,
+                          gral_fields *f, gral_stats *stats);
+
+/* Split form of gral_prog_solve_batch for callers that keep fields resident on the device:
+ * load copies inputs to HBM and runs the set-up, iterate runs the SIMPLE loop on the loaded
+ * situations, store copies results back.  solve_batch = load + iterate + store. */
+int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s,
+                   gral_fields *f);
+int gral_prog_iterate(gral_ctx *ctx);
+int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats);
+
+/* Text of the last error on this context (never NULL). */
+const char *gral_prog_last_error(gral_ctx *ctx);
+
+/* Release the context and its device memory. */
+void gral_prog_destroy(gral_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAL_PROG_H */

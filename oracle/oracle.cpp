@@ -1,0 +1,477 @@
+/*
+ * oracle.cpp -- TEST INFRASTRUCTURE ONLY (CPU oracle, see oracle_common.h).
+ *
+ * Restates PrognosticFlowfield.Calculate() (PrognosticFlowfield.cs:32-1245) in its deterministic
+ * form: set-up (:45-579), the SIMPLE iteration loop (:583-1182) and the post-checks
+ * (:1187-1245).  Exported as oracle_solve() with the same argument structs as the product's
+ * gral_prog_solve(), so tests feed both the same inputs.
+ */
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "oracle_common.h"
+
+using namespace oracle;
+
+namespace {
+
+int validate(const gral_params *p, const gral_static *s, const gral_fields *f) {
+    if (!p || !s || !f || !f->uk || !f->vk || !f->wk) return GRAL_EINVAL;
+    if (p->nii < 4 || p->njj < 4 || p->nkk < 3) return GRAL_EINVAL;
+    if (!s->kkart || !s->advdom || !s->cutk || !s->z0 || !s->dzk || !s->hokart) return GRAL_EINVAL;
+    if (p->turbulence_model < 0 || p->turbulence_model > 2) return GRAL_EINVAL;
+    if (p->turbulence_model == 1 && p->simd_width != 8) return GRAL_EINVAL;
+    if (p->turbulence_model != 1 && (!f->turb || !f->tdiss)) return GRAL_EINVAL;
+    if (p->turbulence_model != 1 && p->turb_init == 0 &&
+        (!s->z0_init || !s->ob_init || !s->ust_init)) return GRAL_EINVAL;
+    if (p->conv_cadence < 1) return GRAL_EINVAL;
+    return GRAL_OK;
+}
+
+/* Lateral boundary conditions at the west/east and south/north borders of the prognostic
+ * sub-domains (PrognosticFlowfield.cs:595-696) and at the top (:699-714). */
+void boundary_conditions(State &st) {
+    const int NII = st.nii, NJJ = st.njj;
+    for (int j = 2; j < NJJ + 1; ++j) {
+        for (int i = 3; i < NII; ++i) {
+            if (st.advdom(i, j) != 1) continue;
+            const int VI = st.vert_index[st.i2(i, j)];
+            const bool iM = (st.advdom(i - 1, j) < 1) || (i == 3);
+            const bool iP = (st.advdom(i + 1, j) < 1) || (i == NII - 1);
+            if (iM) {
+                for (int k = 1; k <= VI; ++k) {
+                    float u = st.uk[st.i3(i - 2, j, k)];
+                    if (u >= 0) st.uk[st.i3(i - 1, j, k)] = u;
+                    st.vk[st.i3(i - 2, j, k)] = st.vk[st.i3(i - 1, j, k)];
+                    st.wk[st.i3(i - 2, j, k)] = st.wk[st.i3(i - 1, j, k)];
+                }
+            }
+            if (iP) {
+                for (int k = 1; k <= VI; ++k) {
+                    float u = st.uk[st.i3(i + 2, j, k)];
+                    if (u <= 0) st.uk[st.i3(i + 1, j, k)] = u;
+                    st.vk[st.i3(i + 1, j, k)] = st.vk[st.i3(i, j, k)];
+                    st.wk[st.i3(i + 1, j, k)] = st.wk[st.i3(i, j, k)];
+                }
+            }
+        }
+    }
+    for (int i = 2; i < NII + 1; ++i) {
+        for (int j = 3; j <= NJJ - 1; ++j) {
+            if (st.advdom(i, j) != 1) continue;
+            const int VI = st.vert_index[st.i2(i, j)];
+            const bool jM = (st.advdom(i, j - 1) < 1) || (j == 3);
+            const bool jP = (st.advdom(i, j + 1) < 1) || (j == NJJ - 1);
+            if (jM) {
+                for (int k = 1; k <= VI; ++k) {
+                    float v = st.vk[st.i3(i, j - 2, k)];
+                    if (v >= 0) st.vk[st.i3(i, j - 1, k)] = v;
+                    st.uk[st.i3(i, j - 2, k)] = st.uk[st.i3(i, j - 1, k)];
+                    st.wk[st.i3(i, j - 2, k)] = st.wk[st.i3(i, j - 1, k)];
+                }
+            }
+            if (jP) {
+                for (int k = 1; k <= VI; ++k) {
+                    float v = st.vk[st.i3(i, j + 2, k)];
+                    if (v <= 0) st.vk[st.i3(i, j + 1, k)] = v;
+                    st.uk[st.i3(i, j + 1, k)] = st.uk[st.i3(i, j, k)];
+                    st.wk[st.i3(i, j + 1, k)] = st.wk[st.i3(i, j, k)];
+                }
+            }
+        }
+    }
+    for (int i = 2; i < NII; ++i) {
+        for (int j = 2; j <= NJJ - 1; ++j) {
+            if (st.advdom(i, j) != 1) continue;
+            const int k = st.vert_index[st.i2(i, j)];
+            st.wk[st.i3(i, j, k + 1)] = st.wk[st.i3(i, j, k)];
+            st.uk[st.i3(i, j, k + 1)] = st.uk[st.i3(i, j, k)];
+            st.vk[st.i3(i, j, k + 1)] = st.vk[st.i3(i, j, k)];
+        }
+    }
+}
+
+/* Round to multiples of 1/Frund in double (PrognosticFlowfield.cs:880, 930-940). */
+inline double quant(double x, double Frund, bool on) {
+    if (!on) return x;
+    return conv_to_int(x * Frund) / Frund;
+}
+
+}  // namespace
+
+extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fields *f,
+                            gral_stats *stats) {
+    int rc = validate(p, s, f);
+    if (rc != GRAL_OK) return rc;
+
+    State st;
+    st.p = p; st.s = s;
+    st.nii = p->nii; st.njj = p->njj; st.nkk = p->nkk;
+    st.kadvmax = p->kadvmax; st.vcff = p->vert_cells_ff;
+    st.ni2 = p->nii + 2; st.nj2 = p->njj + 2; st.nk2 = p->nkk + 2;
+    st.dxk = p->dxk; st.dyk = p->dyk;
+    const size_t n3 = (size_t)st.ni2 * st.nj2 * st.nk2, n2 = (size_t)st.ni2 * st.nj2;
+    st.uk = f->uk; st.vk = f->vk; st.wk = f->wk;
+    st.uks.assign(n3, 0.f); st.vks.assign(n3, 0.f); st.wks.assign(n3, 0.f);
+    st.dpm.assign(n3, 0.f); st.dpmnew.assign(n3, 0.f); st.div.assign(n3, 0.f);
+    st.vert_index.assign(n2, 0);
+    st.ustern_terrain.assign(n2, 0.f); st.ustern_obst.assign(n2, 0.f);
+    st.ap0.assign(st.nk2 + 1, 0.f);
+    const int model = p->turbulence_model;
+    if (model != 1) { st.turb = f->turb; st.tdiss = f->tdiss; }
+    else {
+        st.turb_own.assign(n3, 0.f); st.tdiss_own.assign(n3, 0.f);
+        st.turb = st.turb_own.data(); st.tdiss = st.tdiss_own.data();
+    }
+
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    const float DXK = st.dxk, DYK = st.dyk;
+    const float *DZK = s->dzk;
+    const int rx = p->ref_i, ry = p->ref_j;
+
+    /* UKS/VKS/WKS/DPMNEW exist only where ADVDOM is set in the 3x3 neighbourhood (:64-86). */
+    auto alloc3x3 = [&](int i, int j) {
+        const int ip = std::min(i + 1, NII + 1), jp = std::min(j + 1, NJJ + 1);
+        return st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(ip, j) == 1 ||
+               st.advdom(i, j - 1) == 1 || st.advdom(i - 1, j - 1) == 1 || st.advdom(ip, j - 1) == 1 ||
+               st.advdom(i, jp) == 1 || st.advdom(i - 1, jp) == 1 || st.advdom(ip, jp) == 1;
+    };
+
+    /* topwind, DTIME, AP0 (:146-163) */
+    float topwind = (float)std::sqrt((double)(pow2f(st.uk[st.i3(rx, ry, NKK - 1)]) +
+                                              pow2f(st.vk[st.i3(rx, ry, NKK - 1)])));
+    topwind = net_max(topwind, 0.01f);
+    int IterationLoops = 1;
+    float DTIME = 0.5f * net_min(DXK, DZK[1]) /
+                  net_max(0.01f, std::sqrt(pow2f(st.uk[st.i3(rx, ry, st.kadvmax)]) +
+                                           pow2f(st.vk[st.i3(rx, ry, st.kadvmax)])));
+    DTIME = net_min(DTIME, 5);
+    float DeltaUMax = 0, DeltaFinish = 0, DeltaFirst = 0;
+    const float AREAxy = DXK * DYK;
+    for (int k = 1; k <= st.kadvmax; ++k) st.ap0[k] = AREAxy * DZK[k] / DTIME;
+    const int MaxProgCellCount = st.vcff;
+    const float building_Z0 = p->building_z0;
+    double DeltaMean = 0;
+    const float Cmueh = 0.09f, Ceps = 1, Ceps1 = 1.44f, Ceps2 = 1.92f;
+
+    /* DPM = 0 (:198-209), TURB/TDISS initial constants (:211-227) */
+    if (model != 1 && p->turb_init == 0) {
+        for (int i = 1; i < NII + 1; ++i)
+            for (int j = 1; j <= NJJ; ++j)
+                for (int k = 1; k <= NKK + 1; ++k) {
+                    st.turb[st.i3(i, j, k)] = 0.001f;
+                    st.tdiss[st.i3(i, j, k)] = 0.0000001f;
+                }
+    }
+
+    /* Frund (:231-240): 8000 / topwind is a float division widened to double */
+    double Frund = (double)(8000 / topwind);
+    if (model == 2) Frund = (double)(10000 / topwind);
+    const bool quantise = p->quantise != 0;
+
+    const int IterationStepsMin = p->iteration_steps_min, IterationStepsMax = p->iteration_steps_max;
+    const float relax = p->relax, relaxp = p->relaxp;
+
+    /* initial staggered-grid velocities and GESCHW_MAX (:295-329) */
+    double GESCHW_MAX = 0;
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            if (!alloc3x3(i, j)) continue;
+            for (int k = 1; k <= NKK - 1; ++k) {
+                float u = 0.5f * (st.uk[st.i3(i, j, k)] + st.uk[st.i3(i + 1, j, k)]);
+                float v = 0.5f * (st.vk[st.i3(i, j, k)] + st.vk[st.i3(i, j + 1, k)]);
+                float w = 0.5f * (st.wk[st.i3(i, j, k)] + st.wk[st.i3(i, j, k + 1)]);
+                st.uks[st.i3(i, j, k)] = u; st.vks[st.i3(i, j, k)] = v; st.wks[st.i3(i, j, k)] = w;
+                GESCHW_MAX = net_maxd(GESCHW_MAX, std::sqrt((double)(pow2f(u) + pow2f(v))));
+            }
+        }
+    }
+
+    /* VerticalIndex (:333-344) */
+    for (int i = 1; i < NII + 1; ++i)
+        for (int j = 1; j <= NJJ; ++j)
+            st.vert_index[st.i2(i, j)] = std::min(NKK - 1, st.kkart(i, j) + MaxProgCellCount);
+
+    /* friction-velocity help terms (:347-403) */
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            int KSTART = 1;
+            if (st.cutk(i, j) == 0) KSTART = st.kkart(i, j) + 1;
+            const int VI = st.vert_index[st.i2(i, j)];
+            const int KK = st.kkart(i, j);
+            const float CUTK_L = st.cutk(i, j);
+            const float rough = st.z0(i, j);
+            for (int k = KSTART; k <= VI; ++k) {
+                if (k != KK + 1) continue;
+                if (CUTK_L < 1) {
+                    if ((double)rough >= (double)DZK[k] * 0.1)
+                        st.ustern_terrain[st.i2(i, j)] = 0.4f / std::log((DZK[k] + DZK[k + 1] * 0.5f) / DZK[k] * 0.1f);
+                    else
+                        st.ustern_terrain[st.i2(i, j)] = 0.4f / std::log(DZK[k] * 0.5f / rough);
+                } else {
+                    st.ustern_obst[st.i2(i, j)] = 0.4f / std::log(DZK[k] * 0.5f / building_Z0);
+                }
+            }
+        }
+    }
+
+    /* geostrophic wind at the reference point (:406-407) */
+    const float UG = st.uks[st.i3(rx, ry, NKK - 1)];
+    const float VG = st.vks[st.i3(rx, ry, NKK - 1)];
+
+    /* border copies and TURB initialisation (:410-510) */
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            const size_t c = st.i2(i, j);
+            for (int k = 1; k <= NKK - 1; ++k) {
+                if (i == 1) st.uk[st.i3(NII + 1, j, k)] = st.uk[st.i3(NII, j, k)];
+                if (j == 1) st.vk[st.i3(i, NJJ + 1, k)] = st.vk[st.i3(i, NJJ, k)];
+                if (model != 1 && p->turb_init == 0) {
+                    const float ObLength = s->ob_init[c], ust = s->ust_init[c], rough = s->z0_init[c];
+                    float V0int = p->v0_1;
+                    double windhilf = net_maxd(std::sqrt((double)(pow2f(st.uk[st.i3(i, j, k)]) +
+                                                                  pow2f(st.vk[st.i3(i, j, k)]))), 0.01);
+                    float U0int = (float)(windhilf * (0.2 * std::pow(windhilf, -0.9) + 0.32 * (double)rough + 0.18));
+                    U0int = (float)net_maxd((double)U0int, 0.3) * p->std_dev_v;
+                    float varw;
+                    if (ObLength < 0)
+                        varw = pow2f(ust) * pow2f(1.15f + 0.1f * std::pow(p->bd_lay_height / (-ObLength), 0.67f)) *
+                               pow2f(p->std_dev_w);
+                    else
+                        varw = pow2f(ust * p->std_dev_w * 1.25f);
+                    st.turb[st.i3(i, j, k)] = (float)(0.5 * (double)(pow2f(U0int) + pow2f(V0int) + varw));
+                }
+            }
+        }
+    }
+
+    float VISHMIN = 0.0f, VISVMIN = 0.0f;
+    if (model == 2) { VISHMIN = 0.01f; VISVMIN = 0.01f; }
+    const float Ustern_factorX = (float)(0.4 / std::log((double)DXK * 0.5 / (double)building_Z0));
+
+    /* velocities, TKE inside buildings set to zero (:518-575) */
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            if (st.advdom(i, j) != 1) continue;
+            const int VI = st.vert_index[st.i2(i, j)];
+            const int KK = st.kkart(i, j);
+            for (int k = 1; k <= VI; ++k) {
+                if (KK >= k) {
+                    st.uk[st.i3(i, j, k)] = 0;
+                    if (i == NII) st.uk[st.i3(i + 1, j, k)] = 0;
+                    st.vk[st.i3(i, j, k)] = 0;
+                    if (j == NJJ) st.vk[st.i3(i, j + 1, k)] = 0;
+                    st.wk[st.i3(i, j, k)] = 0;
+                    if (k == VI) st.wk[st.i3(i, j, k + 1)] = 0;
+                    if (model != 1) { st.turb[st.i3(i, j, k)] = 0; st.tdiss[st.i3(i, j, k)] = 0; }
+                    st.uks[st.i3(i, j, k)] = 0; st.vks[st.i3(i, j, k)] = 0; st.wks[st.i3(i, j, k)] = 0;
+                }
+            }
+        }
+    }
+
+    int iterations = 0;
+    int n_hist = 0;
+    bool converged = false;
+    /* ------------------------------ SIMPLE loop (:584-1182) ------------------------------ */
+    while (IterationLoops <= IterationStepsMax) {
+        boundary_conditions(st);
+
+        /* mass divergence; DPM = 0 on the prognostic levels (:723-758) */
+        for (int i = 2; i < NII; ++i) {
+            for (int j = 2; j < NJJ; ++j) {
+                if (st.advdom(i, j) != 1) continue;
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                const float *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
+                const float *UKip = st.col(st.uk, i + 1, j), *VKjp = st.col(st.vk, i, j + 1);
+                float *DIV_L = st.col(st.div, i, j), *DPM_L = st.col(st.dpm, i, j);
+                for (int k = KK + 1; k <= VI; ++k) {
+                    if (k > KK + 1)
+                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] +
+                                   (WK_L[k] - WK_L[k + 1]) * AREAxy;
+                    else
+                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] -
+                                   WK_L[k + 1] * AREAxy;
+                    DPM_L[k] = 0;
+                }
+            }
+        }
+
+        /* sweep direction (:770-802) */
+        int IS = 1, JS = 1;
+        if (IterationLoops % 4 == 0) { IS = -1; JS = 1; }
+        else if (IterationLoops % 4 == 1) { IS = -1; JS = -1; }
+        else if (IterationLoops % 4 == 2) { IS = 1; JS = -1; }
+
+        /* pressure correction, vertical TDMA per column, rows in order (:804-901) */
+        DeltaUMax = 0;
+        {
+            std::vector<float> PIMP(st.nk2), QIMP(st.nk2);
+            for (int j1 = 2; j1 < NJJ; ++j1) {
+                std::fill(PIMP.begin(), PIMP.end(), 0.0f);   /* new float[NKK + 2] per row */
+                std::fill(QIMP.begin(), QIMP.end(), 0.0f);
+                float DeltaUMaxIntern = 0;
+                const int j = (JS == -1) ? NJJ - j1 + 1 : j1;
+                for (int i1 = 2; i1 <= NII - 1; ++i1) {
+                    const int i = (IS == -1) ? NII - i1 + 1 : i1;
+                    if (st.advdom(i, j) != 1) continue;
+                    const float *DIV_L = st.col(st.div, i, j);
+                    float *DPM_L = st.col(st.dpm, i, j);
+                    const float *DPMim = st.col(st.dpm, i - 1, j), *DPMip = st.col(st.dpm, i + 1, j);
+                    const float *DPMjm = st.col(st.dpm, i, j - 1), *DPMjp = st.col(st.dpm, i, j + 1);
+                    float *DPMNEW_L = st.col(st.dpmnew, i, j);
+                    const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                    for (int k = VI; k > KK; --k) {
+                        float DIM = DIV_L[k] / DTIME + (DPMim[k] + DPMip[k]) / DXK * DYK * DZK[k] +
+                                    (DPMjm[k] - DPMjp[k]) / DYK * DXK * DZK[k];
+                        float APP = 2.0f * (DYK * DZK[k] / DXK + DXK * DZK[k] / DYK + AREAxy / DZK[k]);
+                        float ABP = (k > 1) ? AREAxy / (0.5f * (DZK[k - 1] + DZK[k])) : AREAxy / DZK[k];
+                        float ATP = AREAxy / (0.5f * (DZK[k + 1] + DZK[k]));
+                        float TERMP = 1 / (APP - ATP * PIMP[k + 1]);
+                        PIMP[k] = ABP * TERMP;
+                        QIMP[k] = (ATP * QIMP[k + 1] + DIM) * TERMP;
+                    }
+                    for (int k = KK + 1; k <= VI; ++k) {
+                        float temp = PIMP[k] * DPM_L[k - 1] + QIMP[k];
+                        DeltaUMaxIntern = (float)net_maxd((double)DeltaUMaxIntern,
+                            std::fabs((double)DPM_L[k] - quant((double)temp, Frund, quantise)));
+                        DPM_L[k] = temp;
+                        DPMNEW_L[k] += relaxp * DPM_L[k];
+                    }
+                }
+                if (DeltaUMaxIntern > DeltaUMax) DeltaUMax = DeltaUMaxIntern;
+            }
+        }
+
+        /* velocity correction with Frund quantisation in double (:904-949) */
+        for (int i = 2; i < NII; ++i) {
+            for (int j = 2; j <= NJJ - 1; ++j) {
+                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
+                const float *DPMim = st.col(st.dpm, i - 1, j), *DPMjm = st.col(st.dpm, i, j - 1);
+                const float *DPM_L = st.col(st.dpm, i, j);
+                float *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                const int KKim = st.kkart(i - 1, j), KKjm = st.kkart(i, j - 1);
+                for (int k = 1; k <= VI; ++k) {
+                    const float d = DPM_L[k];
+                    if (i > 2 && KK < k && KKim < k)
+                        UK_L[k] = (float)quant((double)(UK_L[k] + (DPMim[k] - d) / DXK * DTIME), Frund, quantise);
+                    if (j > 2 && KK < k && KKjm < k)
+                        VK_L[k] = (float)quant((double)(VK_L[k] + (DPMjm[k] - d) / DYK * DTIME), Frund, quantise);
+                    if (KK + 1 < k)
+                        WK_L[k] = (float)quant((double)(WK_L[k] + (DPM_L[k - 1] - d) / (DZK[k] + DZK[k - 1]) * 2 * DTIME),
+                                               Frund, quantise);
+                    else
+                        WK_L[k] = 0;
+                }
+            }
+        }
+
+        /* staggered -> cell-centre averages and border copies (:958-1039) */
+        for (int i = 2; i < NII; ++i) {
+            for (int j = 2; j <= NJJ - 1; ++j) {
+                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
+                const float *UK_L = st.col(st.uk, i, j), *UKip = st.col(st.uk, i + 1, j);
+                const float *VK_L = st.col(st.vk, i, j), *VKjp = st.col(st.vk, i, j + 1);
+                const float *WK_L = st.col(st.wk, i, j);
+                float *UKS_L = st.col(st.uks, i, j), *VKS_L = st.col(st.vks, i, j), *WKS_L = st.col(st.wks, i, j);
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                int KSTART = 1;
+                if (st.cutk(i, j) == 0) KSTART = KK + 1;
+                for (int k = KSTART; k <= VI; ++k) {
+                    if (KK < k) {
+                        UKS_L[k] = 0.5f * (UK_L[k] + UKip[k]);
+                        VKS_L[k] = 0.5f * (VK_L[k] + VKjp[k]);
+                    }
+                    if (KK + 1 < k) WKS_L[k] = 0.5f * (WK_L[k] + WK_L[k + 1]);
+                }
+                if (j == 2) {
+                    float *UKS1 = st.col(st.uks, i, 1);
+                    for (int k = KSTART; k <= VI; ++k) UKS1[k] = UKS_L[k];
+                }
+                if (j == NJJ - 1 && st.advdom(i, NJJ) == 1) {
+                    float *UKSN = st.col(st.uks, i, NJJ);
+                    for (int k = KSTART; k <= VI; ++k) UKSN[k] = UKS_L[k];
+                }
+            }
+        }
+        for (int j = 2; j < NJJ; ++j) {
+            if (st.advdom(1, j) == 1) {
+                float *a = st.col(st.vks, 1, j); const float *b = st.col(st.vks, 2, j);
+                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
+            }
+            if (st.advdom(NII - 1, j) == 1) {
+                float *a = st.col(st.vks, NII, j); const float *b = st.col(st.vks, NII - 1, j);
+                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
+            }
+        }
+
+        /* momentum equations (:1049-1137), deterministic order */
+        if (model == 0) {
+            u_mom_nd(st, IS, JS, AREAxy, UG, relax);
+            v_mom_nd(st, IS, JS, AREAxy, VG, relax);
+            w_mom_nd(st, IS, JS, AREAxy, relax);
+        } else if (model == 1) {
+            u_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, UG, relax);
+            v_mom_ml(st, p->simd_width, -IS, -JS, VISHMIN, AREAxy, VG, relax);
+            w_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, relax);
+        } else {
+            u_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, UG, relax);
+            v_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, VG, relax);
+            w_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, relax);
+            tke_ke(st, IS, JS, Cmueh, Ceps, Ceps1, Ceps2, VISHMIN, VISVMIN, AREAxy, building_Z0, relax,
+                   Ustern_factorX);
+        }
+        iterations++;
+        if (stats && stats->trace_delta_umax && iterations <= stats->trace_capacity)
+            stats->trace_delta_umax[iterations - 1] = DeltaUMax;
+
+        /* convergence bookkeeping (:1144-1170) */
+        if (IterationLoops >= IterationStepsMax) DeltaFinish = (float)(DeltaMean / (double)pow2f(topwind));
+        if ((IterationLoops % p->conv_cadence == 0) && (IterationLoops > 1)) {
+            double _delta = DeltaMean / (double)pow2f(topwind);
+            if (IterationLoops == p->conv_cadence) DeltaFirst = (float)_delta;
+            if (stats && n_hist < GRAL_MAX_HISTORY) stats->delta_history[n_hist] = _delta;
+            n_hist++;
+            if (_delta < p->conv_threshold && (IterationLoops >= IterationStepsMin)) { converged = true; break; }
+            DeltaMean = 0;
+        } else {
+            DeltaMean += DeltaUMax;
+        }
+        IterationLoops++;
+    }
+
+    /* post-checks (:1187-1243) */
+    int UKun = 0, VKun = 0, WKun = 0;
+    for (int i = 1; i <= NII; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            if (st.advdom(i, j) != 1) continue;
+            const float limit = (float)(10 * GESCHW_MAX);
+            const int kmax = std::min(NKK - 1, st.kkart(i, j) + MaxProgCellCount);
+            for (int k = 1; k <= kmax; ++k) {
+                const float u = std::fabs(st.uk[st.i3(i, j, k)]), v = std::fabs(st.vk[st.i3(i, j, k)]);
+                const float w = std::fabs(st.wk[st.i3(i, j, k)]);
+                if (u > 55 || u > limit) UKun++;
+                if (v > 55 || v > limit) VKun++;
+                if (w > 20 || w > limit) WKun++;
+            }
+        }
+    }
+
+    if (stats) {
+        stats->iterations = iterations;
+        stats->iteration_loops = IterationLoops;
+        stats->converged = converged ? 1 : 0;
+        stats->convergence_problem = (DeltaFinish > DeltaFirst) ? 1 : 0;
+        stats->delta_first = DeltaFirst;
+        stats->delta_finish = DeltaFinish;
+        stats->n_history = std::min(n_hist, GRAL_MAX_HISTORY);
+        stats->uk_unrealistic = UKun; stats->vk_unrealistic = VKun; stats->wk_unrealistic = WKun;
+        stats->geschw_max = GESCHW_MAX;
+        stats->topwind = topwind; stats->dtime = DTIME; stats->frund = Frund;
+        stats->last_delta_umax = DeltaUMax;
+    }
+    return GRAL_OK;
+}

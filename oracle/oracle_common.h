@@ -1,0 +1,118 @@
+/*
+ * oracle_common.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Shared state and scalar helpers of the CPU oracle for GRAL's prognostic microscale flow
+ * solver.  The oracle is a from-scratch C++ restatement of the reference's deterministic path
+ * (in.dat UseFixedRndSeedVal=1, ReadInDat.cs:270-287, which serialises every Gauss-Seidel phase,
+ * PrognosticFlowfield.cs:806-811, 1060-1065, 1085-1090, 1106-1111, 1129-1135).  Only tests/,
+ * the smoke check and the CPU-baseline leg of bench.py may load it; the product never does.
+ *
+ * Parity status: unpinned.  The reference is C#/.NET 8 and cannot be built or run in this
+ * environment, and it ships no tests or golden vectors for this path.  The oracle follows the
+ * reference's source operation by operation (float vs double promotion, association order, .NET 8
+ * Math.Max/Min and Vector.Max/Min semantics), and is built without floating-point contraction.
+ */
+#ifndef GRAL_ORACLE_COMMON_H
+#define GRAL_ORACLE_COMMON_H
+
+#include <climits>
+#include <cmath>
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "gral_prog.h"
+
+namespace oracle {
+
+/* ---- .NET 8 scalar semantics (ProgramFunctions.cs:768-849 and System.Math) ---- */
+
+/* Math.Max(float, float) / MathF.Max: IEEE 754:2019 maximum (NaN propagates, +0 > -0). */
+static inline float net_max(float a, float b) {
+    if (a != b) {
+        if (!std::isnan(a)) return (b < a) ? a : b;
+        return a;
+    }
+    return std::signbit(b) ? a : b;
+}
+static inline float net_min(float a, float b) {
+    if (a != b) {
+        if (!std::isnan(a)) return (a < b) ? a : b;
+        return a;
+    }
+    return std::signbit(a) ? a : b;
+}
+static inline double net_maxd(double a, double b) {
+    if (a != b) {
+        if (!std::isnan(a)) return (b < a) ? a : b;
+        return a;
+    }
+    return std::signbit(b) ? a : b;
+}
+/* Program.FloatMax (ProgramFunctions.cs:768): val1 > val2 ? val1 : val2. */
+static inline float float_max(float a, float b) { return (a > b) ? a : b; }
+/* Vector.Max / Vector.Min on .NET 8 x64 (maxps / minps): left > right ? left : right. */
+static inline float vmax(float a, float b) { return (a > b) ? a : b; }
+static inline float vmin(float a, float b) { return (a < b) ? a : b; }
+
+/* Program.ConvToInt(double) (ProgramFunctions.cs:798): round half away from zero through a
+ * truncating (int) cast.  An out-of-range or NaN operand converts to int.MinValue, as the x64
+ * cvttsd2si conversion of .NET 8 does. */
+static inline int conv_to_int(double v) {
+    double t = (v < 0) ? (v - 0.5) : (v + 0.5);
+    if (!(t > -2147483649.0 && t < 2147483648.0)) return INT_MIN;
+    return (int)t;
+}
+
+static inline float pow2f(float x) { return x * x; }
+static inline double pow2d(double x) { return x * x; }
+static inline float pow3f(float x) { return x * x * x; }
+static inline float pow5f(float x) { return x * x * x * x * x; }
+static inline double pow5d(double x) { return x * x * x * x * x; }
+
+/* ---- solver state: every 3-D array is [NII+2][NJJ+2][NKK+2], k fastest ---- */
+struct State {
+    int nii, njj, nkk, kadvmax, vcff;
+    int ni2, nj2, nk2;
+    float dxk, dyk;
+    const gral_params *p;
+    const gral_static *s;
+    float *uk, *vk, *wk, *turb, *tdiss;           /* caller fields */
+    std::vector<float> uks, vks, wks, dpm, dpmnew, div;
+    std::vector<float> turb_own, tdiss_own;        /* used when model == 1 (never read) */
+    std::vector<int> vert_index;                   /* Program.VerticalIndex [NII+2][NJJ+2] */
+    std::vector<float> ustern_terrain, ustern_obst;/* UsternTerrain/ObstaclesHelpterm */
+    std::vector<float> ap0;                        /* PrognosticFlowfield.AP0 */
+
+    size_t i3(int i, int j, int k) const { return ((size_t)i * nj2 + j) * nk2 + k; }
+    size_t i2(int i, int j) const { return (size_t)i * nj2 + j; }
+    int kkart(int i, int j) const { return s->kkart[i2(i, j)]; }
+    int advdom(int i, int j) const { return s->advdom[i2(i, j)]; }
+    float cutk(int i, int j) const { return s->cutk[i2(i, j)]; }
+    float cov(int i, int j) const { return s->cov ? s->cov[i2(i, j)] : 0.0f; }
+    float z0(int i, int j) const { return s->z0[i2(i, j)]; }
+    bool has_veg(int i, int j) const { return s->veg && s->veg_mask && s->veg_mask[i2(i, j)]; }
+    float *col(float *a, int i, int j) const { return a + i3(i, j, 0); }
+    float *col(std::vector<float> &a, int i, int j) { return a.data() + i3(i, j, 0); }
+    const float *vegcol(int i, int j) const { return s->veg + i3(i, j, 0); }
+    const float *dzk() const { return s->dzk; }
+    const float *hokart() const { return s->hokart; }
+};
+
+/* Momentum routines (one translation unit each model family). */
+void u_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float UG, float relax);
+void v_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float VG, float relax);
+void w_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float relax);
+void u_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float UG, float relax);
+void v_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float VG, float relax);
+void w_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float relax);
+void tke_ke(State &st, int IS, int JS, float Cmueh, float Ceps, float Ceps1, float Ceps2,
+            float VISHMIN, float VISVMIN, float AREAxy, float building_Z0, float relax,
+            float Ustern_factorX);
+void u_mom_nd(State &st, int IS, int JS, float AREAxy, float UG, float relax);
+void v_mom_nd(State &st, int IS, int JS, float AREAxy, float VG, float relax);
+void w_mom_nd(State &st, int IS, int JS, float AREAxy, float relax);
+
+}  // namespace oracle
+
+#endif
