@@ -1,0 +1,178 @@
+// prog_common.cuh -- device-side data structures and helpers of the B200 prognostic solver.
+//
+// Device layout (private to the library): every 3-D field of one situation is a slab
+// [col][KS] float, col = i*(NJJ+2) + j, k fastest, holding levels 0..KS-1 with
+// KS >= KADVMAX+2 (every level the SIMPLE loop reads or writes, PrognosticFlowfield.cs:584-1182).
+// Situations of a batch are consecutive slabs.  Per-column constants live in ColMeta/ColF,
+// per-situation scalars in SitDev.
+//
+// Arithmetic follows the reference's float/double evaluation exactly: the library is built with
+// --fmad=false (no contraction, like .NET RyuJIT), IEEE division and square root, and the
+// max/min helpers below reproduce .NET 8 semantics.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gral {
+
+constexpr int KMAX_LEVELS = 64;   // largest KS the column kernels handle (two rounds of 32 lanes)
+constexpr int MAX_HIST = 64;
+
+// ---- per-column flag bits (ColMeta::flags) ----
+enum : uint32_t {
+    F_ADV = 1u << 0,      // ADVDOM[i][j] == 1
+    F_ALLOC3 = 1u << 1,   // ADVDOM set in the 3x3 neighbourhood (staggered arrays exist), :64-86
+    F_VEG = 1u << 2,      // VEG[i][j] != null
+    F_CUTK0 = 1u << 3,    // CUTK == 0   (KSTART = KKART+1)
+    F_CUTKLT1 = 1u << 4,  // CUTK < 1    (terrain wall law instead of building law)
+    F_CUTKGT0 = 1u << 5,  // CUTK > 0
+    F_VC = 1u << 6,       // ADVDOM(i,j) | ADVDOM(i-1,j) | ADVDOM(i,j-1): velocity correction, :965
+    F_BS = 1u << 7,       // ADVDOM[i][j-1] < 1 || j == 2     (diffusion boundary, U-...1.cs:145-148)
+    F_BN = 1u << 8,       // ADVDOM[i][j+1] < 1 || j == NJJ-1
+    F_BW = 1u << 9,       // ADVDOM[i-1][j] < 1 || i == 2
+    F_BE = 1u << 10,      // ADVDOM[i+1][j] < 1 || i == NII-1
+    F_Z0GE = 1u << 11,    // Z0 >= DZK[KKART+1]*0.1F (float test of the model-1 wall law)
+    F_Z0GED = 1u << 12,   // Z0 >= DZK[KKART+1]*0.1 (double test of the model-0/2 wall law)
+};
+
+struct ColMeta {          // 16 bytes
+    int16_t kkart, vi, kstart, kad;   // KKART, VerticalIndex, KSTART, first level with ADD_DIFF
+    int16_t wc_lo, wc_hi;             // levels whose SIMD chunk holds KKART+1 (wall chunk)
+    int16_t kkm_u, kkm_v;             // max(KKART, KKART[i-1][j]), max(KKART, KKART[i][j-1])
+};
+
+struct ColF {             // 16 bytes
+    float cov, z0, help_t, help_o;    // COV, roughness, UsternTerrain/ObstaclesHelpterm
+};
+
+// Per-situation scalars and convergence state (PrognosticFlowfield.cs:146-163, 231-240, 1144-1170).
+struct SitDev {
+    double frund;
+    double delta_mean;
+    double conv_threshold;
+    double hist[MAX_HIST];
+    unsigned long long geschw_bits;   // GESCHW_MAX as non-negative double bits (atomicMax)
+    float dtime, topwind, ug, vg;
+    float delta_first, delta_finish, last_dumax;
+    uint32_t dumax_bits;     // running max of DeltaUMax (non-negative float bits), reset each iteration
+    int32_t it;              // IterationLoops
+    int32_t active;          // 1 while the SIMPLE loop runs for this situation
+    int32_t iters_done;
+    int32_t converged;
+    int32_t n_hist;
+    int32_t it_min, it_max, cadence;
+    int32_t quantise;
+    int32_t pad_;
+};
+
+// Everything a kernel needs, passed by value (all pointers are device pointers).
+struct KArgs {
+    // geometry
+    int nii, njj, nkk, ks, nj2, ncols, nb;
+    float dxk, dyk, areaxy;
+    float relax, relaxp, coriolis, vishmin;
+    int simd;
+    // static tables (device)
+    const ColMeta *meta;
+    const uint32_t *cflags;              // F_* bits per column
+    const ColF *colf;
+    const float *dzk, *hokart;           // [ks]
+    const float *app, *abp, *atp;        // pressure coefficients per level [ks]
+    const float *veg;                    // [ncols][ks] or null
+    // per-situation state
+    SitDev *sit;                         // [nb]
+    const float *ap0;                    // [nb][ks]
+    // fields [nb][ncols][ks]
+    float *uk, *vk, *wk, *dpm, *dpmnew, *uks, *vks, *wks, *turb, *tdiss;
+    // scheduling
+    int *flags;                          // [nb][ncols] stamps
+    unsigned int *counters;              // task counters, one per GS phase kind
+    float *rowcarry;                     // [nb][nj2][2][ks] pressure row carry (P, Q)
+    int *err;                            // device error word (0 = ok)
+    const int *act;                      // active situation list
+    const int *nact;                     // number of active situations
+    unsigned long long wait_limit_ns;    // bound of every spin wait
+    int chunk;                           // tasks claimed per atomic
+    float *trace;                        // [nb][trace_cap] DeltaUMax per iteration, or null
+    int trace_cap;
+    int vi_min;                          // smallest VerticalIndex of an active column
+};
+
+// Geometry of a Gauss-Seidel sweep: sweep coordinates i1 in [ia, ia+ni), j1 in [ja, ja+nj);
+// tasks are numbered diagonal by diagonal (d = (i1-ia) + (j1-ja)), then situation, then position.
+struct SweepGeom {
+    int ia, ni, ja, nj, ndiag;
+    const int *diag_start;   // [ndiag+1] cells on diagonals < d (device)
+};
+
+enum : int { ERR_NONE = 0, ERR_TIMEOUT = 1, ERR_NONFINITE = 2 };
+
+enum : int { PH_PRESSURE = 1, PH_U = 2, PH_V = 3, PH_W = 4, PH_TKE = 5 };
+
+__host__ __device__ inline size_t fidx(int s, int col, int ncols, int ks) {
+    return ((size_t)s * ncols + col) * ks;
+}
+
+// ---- .NET 8 semantics ----
+// Vector.Max / Vector.Min / Program.FloatMax: left > right ? left : right.
+__device__ __forceinline__ float vmaxf(float a, float b) { return (a > b) ? a : b; }
+__device__ __forceinline__ float vminf(float a, float b) { return (a < b) ? a : b; }
+// Math.Max(float,float) / Math.Min (IEEE 754:2019 maximum/minimum).
+__device__ __forceinline__ float net_maxf(float a, float b) {
+    if (a != b) { if (!isnan(a)) return (b < a) ? a : b; return a; }
+    return signbit(b) ? a : b;
+}
+__device__ __forceinline__ float net_minf(float a, float b) {
+    if (a != b) { if (!isnan(a)) return (a < b) ? a : b; return a; }
+    return signbit(a) ? a : b;
+}
+__device__ __forceinline__ double net_maxd(double a, double b) {
+    if (a != b) { if (!isnan(a)) return (b < a) ? a : b; return a; }
+    return signbit(b) ? a : b;
+}
+// Program.ConvToInt(double): round half away from zero through a truncating cast; out of
+// range or NaN gives int.MinValue as .NET 8 on x64.
+__device__ __forceinline__ int conv_to_int(double v) {
+    double t = (v < 0) ? (v - 0.5) : (v + 0.5);
+    if (!(t > -2147483649.0 && t < 2147483648.0)) return INT32_MIN;
+    return (int)t;
+}
+__device__ __forceinline__ double quantd(double x, double frund, int on) {
+    return on ? (double)conv_to_int(x * frund) / frund : x;
+}
+
+// ---- inter-warp ordering of the Gauss-Seidel wavefront ----
+__device__ __forceinline__ int ld_acquire(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int *p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Spin (lane 0 only) until *flag >= stamp.  Gives up after limit_ns, or as soon as another warp
+// reported an error; returns false then.  Never waits unboundedly.
+__device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned long long limit_ns) {
+    if (ld_acquire(flag) >= stamp) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned ns = 20;
+    for (;;) {
+        __nanosleep(ns);
+        if (ns < 200) ns += ns;
+        if (ld_acquire(flag) >= stamp) return true;
+        if (*(volatile int *)err != ERR_NONE) return false;
+        if (globaltimer_ns() - t0 > limit_ns) {
+            atomicCAS(err, ERR_NONE, ERR_TIMEOUT);
+            return false;
+        }
+    }
+}
+
+}  // namespace gral

@@ -1,0 +1,694 @@
+// prog_host.cu -- C ABI of the B200 prognostic solver (include/gral_prog.h).
+//
+// A context owns the device memory of a batch of situations on one grid.  load() copies the host
+// fields into full-height staging buffers, runs the per-situation set-up of
+// PrognosticFlowfield.Calculate (PrognosticFlowfield.cs:45-579) and extracts the level slab the
+// SIMPLE loop works on; iterate() replays a CUDA graph of one SIMPLE iteration (:584-1182) until
+// every situation has converged or reached its iteration limit, deciding only at the iterations
+// where the reference tests convergence; store() runs the post-checks (:1187-1245) and copies the
+// fields back.  Per-column constants (VerticalIndex, KSTART, the friction-velocity help terms,
+// the SIMD-chunk positions of the reference's Vector<float> loops) are computed here on the host
+// in float, with the same expressions as the reference, once per load.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gral_prog.h"
+#include "prog_common.cuh"
+#include "prog_kernels.cuh"
+
+using namespace gral;
+
+namespace {
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t count) {
+        if (count <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(count, 1) * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Geom {
+    SweepGeom g;
+    std::vector<int> ds;
+};
+
+}  // namespace
+
+struct gral_ctx {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {};
+    int cap_nii = 0, cap_njj = 0, cap_nkk = 0, cap_kadv = 0, cap_batch = 0;
+    std::string err = "no error";
+
+    // current load
+    bool loaded = false;
+    int nii = 0, njj = 0, nkk = 0, ks = 0, nb = 0, ncols = 0, nj2 = 0, model = 1;
+    int it_host = 1, it_max = 0, it_min = 0, cadence = 100;
+    std::vector<gral_params> params;
+    std::vector<gral_fields> fields;
+    KArgs ka{};
+    Staging sg{};
+    BcLists bc{};
+    Geom geo_p, geo_u, geo_v;
+    int grid_gs[4] = {0, 0, 0, 0};
+    cudaGraphExec_t graph = nullptr;
+    float ms_upload = 0.f;
+
+    // device buffers
+    DevBuf<float> slab, stage, veg, tables, ap0, rowcarry, trace;
+    DevBuf<ColMeta> meta;
+    DevBuf<uint32_t> cflags;
+    DevBuf<ColF> colf;
+    DevBuf<SitDev> sit;
+    DevBuf<int> flags, misc, diag, bcl, counts;
+    DevBuf<unsigned int> counters;
+    std::vector<SitDev> h_sit;
+    std::vector<int> h_act;
+
+    ~gral_ctx() {
+        if (graph) cudaGraphExecDestroy(graph);
+        DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
+        for (auto *b : fb) b->release();
+        meta.release(); cflags.release(); colf.release(); sit.release();
+        flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
+        counters.release();
+        for (auto &e : ev) if (e) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+int fail(gral_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                      \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? GRAL_ENOMEM : GRAL_ECUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+inline float f32(float x) { return x; }
+
+// Math.Max/Math.Min(float, float) of .NET 8 (IEEE 754:2019 maximum/minimum)
+inline float net_max(float a, float b) {
+    if (a != b) { if (!std::isnan(a)) return (b < a) ? a : b; return a; }
+    return std::signbit(b) ? a : b;
+}
+inline float net_min(float a, float b) {
+    if (a != b) { if (!std::isnan(a)) return (a < b) ? a : b; return a; }
+    return std::signbit(a) ? a : b;
+}
+
+// ---- per-column constants (host) ----------------------------------------------------------
+
+// Levels of the reference's Vector<float> chunk loop (U-prognostic-microscale_1.cs:194-202):
+// chunk bases KSTART, KSTART+W, ..., the last one pulled back to KEND-W.  kad is the first level
+// processed by a chunk whose base lies above KKART+1 (extra eddy-viscosity terms, :453); wc_lo..
+// wc_hi are the levels processed by chunks that contain KKART+1 (masked wall term, :419).
+void chunk_levels(int K0, int KEND, int KK, int W, int &kad, int &wlo, int &whi) {
+    kad = KEND;
+    wlo = 1;
+    whi = 0;
+    for (int s = K0; s < KEND; s += W) {
+        int base = s;
+        if (s > KEND - W) base = KEND - W;
+        const int hi = std::min(s + W - 1, KEND - 1);
+        if (base > KK + 1) kad = std::min(kad, s);
+        if (base <= KK + 1 && KK + 1 < base + W) {
+            if (whi < wlo) { wlo = s; whi = hi; }
+            else { wlo = std::min(wlo, s); whi = std::max(whi, hi); }
+        }
+    }
+}
+
+int build_meta(gral_ctx *ctx, const gral_params &p, const gral_static &s, std::vector<ColMeta> &meta,
+               std::vector<uint32_t> &cfl, std::vector<ColF> &colf, int &vi_min, int &vi_max) {
+    const int NII = p.nii, NJJ = p.njj, NKK = p.nkk, nj2 = NJJ + 2;
+    const int ncols = (NII + 2) * nj2;
+    meta.assign(ncols, ColMeta{});
+    cfl.assign(ncols, 0u);
+    colf.assign(ncols, ColF{});
+    auto adv = [&](int i, int j) { return (i >= 0 && i <= NII + 1 && j >= 0 && j <= NJJ + 1) ? s.advdom[i * nj2 + j] : 0; };
+    auto kk = [&](int i, int j) { return (int)s.kkart[i * nj2 + j]; };
+    const float *DZK = s.dzk;
+    vi_min = 1 << 20;
+    vi_max = 0;
+    for (int i = 0; i <= NII + 1; ++i) {
+        for (int j = 0; j <= NJJ + 1; ++j) {
+            const int c = i * nj2 + j;
+            ColMeta &m = meta[c];
+            const int KK = kk(i, j);
+            const float cutk = s.cutk[c];
+            const bool inner = (i >= 1 && i <= NII && j >= 1 && j <= NJJ);
+            const int VI = inner ? std::min(NKK - 1, KK + p.vert_cells_ff) : 0;   // :339
+            const int K0 = (cutk == 0) ? KK + 1 : 1;
+            m.kkart = (int16_t)KK;
+            m.vi = (int16_t)VI;
+            m.kstart = (int16_t)K0;
+            m.kkm_u = (int16_t)std::max(KK, i >= 1 ? kk(i - 1, j) : KK);
+            m.kkm_v = (int16_t)std::max(KK, j >= 1 ? kk(i, j - 1) : KK);
+            int kad = VI + 1, wlo = 1, whi = 0;
+            if (p.turbulence_model == 1 && inner) chunk_levels(K0, VI + 1, KK, p.simd_width, kad, wlo, whi);
+            m.kad = (int16_t)kad;
+            m.wc_lo = (int16_t)wlo;
+            m.wc_hi = (int16_t)whi;
+            uint32_t f = 0;
+            if (adv(i, j) == 1) f |= F_ADV;
+            if (inner) {
+                const int ip = std::min(i + 1, NII + 1), jp = std::min(j + 1, NJJ + 1);
+                if (adv(i, j) == 1 || adv(i - 1, j) == 1 || adv(ip, j) == 1 || adv(i, j - 1) == 1 ||
+                    adv(i - 1, j - 1) == 1 || adv(ip, j - 1) == 1 || adv(i, jp) == 1 || adv(i - 1, jp) == 1 ||
+                    adv(ip, jp) == 1)
+                    f |= F_ALLOC3;
+            }
+            if (s.veg && s.veg_mask && s.veg_mask[c]) f |= F_VEG;
+            if (cutk == 0) f |= F_CUTK0;
+            if (cutk < 1) f |= F_CUTKLT1;
+            if (cutk > 0) f |= F_CUTKGT0;
+            if (i >= 1 && j >= 1 && (adv(i, j) == 1 || adv(i - 1, j) == 1 || adv(i, j - 1) == 1)) f |= F_VC;
+            if (adv(i, j - 1) < 1 || j == 2) f |= F_BS;
+            if (adv(i, j + 1) < 1 || j == NJJ - 1) f |= F_BN;
+            if (adv(i - 1, j) < 1 || i == 2) f |= F_BW;
+            if (adv(i + 1, j) < 1 || i == NII - 1) f |= F_BE;
+            const float z0 = s.z0[c];
+            ColF &cf = colf[c];
+            cf.cov = s.cov ? s.cov[c] : 0.0f;
+            cf.z0 = z0;
+            if (inner && KK + 1 <= NKK) {
+                const int k = KK + 1;
+                if (z0 >= f32(DZK[k] * 0.1f)) f |= F_Z0GE;
+                if ((double)z0 >= (double)DZK[k] * 0.1) f |= F_Z0GED;
+                if (K0 <= k && k <= VI) {                                         // :347-403
+                    if (cutk < 1) {
+                        if ((double)z0 >= (double)DZK[k] * 0.1)
+                            cf.help_t = 0.4f / logf((DZK[k] + DZK[k + 1] * 0.5f) / DZK[k] * 0.1f);
+                        else
+                            cf.help_t = 0.4f / logf(DZK[k] * 0.5f / z0);
+                    } else {
+                        cf.help_o = 0.4f / logf(DZK[k] * 0.5f / p.building_z0);
+                    }
+                }
+            }
+            cfl[c] = f;
+            vi_max = std::max(vi_max, VI);
+            if ((f & F_ADV) && i >= 2 && i <= NII - 1 && j >= 2 && j <= NJJ - 1) {
+                vi_min = std::min(vi_min, VI);
+                if (p.turbulence_model == 1 && VI + 1 - p.simd_width < 1)
+                    return fail(ctx, GRAL_EINVAL, "VerticalIndex below the SIMD width of the model-1 parity path");
+            }
+        }
+    }
+    if (vi_min == (1 << 20)) vi_min = 0;
+    return GRAL_OK;
+}
+
+Geom make_geom(int ia, int ni, int ja, int nj) {
+    Geom G;
+    G.g.ia = ia; G.g.ni = std::max(ni, 0); G.g.ja = ja; G.g.nj = std::max(nj, 0);
+    const int nd = (G.g.ni > 0 && G.g.nj > 0) ? G.g.ni + G.g.nj - 1 : 0;
+    G.g.ndiag = nd;
+    G.ds.assign(nd + 1, 0);
+    for (int d = 0; d < nd; ++d) {
+        const int lo = std::max(0, d - (G.g.nj - 1)), hi = std::min(d, G.g.ni - 1);
+        G.ds[d + 1] = G.ds[d] + (hi - lo + 1);
+    }
+    return G;
+}
+
+int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, const gral_fields *f) {
+    if (!ctx) return GRAL_EINVAL;
+    if (n < 1 || n > ctx->cap_batch) return fail(ctx, GRAL_EINVAL, "batch size outside 1..max_batch");
+    if (!p || !s || !f) return fail(ctx, GRAL_EINVAL, "null argument");
+    if (!s->kkart || !s->advdom || !s->cutk || !s->z0 || !s->dzk || !s->hokart)
+        return fail(ctx, GRAL_EINVAL, "missing static array");
+    const gral_params &p0 = p[0];
+    if (p0.nii < 4 || p0.njj < 4 || p0.nkk < 3) return fail(ctx, GRAL_EINVAL, "grid too small");
+    if (p0.nii > ctx->cap_nii || p0.njj > ctx->cap_njj || p0.nkk > ctx->cap_nkk || p0.kadvmax > ctx->cap_kadv)
+        return fail(ctx, GRAL_EINVAL, "grid larger than the context capacity");
+    if (p0.nii > 0xffff || p0.njj > 0xffff) return fail(ctx, GRAL_EINVAL, "grid dimension above 65535");
+    if (p0.kadvmax < 2 || p0.kadvmax + 2 > KMAX_LEVELS || p0.kadvmax > p0.nkk)
+        return fail(ctx, GRAL_EINVAL, "KADVMAX outside 2..62 or above NKK");
+    if (p0.turbulence_model != 1) return fail(ctx, GRAL_EINVAL, "only turbulence_model 1 is built on the GPU yet");
+    if (p0.simd_width != 8) return fail(ctx, GRAL_EINVAL, "simd_width must be 8 (Vector<float> path)");
+    for (int b = 0; b < n; ++b) {
+        const gral_params &q = p[b];
+        if (q.nii != p0.nii || q.njj != p0.njj || q.nkk != p0.nkk || q.kadvmax != p0.kadvmax ||
+            q.vert_cells_ff != p0.vert_cells_ff || q.turbulence_model != p0.turbulence_model ||
+            q.simd_width != p0.simd_width || q.dxk != p0.dxk || q.dyk != p0.dyk ||
+            q.iteration_steps_min != p0.iteration_steps_min || q.iteration_steps_max != p0.iteration_steps_max ||
+            q.conv_cadence != p0.conv_cadence || q.relax != p0.relax || q.relaxp != p0.relaxp ||
+            q.building_z0 != p0.building_z0 || q.coriolis != p0.coriolis)
+            return fail(ctx, GRAL_EINVAL, "situations of a batch must share grid and solver controls");
+        if (q.conv_cadence < 1 || q.iteration_steps_max < 1) return fail(ctx, GRAL_EINVAL, "bad iteration controls");
+        if (q.ref_i < 1 || q.ref_i > q.nii || q.ref_j < 1 || q.ref_j > q.njj)
+            return fail(ctx, GRAL_EINVAL, "reference point outside the grid");
+        if (!f[b].uk || !f[b].vk || !f[b].wk) return fail(ctx, GRAL_EINVAL, "null field");
+    }
+    return GRAL_OK;
+}
+
+int build_graph(gral_ctx *ctx) {
+    if (ctx->graph) { cudaGraphExecDestroy(ctx->graph); ctx->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    cudaStream_t st = ctx->stream;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const KArgs &a = ctx->ka;
+    cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st);
+    launch_bc(a, ctx->bc, st);
+    launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
+    launch_velcorr(a, st);
+    launch_average(a, st);
+    launch_mom_ml(0, a, ctx->geo_u.g, ctx->grid_gs[1], st);
+    launch_mom_ml(1, a, ctx->geo_v.g, ctx->grid_gs[2], st);
+    launch_mom_ml(2, a, ctx->geo_p.g, ctx->grid_gs[3], st);
+    launch_bookkeeping(a, st);
+    cudaError_t e = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess) return fail(ctx, GRAL_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ctx->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(ctx, GRAL_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return GRAL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gral_prog_version(void) { return GRAL_PROG_ABI_VERSION; }
+
+int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int32_t max_batch, gral_ctx **out) {
+    if (!out || nii < 4 || njj < 4 || nkk < 3 || kadvmax < 2 || max_batch < 1) return GRAL_EINVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return GRAL_ENODEV;
+    gral_ctx *ctx = new gral_ctx();
+    ctx->cap_nii = nii; ctx->cap_njj = njj; ctx->cap_nkk = nkk; ctx->cap_kadv = kadvmax; ctx->cap_batch = max_batch;
+    cudaGetDevice(&ctx->device);
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
+    for (auto &e : ctx->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
+    *out = ctx;
+    return GRAL_OK;
+}
+
+const char *gral_prog_last_error(gral_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void gral_prog_destroy(gral_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s, gral_fields *f) {
+    int rc = validate(ctx, n, p, s, f);
+    if (rc != GRAL_OK) return rc;
+    CK(cudaSetDevice(ctx->device));
+    const gral_params &p0 = p[0];
+    const int NII = p0.nii, NJJ = p0.njj, NKK = p0.nkk, nj2 = NJJ + 2, ncols = (NII + 2) * nj2;
+    const int nk2 = NKK + 2;
+    const int ks = ((p0.kadvmax + 2) + 7) / 8 * 8;
+    ctx->loaded = false;
+    ctx->nii = NII; ctx->njj = NJJ; ctx->nkk = NKK; ctx->ks = ks; ctx->nb = n; ctx->ncols = ncols; ctx->nj2 = nj2;
+    ctx->model = p0.turbulence_model;
+    ctx->params.assign(p, p + n);
+    ctx->fields.assign(f, f + n);
+    ctx->it_min = p0.iteration_steps_min; ctx->it_max = p0.iteration_steps_max; ctx->cadence = p0.conv_cadence;
+
+    // ---- per-column constants ----
+    std::vector<ColMeta> meta;
+    std::vector<uint32_t> cfl;
+    std::vector<ColF> colf;
+    int vi_min = 0, vi_max = 0;
+    rc = build_meta(ctx, p0, *s, meta, cfl, colf, vi_min, vi_max);
+    if (rc != GRAL_OK) return rc;
+    if (vi_max + 1 >= ks) return fail(ctx, GRAL_EINVAL, "VerticalIndex above KADVMAX");
+
+    // ---- level tables (float, reference expressions) ----
+    const float DXK = p0.dxk, DYK = p0.dyk, AREA = DXK * DYK;
+    std::vector<float> tab(5 * ks, 0.0f);   // dzk, hokart, app, abp, atp
+    for (int k = 0; k < ks; ++k) {
+        tab[k] = (k < nk2) ? s->dzk[k] : 0.0f;
+        tab[ks + k] = (k < nk2) ? s->hokart[k] : 0.0f;
+    }
+    for (int k = 1; k < ks - 1 && k + 1 < nk2; ++k) {                    // PrognosticFlowfield.cs:857-866
+        const float *DZ = s->dzk;
+        tab[2 * ks + k] = 2.0f * (DYK * DZ[k] / DXK + DXK * DZ[k] / DYK + AREA / DZ[k]);
+        tab[3 * ks + k] = (k > 1) ? AREA / (0.5f * (DZ[k - 1] + DZ[k])) : AREA / DZ[k];
+        tab[4 * ks + k] = AREA / (0.5f * (DZ[k + 1] + DZ[k]));
+    }
+
+    // ---- per-situation scalars (:146-163, 231-240, 406-407) ----
+    ctx->h_sit.assign(n, SitDev{});
+    std::vector<float> ap0((size_t)n * ks, 0.0f);
+    for (int b = 0; b < n; ++b) {
+        const gral_params &q = p[b];
+        const int rx = q.ref_i, ry = q.ref_j;
+        auto I3 = [&](int i, int j, int k) { return ((size_t)i * nj2 + j) * nk2 + k; };
+        const float *UK = f[b].uk, *VK = f[b].vk;
+        const float u1 = UK[I3(rx, ry, NKK - 1)], v1 = VK[I3(rx, ry, NKK - 1)];
+        float topwind = (float)std::sqrt((double)(u1 * u1 + v1 * v1));
+        topwind = net_max(topwind, 0.01f);
+        const float u2 = UK[I3(rx, ry, q.kadvmax)], v2 = VK[I3(rx, ry, q.kadvmax)];
+        float DT = 0.5f * net_min(DXK, s->dzk[1]) / net_max(0.01f, sqrtf(u2 * u2 + v2 * v2));
+        DT = net_min(DT, 5.0f);
+        for (int k = 1; k <= q.kadvmax; ++k) ap0[(size_t)b * ks + k] = AREA * s->dzk[k] / DT;
+        SitDev &S = ctx->h_sit[b];
+        S.frund = (double)((q.turbulence_model == 2 ? 10000 : 8000) / topwind);
+        S.conv_threshold = q.conv_threshold;
+        S.dtime = DT;
+        S.topwind = topwind;
+        const bool alloc = (cfl[rx * nj2 + ry] & F_ALLOC3) != 0;
+        S.ug = alloc ? 0.5f * (UK[I3(rx, ry, NKK - 1)] + UK[I3(rx + 1, ry, NKK - 1)]) : 0.0f;
+        S.vg = alloc ? 0.5f * (VK[I3(rx, ry, NKK - 1)] + VK[I3(rx, ry + 1, NKK - 1)]) : 0.0f;
+        S.it = 1;
+        S.active = 1;
+        S.it_min = q.iteration_steps_min;
+        S.it_max = q.iteration_steps_max;
+        S.cadence = q.conv_cadence;
+        S.quantise = q.quantise;
+    }
+
+    // ---- boundary-condition event lists ----
+    std::vector<int> wptr(nj2 + 1, 0), wev, sptr(NII + 3, 0), sev;
+    auto adv = [&](int i, int j) { return s->advdom[i * nj2 + j]; };
+    for (int j = 0; j <= NJJ + 1; ++j) {
+        wptr[j] = (int)wev.size();
+        if (j >= 2 && j <= NJJ)
+            for (int i = 3; i <= NII - 1; ++i) {
+                if (adv(i, j) != 1) continue;
+                const bool iM = (adv(i - 1, j) < 1) || (i == 3), iP = (adv(i + 1, j) < 1) || (i == NII - 1);
+                if (iM || iP) wev.push_back(i | (iM << 16) | (iP << 17));
+            }
+    }
+    wptr[nj2] = (int)wev.size();
+    for (int i = 0; i <= NII + 1; ++i) {
+        sptr[i] = (int)sev.size();
+        if (i >= 2 && i <= NII)
+            for (int j = 3; j <= NJJ - 1; ++j) {
+                if (adv(i, j) != 1) continue;
+                const bool jM = (adv(i, j - 1) < 1) || (j == 3), jP = (adv(i, j + 1) < 1) || (j == NJJ - 1);
+                if (jM || jP) sev.push_back(j | (jM << 16) | (jP << 17));
+            }
+    }
+    sptr[NII + 2] = (int)sev.size();
+
+    // ---- sweeps ----
+    ctx->geo_p = make_geom(2, NII - 2, 2, NJJ - 2);
+    ctx->geo_u = make_geom(3, NII - 3, 2, NJJ - 2);
+    ctx->geo_v = make_geom(2, NII - 2, 3, NJJ - 3);
+
+    // ---- device memory ----
+    const size_t fsz = (size_t)n * ncols * ks;
+    const int nfields = 10;
+    const size_t ssz = (size_t)ncols * nk2;
+    const int nstage = (ctx->model != 1) ? 5 : 3;
+    const int tcap = ctx->it_max;
+    CK(ctx->slab.ensure(fsz * nfields));
+    CK(ctx->stage.ensure(ssz * nstage * n));
+    CK(ctx->meta.ensure(ncols));
+    CK(ctx->cflags.ensure(ncols));
+    CK(ctx->colf.ensure(ncols));
+    CK(ctx->tables.ensure(5 * ks));
+    CK(ctx->ap0.ensure((size_t)n * ks));
+    CK(ctx->sit.ensure(n));
+    CK(ctx->flags.ensure((size_t)n * ncols));
+    CK(ctx->rowcarry.ensure((size_t)n * nj2 * 2 * ks));
+    CK(ctx->trace.ensure((size_t)n * tcap));
+    CK(ctx->misc.ensure(2 + n));                      // err, nact, act[n]
+    CK(ctx->counters.ensure(8));
+    CK(ctx->counts.ensure(4 * (size_t)n));
+    const size_t dsz = ctx->geo_p.ds.size() + ctx->geo_u.ds.size() + ctx->geo_v.ds.size();
+    CK(ctx->diag.ensure(dsz));
+    CK(ctx->bcl.ensure(wptr.size() + wev.size() + sptr.size() + sev.size() + 4));
+    const bool has_veg = s->veg && s->veg_mask;
+    if (has_veg) CK(ctx->veg.ensure((size_t)ncols * ks));
+
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    float *slab = ctx->slab.p;
+    KArgs &a = ctx->ka;
+    a = KArgs{};
+    a.nii = NII; a.njj = NJJ; a.nkk = NKK; a.ks = ks; a.nj2 = nj2; a.ncols = ncols; a.nb = n;
+    a.dxk = DXK; a.dyk = DYK; a.areaxy = AREA;
+    a.relax = p0.relax; a.relaxp = p0.relaxp; a.coriolis = p0.coriolis;
+    a.vishmin = (p0.turbulence_model == 2) ? 0.01f : 0.0f;
+    a.simd = p0.simd_width;
+    a.meta = ctx->meta.p; a.cflags = ctx->cflags.p; a.colf = ctx->colf.p;
+    a.dzk = ctx->tables.p; a.hokart = ctx->tables.p + ks;
+    a.app = ctx->tables.p + 2 * ks; a.abp = ctx->tables.p + 3 * ks; a.atp = ctx->tables.p + 4 * ks;
+    a.veg = has_veg ? ctx->veg.p : nullptr;
+    a.sit = ctx->sit.p;
+    a.ap0 = ctx->ap0.p;
+    float **fp[10] = {&a.uk, &a.vk, &a.wk, &a.dpm, &a.dpmnew, &a.uks, &a.vks, &a.wks, &a.turb, &a.tdiss};
+    for (int q = 0; q < nfields; ++q) *fp[q] = slab + fsz * q;
+    a.flags = ctx->flags.p;
+    a.counters = ctx->counters.p;
+    a.rowcarry = ctx->rowcarry.p;
+    a.err = ctx->misc.p;
+    a.nact = ctx->misc.p + 1;
+    a.act = ctx->misc.p + 2;
+    a.wait_limit_ns = 2000000000ull;
+    a.trace = ctx->trace.p;
+    a.trace_cap = tcap;
+    a.vi_min = vi_min;
+
+    Staging &sg = ctx->sg;
+    sg.stride = ssz;
+    sg.uk = ctx->stage.p;
+    sg.vk = sg.uk + ssz * n;
+    sg.wk = sg.vk + ssz * n;
+    sg.turb = (nstage == 5) ? sg.wk + ssz * n : nullptr;
+    sg.tdiss = (nstage == 5) ? sg.turb + ssz * n : nullptr;
+    sg.stride = ssz;
+    // situation b's staging block is at sg.X + b*ssz: fields are grouped per field, per situation.
+
+    // geometry tables
+    int *dp = ctx->diag.p;
+    auto put_geom = [&](Geom &G) {
+        G.g.diag_start = dp;
+        cudaMemcpyAsync(dp, G.ds.data(), G.ds.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+        dp += G.ds.size();
+    };
+    put_geom(ctx->geo_p);
+    put_geom(ctx->geo_u);
+    put_geom(ctx->geo_v);
+    int *bp = ctx->bcl.p;
+    auto put_ints = [&](const std::vector<int> &v) {
+        int *dst = bp;
+        if (!v.empty()) cudaMemcpyAsync(bp, v.data(), v.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+        bp += v.size() + 1;
+        return (const int *)dst;
+    };
+    ctx->bc.we_ptr = put_ints(wptr);
+    ctx->bc.we_ev = put_ints(wev);
+    ctx->bc.sn_ptr = put_ints(sptr);
+    ctx->bc.sn_ev = put_ints(sev);
+
+    CK(cudaMemcpyAsync(ctx->meta.p, meta.data(), ncols * sizeof(ColMeta), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->cflags.p, cfl.data(), ncols * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->colf.p, colf.data(), ncols * sizeof(ColF), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->tables.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->ap0.p, ap0.data(), ap0.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->sit.p, ctx->h_sit.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
+    ctx->h_act.resize(2 + n);
+    ctx->h_act[0] = 0;
+    ctx->h_act[1] = n;
+    for (int b = 0; b < n; ++b) ctx->h_act[2 + b] = b;
+    CK(cudaMemcpyAsync(ctx->misc.p, ctx->h_act.data(), (2 + n) * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (has_veg) {
+        std::vector<float> vs((size_t)ncols * ks, 0.0f);
+        for (int c = 0; c < ncols; ++c)
+            for (int k = 0; k < ks && k < nk2; ++k) vs[(size_t)c * ks + k] = s->veg[(size_t)c * nk2 + k];
+        CK(cudaMemcpyAsync(ctx->veg.p, vs.data(), vs.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    CK(cudaMemsetAsync(slab, 0, fsz * nfields * sizeof(float), st));
+    CK(cudaMemsetAsync(ctx->flags.p, 0, (size_t)n * ncols * sizeof(int), st));
+    CK(cudaMemsetAsync(ctx->rowcarry.p, 0, (size_t)n * nj2 * 2 * ks * sizeof(float), st));
+    CK(cudaMemsetAsync(ctx->trace.p, 0, (size_t)n * tcap * sizeof(float), st));
+    // host fields -> staging (one contiguous copy per field and situation)
+    for (int b = 0; b < n; ++b) {
+        CK(cudaMemcpyAsync(sg.uk + ssz * b, f[b].uk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(sg.vk + ssz * b, f[b].vk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(sg.wk + ssz * b, f[b].wk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+    }
+    launch_setup(a, sg, ctx->model, st);
+    launch_gather(a, sg, ctx->model, st);
+    CK(cudaGetLastError());
+
+    // ---- launch shapes of the wavefront kernels ----
+    const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
+    for (int q = 0; q < 4; ++q) {
+        int bps = 0;
+        CK(gs_occupancy(kinds[q], &bps));
+        ctx->grid_gs[q] = std::max(1, bps) * ctx->num_sms;
+    }
+    const int warps = ctx->grid_gs[0] * gs_block_threads() / 32;
+    const long long per_diag = (long long)n * std::min(NII, NJJ);
+    a.chunk = (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
+    ctx->it_host = 1;
+    int brc = build_graph(ctx);
+    if (brc != GRAL_OK) return brc;
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaEventElapsedTime(&ctx->ms_upload, ctx->ev[0], ctx->ev[1]));
+    ctx->loaded = true;
+    return GRAL_OK;
+}
+
+int gral_prog_iterate(gral_ctx *ctx) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "iterate before load");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int nact = ctx->h_act[1];
+    while (nact > 0 && ctx->it_host <= ctx->it_max) {
+        // run up to the next iteration where the reference can stop (a convergence test or the limit)
+        const int c = ctx->cadence;
+        int stop = ((ctx->it_host + c - 1) / c) * c;
+        if (stop < ctx->it_host) stop = ctx->it_host;
+        stop = std::min(stop, ctx->it_max);
+        for (int it = ctx->it_host; it <= stop; ++it) CK(cudaGraphLaunch(ctx->graph, st));
+        ctx->it_host = stop + 1;
+        int herr = 0;
+        CK(cudaMemcpyAsync(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(ctx->h_sit.data(), ctx->sit.p, ctx->nb * sizeof(SitDev), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "a wavefront wait exceeded its time limit");
+        std::vector<int> act;
+        for (int b = 0; b < ctx->nb; ++b)
+            if (ctx->h_sit[b].active) act.push_back(b);
+        if ((int)act.size() != nact) {
+            nact = (int)act.size();
+            ctx->h_act[1] = nact;
+            for (int q = 0; q < nact; ++q) ctx->h_act[2 + q] = act[q];
+            CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, (1 + std::max(nact, 1)) * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+        }
+    }
+    return GRAL_OK;
+}
+
+int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "store before load");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const int n = ctx->nb;
+    if (!f) f = ctx->fields.data();
+    // post-checks run on every situation regardless of its loop state
+    for (int b = 0; b < n; ++b) ctx->h_act[2 + b] = b;
+    ctx->h_act[1] = n;
+    std::vector<SitDev> hs(n);
+    CK(cudaMemcpyAsync(hs.data(), ctx->sit.p, n * sizeof(SitDev), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    std::vector<SitDev> tmp = hs;
+    for (auto &x : tmp) x.active = 1;
+    CK(cudaMemcpyAsync(ctx->sit.p, tmp.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, (1 + n) * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->counts.p, 0, 4 * n * sizeof(int), st));
+    CK(cudaEventRecord(ctx->ev[2], st));
+    launch_postcheck(ctx->ka, ctx->counts.p, st);
+    launch_scatter(ctx->ka, ctx->sg, ctx->model, st);
+    CK(cudaGetLastError());
+    const size_t ssz = ctx->sg.stride;
+    for (int b = 0; b < n; ++b) {
+        CK(cudaMemcpyAsync(f[b].uk, ctx->sg.uk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(f[b].vk, ctx->sg.vk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(f[b].wk, ctx->sg.wk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
+    std::vector<int> counts(4 * n);
+    CK(cudaMemcpyAsync(counts.data(), ctx->counts.p, 4 * n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ctx->sit.p, hs.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
+    CK(cudaEventRecord(ctx->ev[3], st));
+    CK(cudaStreamSynchronize(st));
+    float ms_down = 0.f;
+    cudaEventElapsedTime(&ms_down, ctx->ev[2], ctx->ev[3]);
+    int rc = GRAL_OK;
+    for (int b = 0; b < n; ++b) {
+        const SitDev &S = hs[b];
+        if (counts[4 * b + 3] > 0) rc = GRAL_ENONFINITE;
+        if (!stats) continue;
+        gral_stats &o = stats[b];
+        o.iterations = S.iters_done;
+        o.iteration_loops = S.it;
+        o.converged = S.converged;
+        o.delta_first = S.delta_first;
+        o.delta_finish = S.delta_finish;
+        o.convergence_problem = (S.delta_finish > S.delta_first) ? 1 : 0;
+        o.n_history = std::min(S.n_hist, GRAL_MAX_HISTORY);
+        for (int q = 0; q < o.n_history; ++q) o.delta_history[q] = S.hist[q];
+        o.uk_unrealistic = counts[4 * b + 0];
+        o.vk_unrealistic = counts[4 * b + 1];
+        o.wk_unrealistic = counts[4 * b + 2];
+        double g;
+        std::memcpy(&g, &S.geschw_bits, sizeof(double));
+        o.geschw_max = g;
+        o.topwind = S.topwind;
+        o.dtime = S.dtime;
+        o.frund = S.frund;
+        o.last_delta_umax = S.last_dumax;
+        if (o.trace_delta_umax && o.trace_capacity > 0) {
+            const int m = std::min(o.trace_capacity, ctx->it_max);
+            CK(cudaMemcpy(o.trace_delta_umax, ctx->trace.p + (size_t)b * ctx->it_max, m * sizeof(float),
+                          cudaMemcpyDeviceToHost));
+        }
+        o.ms_upload = ctx->ms_upload;
+        o.ms_download = ms_down;
+    }
+    if (rc != GRAL_OK) fail(ctx, rc, "non-finite values in the solved fields");
+    return rc;
+}
+
+int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s, gral_fields *f,
+                          gral_stats *stats) {
+    int rc = gral_prog_load(ctx, n, p, s, f);
+    if (rc != GRAL_OK) return rc;
+    cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1];
+    cudaEventRecord(e0, ctx->stream);
+    rc = gral_prog_iterate(ctx);
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms_it = 0.f;
+    cudaEventElapsedTime(&ms_it, e0, e1);
+    if (rc != GRAL_OK) return rc;
+    rc = gral_prog_store(ctx, f, stats);
+    if (stats)
+        for (int b = 0; b < n; ++b) {
+            stats[b].ms_iterate = ms_it;
+            stats[b].ms_total = stats[b].ms_upload + ms_it + stats[b].ms_download;
+        }
+    return rc;
+}
+
+int gral_prog_solve(gral_ctx *ctx, const gral_params *p, const gral_static *s, gral_fields *f, gral_stats *stats) {
+    return gral_prog_solve_batch(ctx, 1, p, s, f, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,42 @@
+// prog_kernels.cuh -- host-side launchers of the solver kernels (implemented in prog_gs.cu and
+// prog_kernels.cu).  Every launcher enqueues on the given stream and returns immediately.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "prog_common.cuh"
+
+namespace gral {
+
+// Boundary-condition event lists (PrognosticFlowfield.cs:595-696): for the W/E pass one list per
+// row j of the columns i (ascending) that copy inflow; for the S/N pass one list per column i.
+// Entry = index | (west_or_south << 16) | (east_or_north << 17).
+struct BcLists {
+    const int *we_ptr, *we_ev;   // we_ptr[j]..we_ptr[j+1]
+    const int *sn_ptr, *sn_ev;   // sn_ptr[i]..sn_ptr[i+1]
+};
+
+// Full-height staging copies of the host fields of one situation: [NII+2][NJJ+2][NKK+2].
+struct Staging {
+    float *uk, *vk, *wk, *turb, *tdiss;
+    size_t stride;   // floats between situations
+};
+
+int gs_block_threads();
+cudaError_t gs_occupancy(int kind, int *blocks_per_sm);
+void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
+void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
+
+void launch_bc(const KArgs &a, const BcLists &bc, cudaStream_t st);
+void launch_velcorr(const KArgs &a, cudaStream_t st);
+void launch_average(const KArgs &a, cudaStream_t st);
+void launch_bookkeeping(const KArgs &a, cudaStream_t st);
+
+// set-up and tear-down of a batch (PrognosticFlowfield.cs:295-329, 410-579)
+void launch_setup(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
+void launch_gather(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
+void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
+// post-checks (PrognosticFlowfield.cs:1193-1243); counts[s*4 + 0..3] = UK, VK, WK, non-finite
+void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st);
+
+}  // namespace gral

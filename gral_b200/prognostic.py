@@ -1,0 +1,147 @@
+"""Host-side mirror of ``PrognosticFlowfield.Calculate()`` over the C ABI of ``libgralprog.so``.
+
+``PrognosticSolver.calculate`` is the drop-in for one weather situation: it reads the fields,
+runs the SIMPLE loop on the GPU and writes UK/VK/WK (and TURB/TDISS) back in place, like the
+reference's static method does with ``Program.UK/VK/WK`` (PrognosticFlowfield.cs:32).
+``calculate_batch`` solves many situations of one grid together.  There is no CPU fallback:
+a missing library or GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import build as _build
+from .abi import (GRAL_OK, STATUS_NAMES, FieldArrays, GralFields, GralParams, GralStatic, GralStats,
+                  StaticArrays, params_to_c, stats_to_dict)
+
+_lib = None
+
+EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_prog_solve_batch",
+           "gral_prog_load", "gral_prog_iterate", "gral_prog_store", "gral_prog_last_error",
+           "gral_prog_destroy"]
+
+
+class GralError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {message}")
+        self.code = code
+
+
+def lib(build_if_stale: bool = True):
+    """Load libgralprog.so (building it first when the sources are newer and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if build_if_stale and _build.stale():
+        try:
+            _build.build()
+        except RuntimeError:
+            if not os.path.exists(path):
+                raise
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing; run `python -m gral_b200.build`")
+    L = C.CDLL(path)
+    L.gral_prog_version.restype = C.c_int
+    L.gral_prog_create.argtypes = [C.c_int32] * 5 + [C.POINTER(C.c_void_p)]
+    L.gral_prog_create.restype = C.c_int
+    L.gral_prog_solve.argtypes = [C.c_void_p, C.POINTER(GralParams), C.POINTER(GralStatic),
+                                  C.POINTER(GralFields), C.POINTER(GralStats)]
+    L.gral_prog_solve.restype = C.c_int
+    L.gral_prog_solve_batch.argtypes = [C.c_void_p, C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic),
+                                        C.POINTER(GralFields), C.POINTER(GralStats)]
+    L.gral_prog_solve_batch.restype = C.c_int
+    L.gral_prog_load.argtypes = [C.c_void_p, C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic),
+                                 C.POINTER(GralFields)]
+    L.gral_prog_load.restype = C.c_int
+    L.gral_prog_iterate.argtypes = [C.c_void_p]
+    L.gral_prog_iterate.restype = C.c_int
+    L.gral_prog_store.argtypes = [C.c_void_p, C.POINTER(GralFields), C.POINTER(GralStats)]
+    L.gral_prog_store.restype = C.c_int
+    L.gral_prog_last_error.argtypes = [C.c_void_p]
+    L.gral_prog_last_error.restype = C.c_char_p
+    L.gral_prog_destroy.argtypes = [C.c_void_p]
+    L.gral_prog_destroy.restype = None
+    _lib = L
+    return L
+
+
+class PrognosticSolver:
+    """A solver context for grids up to (nii, njj, nkk, kadvmax) and up to max_batch situations."""
+
+    def __init__(self, nii: int, njj: int, nkk: int, kadvmax: int, max_batch: int = 1):
+        self._L = lib()
+        self._ctx = C.c_void_p()
+        rc = self._L.gral_prog_create(nii, njj, nkk, kadvmax, max_batch, C.byref(self._ctx))
+        if rc != GRAL_OK:
+            raise GralError(rc, "gral_prog_create failed")
+        self._keep: list = []
+
+    def _check(self, rc: int):
+        if rc != GRAL_OK:
+            msg = self._L.gral_prog_last_error(self._ctx).decode()
+            raise GralError(rc, msg)
+
+    def close(self):
+        if self._ctx:
+            self._L.gral_prog_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _stats_array(n: int, traces: Optional[Sequence[np.ndarray]]):
+        st = (GralStats * n)()
+        if traces is not None:
+            for b, t in enumerate(traces):
+                st[b].trace_delta_umax = t.ctypes.data_as(C.POINTER(C.c_float))
+                st[b].trace_capacity = t.size
+        return st
+
+    def calculate(self, params: dict, static: StaticArrays, fields: FieldArrays,
+                  trace: Optional[np.ndarray] = None) -> dict:
+        """One situation, in place on ``fields``; returns the run statistics."""
+        return self.calculate_batch([params], static, [fields], None if trace is None else [trace])[0]
+
+    def calculate_batch(self, params: Sequence[dict], static: StaticArrays, fields: Sequence[FieldArrays],
+                        traces: Optional[Sequence[np.ndarray]] = None) -> List[dict]:
+        n = len(params)
+        pa = (GralParams * n)(*[params_to_c(p) for p in params])
+        s = static.to_c()
+        fa = (GralFields * n)(*[f.to_c() for f in fields])
+        st = self._stats_array(n, traces)
+        self._check(self._L.gral_prog_solve_batch(self._ctx, n, pa, C.byref(s), fa, st))
+        return [stats_to_dict(st[b]) for b in range(n)]
+
+    # split form: inputs resident on the device between load and store
+    def load(self, params: Sequence[dict], static: StaticArrays, fields: Sequence[FieldArrays]):
+        n = len(params)
+        pa = (GralParams * n)(*[params_to_c(p) for p in params])
+        s = static.to_c()
+        fa = (GralFields * n)(*[f.to_c() for f in fields])
+        self._keep = [pa, s, fa, static, fields]
+        self._check(self._L.gral_prog_load(self._ctx, n, pa, C.byref(s), fa))
+
+    def iterate(self):
+        self._check(self._L.gral_prog_iterate(self._ctx))
+
+    def store(self, fields: Sequence[FieldArrays], traces=None) -> List[dict]:
+        n = len(fields)
+        fa = (GralFields * n)(*[f.to_c() for f in fields])
+        st = self._stats_array(n, traces)
+        self._check(self._L.gral_prog_store(self._ctx, fa, st))
+        return [stats_to_dict(st[b]) for b in range(n)]
