@@ -1,0 +1,327 @@
+"""Benchmark of the B200 prognostic microscale flow solver.
+
+Metric: Mcell-iterations/s (nominal cells = ADVDOM columns x VertCellsFF, per SIMPLE iteration).
+A "step" is one SIMPLE iteration over the whole workload.  Default workload: the production-size
+plain solve, 400x400 cells at 2 m with 30 prognostic levels (stretch 1.05, NKK 63, KADVMAX 41),
+64 seeded buildings 10-30 m tall, inflow from 225 deg at 2 m/s (z0 0.5 m, neutral), mixing-length
+model; synthetic, seeded inputs.
+
+  value      device-resident throughput: K timed iterations after W warm-up iterations, CUDA
+             events on the solver's stream, inputs already in HBM (working set > L2).
+  e2e        one full solve through the public C ABI (gral_prog_solve: pinned host buffers in,
+             set-up, 500 SIMPLE iterations, post-checks, fields back to the host), host-timed.
+  roofline   dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration,
+             against the measured HBM copy bandwidth.
+  cpu_baseline  the CPU oracle (a single-threaded restatement of the reference's deterministic
+             solver) on a bounded sample of the same workload.
+
+`--impl reference` times that CPU restatement on all host cores (one independent situation per
+worker process) on the same workload and prints the same metric.
+Multi-GPU (torchrun): every rank solves its own replica of the workload (a single situation does
+not shard); value = all ranks' cell-iterations / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mcell-iterations/s on 1 B200 (batched vs plain, ≤1e-4 rel err); HBM fraction"
+UNIT = "Mcell-iterations/s"
+BYTES_PER_CELL = {"pressure": 24, "velcorr": 28, "u": 20, "v": 20, "w": 20}   # model 1
+
+
+def workload(name: str):
+    from gral_b200 import prep
+    if name == "production":
+        dom = prep.city_domain(n=400, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30, n_buildings=64, seed=2)
+        sit = prep.Situation(direction_deg=225.0, speed_10m=2.0, z0=0.5, ustar=0.3)
+        return dom, sit, 500, "400x400x30 at 2 m, stretch 1.05, 64 buildings, 225 deg 2 m/s, z0 0.5, 500 iterations"
+    if name == "cube":
+        dom = prep.cube_domain(n=100, dx=2.0, dz1=2.0, stretch=1.01, vert_cells_ff=20, z0=0.2, ustar=0.3)
+        sit = prep.Situation(direction_deg=270.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+        return dom, sit, 100, "100x100x20 at 2 m, stretch 1.01, one 20 m cube, 270 deg 3 m/s, z0 0.2, 100 iterations"
+    raise SystemExit(f"unknown workload {name}")
+
+
+def nominal_cells(dom) -> int:
+    adv = dom.static.advdom[1:dom.nii + 1, 1:dom.njj + 1]
+    return int((adv == 1).sum()) * dom.vert_cells_ff
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str):
+    """dram bytes per launch of `kernel` from a committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                parts = line.split()
+                if len(parts) >= 2 and parts[0] == kernel:
+                    return float(parts[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "", 1).isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def pinned_fields(f):
+    """Copies of the initial fields in page-locked host memory (torch pinned tensors)."""
+    import torch
+    from gral_b200.abi import FieldArrays
+
+    def pin(a):
+        if a is None:
+            return None
+        t = torch.empty(a.shape, dtype=torch.float32, pin_memory=True)
+        n = t.numpy()
+        n[...] = a
+        return n
+    return FieldArrays(pin(f.uk), pin(f.vk), pin(f.wk), pin(f.turb), pin(f.tdiss))
+
+
+def cpu_sample(workload_name: str, iterations: int):
+    """The CPU oracle on `iterations` SIMPLE iterations of the workload; returns (Mcell-it/s, s)."""
+    from gral_b200 import prep
+    from oracle import oracle as O
+    dom, sit, _, _ = workload(workload_name)
+    p = dom.params(sit, model=1, iterations=iterations)
+    f = prep.initial_fields(dom, sit)
+    t0 = time.perf_counter()
+    O.solve(p, dom.static, f)
+    dt = time.perf_counter() - t0
+    return nominal_cells(dom) * iterations / dt / 1e6, dt
+
+
+def _cpu_worker(args):
+    name, iters = args
+    return cpu_sample(name, iters)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from oracle import oracle as O
+    O.build()
+    cores = min(os.cpu_count() or 1, args.ref_procs)
+    iters = args.ref_iters
+    ctx = mp.get_context("spawn")
+    times = []
+    total_cells = 0
+    t_all = time.perf_counter()
+    for _ in range(args.warmup if args.ref_warmup else 0):
+        pass
+    for step in range(args.steps):
+        t0 = time.perf_counter()
+        with ctx.Pool(cores) as pool:
+            res = pool.map(_cpu_worker, [(args.workload, iters)] * cores)
+        dt = time.perf_counter() - t0
+        times.append(max(r[1] for r in res))
+    dom, _, _, desc = workload(args.workload)
+    cells = nominal_cells(dom)
+    per_step = statistics.median(times)
+    value = cells * iters * cores / per_step / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": {"workload": args.workload, "description": desc,
+                                       "cells_per_situation": cells, "situations_per_step": cores,
+                                       "iterations_per_situation": iters},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{cores} independent situations x {iters} SIMPLE iterations each, "
+                                   f"one process per core (deterministic single-thread restatement)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from gral_b200 import prep
+    from gral_b200.prognostic import PHASES, PrognosticSolver
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist = world > 1
+    if dist:
+        import datetime
+        import torch.distributed as td
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    dom, sit, full_iters, desc = workload(args.workload)
+    cells = nominal_cells(dom)
+    total_iters = args.warmup + args.steps
+    p = dom.params(sit, model=1, iterations=total_iters + 1, iter_min=total_iters + 1)
+    f0 = prep.initial_fields(dom, sit)
+    solver = PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=1)
+    f = f0.copy()
+    solver.load([p], dom.static, [f])
+    solver.iterate_timed(args.warmup)
+    if dist:
+        td.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        tot_ms, phases = solver.iterate_timed(args.steps)
+    torch.cuda.synchronize()
+    t_max = tot_ms
+    if dist:
+        tt = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
+        td.all_reduce(tt, op=td.ReduceOp.MAX)
+        t_max = float(tt.item())
+    value = cells * args.steps * world / (t_max / 1e3) / 1e6
+    ms_per_step = t_max / args.steps
+
+    # roofline of the dominant kernel
+    cand = {k: v for k, v in phases.items() if k in BYTES_PER_CELL}
+    dom_k = max(cand, key=cand.get)
+    per_launch_s = cand[dom_k] / args.steps / 1e3
+    alg_bytes = cells * BYTES_PER_CELL[dom_k]
+    achieved = alg_bytes / per_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = profile_traffic({"pressure": "k_pressure", "u": "k_mom_u1", "v": "k_mom_v1",
+                               "w": "k_mom_w1", "velcorr": "k_velcorr"}[dom_k])
+    it_bytes = cells * sum(BYTES_PER_CELL.values())
+    hbm_frac_iteration = it_bytes / (ms_per_step / 1e3) / 1e9 / peak
+    solver.store([f])
+    solver.close()
+
+    # end to end through the public ABI: pinned host buffers, full solve, fields back
+    e2e = None
+    if not args.no_e2e:
+        pe = dom.params(sit, model=1, iterations=args.e2e_iters, iter_min=args.e2e_iters)
+        fp = pinned_fields(f0)
+        with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=1) as s2:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = s2.calculate(pe, dom.static, fp)
+            dt = time.perf_counter() - t0
+        if dist:
+            tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
+            td.all_reduce(tt, op=td.ReduceOp.MAX)
+            dt = float(tt.item())
+        nbytes = sum(a.nbytes for a in (fp.uk, fp.vk, fp.wk))
+        e2e = {"value": round(cells * st["iterations"] * world / dt / 1e6, 3), "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "iterations": st["iterations"], "seconds": round(dt, 4)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, dt = cpu_sample(args.workload, args.cpu_iters)
+        cpu = {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s), "
+                         "single-threaded deterministic restatement"}
+
+    launches = {"bc": 3, "pressure": 1, "velcorr": 1, "average": 1, "u": 1, "v": 1, "w": 1, "bookkeeping": 1}
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "description": desc, "cells": cells,
+                   "grid": [dom.nii, dom.njj, dom.nkk], "kadvmax": dom.kadvmax, "model": 1,
+                   "simd_parity_width": 8, "l2": "working set above L2 (8 fields x 31 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
+        "roofline": {"bound": "hbm", "kernel": dom_k, "achieved": round(achieved, 2), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 5),
+                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                     "hbm_frac_iteration": round(hbm_frac_iteration, 5)},
+        "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": sum(launches.values()) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        td.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["production", "cube"], default="production")
+    ap.add_argument("--e2e-iters", type=int, default=500)
+    ap.add_argument("--cpu-iters", type=int, default=8)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iters", type=int, default=4)
+    ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--ref-warmup", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", args.gpus))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -595,6 +595,61 @@ int gral_prog_iterate(gral_ctx *ctx) {
     return GRAL_OK;
 }
 
+int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms, double *total_ms) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "iterate before load");
+    if (iterations < 1) return fail(ctx, GRAL_EINVAL, "iterations must be >= 1");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const KArgs &a = ctx->ka;
+    const int marks = GRAL_NUM_PHASES + 1;
+    std::vector<cudaEvent_t> ev((size_t)iterations * marks, nullptr);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    for (int it = 0; it < iterations; ++it) {
+        cudaEvent_t *E = ev.data() + (size_t)it * marks;
+        CK(cudaEventRecord(E[GRAL_PHASE_BC], st));
+        CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st));
+        launch_bc(a, ctx->bc, st);
+        CK(cudaEventRecord(E[GRAL_PHASE_PRESSURE], st));
+        launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
+        CK(cudaEventRecord(E[GRAL_PHASE_VELCORR], st));
+        launch_velcorr(a, st);
+        CK(cudaEventRecord(E[GRAL_PHASE_AVERAGE], st));
+        launch_average(a, st);
+        CK(cudaEventRecord(E[GRAL_PHASE_U], st));
+        launch_mom_ml(0, a, ctx->geo_u.g, ctx->grid_gs[1], st);
+        CK(cudaEventRecord(E[GRAL_PHASE_V], st));
+        launch_mom_ml(1, a, ctx->geo_v.g, ctx->grid_gs[2], st);
+        CK(cudaEventRecord(E[GRAL_PHASE_W], st));
+        launch_mom_ml(2, a, ctx->geo_p.g, ctx->grid_gs[3], st);
+        CK(cudaEventRecord(E[GRAL_PHASE_TKE], st));
+        CK(cudaEventRecord(E[GRAL_PHASE_BOOKKEEPING], st));
+        launch_bookkeeping(a, st);
+        CK(cudaEventRecord(E[GRAL_NUM_PHASES], st));
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    int herr = 0;
+    CK(cudaMemcpy(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost));
+    double ph[GRAL_NUM_PHASES] = {0};
+    for (int it = 0; it < iterations; ++it) {
+        cudaEvent_t *E = ev.data() + (size_t)it * marks;
+        for (int q = 0; q < GRAL_NUM_PHASES; ++q) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, E[q], E[q + 1]));
+            ph[q] += ms;
+        }
+    }
+    float tot = 0.f;
+    CK(cudaEventElapsedTime(&tot, ev.front(), ev.back()));
+    for (auto &e : ev) cudaEventDestroy(e);
+    ctx->it_host += iterations;
+    if (phase_ms) for (int q = 0; q < GRAL_NUM_PHASES; ++q) phase_ms[q] = ph[q];
+    if (total_ms) *total_ms = tot;
+    if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "a wavefront wait exceeded its time limit");
+    return GRAL_OK;
+}
+
 int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
     if (!ctx) return GRAL_EINVAL;
     if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "store before load");

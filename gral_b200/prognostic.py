@@ -21,8 +21,10 @@ from .abi import (GRAL_OK, STATUS_NAMES, FieldArrays, GralFields, GralParams, Gr
 _lib = None
 
 EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_prog_solve_batch",
-           "gral_prog_load", "gral_prog_iterate", "gral_prog_store", "gral_prog_last_error",
-           "gral_prog_destroy"]
+           "gral_prog_load", "gral_prog_iterate", "gral_prog_iterate_timed", "gral_prog_store",
+           "gral_prog_last_error", "gral_prog_destroy"]
+
+PHASES = ["bc", "pressure", "velcorr", "average", "u", "v", "w", "tke", "bookkeeping"]
 
 
 class GralError(RuntimeError):
@@ -60,6 +62,8 @@ def lib(build_if_stale: bool = True):
     L.gral_prog_load.restype = C.c_int
     L.gral_prog_iterate.argtypes = [C.c_void_p]
     L.gral_prog_iterate.restype = C.c_int
+    L.gral_prog_iterate_timed.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.gral_prog_iterate_timed.restype = C.c_int
     L.gral_prog_store.argtypes = [C.c_void_p, C.POINTER(GralFields), C.POINTER(GralStats)]
     L.gral_prog_store.restype = C.c_int
     L.gral_prog_last_error.argtypes = [C.c_void_p]
@@ -138,6 +142,13 @@ class PrognosticSolver:
 
     def iterate(self):
         self._check(self._L.gral_prog_iterate(self._ctx))
+
+    def iterate_timed(self, iterations: int):
+        """Run exactly `iterations` SIMPLE iterations; returns (total_ms, {phase: summed ms})."""
+        ph = (C.c_double * len(PHASES))()
+        tot = C.c_double()
+        self._check(self._L.gral_prog_iterate_timed(self._ctx, iterations, ph, C.byref(tot)))
+        return tot.value, {name: ph[q] for q, name in enumerate(PHASES)}
 
     def store(self, fields: Sequence[FieldArrays], traces=None) -> List[dict]:
         n = len(fields)

@@ -143,6 +143,25 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
 int gral_prog_iterate(gral_ctx *ctx);
 int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats);
 
+/* Phases of one SIMPLE iteration, in launch order, as reported by gral_prog_iterate_timed. */
+#define GRAL_NUM_PHASES 9
+#define GRAL_PHASE_BC 0          /* lateral and top boundary conditions, PrognosticFlowfield.cs:595-714 */
+#define GRAL_PHASE_PRESSURE 1    /* divergence + pressure-correction TDMA sweep, :723-901 */
+#define GRAL_PHASE_VELCORR 2     /* velocity correction with Frund rounding, :904-949 */
+#define GRAL_PHASE_AVERAGE 3     /* staggered-grid averages, :958-1039 */
+#define GRAL_PHASE_U 4           /* U momentum (U-prognostic-microscale_*.cs) */
+#define GRAL_PHASE_V 5           /* V momentum */
+#define GRAL_PHASE_W 6           /* W momentum */
+#define GRAL_PHASE_TKE 7         /* k and eps transport (model 2) */
+#define GRAL_PHASE_BOOKKEEPING 8 /* convergence bookkeeping, :1144-1178 */
+
+/* Instrumentation: runs exactly `iterations` SIMPLE iterations on the loaded situations (the
+ * convergence bookkeeping still runs, so a situation that meets the reference's stop rule stops
+ * updating), launching each phase separately with CUDA events between phases and no host
+ * synchronisation inside the run.  phase_ms[GRAL_NUM_PHASES] receives the summed device time of
+ * each phase, total_ms the device time of the whole run.  Either pointer may be NULL. */
+int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms, double *total_ms);
+
 /* Text of the last error on this context (never NULL). */
 const char *gral_prog_last_error(gral_ctx *ctx);
 
