@@ -45,6 +45,10 @@ def workload(name: str):
         dom = prep.city_domain(n=400, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30, n_buildings=64, seed=2)
         sit = prep.Situation(direction_deg=225.0, speed_10m=2.0, z0=0.5, ustar=0.3)
         return dom, sit, 500, "400x400x30 at 2 m, stretch 1.05, 64 buildings, 225 deg 2 m/s, z0 0.5, 500 iterations"
+    if name == "batched":
+        dom = prep.city_domain(n=400, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30, n_buildings=64, seed=2)
+        return dom, None, 800, ("144 situations (36 directions x 4 speeds, seeded stability) on the 400x400x30 "
+                                "production grid, up to 800 iterations")
     if name == "cube":
         dom = prep.cube_domain(n=100, dx=2.0, dz1=2.0, stretch=1.01, vert_cells_ff=20, z0=0.2, ustar=0.3)
         sit = prep.Situation(direction_deg=270.0, speed_10m=3.0, z0=0.2, ustar=0.3)
@@ -229,13 +233,15 @@ def run_ours(args, rank, world):
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     dom, sit, full_iters, desc = workload(args.workload)
-    cells = nominal_cells(dom)
+    sits = batched_situations(args.batch) if sit is None else [sit]
+    nsit = len(sits)
+    cells = nominal_cells(dom) * nsit
     total_iters = args.warmup + args.steps
-    p = dom.params(sit, model=1, iterations=total_iters + 1, iter_min=total_iters + 1)
-    f0 = prep.initial_fields(dom, sit)
-    solver = PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=1)
-    f = f0.copy()
-    solver.load([p], dom.static, [f])
+    ps = [dom.params(x, model=1, iterations=total_iters + 1, iter_min=total_iters + 1) for x in sits]
+    f0s = [prep.initial_fields(dom, x) for x in sits]
+    solver = PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=nsit)
+    fs = [x.copy() for x in f0s]
+    solver.load(ps, dom.static, fs)
     solver.iterate_timed(args.warmup)
     if dist:
         td.barrier()
@@ -262,31 +268,34 @@ def run_ours(args, rank, world):
                                "w": "k_mom_w1", "velcorr": "k_velcorr"}[dom_k])
     it_bytes = cells * sum(BYTES_PER_CELL.values())
     hbm_frac_iteration = it_bytes / (ms_per_step / 1e3) / 1e9 / peak
-    solver.store([f])
+    solver.store(fs)
     solver.close()
 
     # end to end through the public ABI: pinned host buffers, full solve, fields back
     e2e = None
     if not args.no_e2e:
-        pe = dom.params(sit, model=1, iterations=args.e2e_iters, iter_min=args.e2e_iters)
-        fp = pinned_fields(f0)
-        with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=1) as s2:
+        e2e_iters = args.e2e_iters if args.e2e_iters > 0 else full_iters
+        pes = [dom.params(x, model=1, iterations=e2e_iters, iter_min=e2e_iters) for x in sits]
+        fps = [pinned_fields(x) for x in f0s]
+        del f0s
+        with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=nsit) as s2:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            st = s2.calculate(pe, dom.static, fp)
+            sts = s2.calculate_batch(pes, dom.static, fps)
             dt = time.perf_counter() - t0
+        st = {"iterations": sum(x["iterations"] for x in sts) / nsit}
         if dist:
             tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
             td.all_reduce(tt, op=td.ReduceOp.MAX)
             dt = float(tt.item())
-        nbytes = sum(a.nbytes for a in (fp.uk, fp.vk, fp.wk))
+        nbytes = sum(a.nbytes for fp in fps for a in (fp.uk, fp.vk, fp.wk))
         e2e = {"value": round(cells * st["iterations"] * world / dt / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                "iterations": st["iterations"], "seconds": round(dt, 4)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt = cpu_sample(args.workload, args.cpu_iters)
+        v, dt = cpu_sample("production" if args.workload == "batched" else args.workload, args.cpu_iters)
         cpu = {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"{args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s), "
                          "single-threaded deterministic restatement"}
@@ -296,7 +305,7 @@ def run_ours(args, rank, world):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "description": desc, "cells": cells,
+        "config": {"workload": args.workload, "description": desc, "cells": cells, "situations": nsit,
                    "grid": [dom.nii, dom.njj, dom.nkk], "kadvmax": dom.kadvmax, "model": 1,
                    "simd_parity_width": 8, "l2": "working set above L2 (8 fields x 31 MB)",
                    "parallelism": f"replicas x{world}"},
@@ -321,8 +330,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["production", "cube"], default="production")
-    ap.add_argument("--e2e-iters", type=int, default=500)
+    ap.add_argument("--workload", choices=["production", "batched", "cube"], default="production")
+    ap.add_argument("--batch", type=int, default=144, help="situations of the batched workload")
+    ap.add_argument("--e2e-iters", type=int, default=0, help="iterations of the e2e solve (0: the workload's)")
     ap.add_argument("--cpu-iters", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
