@@ -70,6 +70,8 @@ struct SitDev {
 struct KArgs {
     // geometry
     int nii, njj, nkk, ks, nj2, ncols, nb;
+    int il;                              // 1: interleaved layout (batched family), 0: slab layout
+    int ngroups;                         // groups of 32 situations (interleaved layout)
     float dxk, dyk, areaxy;
     float relax, relaxp, coriolis, vishmin;
     int simd;
@@ -90,8 +92,9 @@ struct KArgs {
     unsigned int *counters;              // task counters, one per GS phase kind
     float *rowcarry;                     // [nb][nj2][2][ks] pressure row carry (P, Q)
     int *err;                            // device error word (0 = ok)
-    const int *act;                      // active situation list
+    const int *act;                      // active situation list (slab layout)
     const int *nact;                     // number of active situations
+    int *it_global;                      // IterationLoops of the batch (all situations in lockstep)
     unsigned long long wait_limit_ns;    // bound of every spin wait
     int chunk;                           // tasks claimed per atomic
     float *trace;                        // [nb][trace_cap] DeltaUMax per iteration, or null

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -57,11 +58,14 @@ struct gral_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {};
     int cap_nii = 0, cap_njj = 0, cap_nkk = 0, cap_kadv = 0, cap_batch = 0;
+    int il_min_batch = 32;
     std::string err = "no error";
 
     // current load
     bool loaded = false;
     int nii = 0, njj = 0, nkk = 0, ks = 0, nb = 0, ncols = 0, nj2 = 0, model = 1;
+    bool il = false;     // interleaved layout + batched kernel family
+    int ngroups = 0;
     int it_host = 1, it_max = 0, it_min = 0, cadence = 100;
     std::vector<gral_params> params;
     std::vector<gral_fields> fields;
@@ -308,6 +312,11 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
     gral_ctx *ctx = new gral_ctx();
     ctx->cap_nii = nii; ctx->cap_njj = njj; ctx->cap_nkk = nkk; ctx->cap_kadv = kadvmax; ctx->cap_batch = max_batch;
     cudaGetDevice(&ctx->device);
+    // GRAL_PROG_LAYOUT=interleaved|slab forces the kernel family regardless of the batch size.
+    if (const char *lay = std::getenv("GRAL_PROG_LAYOUT")) {
+        if (std::strcmp(lay, "interleaved") == 0) ctx->il_min_batch = 1;
+        else if (std::strcmp(lay, "slab") == 0) ctx->il_min_batch = 1 << 30;
+    }
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
     for (auto &e : ctx->ev)
@@ -333,6 +342,12 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     const int NII = p0.nii, NJJ = p0.njj, NKK = p0.nkk, nj2 = NJJ + 2, ncols = (NII + 2) * nj2;
     const int nk2 = NKK + 2;
     const int ks = ((p0.kadvmax + 2) + 7) / 8 * 8;
+    // Layout: batches of at least il_min_batch situations use the interleaved layout and the
+    // lane-per-situation kernels; smaller ones the slab layout and the warp-per-column kernels.
+    const bool il = n >= ctx->il_min_batch;
+    const int ngroups = (n + 31) / 32;
+    ctx->il = il;
+    ctx->ngroups = ngroups;
     ctx->loaded = false;
     ctx->nii = NII; ctx->njj = NJJ; ctx->nkk = NKK; ctx->ks = ks; ctx->nb = n; ctx->ncols = ncols; ctx->nj2 = nj2;
     ctx->model = p0.turbulence_model;
@@ -424,7 +439,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     ctx->geo_v = make_geom(2, NII - 2, 3, NJJ - 3);
 
     // ---- device memory ----
-    const size_t fsz = (size_t)n * ncols * ks;
+    const size_t units = il ? (size_t)ngroups * 32 : (size_t)n;     // situation slots
+    const size_t fsz = units * ncols * ks;
     const int nfields = 10;
     const size_t ssz = (size_t)ncols * nk2;
     const int nstage = (ctx->model != 1) ? 5 : 3;
@@ -437,10 +453,11 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(ctx->tables.ensure(5 * ks));
     CK(ctx->ap0.ensure((size_t)n * ks));
     CK(ctx->sit.ensure(n));
-    CK(ctx->flags.ensure((size_t)n * ncols));
-    CK(ctx->rowcarry.ensure((size_t)n * nj2 * 2 * ks));
+    const size_t flag_units = il ? (size_t)ngroups : (size_t)n;
+    CK(ctx->flags.ensure(flag_units * ncols));
+    CK(ctx->rowcarry.ensure(units * nj2 * 2 * ks));
     CK(ctx->trace.ensure((size_t)n * tcap));
-    CK(ctx->misc.ensure(2 + n));                      // err, nact, act[n]
+    CK(ctx->misc.ensure(3 + n));                      // err, nact, it, act[n]
     CK(ctx->counters.ensure(8));
     CK(ctx->counts.ensure(4 * (size_t)n));
     const size_t dsz = ctx->geo_p.ds.size() + ctx->geo_u.ds.size() + ctx->geo_v.ds.size();
@@ -455,6 +472,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     KArgs &a = ctx->ka;
     a = KArgs{};
     a.nii = NII; a.njj = NJJ; a.nkk = NKK; a.ks = ks; a.nj2 = nj2; a.ncols = ncols; a.nb = n;
+    a.il = il ? 1 : 0;
+    a.ngroups = ngroups;
     a.dxk = DXK; a.dyk = DYK; a.areaxy = AREA;
     a.relax = p0.relax; a.relaxp = p0.relaxp; a.coriolis = p0.coriolis;
     a.vishmin = (p0.turbulence_model == 2) ? 0.01f : 0.0f;
@@ -472,7 +491,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     a.rowcarry = ctx->rowcarry.p;
     a.err = ctx->misc.p;
     a.nact = ctx->misc.p + 1;
-    a.act = ctx->misc.p + 2;
+    a.it_global = ctx->misc.p + 2;
+    a.act = ctx->misc.p + 3;
     a.wait_limit_ns = 2000000000ull;
     a.trace = ctx->trace.p;
     a.trace_cap = tcap;
@@ -516,11 +536,12 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemcpyAsync(ctx->tables.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->ap0.p, ap0.data(), ap0.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->sit.p, ctx->h_sit.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
-    ctx->h_act.resize(2 + n);
+    ctx->h_act.resize(3 + n);
     ctx->h_act[0] = 0;
     ctx->h_act[1] = n;
-    for (int b = 0; b < n; ++b) ctx->h_act[2 + b] = b;
-    CK(cudaMemcpyAsync(ctx->misc.p, ctx->h_act.data(), (2 + n) * sizeof(int), cudaMemcpyHostToDevice, st));
+    ctx->h_act[2] = 1;
+    for (int b = 0; b < n; ++b) ctx->h_act[3 + b] = b;
+    CK(cudaMemcpyAsync(ctx->misc.p, ctx->h_act.data(), (3 + n) * sizeof(int), cudaMemcpyHostToDevice, st));
     if (has_veg) {
         std::vector<float> vs((size_t)ncols * ks, 0.0f);
         for (int c = 0; c < ncols; ++c)
@@ -529,8 +550,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         CK(cudaStreamSynchronize(st));
     }
     CK(cudaMemsetAsync(slab, 0, fsz * nfields * sizeof(float), st));
-    CK(cudaMemsetAsync(ctx->flags.p, 0, (size_t)n * ncols * sizeof(int), st));
-    CK(cudaMemsetAsync(ctx->rowcarry.p, 0, (size_t)n * nj2 * 2 * ks * sizeof(float), st));
+    CK(cudaMemsetAsync(ctx->flags.p, 0, flag_units * ncols * sizeof(int), st));
+    CK(cudaMemsetAsync(ctx->rowcarry.p, 0, units * nj2 * 2 * ks * sizeof(float), st));
     CK(cudaMemsetAsync(ctx->trace.p, 0, (size_t)n * tcap * sizeof(float), st));
     // host fields -> staging (one contiguous copy per field and situation)
     for (int b = 0; b < n; ++b) {
@@ -544,13 +565,14 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
 
     // ---- launch shapes of the wavefront kernels ----
     const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
+    CK(gs_prepare(il, ks));
     for (int q = 0; q < 4; ++q) {
         int bps = 0;
-        CK(gs_occupancy(kinds[q], &bps));
+        CK(gs_occupancy(il, kinds[q], ks, &bps));
         ctx->grid_gs[q] = std::max(1, bps) * ctx->num_sms;
     }
-    const int warps = ctx->grid_gs[0] * gs_block_threads() / 32;
-    const long long per_diag = (long long)n * std::min(NII, NJJ);
+    const int warps = ctx->grid_gs[0] * gs_block_threads(il) / 32;
+    const long long per_diag = (long long)(il ? ngroups : n) * std::min(NII, NJJ);
     a.chunk = (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
     ctx->it_host = 1;
     int brc = build_graph(ctx);
@@ -587,9 +609,10 @@ int gral_prog_iterate(gral_ctx *ctx) {
         if ((int)act.size() != nact) {
             nact = (int)act.size();
             ctx->h_act[1] = nact;
-            for (int q = 0; q < nact; ++q) ctx->h_act[2 + q] = act[q];
-            CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, (1 + std::max(nact, 1)) * sizeof(int),
-                               cudaMemcpyHostToDevice, st));
+            for (int q = 0; q < nact; ++q) ctx->h_act[3 + q] = act[q];
+            CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, sizeof(int), cudaMemcpyHostToDevice, st));
+            if (nact > 0)
+                CK(cudaMemcpyAsync(ctx->misc.p + 3, ctx->h_act.data() + 3, nact * sizeof(int), cudaMemcpyHostToDevice, st));
         }
     }
     return GRAL_OK;
@@ -658,7 +681,7 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
     const int n = ctx->nb;
     if (!f) f = ctx->fields.data();
     // post-checks run on every situation regardless of its loop state
-    for (int b = 0; b < n; ++b) ctx->h_act[2 + b] = b;
+    for (int b = 0; b < n; ++b) ctx->h_act[3 + b] = b;
     ctx->h_act[1] = n;
     std::vector<SitDev> hs(n);
     CK(cudaMemcpyAsync(hs.data(), ctx->sit.p, n * sizeof(SitDev), cudaMemcpyDeviceToHost, st));
@@ -666,7 +689,8 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
     std::vector<SitDev> tmp = hs;
     for (auto &x : tmp) x.active = 1;
     CK(cudaMemcpyAsync(ctx->sit.p, tmp.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, (1 + n) * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->misc.p + 1, ctx->h_act.data() + 1, sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->misc.p + 3, ctx->h_act.data() + 3, n * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->counts.p, 0, 4 * n * sizeof(int), st));
     CK(cudaEventRecord(ctx->ev[2], st));
     launch_postcheck(ctx->ka, ctx->counts.p, st);

@@ -1,10 +1,14 @@
 // prog_kernels.cu -- the Jacobi-style passes of one SIMPLE iteration (boundary conditions,
 // velocity correction, staggered averages, convergence bookkeeping), the per-situation set-up and
-// the post-checks.  One warp per column with lanes over k unless stated otherwise; every pass
-// only writes values no other thread of the same launch reads, exactly as the reference's
-// parallel loops do (their results do not depend on thread order).
+// the post-checks.  Every pass only writes values that no other thread of the same launch reads,
+// exactly as the reference's parallel loops do (their results do not depend on thread order).
+//
+// Thread mapping follows the layout so that a warp's loads are contiguous:
+//   slab layout        one warp per (situation, column), lanes over levels;
+//   interleaved layout one warp per (group, column), lane = situation, each lane loops over levels.
 #include "prog_common.cuh"
 #include "prog_kernels.cuh"
+#include "prog_level.cuh"
 
 namespace gral {
 
@@ -12,178 +16,197 @@ namespace {
 
 constexpr int COL_WARPS = 8;   // warps per block of the column kernels
 
-struct ColTask {
-    int s, col, i, j;
-};
-
-// Maps the calling warp to (active situation, column); false when out of range or inactive.
-__device__ __forceinline__ bool col_task(const KArgs &a, ColTask &t) {
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nact = *a.nact;
-    const long long sidx = gw / a.ncols;
-    if (sidx >= nact) return false;
-    t.s = a.act[sidx];
-    if (!a.sit[t.s].active) return false;
-    t.col = (int)(gw - sidx * a.ncols);
-    t.i = t.col / a.nj2;
-    t.j = t.col - t.i * a.nj2;
-    return true;
-}
-
+template <bool IL>
 inline int col_grid(const KArgs &a) {
-    const long long warps = (long long)a.nb * a.ncols;
+    const long long units = IL ? a.ngroups : a.nb;
+    const long long warps = units * a.ncols;
     return (int)((warps + COL_WARPS - 1) / COL_WARPS);
 }
 
+// Calls body(s, col, i, j, x, kbeg, kstep) for every active (situation, column): the body loops
+// `for (k = kbeg; k <= hi; k += kstep)` over the levels it needs.
+template <bool IL, class Body>
+__device__ __forceinline__ void col_loop(const KArgs &a, bool need_active, Body &&body) {
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long unit = gw / a.ncols;
+    const int col = (int)(gw - unit * a.ncols);
+    int s;
+    if (IL) {
+        if (unit >= a.ngroups) return;
+        s = (int)unit * 32 + lane;
+        if (s >= a.nb) return;
+    } else {
+        if (unit >= *a.nact) return;
+        s = a.act[unit];
+    }
+    if (need_active && !a.sit[s].active) return;
+    const int i = col / a.nj2, j = col - (col / a.nj2) * a.nj2;
+    const Acc<IL> x = make_acc<IL>(a, s, col);
+    body(s, col, i, j, x, IL ? 0 : lane, IL ? 1 : 32);
+}
+
 // ---- boundary conditions (PrognosticFlowfield.cs:595-714) ----
-// W/E: one thread per (situation, row j, level k) walks the row's events in ascending i, which is
+// W/E: one thread per (situation, row j, level) walks the row's events in ascending i, which is
 // the reference's sequential i loop; rows and levels are independent.
+template <bool IL>
 __global__ void k_bc_we(KArgs a, BcLists bc) {
     const int j = 2 + blockIdx.x * blockDim.y + threadIdx.y;
-    const int sidx = blockIdx.y;
-    if (j > a.njj || sidx >= *a.nact) return;
-    const int s = a.act[sidx];
+    if (j > a.njj) return;
+    int s, kbeg, kstep;
+    if (IL) {
+        s = blockIdx.y * 32 + threadIdx.x;
+        if (blockIdx.y >= a.ngroups || s >= a.nb) return;
+        kbeg = 0; kstep = 1;
+    } else {
+        if ((int)blockIdx.y >= *a.nact) return;
+        s = a.act[blockIdx.y];
+        kbeg = threadIdx.x; kstep = 32;
+    }
     if (!a.sit[s].active) return;
-    const size_t sb = (size_t)s * a.ncols;
-    const int ks = a.ks, nj2 = a.nj2;
+    const int nj2 = a.nj2;
     for (int e = bc.we_ptr[j]; e < bc.we_ptr[j + 1]; ++e) {
         const int ev = bc.we_ev[e];
         const int i = ev & 0xffff;
         const int VI = a.meta[i * nj2 + j].vi;
-        for (int k = threadIdx.x; k <= VI; k += 32) {
+        const Acc<IL> x = make_acc<IL>(a, s, i * nj2 + j);
+        const long long dW = -(long long)nj2, dE = nj2;
+        for (int k = kbeg; k <= VI; k += kstep) {
             if (k < 1) continue;
-            auto at = [&](int ii) { return (sb + (size_t)ii * nj2 + j) * ks + k; };
             if (ev & (1 << 16)) {
-                const float u = a.uk[at(i - 2)];
-                if (u >= 0) a.uk[at(i - 1)] = u;
-                a.vk[at(i - 2)] = a.vk[at(i - 1)];
-                a.wk[at(i - 2)] = a.wk[at(i - 1)];
+                const float u = a.uk[x.at(2 * dW, k)];
+                if (u >= 0) a.uk[x.at(dW, k)] = u;
+                a.vk[x.at(2 * dW, k)] = a.vk[x.at(dW, k)];
+                a.wk[x.at(2 * dW, k)] = a.wk[x.at(dW, k)];
             }
             if (ev & (1 << 17)) {
-                const float u = a.uk[at(i + 2)];
-                if (u <= 0) a.uk[at(i + 1)] = u;
-                a.vk[at(i + 1)] = a.vk[at(i)];
-                a.wk[at(i + 1)] = a.wk[at(i)];
+                const float u = a.uk[x.at(2 * dE, k)];
+                if (u <= 0) a.uk[x.at(dE, k)] = u;
+                a.vk[x.at(dE, k)] = a.vk[x.at(0, k)];
+                a.wk[x.at(dE, k)] = a.wk[x.at(0, k)];
             }
         }
     }
 }
 
+template <bool IL>
 __global__ void k_bc_sn(KArgs a, BcLists bc) {
     const int i = 2 + blockIdx.x * blockDim.y + threadIdx.y;
-    const int sidx = blockIdx.y;
-    if (i > a.nii || sidx >= *a.nact) return;
-    const int s = a.act[sidx];
+    if (i > a.nii) return;
+    int s, kbeg, kstep;
+    if (IL) {
+        s = blockIdx.y * 32 + threadIdx.x;
+        if (blockIdx.y >= a.ngroups || s >= a.nb) return;
+        kbeg = 0; kstep = 1;
+    } else {
+        if ((int)blockIdx.y >= *a.nact) return;
+        s = a.act[blockIdx.y];
+        kbeg = threadIdx.x; kstep = 32;
+    }
     if (!a.sit[s].active) return;
-    const size_t sb = (size_t)s * a.ncols;
-    const int ks = a.ks, nj2 = a.nj2;
+    const int nj2 = a.nj2;
     for (int e = bc.sn_ptr[i]; e < bc.sn_ptr[i + 1]; ++e) {
         const int ev = bc.sn_ev[e];
         const int j = ev & 0xffff;
         const int VI = a.meta[i * nj2 + j].vi;
-        for (int k = threadIdx.x; k <= VI; k += 32) {
+        const Acc<IL> x = make_acc<IL>(a, s, i * nj2 + j);
+        for (int k = kbeg; k <= VI; k += kstep) {
             if (k < 1) continue;
-            auto at = [&](int jj) { return (sb + (size_t)i * nj2 + jj) * ks + k; };
             if (ev & (1 << 16)) {
-                const float v = a.vk[at(j - 2)];
-                if (v >= 0) a.vk[at(j - 1)] = v;
-                a.uk[at(j - 2)] = a.uk[at(j - 1)];
-                a.wk[at(j - 2)] = a.wk[at(j - 1)];
+                const float v = a.vk[x.at(-2, k)];
+                if (v >= 0) a.vk[x.at(-1, k)] = v;
+                a.uk[x.at(-2, k)] = a.uk[x.at(-1, k)];
+                a.wk[x.at(-2, k)] = a.wk[x.at(-1, k)];
             }
             if (ev & (1 << 17)) {
-                const float v = a.vk[at(j + 2)];
-                if (v <= 0) a.vk[at(j + 1)] = v;
-                a.uk[at(j + 1)] = a.uk[at(j)];
-                a.wk[at(j + 1)] = a.wk[at(j)];
+                const float v = a.vk[x.at(2, k)];
+                if (v <= 0) a.vk[x.at(1, k)] = v;
+                a.uk[x.at(1, k)] = a.uk[x.at(0, k)];
+                a.wk[x.at(1, k)] = a.wk[x.at(0, k)];
             }
         }
     }
 }
 
-// top: level VerticalIndex copied to VerticalIndex+1 (:699-714); one thread per column
+// top: level VerticalIndex copied to VerticalIndex+1 (:699-714)
+template <bool IL>
 __global__ void k_bc_top(KArgs a) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long sidx = t / a.ncols;
-    if (sidx >= *a.nact) return;
-    const int s = a.act[sidx];
-    if (!a.sit[s].active) return;
-    const int col = (int)(t - sidx * a.ncols);
-    const int i = col / a.nj2, j = col - (col / a.nj2) * a.nj2;
-    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
-    if (!(a.cflags[col] & F_ADV)) return;
-    const int k = a.meta[col].vi;
-    const size_t o = fidx(s, col, a.ncols, a.ks);
-    a.wk[o + k + 1] = a.wk[o + k];
-    a.uk[o + k + 1] = a.uk[o + k];
-    a.vk[o + k + 1] = a.vk[o + k];
+    col_loop<IL>(a, true, [&](int, int col, int i, int j, const Acc<IL> &x, int kbeg, int) {
+        if (kbeg != 0) return;
+        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+        if (!(a.cflags[col] & F_ADV)) return;
+        const int k = a.meta[col].vi;
+        a.wk[x.at(0, k + 1)] = a.wk[x.at(0, k)];
+        a.uk[x.at(0, k + 1)] = a.uk[x.at(0, k)];
+        a.vk[x.at(0, k + 1)] = a.vk[x.at(0, k)];
+    });
 }
 
 // ---- velocity correction with Frund quantisation in double (:904-949) ----
+template <bool IL>
 __global__ void k_velcorr(KArgs a) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    if (t.i < 2 || t.i > a.nii - 1 || t.j < 2 || t.j > a.njj - 1) return;
-    if (!(a.cflags[t.col] & F_VC)) return;
-    const int lane = threadIdx.x & 31;
-    const ColMeta m = a.meta[t.col];
-    const SitDev &sd = a.sit[t.s];
-    const float DT = sd.dtime, DXK = a.dxk, DYK = a.dyk;
-    const double fr = sd.frund;
-    const int q = sd.quantise;
-    const size_t o = fidx(t.s, t.col, a.ncols, a.ks);
-    const size_t oW = o - (size_t)a.nj2 * a.ks, oS = o - a.ks;
-    const float *DPM = a.dpm;
-    for (int k = lane; k <= m.vi; k += 32) {
-        if (k < 1) continue;
-        const float d = DPM[o + k];
-        if (t.i > 2 && m.kkm_u < k)
-            a.uk[o + k] = (float)quantd((double)(a.uk[o + k] + (DPM[oW + k] - d) / DXK * DT), fr, q);
-        if (t.j > 2 && m.kkm_v < k)
-            a.vk[o + k] = (float)quantd((double)(a.vk[o + k] + (DPM[oS + k] - d) / DYK * DT), fr, q);
-        if (m.kkart + 1 < k)
-            a.wk[o + k] = (float)quantd(
-                (double)(a.wk[o + k] + (DPM[o + k - 1] - d) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, q);
-        else
-            a.wk[o + k] = 0;
-    }
+    col_loop<IL>(a, true, [&](int s, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+        if (!(a.cflags[col] & F_VC)) return;
+        const ColMeta m = a.meta[col];
+        const SitDev &sd = a.sit[s];
+        const float DT = sd.dtime, DXK = a.dxk, DYK = a.dyk;
+        const double fr = sd.frund;
+        const int q = sd.quantise;
+        const long long dW = -(long long)a.nj2;
+        for (int k = kbeg; k <= m.vi; k += kstep) {
+            if (k < 1) continue;
+            const float d = a.dpm[x.at(0, k)];
+            if (i > 2 && m.kkm_u < k)
+                a.uk[x.at(0, k)] = (float)quantd((double)(a.uk[x.at(0, k)] + (a.dpm[x.at(dW, k)] - d) / DXK * DT), fr, q);
+            if (j > 2 && m.kkm_v < k)
+                a.vk[x.at(0, k)] = (float)quantd((double)(a.vk[x.at(0, k)] + (a.dpm[x.at(-1, k)] - d) / DYK * DT), fr, q);
+            if (m.kkart + 1 < k)
+                a.wk[x.at(0, k)] = (float)quantd(
+                    (double)(a.wk[x.at(0, k)] + (a.dpm[x.at(0, k - 1)] - d) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, q);
+            else
+                a.wk[x.at(0, k)] = 0;
+        }
+    });
 }
 
 // ---- staggered -> cell-centre averages and the border copies (:958-1039) ----
+template <bool IL>
 __global__ void k_average(KArgs a) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    if (t.i < 2 || t.i > a.nii - 1 || t.j < 2 || t.j > a.njj - 1) return;
-    if (!(a.cflags[t.col] & F_VC)) return;
-    const int lane = threadIdx.x & 31;
-    const ColMeta m = a.meta[t.col];
-    const int ks = a.ks, nj2 = a.nj2;
-    const size_t o = fidx(t.s, t.col, a.ncols, ks);
-    const size_t oE = o + (size_t)nj2 * ks, oN = o + ks;
-    const int KK = m.kkart;
-    for (int k = lane; k <= m.vi; k += 32) {
-        if (k < m.kstart) continue;
-        if (KK < k) {
-            a.uks[o + k] = 0.5f * (a.uk[o + k] + a.uk[oE + k]);
-            a.vks[o + k] = 0.5f * (a.vk[o + k] + a.vk[oN + k]);
+    col_loop<IL>(a, true, [&](int, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+        if (!(a.cflags[col] & F_VC)) return;
+        const ColMeta m = a.meta[col];
+        const int nj2 = a.nj2;
+        const long long dE = nj2;
+        const int KK = m.kkart;
+        const bool cpS = (j == 2);
+        const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
+        for (int k = kbeg; k <= m.vi; k += kstep) {
+            if (k < m.kstart) continue;
+            if (KK < k) {
+                a.uks[x.at(0, k)] = 0.5f * (a.uk[x.at(0, k)] + a.uk[x.at(dE, k)]);
+                a.vks[x.at(0, k)] = 0.5f * (a.vk[x.at(0, k)] + a.vk[x.at(1, k)]);
+            }
+            if (KK + 1 < k) a.wks[x.at(0, k)] = 0.5f * (a.wk[x.at(0, k)] + a.wk[x.at(0, k + 1)]);
+            if (cpS) a.uks[x.at(-1, k)] = a.uks[x.at(0, k)];
+            if (cpN) a.uks[x.at(1, k)] = a.uks[x.at(0, k)];
         }
-        if (KK + 1 < k) a.wks[o + k] = 0.5f * (a.wk[o + k] + a.wk[o + k + 1]);
-        if (t.j == 2) a.uks[o - ks + k] = a.uks[o + k];
-        if (t.j == a.njj - 1 && (a.cflags[t.i * nj2 + a.njj] & F_ADV)) a.uks[o + ks + k] = a.uks[o + k];
-    }
-    // VKS[1][j] = VKS[2][j] and VKS[NII][j] = VKS[NII-1][j] over all levels (:1018-1036)
-    const bool west = (t.i == 2) && (a.cflags[1 * nj2 + t.j] & F_ADV);
-    const bool east = (t.i == a.nii - 1) && (a.cflags[t.col] & F_ADV);
-    if (west || east) {
-        const size_t od = west ? o - (size_t)nj2 * ks : oE;
-        for (int k = lane; k < ks; k += 32) a.vks[od + k] = a.vks[o + k];
-    }
+        // VKS[1][j] = VKS[2][j] and VKS[NII][j] = VKS[NII-1][j] on every level (:1018-1036)
+        const bool west = (i == 2) && (a.cflags[1 * nj2 + j] & F_ADV);
+        const bool east = (i == a.nii - 1) && (a.cflags[col] & F_ADV);
+        if (west || east) {
+            const long long dd = west ? -(long long)nj2 : dE;
+            for (int k = kbeg; k < a.ks; k += kstep) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
+        }
+    });
 }
 
 // ---- convergence bookkeeping (:1144-1178), one thread per situation ----
 __global__ void k_bookkeeping(KArgs a) {
-    const int sidx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (sidx >= *a.nact) return;
-    const int s = a.act[sidx];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) *a.it_global += 1;   // kernels of this launch read SitDev::it, never it_global
+    if (s >= a.nb) return;
     SitDev &S = a.sit[s];
     if (!S.active) return;
     const float dumax = __uint_as_float(S.dumax_bits);
@@ -218,25 +241,25 @@ __device__ __forceinline__ size_t sidx3(const KArgs &a, int i, int j, int k) {
 }
 
 // staggered-grid initial values and GESCHW_MAX (:295-329)
+template <bool IL>
 __global__ void k_setup_uks(KArgs a, Staging sg) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    if (t.i < 1 || t.i > a.nii || t.j < 1 || t.j > a.njj) return;
-    if (!(a.cflags[t.col] & F_ALLOC3)) return;
-    const int lane = threadIdx.x & 31;
-    const float *U = sg.uk + sg.stride * t.s, *V = sg.vk + sg.stride * t.s, *W = sg.wk + sg.stride * t.s;
-    const size_t o = fidx(t.s, t.col, a.ncols, a.ks);
-    double g = 0.0;
-    for (int k = 1 + lane; k <= a.nkk - 1; k += 32) {
-        const float u = 0.5f * (U[sidx3(a, t.i, t.j, k)] + U[sidx3(a, t.i + 1, t.j, k)]);
-        const float v = 0.5f * (V[sidx3(a, t.i, t.j, k)] + V[sidx3(a, t.i, t.j + 1, k)]);
-        const float w = 0.5f * (W[sidx3(a, t.i, t.j, k)] + W[sidx3(a, t.i, t.j, k + 1)]);
-        if (k < a.ks) { a.uks[o + k] = u; a.vks[o + k] = v; a.wks[o + k] = w; }
-        g = net_maxd(g, sqrt((double)(u * u + v * v)));
-    }
-    for (int d = 16; d > 0; d >>= 1) g = fmax(g, __shfl_xor_sync(0xffffffffu, g, d));
-    if (lane == 0 && g > 0.0)
-        atomicMax(&a.sit[t.s].geschw_bits, (unsigned long long)__double_as_longlong(g));
+    col_loop<IL>(a, false, [&](int s, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+        double g = 0.0;
+        if (i >= 1 && i <= a.nii && j >= 1 && j <= a.njj && (a.cflags[col] & F_ALLOC3)) {
+            const float *U = sg.uk + sg.stride * s, *V = sg.vk + sg.stride * s, *Wf = sg.wk + sg.stride * s;
+            for (int k = 1 + kbeg; k <= a.nkk - 1; k += kstep) {
+                const float u = 0.5f * (U[sidx3(a, i, j, k)] + U[sidx3(a, i + 1, j, k)]);
+                const float v = 0.5f * (V[sidx3(a, i, j, k)] + V[sidx3(a, i, j + 1, k)]);
+                const float w = 0.5f * (Wf[sidx3(a, i, j, k)] + Wf[sidx3(a, i, j, k + 1)]);
+                if (k < a.ks) { a.uks[x.at(0, k)] = u; a.vks[x.at(0, k)] = v; a.wks[x.at(0, k)] = w; }
+                g = net_maxd(g, sqrt((double)(u * u + v * v)));
+            }
+        }
+        if (!IL)
+            for (int d = 16; d > 0; d >>= 1) g = fmax(g, __shfl_xor_sync(0xffffffffu, g, d));
+        if ((IL || kbeg == 0) && g > 0.0)
+            atomicMax(&a.sit[s].geschw_bits, (unsigned long long)__double_as_longlong(g));
+    });
 }
 
 // border copies UK[NII+1] = UK[NII], VK[.][NJJ+1] = VK[.][NJJ] on levels 1..NKK-1 (:422-429)
@@ -244,10 +267,9 @@ __global__ void k_setup_border(KArgs a, Staging sg) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int nk = a.nkk - 1;
     const long long per = (long long)(a.njj + a.nii) * nk;
-    const long long sidx = t / per;
-    if (sidx >= *a.nact) return;
-    const int s = a.act[sidx];
-    const long long r = t - sidx * per;
+    const long long s = t / per;
+    if (s >= a.nb) return;
+    const long long r = t - s * per;
     float *U = sg.uk + sg.stride * s, *V = sg.vk + sg.stride * s;
     const int k = 1 + (int)(r % nk);
     const int q = (int)(r / nk);
@@ -261,122 +283,117 @@ __global__ void k_setup_border(KArgs a, Staging sg) {
 }
 
 // velocities (and k, eps) inside buildings set to zero (:518-575)
+template <bool IL>
 __global__ void k_setup_zero(KArgs a, Staging sg, int model) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    if (t.i < 1 || t.i > a.nii || t.j < 1 || t.j > a.njj) return;
-    if (!(a.cflags[t.col] & F_ADV)) return;
-    const int lane = threadIdx.x & 31;
-    const ColMeta m = a.meta[t.col];
-    float *U = sg.uk + sg.stride * t.s, *V = sg.vk + sg.stride * t.s, *W = sg.wk + sg.stride * t.s;
-    const size_t o = fidx(t.s, t.col, a.ncols, a.ks);
-    for (int k = 1 + lane; k <= m.vi; k += 32) {
-        if (m.kkart < k) continue;
-        U[sidx3(a, t.i, t.j, k)] = 0;
-        if (t.i == a.nii) U[sidx3(a, t.i + 1, t.j, k)] = 0;
-        V[sidx3(a, t.i, t.j, k)] = 0;
-        if (t.j == a.njj) V[sidx3(a, t.i, t.j + 1, k)] = 0;
-        W[sidx3(a, t.i, t.j, k)] = 0;
-        if (k == m.vi) W[sidx3(a, t.i, t.j, k + 1)] = 0;
-        if (model != 1) {
-            sg.turb[sg.stride * t.s + sidx3(a, t.i, t.j, k)] = 0;
-            sg.tdiss[sg.stride * t.s + sidx3(a, t.i, t.j, k)] = 0;
+    col_loop<IL>(a, false, [&](int s, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+        if (i < 1 || i > a.nii || j < 1 || j > a.njj) return;
+        if (!(a.cflags[col] & F_ADV)) return;
+        const ColMeta m = a.meta[col];
+        float *U = sg.uk + sg.stride * s, *V = sg.vk + sg.stride * s, *Wf = sg.wk + sg.stride * s;
+        for (int k = 1 + kbeg; k <= m.vi; k += kstep) {
+            if (m.kkart < k) continue;
+            U[sidx3(a, i, j, k)] = 0;
+            if (i == a.nii) U[sidx3(a, i + 1, j, k)] = 0;
+            V[sidx3(a, i, j, k)] = 0;
+            if (j == a.njj) V[sidx3(a, i, j + 1, k)] = 0;
+            Wf[sidx3(a, i, j, k)] = 0;
+            if (k == m.vi) Wf[sidx3(a, i, j, k + 1)] = 0;
+            if (model != 1) {
+                sg.turb[sg.stride * s + sidx3(a, i, j, k)] = 0;
+                sg.tdiss[sg.stride * s + sidx3(a, i, j, k)] = 0;
+            }
+            a.uks[x.at(0, k)] = 0; a.vks[x.at(0, k)] = 0; a.wks[x.at(0, k)] = 0;
         }
-        a.uks[o + k] = 0; a.vks[o + k] = 0; a.wks[o + k] = 0;
-    }
+    });
 }
 
-// staging (full height) <-> slab (levels 0..KS-1)
-__global__ void k_gather(KArgs a, Staging sg, int model, int to_slab) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    const int lane = threadIdx.x & 31;
-    const size_t o = fidx(t.s, t.col, a.ncols, a.ks);
-    const size_t so = sg.stride * t.s + (size_t)t.col * (a.nkk + 2);
-    const int nk2 = a.nkk + 2;
-    const int nf = (model != 1) ? 5 : 3;
-    float *slab[5] = {a.uk, a.vk, a.wk, a.turb, a.tdiss};
-    float *stag[5] = {sg.uk, sg.vk, sg.wk, sg.turb, sg.tdiss};
-    for (int f = 0; f < nf; ++f) {
-        for (int k = lane; k < a.ks; k += 32) {
-            if (to_slab) slab[f][o + k] = (k < nk2) ? stag[f][so + k] : 0.0f;
-            else if (k < nk2) stag[f][so + k] = slab[f][o + k];
+// staging (full height) <-> device layout (levels 0..KS-1)
+template <bool IL>
+__global__ void k_gather(KArgs a, Staging sg, int model, int to_dev) {
+    col_loop<IL>(a, false, [&](int s, int col, int, int, const Acc<IL> &x, int kbeg, int kstep) {
+        const size_t so = sg.stride * s + (size_t)col * (a.nkk + 2);
+        const int nk2 = a.nkk + 2;
+        const int nf = (model != 1) ? 5 : 3;
+        float *dev[5] = {a.uk, a.vk, a.wk, a.turb, a.tdiss};
+        float *stag[5] = {sg.uk, sg.vk, sg.wk, sg.turb, sg.tdiss};
+        for (int f = 0; f < nf; ++f) {
+            for (int k = kbeg; k < a.ks; k += kstep) {
+                if (to_dev) dev[f][x.at(0, k)] = (k < nk2) ? stag[f][so + k] : 0.0f;
+                else if (k < nk2) stag[f][so + k] = dev[f][x.at(0, k)];
+            }
         }
-    }
+    });
 }
 
 // unrealistic-speed counts and non-finite values (:1193-1243)
+template <bool IL>
 __global__ void k_postcheck(KArgs a, int *counts) {
-    ColTask t;
-    if (!col_task(a, t)) return;
-    if (t.i < 1 || t.i > a.nii || t.j < 1 || t.j > a.njj) return;
-    if (!(a.cflags[t.col] & F_ADV)) return;
-    const int lane = threadIdx.x & 31;
-    const ColMeta m = a.meta[t.col];
-    const SitDev &sd = a.sit[t.s];
-    const float limit = (float)(10 * __longlong_as_double((long long)sd.geschw_bits));
-    const size_t o = fidx(t.s, t.col, a.ncols, a.ks);
-    int cu = 0, cv = 0, cw = 0, cn = 0;
-    for (int k = 1 + lane; k <= m.vi; k += 32) {
-        const float u = a.uk[o + k], v = a.vk[o + k], w = a.wk[o + k];
-        if (fabsf(u) > 55 || fabsf(u) > limit) cu++;
-        if (fabsf(v) > 55 || fabsf(v) > limit) cv++;
-        if (fabsf(w) > 20 || fabsf(w) > limit) cw++;
-        if (!isfinite(u) || !isfinite(v) || !isfinite(w)) cn++;
-    }
-    for (int d = 16; d > 0; d >>= 1) {
-        cu += __shfl_xor_sync(0xffffffffu, cu, d);
-        cv += __shfl_xor_sync(0xffffffffu, cv, d);
-        cw += __shfl_xor_sync(0xffffffffu, cw, d);
-        cn += __shfl_xor_sync(0xffffffffu, cn, d);
-    }
-    if (lane == 0 && (cu | cv | cw | cn)) {
-        atomicAdd(counts + 4 * t.s + 0, cu);
-        atomicAdd(counts + 4 * t.s + 1, cv);
-        atomicAdd(counts + 4 * t.s + 2, cw);
-        atomicAdd(counts + 4 * t.s + 3, cn);
-    }
+    col_loop<IL>(a, false, [&](int s, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+        if (i < 1 || i > a.nii || j < 1 || j > a.njj) return;
+        if (!(a.cflags[col] & F_ADV)) return;
+        const ColMeta m = a.meta[col];
+        const float limit = (float)(10 * __longlong_as_double((long long)a.sit[s].geschw_bits));
+        int cu = 0, cv = 0, cw = 0, cn = 0;
+        for (int k = 1 + kbeg; k <= m.vi; k += kstep) {
+            const float u = a.uk[x.at(0, k)], v = a.vk[x.at(0, k)], w = a.wk[x.at(0, k)];
+            if (fabsf(u) > 55 || fabsf(u) > limit) cu++;
+            if (fabsf(v) > 55 || fabsf(v) > limit) cv++;
+            if (fabsf(w) > 20 || fabsf(w) > limit) cw++;
+            if (!isfinite(u) || !isfinite(v) || !isfinite(w)) cn++;
+        }
+        if (cu) atomicAdd(counts + 4 * s + 0, cu);
+        if (cv) atomicAdd(counts + 4 * s + 1, cv);
+        if (cw) atomicAdd(counts + 4 * s + 2, cw);
+        if (cn) atomicAdd(counts + 4 * s + 3, cn);
+    });
 }
 
 }  // namespace
 
+#define GRAL_COL_LAUNCH(kern, ...)                                                        \
+    do {                                                                                  \
+        if (a.il) kern<true><<<col_grid<true>(a), COL_WARPS * 32, 0, st>>>(__VA_ARGS__);  \
+        else kern<false><<<col_grid<false>(a), COL_WARPS * 32, 0, st>>>(__VA_ARGS__);     \
+    } while (0)
+
 void launch_bc(const KArgs &a, const BcLists &bc, cudaStream_t st) {
     const dim3 blk(32, 8);
-    k_bc_we<<<dim3((a.njj - 1 + 7) / 8, a.nb), blk, 0, st>>>(a, bc);
-    k_bc_sn<<<dim3((a.nii - 1 + 7) / 8, a.nb), blk, 0, st>>>(a, bc);
-    const long long n = (long long)a.nb * a.ncols;
-    k_bc_top<<<(int)((n + 255) / 256), 256, 0, st>>>(a);
+    const int units = a.il ? a.ngroups : a.nb;
+    if (a.il) {
+        k_bc_we<true><<<dim3((a.njj - 1 + 7) / 8, units), blk, 0, st>>>(a, bc);
+        k_bc_sn<true><<<dim3((a.nii - 1 + 7) / 8, units), blk, 0, st>>>(a, bc);
+    } else {
+        k_bc_we<false><<<dim3((a.njj - 1 + 7) / 8, units), blk, 0, st>>>(a, bc);
+        k_bc_sn<false><<<dim3((a.nii - 1 + 7) / 8, units), blk, 0, st>>>(a, bc);
+    }
+    GRAL_COL_LAUNCH(k_bc_top, a);
 }
 
-void launch_velcorr(const KArgs &a, cudaStream_t st) {
-    k_velcorr<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a);
-}
+void launch_velcorr(const KArgs &a, cudaStream_t st) { GRAL_COL_LAUNCH(k_velcorr, a); }
 
-void launch_average(const KArgs &a, cudaStream_t st) {
-    k_average<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a);
-}
+void launch_average(const KArgs &a, cudaStream_t st) { GRAL_COL_LAUNCH(k_average, a); }
 
 void launch_bookkeeping(const KArgs &a, cudaStream_t st) {
     k_bookkeeping<<<(a.nb + 127) / 128, 128, 0, st>>>(a);
 }
 
 void launch_setup(const KArgs &a, const Staging &sg, int model, cudaStream_t st) {
-    k_setup_uks<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a, sg);
+    GRAL_COL_LAUNCH(k_setup_uks, a, sg);
     const long long nb = (long long)a.nb * (a.njj + a.nii) * (a.nkk - 1);
     k_setup_border<<<(int)((nb + 255) / 256), 256, 0, st>>>(a, sg);
-    k_setup_zero<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a, sg, model);
+    GRAL_COL_LAUNCH(k_setup_zero, a, sg, model);
 }
 
 void launch_gather(const KArgs &a, const Staging &sg, int model, cudaStream_t st) {
-    k_gather<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a, sg, model, 1);
+    GRAL_COL_LAUNCH(k_gather, a, sg, model, 1);
 }
 
 void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t st) {
-    k_gather<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a, sg, model, 0);
+    GRAL_COL_LAUNCH(k_gather, a, sg, model, 0);
 }
 
 void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st) {
-    k_postcheck<<<col_grid(a), COL_WARPS * 32, 0, st>>>(a, counts);
+    GRAL_COL_LAUNCH(k_postcheck, a, counts);
 }
 
 }  // namespace gral

@@ -1,9 +1,13 @@
 """GPU parity: the CUDA solver (through the C ABI) against the CPU oracle on the same inputs.
 
 Both implement the reference's deterministic float32 evaluation order, so the expected difference
-is zero; the asserted bound is the north-star tolerance max|dU|/max|U| <= 1e-4 with the
-iteration count and convergence decisions compared exactly.
+is zero; asserted are the north-star bound max|dU|/max|U| <= 1e-4 on U, V, W, bit-identical
+fields, identical DeltaUMax traces and identical iteration counts and convergence decisions.
+Both kernel families are covered: the slab layout (one warp per column, few situations) and the
+interleaved layout (lane per situation, batches), forced with GRAL_PROG_LAYOUT.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -21,27 +25,103 @@ def rel_err(a, b):
     return float(np.abs(a.astype(np.float64) - b.astype(np.float64)).max()) / den
 
 
-def run_both(dom, sit, iterations, model=1, **kw):
-    p = dom.params(sit, model=model, iterations=iterations, **kw)
-    f_gpu = prep.initial_fields(dom, sit, model)
-    f_cpu = f_gpu.copy()
-    tr_g = np.zeros(max(iterations, 1), np.float32)
-    tr_c = np.zeros(max(iterations, 1), np.float32)
-    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
-        sg = s.calculate(p, dom.static, f_gpu, trace=tr_g)
-    sc = O.solve(p, dom.static, f_cpu, trace=tr_c)
-    return f_gpu, f_cpu, sg, sc, tr_g, tr_c
+@pytest.fixture(params=["slab", "interleaved"])
+def layout(request, monkeypatch):
+    monkeypatch.setenv("GRAL_PROG_LAYOUT", request.param)
+    return request.param
+
+
+def solve_gpu(dom, params, fields, traces=None):
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=len(params)) as s:
+        return s.calculate_batch(params, dom.static, fields, traces)
+
+
+def check_same(fg, fc, names=("uk", "vk", "wk")):
+    for name in names:
+        a, b = getattr(fg, name), getattr(fc, name)
+        assert rel_err(a, b) <= TOL, name
+        assert np.array_equal(a, b), f"{name} not bit-identical (max rel err {rel_err(a, b):.3e})"
+
+
+def run_pair(dom, sits, iterations, model=1, **kw):
+    ps = [dom.params(x, model=model, iterations=iterations, **kw) for x in sits]
+    f0 = [prep.initial_fields(dom, x, model) for x in sits]
+    fg = [f.copy() for f in f0]
+    tg = [np.zeros(max(iterations, 1), np.float32) for _ in sits]
+    sg = solve_gpu(dom, ps, fg, tg)
+    out = []
+    for b, x in enumerate(sits):
+        fc = f0[b].copy()
+        tc = np.zeros(max(iterations, 1), np.float32)
+        sc = O.solve(ps[b], dom.static, fc, tc)
+        out.append((fg[b], fc, sg[b], sc, tg[b], tc))
+    return out
 
 
 @pytest.mark.parametrize("iterations", [1, 2, 4, 9])
 @pytest.mark.parametrize("seed", [0, 1])
-def test_model1_small(gpu_required, seed, iterations):
+def test_model1_small(gpu_required, layout, seed, iterations):
     dom = prep.small_domain(16, 14, seed=seed)
     sit = prep.Situation(direction_deg=250.0 + 30 * seed, speed_10m=3.0, z0=0.2, ustar=0.3)
-    fg, fc, sg, sc, tg, tc = run_both(dom, sit, iterations)
-    assert sg["iterations"] == sc["iterations"] == iterations
-    np.testing.assert_array_equal(tg, tc)
-    for name in ("uk", "vk", "wk"):
-        a, b = getattr(fg, name), getattr(fc, name)
-        assert rel_err(a, b) <= TOL, name
-        assert np.array_equal(a, b), f"{name} not bit-identical"
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], iterations):
+        assert sg["iterations"] == sc["iterations"] == iterations
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
+
+
+def test_model1_batch_mixed_directions(gpu_required, layout):
+    """Three situations in one batch, each against its own oracle run (sweep direction, inflow
+    side and boundary events differ per situation)."""
+    dom = prep.small_domain(18, 15, seed=2, n_buildings=4)
+    sits = [prep.Situation(direction_deg=d, speed_10m=v, z0=0.3, ustar=0.25)
+            for d, v in ((15.0, 2.0), (135.0, 4.0), (290.0, 1.0))]
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, sits, 7):
+        assert sg["iterations"] == sc["iterations"] == 7
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
+
+
+def test_model1_vegetation(gpu_required, layout):
+    dom = prep.small_domain(16, 16, seed=3, with_veg=True)
+    assert dom.static.veg_mask.sum() > 0
+    sit = prep.Situation(direction_deg=200.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 6):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
+
+
+def test_model1_convergence_decisions(gpu_required, layout):
+    """The cadence test (every 100 iterations, threshold on DeltaMean/topwind^2) stops both solvers
+    at the same iteration with the same residual history."""
+    dom = prep.small_domain(14, 12, seed=4, n_buildings=2)
+    sit = prep.Situation(direction_deg=260.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    [(fg, fc, sg, sc, tg, tc)] = run_pair(dom, [sit], 400, iter_min=100, conv_threshold=0.05)
+    assert sg["iterations"] == sc["iterations"]
+    assert sg["iteration_loops"] == sc["iteration_loops"]
+    assert sg["converged"] == sc["converged"]
+    assert sg["delta_history"] == sc["delta_history"]
+    assert sg["delta_first"] == sc["delta_first"] and sg["delta_finish"] == sc["delta_finish"]
+    assert sg["convergence_problem"] == sc["convergence_problem"]
+    assert (sg["uk_unrealistic"], sg["vk_unrealistic"], sg["wk_unrealistic"]) == \
+        (sc["uk_unrealistic"], sc["vk_unrealistic"], sc["wk_unrealistic"])
+    assert sg["geschw_max"] == sc["geschw_max"]
+    check_same(fg, fc)
+
+
+def test_cube_domain_config1_geometry(gpu_required, layout):
+    """The 100x100 cube case (2 m cells, 20 m building, stretch 1.01: NKK 162, KADVMAX 30)."""
+    dom = prep.cube_domain()
+    assert (dom.nkk, dom.kadvmax, int(dom.static.kkart.max())) == (162, 30, 10)
+    sit = prep.Situation(direction_deg=270.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 5):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
+
+
+def test_quantise_off(gpu_required, layout):
+    """quantise=0 switches the Frund rounding off on both sides."""
+    dom = prep.small_domain(16, 14, seed=5)
+    sit = prep.Situation(direction_deg=45.0, speed_10m=2.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 5, quantise=0):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
