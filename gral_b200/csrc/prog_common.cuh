@@ -55,7 +55,7 @@ struct SitDev {
     unsigned long long geschw_bits;   // GESCHW_MAX as non-negative double bits (atomicMax)
     float dtime, topwind, ug, vg;
     float delta_first, delta_finish, last_dumax;
-    uint32_t dumax_bits;     // running max of DeltaUMax (non-negative float bits), reset each iteration
+    uint32_t dumax_bits;     // running max of the residual keys of this iteration (see residual_key)
     int32_t it;              // IterationLoops
     int32_t active;          // 1 while the SIMPLE loop runs for this situation
     int32_t iters_done;

@@ -28,7 +28,7 @@ namespace gral {
 namespace {
 
 constexpr int GS_WARPS = 4;      // warps per block, plain family
-constexpr int GB_WARPS = 2;      // warps per block, batched family
+constexpr int GB_WARPS = 8;      // warps per block, batched family (levels split over warps)
 constexpr int SM_ROWS = 5;       // shared rows per warp of the plain family: A, B, C, D, phi
 
 __device__ __forceinline__ void sweep_dir(int it, int &IS, int &JS) {
@@ -221,14 +221,13 @@ __device__ void plain_pressure_column(const KArgs &a, int s, int i, int j, int I
         }
     }
     __syncwarp();
-    float dmax = 0.0f;
+    unsigned dmax = 0;
     const int klo = max(c.KK, a.vi_min);
     for (int r = 0; r < 2; ++r) {
         const int k = lane + 32 * r;
         if (k <= c.KK || k > c.VI) continue;
         const float temp = S[4][k];
-        const double q = quantd((double)temp, sc.frund, sc.quant);
-        dmax = fmaxf(dmax, (float)fabs(0.0 - q));
+        dmax = max(dmax, residual_key(temp, sc));
         __stcg(a.dpm + x.at(0, k), temp);
         a.dpmnew[x.at(0, k)] += a.relaxp * temp;
         if (k > klo) {
@@ -236,8 +235,8 @@ __device__ void plain_pressure_column(const KArgs &a, int s, int i, int j, int I
             __stcg(rc + ks + k, S[2][k]);
         }
     }
-    for (int d = 16; d > 0; d >>= 1) dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
-    if (lane == 0 && dmax > 0.0f) atomicMax(&a.sit[s].dumax_bits, __float_as_uint(dmax));
+    for (int d = 16; d > 0; d >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
+    if (lane == 0 && dmax > 0) atomicMax(&a.sit[s].dumax_bits, dmax);
 }
 
 __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure(KArgs a, SweepGeom g) {
@@ -259,43 +258,99 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_mom_ml(KArgs a, SweepGeom g) 
 }
 
 // ---------------------------- batched family -----------------------------------------------
-// Shared rows per thread: P and Q for every level, [k][thread] (conflict-free).
+// One block per task = (group of 32 situations, column).  The block's warps split the levels for
+// the coefficient assembly (lane = situation, contiguous 128-byte loads in the interleaved layout)
+// and write A, B, C, D, phi rows [k][32] to shared memory; warp 0 then runs the 32 situations'
+// Thomas recurrences and back-substitutions side by side.
 
-template <int COMP>
-__device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, float *sP, float *sQ) {
-    const int lane = threadIdx.x & 31;
+struct BRows {
+    float A[KMAX_LEVELS][32], B[KMAX_LEVELS][32], C[KMAX_LEVELS][32], D[KMAX_LEVELS][32], phi[KMAX_LEVELS][32];
+};
+
+// Block-wide variant of gs_tasks: thread 0 claims and waits, the block works, thread 0 publishes.
+template <int PHASE, bool REVERSE, class Body>
+__device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &g, Body &&body) {
+    __shared__ unsigned s_base;
+    __shared__ int s_ok;
+    const unsigned units = (unsigned)a.ngroups;
+    const unsigned total = (unsigned)g.diag_start[g.ndiag] * units;
+    unsigned int *ctr = a.counters + PHASE;
+    const int it = *a.it_global;
+    int IS, JS;
+    sweep_dir(it, IS, JS);
+    if (REVERSE) { IS = -IS; JS = -JS; }
+    const int stamp = it * 8 + PHASE;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_base = atomicAdd(ctr, (unsigned)a.chunk);
+        __syncthreads();
+        const unsigned base = s_base;
+        if (base >= total) break;
+        if (*(volatile int *)a.err != ERR_NONE) break;
+        const unsigned end = min(total, base + (unsigned)a.chunk);
+        for (unsigned t = base; t < end; ++t) {
+            int grp, i1, j1;
+            decode_task(t, g, units, grp, i1, j1);
+            const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+            const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+            int *fl = a.flags + (size_t)grp * a.ncols;
+            if (threadIdx.x == 0) {
+                int ok = 1;
+                if (i1 > g.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, stamp, a.err, a.wait_limit_ns);
+                if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
+                s_ok = ok;
+            }
+            __syncthreads();
+            if (s_ok) body(grp, i, j, IS, JS, i1 == g.ia);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                st_release(fl + i * a.nj2 + j, stamp);
+            }
+        }
+    }
+}
+
+template <int COMP, int NW>
+__device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV)) return;
-    if (s >= a.nb || !a.sit[s].active) return;
-    const SitCtx sc = make_sit(a, s);
-    const Acc<true> x = make_acc<true>(a, s, c.col);
-    float *F = comp_field<COMP>(a);
-    const int T = blockDim.x, tid = threadIdx.x;
-    float P = 0.0f, Q = 0.0f;
-#pragma unroll 1
-    for (int k = c.K0; k <= c.VI; ++k) {
-        const Coef q = ml_level<COMP, true>(a, x, c, sc, k);
-        if (k > c.KK + 1) {
-            const float Tm = 1.0f / (q.A - q.C * P);
-            P = q.B * Tm;
-            Q = (q.D + q.C * Q) * Tm;
-        } else {
-            const float Tm = 1.0f / q.A;
-            P = q.B * Tm;
-            Q = q.D * Tm;
+    const bool act = (s < a.nb) && a.sit[s].active;
+    const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
+    if (act) {
+        const SitCtx sc = make_sit(a, s);
+        for (int k = c.K0 + warp; k <= c.VI; k += NW) {
+            const Coef q = ml_level<COMP, true>(a, x, c, sc, k);
+            R.A[k][lane] = q.A; R.B[k][lane] = q.B; R.C[k][lane] = q.C; R.D[k][lane] = q.D; R.phi[k][lane] = q.phi;
         }
-        sP[k * T + tid] = P;
-        sQ[k * T + tid] = Q;
+    }
+    __syncthreads();
+    if (warp != 0 || !act) return;
+    float *F = comp_field<COMP>(a);
+    float P = 0.0f, Q = 0.0f;
+    for (int k = c.K0; k <= c.VI; ++k) {
+        const float A = R.A[k][lane], B = R.B[k][lane], C = R.C[k][lane], D = R.D[k][lane];
+        if (k > c.KK + 1) {
+            const float T = 1.0f / (A - C * P);
+            P = B * T;
+            Q = (D + C * Q) * T;
+        } else {
+            const float T = 1.0f / A;
+            P = B * T;
+            Q = D * T;
+        }
+        R.B[k][lane] = P;
+        R.D[k][lane] = Q;
     }
     const int kkm = back_limit<COMP>(c);
-    float up = __ldcg(F + x.at(0, c.VI + 1));
     const float relax = a.relax;
-#pragma unroll 1
+    float up = __ldcg(F + x.at(0, c.VI + 1));
     for (int k = c.VI; k >= c.K0; --k) {
-        float u = __ldcg(F + x.at(0, k));
+        float u = R.phi[k][lane];
         if (kkm < k) {
-            u += relax * (sP[k * T + tid] * up + sQ[k * T + tid] - u);
+            u += relax * (R.B[k][lane] * up + R.D[k][lane] - u);
             __stcg(F + x.at(0, k), u);
         }
         up = u;
@@ -303,76 +358,88 @@ __device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, float *sP
 }
 
 // Row carry of the batched family: [group][j][2][KS][32].
-__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first,
-                                      float *sP, float *sQ, float &dmax_acc) {
-    const int lane = threadIdx.x & 31;
+template <int NW>
+__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first, BRows &R,
+                                      unsigned &nmax_acc) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const int ks = a.ks;
     float *rc = a.rowcarry + (((size_t)grp * a.nj2 + j) * 2 * ks) * 32 + lane;
-    if (first) {
+    if (first && warp == 0)
         for (int k = 0; k < 2 * ks; ++k) __stcg(rc + (size_t)k * 32, 0.0f);
-    }
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV)) return;
-    if (s >= a.nb || !a.sit[s].active) return;
-    const SitCtx sc = make_sit(a, s);
-    const Acc<true> x = make_acc<true>(a, s, c.col);
-    const int T = blockDim.x, tid = threadIdx.x;
-    float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
-#pragma unroll 1
-    for (int k = c.VI; k > c.KK; --k) {
-        const float D = pressure_dim<true>(a, x, c, sc, k, IS, JS);
-        const float Tm = 1.0f / (a.app[k] - a.atp[k] * P);
-        P = a.abp[k] * Tm;
-        Q = (a.atp[k] * Q + D) * Tm;
-        sP[k * T + tid] = P;
-        sQ[k * T + tid] = Q;
+    const bool act = (s < a.nb) && a.sit[s].active;
+    const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
+    const SitCtx sc = make_sit(a, act ? s : grp * 32);
+    if (act)
+        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.D[k][lane] = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+    __syncthreads();
+    if (warp == 0 && act) {
+        float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
+        for (int k = c.VI; k > c.KK; --k) {
+            const float T = 1.0f / (a.app[k] - a.atp[k] * P);
+            P = a.abp[k] * T;
+            Q = (a.atp[k] * Q + R.D[k][lane]) * T;
+            R.B[k][lane] = P;
+            R.C[k][lane] = Q;
+        }
+        float prev = 0.0f;                                         // DPM[KKART] is always 0
+        for (int k = c.KK + 1; k <= c.VI; ++k) {
+            prev = R.B[k][lane] * prev + R.C[k][lane];
+            R.phi[k][lane] = prev;
+        }
     }
+    __syncthreads();
+    if (!act) return;
     const int klo = max(c.KK, a.vi_min);
-    float prev = 0.0f;
-    float dmax = 0.0f;
-#pragma unroll 1
-    for (int k = c.KK + 1; k <= c.VI; ++k) {
-        const float Pk = sP[k * T + tid], Qk = sQ[k * T + tid];
-        prev = Pk * prev + Qk;
-        const double q = quantd((double)prev, sc.frund, sc.quant);
-        dmax = fmaxf(dmax, (float)fabs(0.0 - q));
-        __stcg(a.dpm + x.at(0, k), prev);
-        a.dpmnew[x.at(0, k)] += a.relaxp * prev;
+    unsigned nmax = 0;
+    for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) {
+        const float temp = R.phi[k][lane];
+        nmax = max(nmax, residual_key(temp, sc));
+        __stcg(a.dpm + x.at(0, k), temp);
+        a.dpmnew[x.at(0, k)] += a.relaxp * temp;
         if (k > klo) {
-            __stcg(rc + (size_t)k * 32, Pk);
-            __stcg(rc + (size_t)(ks + k) * 32, Qk);
+            __stcg(rc + (size_t)k * 32, R.B[k][lane]);
+            __stcg(rc + (size_t)(ks + k) * 32, R.C[k][lane]);
         }
     }
-    dmax_acc = fmaxf(dmax_acc, dmax);
+    nmax_acc = max(nmax_acc, nmax);
 }
 
-__global__ void __launch_bounds__(GB_WARPS * 32) k_pressure_b(KArgs a, SweepGeom g) {
-    extern __shared__ float smem[];
-    float *sP = smem, *sQ = smem + (size_t)a.ks * blockDim.x;
-    const int lane = threadIdx.x & 31;
-    float dmax = 0.0f;
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) k_pressure_b(KArgs a, SweepGeom g) {
+    __shared__ BRows R;
+    __shared__ unsigned red[NW][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned nmax = 0;
     int cur = -1;
-    gs_tasks<PH_PRESSURE, false, true>(a, g, [&](int grp, int i, int j, int IS, int JS, bool first) {
-        if (grp != cur) {
+    auto flush = [&]() {
+        // block-reduce the residual keys of the current group and publish one atomic per situation
+        red[warp][lane] = nmax;
+        __syncthreads();
+        if (warp == 0 && cur >= 0) {
+            unsigned m = 0;
+            for (int w = 0; w < NW; ++w) m = max(m, red[w][lane]);
             const int s = cur * 32 + lane;
-            if (cur >= 0 && dmax > 0.0f && s < a.nb) atomicMax(&a.sit[s].dumax_bits, __float_as_uint(dmax));
-            dmax = 0.0f;
-            cur = grp;
+            if (m > 0 && s < a.nb) atomicMax(&a.sit[s].dumax_bits, m);
         }
-        batch_pressure_column(a, grp, i, j, IS, JS, first, sP, sQ, dmax);
+        __syncthreads();
+        nmax = 0;
+    };
+    gs_tasks_block<PH_PRESSURE, false>(a, g, [&](int grp, int i, int j, int IS, int JS, bool first) {
+        if (grp != cur) { flush(); cur = grp; }
+        batch_pressure_column<NW>(a, grp, i, j, IS, JS, first, R, nmax);
     });
-    const int s = cur * 32 + lane;
-    if (cur >= 0 && dmax > 0.0f && s < a.nb) atomicMax(&a.sit[s].dumax_bits, __float_as_uint(dmax));
+    flush();
 }
 
-template <int COMP>
-__global__ void __launch_bounds__(GB_WARPS * 32) k_mom_ml_b(KArgs a, SweepGeom g) {
-    extern __shared__ float smem[];
-    float *sP = smem, *sQ = smem + (size_t)a.ks * blockDim.x;
+template <int COMP, int NW>
+__global__ void __launch_bounds__(NW * 32) k_mom_ml_b(KArgs a, SweepGeom g) {
+    __shared__ BRows R;
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
-    gs_tasks<PH, COMP == COMP_V, true>(a, g, [&](int grp, int i, int j, int, int, bool) {
-        batch_ml_column<COMP>(a, grp, i, j, sP, sQ);
+    gs_tasks_block<PH, COMP == COMP_V>(a, g, [&](int grp, int i, int j, int, int, bool) {
+        batch_ml_column<COMP, NW>(a, grp, i, j, R);
     });
 }
 
@@ -380,21 +447,12 @@ __global__ void __launch_bounds__(GB_WARPS * 32) k_mom_ml_b(KArgs a, SweepGeom g
 
 int gs_block_threads(bool il) { return il ? GB_WARPS * 32 : GS_WARPS * 32; }
 
-size_t gs_smem_bytes(bool il, int ks) { return il ? (size_t)2 * ks * GB_WARPS * 32 * sizeof(float) : 0; }
+size_t gs_smem_bytes(bool, int) { return 0; }
 
-cudaError_t gs_prepare(bool il, int ks) {
-    if (!il) return cudaSuccess;
-    const int bytes = (int)gs_smem_bytes(true, ks);
-    cudaError_t e = cudaFuncSetAttribute(k_pressure_b, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mom_ml_b<COMP_U>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mom_ml_b<COMP_V>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_mom_ml_b<COMP_W>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    return e;
-}
+cudaError_t gs_prepare(bool, int) { return cudaSuccess; }
 
-cudaError_t gs_occupancy(bool il, int kind, int ks, int *blocks_per_sm) {
+cudaError_t gs_occupancy(bool il, int kind, int, int *blocks_per_sm) {
     const int th = gs_block_threads(il);
-    const size_t sm = gs_smem_bytes(il, ks);
     if (!il) {
         switch (kind) {
             case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure, th, 0);
@@ -404,24 +462,23 @@ cudaError_t gs_occupancy(bool il, int kind, int ks, int *blocks_per_sm) {
         }
     }
     switch (kind) {
-        case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure_b, th, sm);
-        case PH_U: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_U>, th, sm);
-        case PH_V: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_V>, th, sm);
-        default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_W>, th, sm);
+        case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure_b<GB_WARPS>, th, 0);
+        case PH_U: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_U, GB_WARPS>, th, 0);
+        case PH_V: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_V, GB_WARPS>, th, 0);
+        default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_W, GB_WARPS>, th, 0);
     }
 }
 
 void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
-    if (a.il) k_pressure_b<<<grid, GB_WARPS * 32, gs_smem_bytes(true, a.ks), st>>>(a, g);
+    if (a.il) k_pressure_b<GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
     else k_pressure<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
 }
 
 void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
-        const size_t sm = gs_smem_bytes(true, a.ks);
-        if (comp == 0) k_mom_ml_b<COMP_U><<<grid, GB_WARPS * 32, sm, st>>>(a, g);
-        else if (comp == 1) k_mom_ml_b<COMP_V><<<grid, GB_WARPS * 32, sm, st>>>(a, g);
-        else k_mom_ml_b<COMP_W><<<grid, GB_WARPS * 32, sm, st>>>(a, g);
+        if (comp == 0) k_mom_ml_b<COMP_U, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
+        else if (comp == 1) k_mom_ml_b<COMP_V, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
+        else k_mom_ml_b<COMP_W, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
     } else {
         if (comp == 0) k_mom_ml<COMP_U><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
         else if (comp == 1) k_mom_ml<COMP_V><<<grid, GS_WARPS * 32, 0, st>>>(a, g);

@@ -209,7 +209,7 @@ __global__ void k_bookkeeping(KArgs a) {
     if (s >= a.nb) return;
     SitDev &S = a.sit[s];
     if (!S.active) return;
-    const float dumax = __uint_as_float(S.dumax_bits);
+    const float dumax = S.quantise ? (float)((double)S.dumax_bits / S.frund) : __uint_as_float(S.dumax_bits);
     S.dumax_bits = 0;
     S.last_dumax = dumax;
     const int it = S.it;

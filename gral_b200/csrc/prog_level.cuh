@@ -75,6 +75,19 @@ __device__ __forceinline__ SitCtx make_sit(const KArgs &a, int s) {
     return q;
 }
 
+// Residual key of one pressure cell.  The reference's DeltaUMax is the float of the maximum over
+// cells of |0 - ConvToInt(temp*Frund)/Frund| (PrognosticFlowfield.cs:880); division by the positive
+// constant Frund is monotonic, so the maximum is taken over the integers |ConvToInt(temp*Frund)|
+// and divided once per iteration (k_bookkeeping).  Without quantisation the key is the bit pattern
+// of |temp| (non-negative floats order like their bits).
+__device__ __forceinline__ unsigned residual_key(float temp, const SitCtx &sc) {
+    if (sc.quant) {
+        const long long n = conv_to_int((double)temp * sc.frund);
+        return (unsigned)(n < 0 ? -n : n);
+    }
+    return __float_as_uint(fabsf(temp));
+}
+
 struct Coef {
     float A, B, C, D, phi;
 };
