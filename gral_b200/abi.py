@@ -78,6 +78,7 @@ class GralStats(C.Structure):
         ("trace_delta_umax", _fp), ("trace_capacity", C.c_int32),
         ("ms_total", C.c_double), ("ms_upload", C.c_double),
         ("ms_iterate", C.c_double), ("ms_download", C.c_double),
+        ("layout", C.c_int32), ("launch_variant", C.c_int32),
     ]
 
 

@@ -72,6 +72,7 @@ struct KArgs {
     int nii, njj, nkk, ks, nj2, ncols, nb;
     int il;                              // 1: interleaved layout (batched family), 0: slab layout
     int ngroups;                         // groups of 32 situations (interleaved layout)
+    int variant;                         // launch variant of the batched wavefront kernels
     float dxk, dyk, areaxy;
     float relax, relaxp, coriolis, vishmin;
     int simd;

@@ -28,7 +28,6 @@ namespace gral {
 namespace {
 
 constexpr int GS_WARPS = 4;      // warps per block, plain family
-constexpr int GB_WARPS = 8;      // warps per block, batched family (levels split over warps)
 constexpr int SM_ROWS = 5;       // shared rows per warp of the plain family: A, B, C, D, phi
 
 __device__ __forceinline__ void sweep_dir(int it, int &IS, int &JS) {
@@ -263,9 +262,21 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_mom_ml(KArgs a, SweepGeom g) 
 // and write A, B, C, D, phi rows [k][32] to shared memory; warp 0 then runs the 32 situations'
 // Thomas recurrences and back-substitutions side by side.
 
+// Shared rows of one task, [k][32] each, carved from dynamic shared memory sized by KS.
 struct BRows {
-    float A[KMAX_LEVELS][32], B[KMAX_LEVELS][32], C[KMAX_LEVELS][32], D[KMAX_LEVELS][32], phi[KMAX_LEVELS][32];
+    float *A, *B, *C, *D, *phi;
+    __device__ __forceinline__ float &a(int k, int l) { return A[k * 32 + l]; }
+    __device__ __forceinline__ float &b(int k, int l) { return B[k * 32 + l]; }
+    __device__ __forceinline__ float &c(int k, int l) { return C[k * 32 + l]; }
+    __device__ __forceinline__ float &d(int k, int l) { return D[k * 32 + l]; }
+    __device__ __forceinline__ float &p(int k, int l) { return phi[k * 32 + l]; }
 };
+
+__device__ __forceinline__ BRows carve_rows(float *smem, int ks) {
+    BRows R;
+    R.A = smem; R.B = R.A + ks * 32; R.C = R.B + ks * 32; R.D = R.C + ks * 32; R.phi = R.D + ks * 32;
+    return R;
+}
 
 // Block-wide variant of gs_tasks: thread 0 claims and waits, the block works, thread 0 publishes.
 template <int PHASE, bool REVERSE, class Body>
@@ -312,7 +323,7 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
 }
 
 template <int COMP, int NW>
-__device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R) {
+__device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows R) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
@@ -321,9 +332,10 @@ __device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R)
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     if (act) {
         const SitCtx sc = make_sit(a, s);
+#pragma unroll 2
         for (int k = c.K0 + warp; k <= c.VI; k += NW) {
             const Coef q = ml_level<COMP, true>(a, x, c, sc, k);
-            R.A[k][lane] = q.A; R.B[k][lane] = q.B; R.C[k][lane] = q.C; R.D[k][lane] = q.D; R.phi[k][lane] = q.phi;
+            R.a(k, lane) = q.A; R.b(k, lane) = q.B; R.c(k, lane) = q.C; R.d(k, lane) = q.D; R.p(k, lane) = q.phi;
         }
     }
     __syncthreads();
@@ -331,7 +343,7 @@ __device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R)
     float *F = comp_field<COMP>(a);
     float P = 0.0f, Q = 0.0f;
     for (int k = c.K0; k <= c.VI; ++k) {
-        const float A = R.A[k][lane], B = R.B[k][lane], C = R.C[k][lane], D = R.D[k][lane];
+        const float A = R.a(k, lane), B = R.b(k, lane), C = R.c(k, lane), D = R.d(k, lane);
         if (k > c.KK + 1) {
             const float T = 1.0f / (A - C * P);
             P = B * T;
@@ -341,16 +353,16 @@ __device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R)
             P = B * T;
             Q = D * T;
         }
-        R.B[k][lane] = P;
-        R.D[k][lane] = Q;
+        R.b(k, lane) = P;
+        R.d(k, lane) = Q;
     }
     const int kkm = back_limit<COMP>(c);
     const float relax = a.relax;
     float up = __ldcg(F + x.at(0, c.VI + 1));
     for (int k = c.VI; k >= c.K0; --k) {
-        float u = R.phi[k][lane];
+        float u = R.p(k, lane);
         if (kkm < k) {
-            u += relax * (R.B[k][lane] * up + R.D[k][lane] - u);
+            u += relax * (R.b(k, lane) * up + R.d(k, lane) - u);
             __stcg(F + x.at(0, k), u);
         }
         up = u;
@@ -359,7 +371,7 @@ __device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows &R)
 
 // Row carry of the batched family: [group][j][2][KS][32].
 template <int NW>
-__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first, BRows &R,
+__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first, BRows R,
                                       unsigned &nmax_acc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
@@ -373,21 +385,21 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     const SitCtx sc = make_sit(a, act ? s : grp * 32);
     if (act)
-        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.D[k][lane] = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.d(k, lane) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
     __syncthreads();
     if (warp == 0 && act) {
         float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
         for (int k = c.VI; k > c.KK; --k) {
             const float T = 1.0f / (a.app[k] - a.atp[k] * P);
             P = a.abp[k] * T;
-            Q = (a.atp[k] * Q + R.D[k][lane]) * T;
-            R.B[k][lane] = P;
-            R.C[k][lane] = Q;
+            Q = (a.atp[k] * Q + R.d(k, lane)) * T;
+            R.b(k, lane) = P;
+            R.c(k, lane) = Q;
         }
         float prev = 0.0f;                                         // DPM[KKART] is always 0
         for (int k = c.KK + 1; k <= c.VI; ++k) {
-            prev = R.B[k][lane] * prev + R.C[k][lane];
-            R.phi[k][lane] = prev;
+            prev = R.b(k, lane) * prev + R.c(k, lane);
+            R.p(k, lane) = prev;
         }
     }
     __syncthreads();
@@ -395,21 +407,22 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
     const int klo = max(c.KK, a.vi_min);
     unsigned nmax = 0;
     for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) {
-        const float temp = R.phi[k][lane];
+        const float temp = R.p(k, lane);
         nmax = max(nmax, residual_key(temp, sc));
         __stcg(a.dpm + x.at(0, k), temp);
         a.dpmnew[x.at(0, k)] += a.relaxp * temp;
         if (k > klo) {
-            __stcg(rc + (size_t)k * 32, R.B[k][lane]);
-            __stcg(rc + (size_t)(ks + k) * 32, R.C[k][lane]);
+            __stcg(rc + (size_t)k * 32, R.b(k, lane));
+            __stcg(rc + (size_t)(ks + k) * 32, R.c(k, lane));
         }
     }
     nmax_acc = max(nmax_acc, nmax);
 }
 
-template <int NW>
-__global__ void __launch_bounds__(NW * 32) k_pressure_b(KArgs a, SweepGeom g) {
-    __shared__ BRows R;
+template <int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_pressure_b(KArgs a, SweepGeom g) {
+    extern __shared__ float smem[];
+    BRows R = carve_rows(smem, a.ks);
     __shared__ unsigned red[NW][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned nmax = 0;
@@ -434,25 +447,57 @@ __global__ void __launch_bounds__(NW * 32) k_pressure_b(KArgs a, SweepGeom g) {
     flush();
 }
 
-template <int COMP, int NW>
-__global__ void __launch_bounds__(NW * 32) k_mom_ml_b(KArgs a, SweepGeom g) {
-    __shared__ BRows R;
+template <int COMP, int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_mom_ml_b(KArgs a, SweepGeom g) {
+    extern __shared__ float smem[];
+    BRows R = carve_rows(smem, a.ks);
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
     gs_tasks_block<PH, COMP == COMP_V>(a, g, [&](int grp, int i, int j, int, int, bool) {
         batch_ml_column<COMP, NW>(a, grp, i, j, R);
     });
 }
 
+// Launch variants of the batched family: (warps per block, minimum resident blocks per SM).
+// The host times them once per context and keeps the fastest (GRAL_PROG_BATCH_VARIANT forces one).
+struct BVariant {
+    int nw, minb;
+    void (*pressure)(KArgs, SweepGeom);
+    void (*mom[3])(KArgs, SweepGeom);
+};
+
+#define GRAL_BV(NW, MB)                                                                          \
+    BVariant{NW, MB, k_pressure_b<NW, MB>,                                                       \
+             {k_mom_ml_b<COMP_U, NW, MB>, k_mom_ml_b<COMP_V, NW, MB>, k_mom_ml_b<COMP_W, NW, MB>}}
+
+const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(8, 3), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(16, 1)};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
 }  // namespace
 
-int gs_block_threads(bool il) { return il ? GB_WARPS * 32 : GS_WARPS * 32; }
+int gs_num_variants() { return kNumVariants; }
 
-size_t gs_smem_bytes(bool, int) { return 0; }
+int gs_block_threads(bool il, int variant) { return il ? kVariants[variant].nw * 32 : GS_WARPS * 32; }
 
-cudaError_t gs_prepare(bool, int) { return cudaSuccess; }
+size_t gs_smem_bytes(bool il, int ks, int variant) {
+    (void)variant;
+    return il ? (size_t)5 * ks * 32 * sizeof(float) : 0;
+}
 
-cudaError_t gs_occupancy(bool il, int kind, int, int *blocks_per_sm) {
-    const int th = gs_block_threads(il);
+cudaError_t gs_prepare(bool il, int ks) {
+    if (!il) return cudaSuccess;
+    const int bytes = (int)gs_smem_bytes(true, ks, 0);
+    for (int v = 0; v < kNumVariants; ++v) {
+        const BVariant &V = kVariants[v];
+        cudaError_t e = cudaFuncSetAttribute(V.pressure, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        for (int q = 0; q < 3 && e == cudaSuccess; ++q)
+            e = cudaFuncSetAttribute(V.mom[q], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t gs_occupancy(bool il, int kind, int ks, int variant, int *blocks_per_sm) {
+    const int th = gs_block_threads(il, variant);
     if (!il) {
         switch (kind) {
             case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure, th, 0);
@@ -461,24 +506,25 @@ cudaError_t gs_occupancy(bool il, int kind, int, int *blocks_per_sm) {
             default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml<COMP_W>, th, 0);
         }
     }
-    switch (kind) {
-        case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure_b<GB_WARPS>, th, 0);
-        case PH_U: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_U, GB_WARPS>, th, 0);
-        case PH_V: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_V, GB_WARPS>, th, 0);
-        default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml_b<COMP_W, GB_WARPS>, th, 0);
-    }
+    const BVariant &V = kVariants[variant];
+    const size_t sm = gs_smem_bytes(true, ks, variant);
+    void (*f)(KArgs, SweepGeom) = (kind == PH_PRESSURE) ? V.pressure : V.mom[kind == PH_U ? 0 : (kind == PH_V ? 1 : 2)];
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, th, sm);
 }
 
 void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
-    if (a.il) k_pressure_b<GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
-    else k_pressure<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
+    if (a.il) {
+        const BVariant &V = kVariants[a.variant];
+        V.pressure<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(a, g);
+    } else {
+        k_pressure<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
+    }
 }
 
 void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
-        if (comp == 0) k_mom_ml_b<COMP_U, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
-        else if (comp == 1) k_mom_ml_b<COMP_V, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
-        else k_mom_ml_b<COMP_W, GB_WARPS><<<grid, GB_WARPS * 32, 0, st>>>(a, g);
+        const BVariant &V = kVariants[a.variant];
+        V.mom[comp]<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(a, g);
     } else {
         if (comp == 0) k_mom_ml<COMP_U><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
         else if (comp == 1) k_mom_ml<COMP_V><<<grid, GS_WARPS * 32, 0, st>>>(a, g);

@@ -59,6 +59,8 @@ struct gral_ctx {
     cudaEvent_t ev[4] = {};
     int cap_nii = 0, cap_njj = 0, cap_nkk = 0, cap_kadv = 0, cap_batch = 0;
     int il_min_batch = 32;
+    int forced_variant = -1;   // GRAL_PROG_BATCH_VARIANT
+    int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
     std::string err = "no error";
 
     // current load
@@ -76,6 +78,7 @@ struct gral_ctx {
     int grid_gs[4] = {0, 0, 0, 0};
     cudaGraphExec_t graph = nullptr;
     float ms_upload = 0.f;
+    float tune_ms[16] = {0};
 
     // device buffers
     DevBuf<float> slab, stage, veg, tables, ap0, rowcarry, trace;
@@ -275,11 +278,8 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
     return GRAL_OK;
 }
 
-int build_graph(gral_ctx *ctx) {
-    if (ctx->graph) { cudaGraphExecDestroy(ctx->graph); ctx->graph = nullptr; }
-    cudaGraph_t g = nullptr;
-    cudaStream_t st = ctx->stream;
-    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+// One SIMPLE iteration (PrognosticFlowfield.cs:584-1182), enqueued on st.
+void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
     cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
@@ -290,12 +290,75 @@ int build_graph(gral_ctx *ctx) {
     launch_mom_ml(1, a, ctx->geo_v.g, ctx->grid_gs[2], st);
     launch_mom_ml(2, a, ctx->geo_p.g, ctx->grid_gs[3], st);
     launch_bookkeeping(a, st);
+}
+
+// Grid sizes of the wavefront kernels for the current family and variant: every resident block
+// slot of the GPU (the kernels are persistent and claim tasks).
+int size_grids(gral_ctx *ctx) {
+    const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
+    const bool il = ctx->il;
+    const int v = il ? std::max(ctx->variant, 0) : 0;
+    for (int q = 0; q < 4; ++q) {
+        int bps = 0;
+        CK(gs_occupancy(il, kinds[q], ctx->ks, v, &bps));
+        ctx->grid_gs[q] = std::max(1, bps) * ctx->num_sms;
+    }
+    const int warps = ctx->grid_gs[0] * gs_block_threads(il, v) / 32;
+    const long long per_diag = (long long)(il ? ctx->ngroups : ctx->nb) * std::min(ctx->nii, ctx->njj);
+    ctx->ka.chunk = il ? 1 : (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
+    ctx->ka.variant = v;
+    return GRAL_OK;
+}
+
+int build_graph(gral_ctx *ctx) {
+    if (ctx->graph) { cudaGraphExecDestroy(ctx->graph); ctx->graph = nullptr; }
+    cudaGraph_t g = nullptr;
+    cudaStream_t st = ctx->stream;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    launch_iteration(ctx, st);
     cudaError_t e = cudaStreamEndCapture(st, &g);
     if (e != cudaSuccess) return fail(ctx, GRAL_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&ctx->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(ctx, GRAL_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     return GRAL_OK;
+}
+
+// Autotuner of the batched family: every launch variant gives bit-identical results, so the first
+// iterations of the solve each run one variant, timed with CUDA events, and the fastest is kept
+// and captured into the iteration graph.  Runs only when enough iterations remain before the
+// first convergence test; otherwise variant 0 is used.
+int tune_variants(gral_ctx *ctx) {
+    if (!ctx->il || ctx->variant >= 0) return GRAL_OK;
+    const int nv = gs_num_variants();
+    const int first_stop = std::min(((ctx->it_host + ctx->cadence - 1) / ctx->cadence) * ctx->cadence, ctx->it_max);
+    if (ctx->forced_variant >= 0 && ctx->forced_variant < nv) {
+        ctx->variant = ctx->forced_variant;
+    } else if (first_stop - ctx->it_host + 1 > nv) {
+        cudaStream_t st = ctx->stream;
+        float best = 1e30f;
+        int best_v = 0;
+        for (int v = 0; v < nv; ++v) {
+            ctx->variant = v;
+            int rc = size_grids(ctx);
+            if (rc != GRAL_OK) return rc;
+            CK(cudaEventRecord(ctx->ev[2], st));
+            launch_iteration(ctx, st);
+            CK(cudaEventRecord(ctx->ev[3], st));
+            CK(cudaEventSynchronize(ctx->ev[3]));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+            ctx->tune_ms[v] = ms;
+            if (ms < best) { best = ms; best_v = v; }
+            ctx->it_host++;
+        }
+        ctx->variant = best_v;
+    } else {
+        ctx->variant = 0;
+    }
+    int rc = size_grids(ctx);
+    if (rc != GRAL_OK) return rc;
+    return build_graph(ctx);
 }
 
 }  // namespace
@@ -317,6 +380,7 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
         if (std::strcmp(lay, "interleaved") == 0) ctx->il_min_batch = 1;
         else if (std::strcmp(lay, "slab") == 0) ctx->il_min_batch = 1 << 30;
     }
+    if (const char *v = std::getenv("GRAL_PROG_BATCH_VARIANT")) ctx->forced_variant = std::atoi(v);
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
     for (auto &e : ctx->ev)
@@ -564,19 +628,15 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaGetLastError());
 
     // ---- launch shapes of the wavefront kernels ----
-    const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
     CK(gs_prepare(il, ks));
-    for (int q = 0; q < 4; ++q) {
-        int bps = 0;
-        CK(gs_occupancy(il, kinds[q], ks, &bps));
-        ctx->grid_gs[q] = std::max(1, bps) * ctx->num_sms;
-    }
-    const int warps = ctx->grid_gs[0] * gs_block_threads(il) / 32;
-    const long long per_diag = (long long)(il ? ngroups : n) * std::min(NII, NJJ);
-    a.chunk = (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
     ctx->it_host = 1;
-    int brc = build_graph(ctx);
+    ctx->variant = -1;
+    int brc = size_grids(ctx);
     if (brc != GRAL_OK) return brc;
+    if (!il) {
+        brc = build_graph(ctx);
+        if (brc != GRAL_OK) return brc;
+    }
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&ctx->ms_upload, ctx->ev[0], ctx->ev[1]));
@@ -589,6 +649,8 @@ int gral_prog_iterate(gral_ctx *ctx) {
     if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "iterate before load");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
+    int trc = tune_variants(ctx);
+    if (trc != GRAL_OK) return trc;
     int nact = ctx->h_act[1];
     while (nact > 0 && ctx->it_host <= ctx->it_max) {
         // run up to the next iteration where the reference can stop (a convergence test or the limit)
@@ -624,6 +686,8 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
     if (iterations < 1) return fail(ctx, GRAL_EINVAL, "iterations must be >= 1");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
+    int trc = tune_variants(ctx);
+    if (trc != GRAL_OK) return trc;
     const KArgs &a = ctx->ka;
     const int marks = GRAL_NUM_PHASES + 1;
     std::vector<cudaEvent_t> ev((size_t)iterations * marks, nullptr);
@@ -740,6 +804,8 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
         }
         o.ms_upload = ctx->ms_upload;
         o.ms_download = ms_down;
+        o.layout = ctx->il ? 1 : 0;
+        o.launch_variant = ctx->il ? ctx->variant : -1;
     }
     if (rc != GRAL_OK) fail(ctx, rc, "non-finite values in the solved fields");
     return rc;

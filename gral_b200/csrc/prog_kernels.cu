@@ -154,7 +154,8 @@ __global__ void k_velcorr(KArgs a) {
         const double fr = sd.frund;
         const int q = sd.quantise;
         const long long dW = -(long long)a.nj2;
-        for (int k = kbeg; k <= m.vi; k += kstep) {
+#pragma unroll 4
+        for (int k = kbeg; k <= m.vi; k += (IL ? 1 : 32)) {
             if (k < 1) continue;
             const float d = a.dpm[x.at(0, k)];
             if (i > 2 && m.kkm_u < k)
@@ -182,7 +183,8 @@ __global__ void k_average(KArgs a) {
         const int KK = m.kkart;
         const bool cpS = (j == 2);
         const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
-        for (int k = kbeg; k <= m.vi; k += kstep) {
+#pragma unroll 4
+        for (int k = kbeg; k <= m.vi; k += (IL ? 1 : 32)) {
             if (k < m.kstart) continue;
             if (KK < k) {
                 a.uks[x.at(0, k)] = 0.5f * (a.uk[x.at(0, k)] + a.uk[x.at(dE, k)]);
@@ -197,7 +199,8 @@ __global__ void k_average(KArgs a) {
         const bool east = (i == a.nii - 1) && (a.cflags[col] & F_ADV);
         if (west || east) {
             const long long dd = west ? -(long long)nj2 : dE;
-            for (int k = kbeg; k < a.ks; k += kstep) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
+#pragma unroll 4
+            for (int k = kbeg; k < a.ks; k += (IL ? 1 : 32)) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
         }
     });
 }

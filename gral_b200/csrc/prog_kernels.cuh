@@ -22,10 +22,11 @@ struct Staging {
     size_t stride;   // floats between situations
 };
 
-int gs_block_threads(bool il);
-size_t gs_smem_bytes(bool il, int ks);
+int gs_num_variants();
+int gs_block_threads(bool il, int variant);
+size_t gs_smem_bytes(bool il, int ks, int variant);
 cudaError_t gs_prepare(bool il, int ks);
-cudaError_t gs_occupancy(bool il, int kind, int ks, int *blocks_per_sm);
+cudaError_t gs_occupancy(bool il, int kind, int ks, int variant, int *blocks_per_sm);
 void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
 void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
 

@@ -111,6 +111,9 @@ typedef struct gral_stats {
     float *trace_delta_umax;     /* optional, caller-owned: DeltaUMax per iteration */
     int32_t trace_capacity;
     double ms_total, ms_upload, ms_iterate, ms_download;
+    int32_t layout;              /* device layout used: 0 slab (one warp per column), 1 interleaved
+                                    (32 situations per group, one block per group-column) */
+    int32_t launch_variant;      /* launch variant the autotuner kept (interleaved layout) */
 } gral_stats;
 
 typedef struct gral_ctx gral_ctx;
