@@ -39,8 +39,17 @@ UNIT = "Mcell-iterations/s"
 BYTES_PER_CELL = {"pressure": 24, "velcorr": 28, "u": 20, "v": 20, "w": 20}   # model 1
 
 
-def workload(name: str):
+def workload(name: str, grid: int = 400):
     from gral_b200 import prep
+    if name == "production" and grid != 400:
+        dom = prep.city_domain(n=grid, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30,
+                               n_buildings=max(1, 64 * grid * grid // 160000), seed=2)
+        sit = prep.Situation(direction_deg=225.0, speed_10m=2.0, z0=0.5, ustar=0.3)
+        return dom, sit, 500, f"{grid}x{grid}x30 at 2 m, stretch 1.05, seeded buildings, 225 deg 2 m/s, 500 iterations"
+    if name == "batched" and grid != 400:
+        dom = prep.city_domain(n=grid, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30,
+                               n_buildings=max(1, 64 * grid * grid // 160000), seed=2)
+        return dom, None, 800, f"batched situations on a {grid}x{grid}x30 grid"
     if name == "production":
         dom = prep.city_domain(n=400, dx=2.0, dz1=2.0, stretch=1.05, vert_cells_ff=30, n_buildings=64, seed=2)
         sit = prep.Situation(direction_deg=225.0, speed_10m=2.0, z0=0.5, ustar=0.3)
@@ -232,7 +241,7 @@ def run_ours(args, rank, world):
         import torch.distributed as td
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    dom, sit, full_iters, desc = workload(args.workload)
+    dom, sit, full_iters, desc = workload(args.workload, args.grid)
     sits = batched_situations(args.batch) if sit is None else [sit]
     nsit = len(sits)
     cells = nominal_cells(dom) * nsit
@@ -335,6 +344,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["production", "batched", "cube"], default="production")
     ap.add_argument("--batch", type=int, default=144, help="situations of the batched workload")
+    ap.add_argument("--grid", type=int, default=400, help="columns per side of the city grid (profiling cases)")
     ap.add_argument("--e2e-iters", type=int, default=0, help="iterations of the e2e solve (0: the workload's)")
     ap.add_argument("--cpu-iters", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")

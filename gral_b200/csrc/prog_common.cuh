@@ -73,6 +73,9 @@ struct KArgs {
     int il;                              // 1: interleaved layout (batched family), 0: slab layout
     int ngroups;                         // groups of 32 situations (interleaved layout)
     int variant;                         // launch variant of the batched wavefront kernels
+    int group_lo, group_n;               // groups swept by one wavefront launch (batched family)
+    int ctr_slot;                        // task-counter slot of the launch
+    int group_set;                       // groups per wavefront launch (0 = all)
     float dxk, dyk, areaxy;
     float relax, relaxp, coriolis, vishmin;
     int simd;

@@ -293,11 +293,11 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
     const int stamp = it * 8 + PHASE;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_base = atomicAdd(ctr, (unsigned)a.chunk);
+        if (threadIdx.x == 0)
+            s_base = (*(volatile int *)a.err != ERR_NONE) ? 0xffffffffu : atomicAdd(ctr, (unsigned)a.chunk);
         __syncthreads();
         const unsigned base = s_base;
         if (base >= total) break;
-        if (*(volatile int *)a.err != ERR_NONE) break;
         const unsigned end = min(total, base + (unsigned)a.chunk);
         for (unsigned t = base; t < end; ++t) {
             int grp, i1, j1;

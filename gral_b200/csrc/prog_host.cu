@@ -45,6 +45,8 @@ struct DevBuf {
     }
 };
 
+constexpr int kCounterSlots = 64;   // wavefront launches per phase (group sets) with own counters
+
 struct Geom {
     SweepGeom g;
     std::vector<int> ds;
@@ -281,7 +283,7 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
 // One SIMPLE iteration (PrognosticFlowfield.cs:584-1182), enqueued on st.
 void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
-    cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st);
+    cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
     launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
     launch_velcorr(a, st);
@@ -297,7 +299,16 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
 int size_grids(gral_ctx *ctx) {
     const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
     const bool il = ctx->il;
-    const int v = il ? std::max(ctx->variant, 0) : 0;
+    const int nkv = gs_num_variants();
+    const int vv = il ? std::max(ctx->variant, 0) : 0;
+    const int v = vv % nkv;                     // kernel variant
+    const int gm = vv / nkv;                    // group-set mode: 0 all groups, 1 two, 2 one
+    ctx->ka.group_set = (gm == 0) ? 0 : (gm == 1 ? 2 : 1);
+    ctx->ka.group_lo = 0;
+    ctx->ka.group_n = ctx->ngroups;
+    ctx->ka.ctr_slot = 0;
+    if (il && (ctx->ngroups + std::max(ctx->ka.group_set, 1) - 1) / std::max(ctx->ka.group_set, 1) > kCounterSlots)
+        ctx->ka.group_set = 0;
     for (int q = 0; q < 4; ++q) {
         int bps = 0;
         CK(gs_occupancy(il, kinds[q], ctx->ks, v, &bps));
@@ -330,7 +341,7 @@ int build_graph(gral_ctx *ctx) {
 // first convergence test; otherwise variant 0 is used.
 int tune_variants(gral_ctx *ctx) {
     if (!ctx->il || ctx->variant >= 0) return GRAL_OK;
-    const int nv = gs_num_variants();
+    const int nv = gs_num_variants() * (ctx->ngroups > 2 ? 3 : (ctx->ngroups > 1 ? 2 : 1));
     const int first_stop = std::min(((ctx->it_host + ctx->cadence - 1) / ctx->cadence) * ctx->cadence, ctx->it_max);
     if (ctx->forced_variant >= 0 && ctx->forced_variant < nv) {
         ctx->variant = ctx->forced_variant;
@@ -522,7 +533,7 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(ctx->rowcarry.ensure(units * nj2 * 2 * ks));
     CK(ctx->trace.ensure((size_t)n * tcap));
     CK(ctx->misc.ensure(3 + n));                      // err, nact, it, act[n]
-    CK(ctx->counters.ensure(8));
+    CK(ctx->counters.ensure(8 * kCounterSlots));
     CK(ctx->counts.ensure(4 * (size_t)n));
     const size_t dsz = ctx->geo_p.ds.size() + ctx->geo_u.ds.size() + ctx->geo_v.ds.size();
     CK(ctx->diag.ensure(dsz));
@@ -695,7 +706,7 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
     for (int it = 0; it < iterations; ++it) {
         cudaEvent_t *E = ev.data() + (size_t)it * marks;
         CK(cudaEventRecord(E[GRAL_PHASE_BC], st));
-        CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st));
+        CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st));
         launch_bc(a, ctx->bc, st);
         CK(cudaEventRecord(E[GRAL_PHASE_PRESSURE], st));
         launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
