@@ -19,6 +19,8 @@
 //   batched (interleaved layout) one warp per (group of 32 situations, column), lane =
 //                                situation; every lane runs its own k loop and Thomas sweep, the
 //                                P/Q rows live in shared memory [k][thread].
+#include <algorithm>
+
 #include "prog_common.cuh"
 #include "prog_kernels.cuh"
 #include "prog_level.cuh"
@@ -283,9 +285,9 @@ template <int PHASE, bool REVERSE, class Body>
 __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &g, Body &&body) {
     __shared__ unsigned s_base;
     __shared__ int s_ok;
-    const unsigned units = (unsigned)a.ngroups;
+    const unsigned units = (unsigned)a.group_n;
     const unsigned total = (unsigned)g.diag_start[g.ndiag] * units;
-    unsigned int *ctr = a.counters + PHASE;
+    unsigned int *ctr = a.counters + 8 * a.ctr_slot + PHASE;
     const int it = *a.it_global;
     int IS, JS;
     sweep_dir(it, IS, JS);
@@ -302,6 +304,7 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
         for (unsigned t = base; t < end; ++t) {
             int grp, i1, j1;
             decode_task(t, g, units, grp, i1, j1);
+            grp += a.group_lo;
             const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
             const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
             int *fl = a.flags + (size_t)grp * a.ncols;
@@ -469,7 +472,7 @@ struct BVariant {
     BVariant{NW, MB, k_pressure_b<NW, MB>,                                                       \
              {k_mom_ml_b<COMP_U, NW, MB>, k_mom_ml_b<COMP_V, NW, MB>, k_mom_ml_b<COMP_W, NW, MB>}}
 
-const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(8, 3), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(16, 1)};
+const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 }  // namespace
@@ -512,10 +515,27 @@ cudaError_t gs_occupancy(bool il, int kind, int ks, int variant, int *blocks_per
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, th, sm);
 }
 
+// Group sets of the batched family: a launch sweeps group_set groups at a time (0 = all groups),
+// each launch with its own task counter.
+template <class F>
+void for_group_sets(const KArgs &a, F &&f) {
+    const int gs = (a.group_set <= 0) ? a.ngroups : a.group_set;
+    int slot = 0;
+    for (int lo = 0; lo < a.ngroups; lo += gs, ++slot) {
+        KArgs b = a;
+        b.group_lo = lo;
+        b.group_n = std::min(gs, a.ngroups - lo);
+        b.ctr_slot = slot;
+        f(b);
+    }
+}
+
 void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
         const BVariant &V = kVariants[a.variant];
-        V.pressure<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(a, g);
+        for_group_sets(a, [&](const KArgs &b) {
+            V.pressure<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(b, g);
+        });
     } else {
         k_pressure<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
     }
@@ -524,7 +544,9 @@ void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t 
 void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
         const BVariant &V = kVariants[a.variant];
-        V.mom[comp]<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(a, g);
+        for_group_sets(a, [&](const KArgs &b) {
+            V.mom[comp]<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(b, g);
+        });
     } else {
         if (comp == 0) k_mom_ml<COMP_U><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
         else if (comp == 1) k_mom_ml<COMP_V><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
