@@ -46,6 +46,14 @@ struct ColF {             // 16 bytes
     float cov, z0, help_t, help_o;    // COV, roughness, UsternTerrain/ObstaclesHelpterm
 };
 
+// k-eps wall functions of the TKE back-substitution (TKE-prognostic-microscale.cs:272-343):
+// gfac = 0.4/ln(z/Z0) of the ground law in double (gmode 1: z = DZK[k]+DZK[k+1]/2, 0: DZK[k]/2);
+// kw_e/w/n/s = KKART+1 of the east/west/north/south neighbour when it is a building, else -1.
+struct ColKE {            // 16 bytes
+    double gfac;
+    int16_t kw_e, kw_w, kw_n, kw_s;
+};
+
 // Per-situation scalars and convergence state (PrognosticFlowfield.cs:146-163, 231-240, 1144-1170).
 struct SitDev {
     double frund;
@@ -54,6 +62,9 @@ struct SitDev {
     double hist[MAX_HIST];
     unsigned long long geschw_bits;   // GESCHW_MAX as non-negative double bits (atomicMax)
     float dtime, topwind, ug, vg;
+    float potdtdz;           // Program.PotdTdz of the situation (k-eps buoyancy)
+    float std_dev_v, v0_1;   // TURB initialisation (PrognosticFlowfield.cs:477-486)
+    int32_t turb_init;       // 0: initialise TURB/TDISS as the reference, 1: keep the caller's
     float delta_first, delta_finish, last_dumax;
     uint32_t dumax_bits;     // running max of the residual keys of this iteration (see residual_key)
     int32_t it;              // IterationLoops
@@ -83,6 +94,9 @@ struct KArgs {
     const ColMeta *meta;
     const uint32_t *cflags;              // F_* bits per column
     const ColF *colf;
+    const ColKE *colke;                  // per column, model 2 only (else null)
+    float ustern_fx, building_z0;        // Ustern_factorX, building roughness (k-eps wall laws)
+    int model;                           // TurbulenceModel 0, 1, 2
     const float *dzk, *hokart;           // [ks]
     const float *app, *abp, *atp;        // pressure coefficients per level [ks]
     const float *veg;                    // [ncols][ks] or null
@@ -116,6 +130,7 @@ struct SweepGeom {
 enum : int { ERR_NONE = 0, ERR_TIMEOUT = 1, ERR_NONFINITE = 2 };
 
 enum : int { PH_PRESSURE = 1, PH_U = 2, PH_V = 3, PH_W = 4, PH_TKE = 5 };
+enum : int { F_GMODE1 = 1 << 13 };   // ColKE ground law uses level k+1 (Z0 >= DZK/2)
 
 __host__ __device__ inline size_t fidx(int s, int col, int ncols, int ks) {
     return ((size_t)s * ncols + col) * ks;

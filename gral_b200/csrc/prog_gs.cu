@@ -155,10 +155,183 @@ __device__ __forceinline__ float *comp_field(const KArgs &a) {
     return COMP == COMP_U ? a.uk : (COMP == COMP_V ? a.vk : a.wk);
 }
 
+// Coefficients of one level for model MODEL (0 no diffusion, 1 mixing length, 2 k-eps).
+template <int MODEL, int COMP, bool IL>
+__device__ __forceinline__ Coef mom_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+    if (MODEL == 1) return ml_level<COMP, IL>(a, x, c, sc, k);
+    if (COMP == COMP_W) return w_scalar_level<MODEL == 2, IL>(a, x, c, sc, k);
+    return uv_scalar_level<MODEL == 2, COMP, IL>(a, x, c, sc, k);
+}
+
+// Vertical Thomas recurrence and relaxed back-substitution of one situation's column on rows
+// R.a/b/c/d/p (A, B, C, D, phi): model 1 multiplies by 1/(A - C*P) (U-prognostic-microscale_1.cs:
+// 485-504), models 2 and 0 divide twice (U-prognostic-microscale_2.cs:247-256), and the model-0
+// W routine keeps P and Q in double (W-prognostic-microscale_0.cs:35-36, 124-139).  phi is
+// replaced by the new values on the levels the reference updates.
+template <int MODEL, int COMP, class Rows>
+__device__ __forceinline__ void mom_sweep(Rows &R, int K0, int KK, int VI, int kkm, float relax, float top) {
+    if (MODEL == 0 && COMP == COMP_W) {
+        double P = 0.0, Q = 0.0;
+        for (int k = K0; k <= VI; ++k) {
+            const float A = R.a(k), B = R.b(k), C = R.c(k), D = R.d(k);
+            if (k > KK + 1) {
+                const double den = (double)A - (double)C * P;
+                const double Pn = (double)B / den;
+                Q = ((double)D + (double)C * Q) / den;
+                P = Pn;
+            } else {
+                P = (double)(B / A);
+                Q = (double)(D / A);
+            }
+            R.pd(k) = P;
+            R.qd(k) = Q;
+        }
+        float up = top;
+        for (int k = VI; k >= K0; --k) {
+            float u = R.p(k);
+            u += (float)((double)relax * (R.pd(k) * (double)up + R.qd(k) - (double)u));
+            R.p(k) = u;
+            up = u;
+        }
+        return;
+    }
+    float P = 0.0f, Q = 0.0f;
+    for (int k = K0; k <= VI; ++k) {
+        const float A = R.a(k), B = R.b(k), C = R.c(k), D = R.d(k);
+        if (k > KK + 1) {
+            if (MODEL == 1) {
+                const float T = 1.0f / (A - C * P);
+                P = B * T;
+                Q = (D + C * Q) * T;
+            } else {
+                const float Pn = B / (A - C * P);
+                Q = (D + C * Q) / (A - C * P);
+                P = Pn;
+            }
+        } else {
+            if (MODEL == 1) {
+                const float T = 1.0f / A;
+                P = B * T;
+                Q = D * T;
+            } else {
+                P = B / A;
+                Q = D / A;
+            }
+        }
+        R.b(k) = P;
+        R.d(k) = Q;
+    }
+    float up = top;
+    for (int k = VI; k >= K0; --k) {
+        float u = R.p(k);
+        if (kkm < k) {
+            u += relax * (R.b(k) * up + R.d(k) - u);
+            R.p(k) = u;
+        }
+        up = u;
+    }
+}
+
+// k and eps: two recurrences with divisions sharing A, then the back-substitution with the wall
+// functions of ground, roof and the four neighbour walls, and the clamps
+// (TKE-prognostic-microscale.cs:255-347).  Rows: a, b1, c1, d1, b2, c2, d2, k1 (TURB), e1 (TDISS);
+// vel(field, dc, k) loads UK/VK/WK of the column (dc = 0) or its east/north neighbour.
+template <class Rows, class Vel>
+__device__ __forceinline__ void tke_sweep(Rows &R, const KArgs &a, const ColCtx &c, const ColKE &ke, float ktop,
+                                          float etop, Vel &&vel) {
+    const int K0 = c.K0, KK = c.KK, VI = c.VI;
+    float PT = 0.0f, QT = 0.0f, PE = 0.0f, QE = 0.0f;
+    for (int k = K0; k <= VI; ++k) {
+        const float A = R.a(k), B1 = R.b1(k), C1 = R.c1(k), D1 = R.d1(k);
+        const float B2 = R.b2(k), C2 = R.c2(k), D2 = R.d2(k);
+        if (k > KK + 1) {
+            const float PTn = B1 / (A - C1 * PT);
+            QT = (D1 + C1 * QT) / (A - C1 * PT);
+            PT = PTn;
+            const float PEn = B2 / (A - C2 * PE);
+            QE = (D2 + C2 * QE) / (A - C2 * PE);
+            PE = PEn;
+        } else {
+            PT = B1 / A; QT = D1 / A; PE = B2 / A; QE = D2 / A;
+        }
+        R.b1(k) = PT; R.d1(k) = QT; R.b2(k) = PE; R.d2(k) = QE;
+    }
+    const long long E = c.nj2, N = 1;
+    auto hyp = [](double p, double q) { return sqrt(p * p + q * q); };
+    float kup = ktop, eup = etop;
+    for (int k = VI; k >= K0; --k) {
+        float kn = R.k1(k), en = R.e1(k);
+        if (KK < k) {
+            float U;
+            bool wall = true;
+            double div;   // TDISS divisor
+            if (k == KK + 1 && (c.fl & F_CUTK0)) {
+                if (c.fl & F_GMODE1) {
+                    U = (float)(ke.gfac * hyp(0.5 * (double)(vel(0, 0, k + 1) + vel(0, E, k + 1)),
+                                              0.5 * (double)(vel(1, 0, k + 1) + vel(1, N, k + 1))));
+                    div = ((double)a.dzk[k] + (double)a.dzk[k + 1] * 0.5) * 0.4;
+                } else {
+                    U = (float)(ke.gfac * hyp(0.5 * (double)((vel(0, 0, k + 1)) + vel(0, E, k)),
+                                              0.5 * (double)((vel(1, 0, k)) + vel(1, N, k))));
+                    div = (double)a.dzk[k] * 0.5 * 0.4;
+                }
+            } else if (k == KK + 1 && (c.fl & F_CUTKGT0)) {
+                U = c.cf.help_o * (float)hyp(0.5 * (double)(vel(0, 0, k) + vel(0, E, k)),
+                                             0.5 * (double)(vel(1, 0, k) + vel(1, N, k)));
+                div = (double)a.dzk[k] * 0.5 * 0.4;
+            } else if (k == ke.kw_e || k == ke.kw_w) {
+                U = (float)((double)a.ustern_fx * hyp(0.5 * (double)(vel(2, 0, k) + vel(2, 0, k + 1)),
+                                                      0.5 * (double)(vel(1, 0, k) + vel(1, N, k))));
+                div = (double)a.building_z0 * 0.4;
+            } else if (k == ke.kw_n || k == ke.kw_s) {
+                U = (float)((double)a.ustern_fx * hyp(0.5 * (double)(vel(2, 0, k) + vel(2, 0, k + 1)),
+                                                      0.5 * (double)(vel(0, 0, k) + vel(0, E, k))));
+                div = (double)a.building_z0 * 0.4;
+            } else {
+                wall = false;
+                kn = R.b1(k) * kup + R.d1(k);
+                en = R.b2(k) * eup + R.d2(k);
+            }
+            if (wall) {
+                kn = (float)(3.33 * (double)(U * U));
+                en = (float)((double)(U * U * U) / div);
+            }
+            kn = (float)net_maxd((double)kn, 0.001);
+            en = (float)net_maxd((double)en, 0.0000001);
+            R.k1(k) = kn;
+            R.e1(k) = en;
+        }
+        kup = kn;
+        eup = en;
+    }
+}
+
 // ---------------------------- plain family -------------------------------------------------
 
-template <int COMP>
-__device__ void plain_ml_column(const KArgs &a, int s, int i, int j, float (*S)[KMAX_LEVELS]) {
+struct PlainRows {
+    float (*S)[KMAX_LEVELS];
+    double (*SD)[KMAX_LEVELS];
+    __device__ __forceinline__ float &a(int k) { return S[0][k]; }
+    __device__ __forceinline__ float &b(int k) { return S[1][k]; }
+    __device__ __forceinline__ float &c(int k) { return S[2][k]; }
+    __device__ __forceinline__ float &d(int k) { return S[3][k]; }
+    __device__ __forceinline__ float &p(int k) { return S[4][k]; }
+    __device__ __forceinline__ double &pd(int k) { return SD[0][k]; }
+    __device__ __forceinline__ double &qd(int k) { return SD[1][k]; }
+    // TKE rows
+    __device__ __forceinline__ float &b1(int k) { return S[1][k]; }
+    __device__ __forceinline__ float &c1(int k) { return S[2][k]; }
+    __device__ __forceinline__ float &d1(int k) { return S[3][k]; }
+    __device__ __forceinline__ float &k1(int k) { return S[4][k]; }
+    __device__ __forceinline__ float &b2(int k) { return S[5][k]; }
+    __device__ __forceinline__ float &c2(int k) { return S[6][k]; }
+    __device__ __forceinline__ float &d2(int k) { return S[7][k]; }
+    __device__ __forceinline__ float &e1(int k) { return S[8][k]; }
+};
+
+template <int MODEL, int COMP>
+__device__ void plain_mom_column(const KArgs &a, int s, int i, int j, float (*S)[KMAX_LEVELS],
+                                 double (*SD)[KMAX_LEVELS]) {
     const int lane = threadIdx.x & 31;
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV) || !a.sit[s].active) return;
@@ -168,17 +341,50 @@ __device__ void plain_ml_column(const KArgs &a, int s, int i, int j, float (*S)[
     for (int r = 0; r < 2; ++r) {
         const int k = lane + 32 * r;
         if (k < c.K0 || k > c.VI) continue;
-        const Coef q = ml_level<COMP, false>(a, x, c, sc, k);
+        const Coef q = mom_level<MODEL, COMP, false>(a, x, c, sc, k);
         S[0][k] = q.A; S[1][k] = q.B; S[2][k] = q.C; S[3][k] = q.D; S[4][k] = q.phi;
     }
-    if (lane == 0) S[4][c.VI + 1] = __ldcg(F + x.at(0, c.VI + 1));
     __syncwarp();
     const int kkm = back_limit<COMP>(c);
-    if (lane == 0) thomas_relax(S, c.K0, c.KK, c.VI, kkm, a.relax);
+    if (lane == 0) {
+        PlainRows R{S, SD};
+        mom_sweep<MODEL, COMP>(R, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x.at(0, c.VI + 1)));
+    }
     __syncwarp();
     for (int r = 0; r < 2; ++r) {
         const int k = lane + 32 * r;
         if (k >= c.K0 && k <= c.VI && kkm < k) __stcg(F + x.at(0, k), S[4][k]);
+    }
+}
+
+__device__ void plain_tke_column(const KArgs &a, int s, int i, int j, float (*S)[KMAX_LEVELS]) {
+    const int lane = threadIdx.x & 31;
+    const ColCtx c = make_col(a, i, j);
+    if (!(c.fl & F_ADV) || !a.sit[s].active) return;
+    const SitCtx sc = make_sit(a, s);
+    const Acc<false> x = make_acc<false>(a, s, c.col);
+    for (int r = 0; r < 2; ++r) {
+        const int k = lane + 32 * r;
+        if (k < c.K0 || k > c.VI) continue;
+        const CoefKE q = tke_level<false>(a, x, c, sc, k);
+        S[0][k] = q.A; S[1][k] = q.B1; S[2][k] = q.C1; S[3][k] = q.D1; S[4][k] = q.k1;
+        S[5][k] = q.B2; S[6][k] = q.C2; S[7][k] = q.D2; S[8][k] = q.e1;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        PlainRows R{S, nullptr};
+        const ColKE ke = a.colke[c.col];
+        const float *vf[3] = {a.uk, a.vk, a.wk};
+        tke_sweep(R, a, c, ke, __ldcg(a.turb + x.at(0, c.VI + 1)), __ldcg(a.tdiss + x.at(0, c.VI + 1)),
+                  [&](int f, long long dc, int k) { return vf[f][x.at(dc, k)]; });
+    }
+    __syncwarp();
+    for (int r = 0; r < 2; ++r) {
+        const int k = lane + 32 * r;
+        if (k >= c.K0 && k <= c.VI && c.KK < k) {
+            __stcg(a.turb + x.at(0, k), S[4][k]);
+            __stcg(a.tdiss + x.at(0, k), S[8][k]);
+        }
     }
 }
 
@@ -248,37 +454,33 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure(KArgs a, SweepGeom g
     });
 }
 
-template <int COMP>
-__global__ void __launch_bounds__(GS_WARPS * 32) k_mom_ml(KArgs a, SweepGeom g) {
+template <int MODEL, int COMP>
+__global__ void __launch_bounds__(GS_WARPS * 32) k_mom(KArgs a, SweepGeom g) {
     __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
-    float (*S)[KMAX_LEVELS] = sm[threadIdx.x >> 5];
+    __shared__ double smd[(MODEL == 0 && COMP == COMP_W) ? GS_WARPS : 1][2][KMAX_LEVELS];
+    const int w = threadIdx.x >> 5;
+    float (*S)[KMAX_LEVELS] = sm[w];
+    double (*SD)[KMAX_LEVELS] = smd[(MODEL == 0 && COMP == COMP_W) ? w : 0];
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
-    gs_tasks<PH, COMP == COMP_V, false>(a, g, [&](int s, int i, int j, int, int, bool) {
-        plain_ml_column<COMP>(a, s, i, j, S);
+    constexpr bool REV = (MODEL == 1 && COMP == COMP_V);     // model-1 V sweeps with (-IS,-JS)
+    gs_tasks<PH, REV, false>(a, g, [&](int s, int i, int j, int, int, bool) {
+        plain_mom_column<MODEL, COMP>(a, s, i, j, S, SD);
+    });
+}
+
+__global__ void __launch_bounds__(GS_WARPS * 32) k_tke(KArgs a, SweepGeom g) {
+    __shared__ float sm[GS_WARPS][9][KMAX_LEVELS];
+    float (*S)[KMAX_LEVELS] = sm[threadIdx.x >> 5];
+    gs_tasks<PH_TKE, false, false>(a, g, [&](int s, int i, int j, int, int, bool) {
+        plain_tke_column(a, s, i, j, S);
     });
 }
 
 // ---------------------------- batched family -----------------------------------------------
 // One block per task = (group of 32 situations, column).  The block's warps split the levels for
 // the coefficient assembly (lane = situation, contiguous 128-byte loads in the interleaved layout)
-// and write A, B, C, D, phi rows [k][32] to shared memory; warp 0 then runs the 32 situations'
-// Thomas recurrences and back-substitutions side by side.
-
-// Shared rows of one task, [k][32] each, carved from dynamic shared memory sized by KS.
-struct BRows {
-    float *A, *B, *C, *D, *phi;
-    __device__ __forceinline__ float &a(int k, int l) { return A[k * 32 + l]; }
-    __device__ __forceinline__ float &b(int k, int l) { return B[k * 32 + l]; }
-    __device__ __forceinline__ float &c(int k, int l) { return C[k * 32 + l]; }
-    __device__ __forceinline__ float &d(int k, int l) { return D[k * 32 + l]; }
-    __device__ __forceinline__ float &p(int k, int l) { return phi[k * 32 + l]; }
-};
-
-__device__ __forceinline__ BRows carve_rows(float *smem, int ks) {
-    BRows R;
-    R.A = smem; R.B = R.A + ks * 32; R.C = R.B + ks * 32; R.D = R.C + ks * 32; R.phi = R.D + ks * 32;
-    return R;
-}
+// and write rows [k][32] to shared memory; warp 0 then runs the 32 situations' Thomas
+// recurrences and back-substitutions side by side.
 
 // Block-wide variant of gs_tasks: thread 0 claims and waits, the block works, thread 0 publishes.
 template <int PHASE, bool REVERSE, class Body>
@@ -325,57 +527,99 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
     }
 }
 
-template <int COMP, int NW>
-__device__ void batch_ml_column(const KArgs &a, int grp, int i, int j, BRows R) {
+// Rows [row][k][32] of one lane (= situation) in dynamic shared memory; the model-0 W rows P/Q
+// in double follow the float rows.
+struct BLane {
+    float *base;
+    double *dbase;
+    int ks, lane;
+    __device__ __forceinline__ float &row(int r, int k) { return base[((size_t)r * ks + k) * 32 + lane]; }
+    __device__ __forceinline__ float &a(int k) { return row(0, k); }
+    __device__ __forceinline__ float &b(int k) { return row(1, k); }
+    __device__ __forceinline__ float &c(int k) { return row(2, k); }
+    __device__ __forceinline__ float &d(int k) { return row(3, k); }
+    __device__ __forceinline__ float &p(int k) { return row(4, k); }
+    __device__ __forceinline__ double &pd(int k) { return dbase[((size_t)0 * ks + k) * 32 + lane]; }
+    __device__ __forceinline__ double &qd(int k) { return dbase[((size_t)1 * ks + k) * 32 + lane]; }
+    __device__ __forceinline__ float &b1(int k) { return row(1, k); }
+    __device__ __forceinline__ float &c1(int k) { return row(2, k); }
+    __device__ __forceinline__ float &d1(int k) { return row(3, k); }
+    __device__ __forceinline__ float &k1(int k) { return row(4, k); }
+    __device__ __forceinline__ float &b2(int k) { return row(5, k); }
+    __device__ __forceinline__ float &c2(int k) { return row(6, k); }
+    __device__ __forceinline__ float &d2(int k) { return row(7, k); }
+    __device__ __forceinline__ float &e1(int k) { return row(8, k); }
+};
+
+__device__ __forceinline__ BLane blane(float *smem, int ks) {
+    BLane R;
+    R.base = smem;
+    R.dbase = reinterpret_cast<double *>(smem + (size_t)9 * ks * 32);
+    R.ks = ks;
+    R.lane = threadIdx.x & 31;
+    return R;
+}
+
+template <int MODEL, int COMP, int NW>
+__device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *smem) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV)) return;
     const bool act = (s < a.nb) && a.sit[s].active;
+    BLane R = blane(smem, a.ks);
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     if (act) {
         const SitCtx sc = make_sit(a, s);
 #pragma unroll 2
         for (int k = c.K0 + warp; k <= c.VI; k += NW) {
-            const Coef q = ml_level<COMP, true>(a, x, c, sc, k);
-            R.a(k, lane) = q.A; R.b(k, lane) = q.B; R.c(k, lane) = q.C; R.d(k, lane) = q.D; R.p(k, lane) = q.phi;
+            const Coef q = mom_level<MODEL, COMP, true>(a, x, c, sc, k);
+            R.a(k) = q.A; R.b(k) = q.B; R.c(k) = q.C; R.d(k) = q.D; R.p(k) = q.phi;
         }
     }
     __syncthreads();
     if (warp != 0 || !act) return;
     float *F = comp_field<COMP>(a);
-    float P = 0.0f, Q = 0.0f;
-    for (int k = c.K0; k <= c.VI; ++k) {
-        const float A = R.a(k, lane), B = R.b(k, lane), C = R.c(k, lane), D = R.d(k, lane);
-        if (k > c.KK + 1) {
-            const float T = 1.0f / (A - C * P);
-            P = B * T;
-            Q = (D + C * Q) * T;
-        } else {
-            const float T = 1.0f / A;
-            P = B * T;
-            Q = D * T;
-        }
-        R.b(k, lane) = P;
-        R.d(k, lane) = Q;
-    }
     const int kkm = back_limit<COMP>(c);
-    const float relax = a.relax;
-    float up = __ldcg(F + x.at(0, c.VI + 1));
-    for (int k = c.VI; k >= c.K0; --k) {
-        float u = R.p(k, lane);
-        if (kkm < k) {
-            u += relax * (R.b(k, lane) * up + R.d(k, lane) - u);
-            __stcg(F + x.at(0, k), u);
+    mom_sweep<MODEL, COMP>(R, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x.at(0, c.VI + 1)));
+    for (int k = c.K0; k <= c.VI; ++k)
+        if (kkm < k) __stcg(F + x.at(0, k), R.p(k));
+}
+
+template <int NW>
+__device__ void batch_tke_column(const KArgs &a, int grp, int i, int j, float *smem) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int s = grp * 32 + lane;
+    const ColCtx c = make_col(a, i, j);
+    if (!(c.fl & F_ADV)) return;
+    const bool act = (s < a.nb) && a.sit[s].active;
+    BLane R = blane(smem, a.ks);
+    const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
+    if (act) {
+        const SitCtx sc = make_sit(a, s);
+        for (int k = c.K0 + warp; k <= c.VI; k += NW) {
+            const CoefKE q = tke_level<true>(a, x, c, sc, k);
+            R.a(k) = q.A; R.b1(k) = q.B1; R.c1(k) = q.C1; R.d1(k) = q.D1; R.k1(k) = q.k1;
+            R.b2(k) = q.B2; R.c2(k) = q.C2; R.d2(k) = q.D2; R.e1(k) = q.e1;
         }
-        up = u;
     }
+    __syncthreads();
+    if (warp != 0 || !act) return;
+    const ColKE ke = a.colke[c.col];
+    const float *vf[3] = {a.uk, a.vk, a.wk};
+    tke_sweep(R, a, c, ke, __ldcg(a.turb + x.at(0, c.VI + 1)), __ldcg(a.tdiss + x.at(0, c.VI + 1)),
+              [&](int f, long long dc, int k) { return vf[f][x.at(dc, k)]; });
+    for (int k = c.K0; k <= c.VI; ++k)
+        if (c.KK < k) {
+            __stcg(a.turb + x.at(0, k), R.k1(k));
+            __stcg(a.tdiss + x.at(0, k), R.e1(k));
+        }
 }
 
 // Row carry of the batched family: [group][j][2][KS][32].
 template <int NW>
-__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first, BRows R,
-                                      unsigned &nmax_acc) {
+__device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first,
+                                      float *smem, unsigned &nmax_acc) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const int ks = a.ks;
@@ -385,24 +629,27 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV)) return;
     const bool act = (s < a.nb) && a.sit[s].active;
+    BLane R = blane(smem, ks);
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     const SitCtx sc = make_sit(a, act ? s : grp * 32);
-    if (act)
-        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.d(k, lane) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+    if (act) {
+#pragma unroll 2
+        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.d(k) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+    }
     __syncthreads();
     if (warp == 0 && act) {
         float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
         for (int k = c.VI; k > c.KK; --k) {
             const float T = 1.0f / (a.app[k] - a.atp[k] * P);
             P = a.abp[k] * T;
-            Q = (a.atp[k] * Q + R.d(k, lane)) * T;
-            R.b(k, lane) = P;
-            R.c(k, lane) = Q;
+            Q = (a.atp[k] * Q + R.d(k)) * T;
+            R.b(k) = P;
+            R.c(k) = Q;
         }
         float prev = 0.0f;                                         // DPM[KKART] is always 0
         for (int k = c.KK + 1; k <= c.VI; ++k) {
-            prev = R.b(k, lane) * prev + R.c(k, lane);
-            R.p(k, lane) = prev;
+            prev = R.b(k) * prev + R.c(k);
+            R.p(k) = prev;
         }
     }
     __syncthreads();
@@ -410,13 +657,13 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
     const int klo = max(c.KK, a.vi_min);
     unsigned nmax = 0;
     for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) {
-        const float temp = R.p(k, lane);
+        const float temp = R.p(k);
         nmax = max(nmax, residual_key(temp, sc));
         __stcg(a.dpm + x.at(0, k), temp);
         a.dpmnew[x.at(0, k)] += a.relaxp * temp;
         if (k > klo) {
-            __stcg(rc + (size_t)k * 32, R.b(k, lane));
-            __stcg(rc + (size_t)(ks + k) * 32, R.c(k, lane));
+            __stcg(rc + (size_t)k * 32, R.b(k));
+            __stcg(rc + (size_t)(ks + k) * 32, R.c(k));
         }
     }
     nmax_acc = max(nmax_acc, nmax);
@@ -425,7 +672,6 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
 template <int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) k_pressure_b(KArgs a, SweepGeom g) {
     extern __shared__ float smem[];
-    BRows R = carve_rows(smem, a.ks);
     __shared__ unsigned red[NW][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned nmax = 0;
@@ -445,74 +691,80 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_pressure_b(KArgs a, SweepGeom
     };
     gs_tasks_block<PH_PRESSURE, false>(a, g, [&](int grp, int i, int j, int IS, int JS, bool first) {
         if (grp != cur) { flush(); cur = grp; }
-        batch_pressure_column<NW>(a, grp, i, j, IS, JS, first, R, nmax);
+        batch_pressure_column<NW>(a, grp, i, j, IS, JS, first, smem, nmax);
     });
     flush();
 }
 
-template <int COMP, int NW, int MINB>
-__global__ void __launch_bounds__(NW * 32, MINB) k_mom_ml_b(KArgs a, SweepGeom g) {
+template <int MODEL, int COMP, int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_mom_b(KArgs a, SweepGeom g) {
     extern __shared__ float smem[];
-    BRows R = carve_rows(smem, a.ks);
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
-    gs_tasks_block<PH, COMP == COMP_V>(a, g, [&](int grp, int i, int j, int, int, bool) {
-        batch_ml_column<COMP, NW>(a, grp, i, j, R);
+    constexpr bool REV = (MODEL == 1 && COMP == COMP_V);
+    gs_tasks_block<PH, REV>(a, g, [&](int grp, int i, int j, int, int, bool) {
+        batch_mom_column<MODEL, COMP, NW>(a, grp, i, j, smem);
     });
 }
 
+template <int NW, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB) k_tke_b(KArgs a, SweepGeom g) {
+    extern __shared__ float smem[];
+    gs_tasks_block<PH_TKE, false>(a, g, [&](int grp, int i, int j, int, int, bool) {
+        batch_tke_column<NW>(a, grp, i, j, smem);
+    });
+}
+
+using KFn = void (*)(KArgs, SweepGeom);
+
 // Launch variants of the batched family: (warps per block, minimum resident blocks per SM).
-// The host times them once per context and keeps the fastest (GRAL_PROG_BATCH_VARIANT forces one).
 struct BVariant {
     int nw, minb;
-    void (*pressure)(KArgs, SweepGeom);
-    void (*mom[3])(KArgs, SweepGeom);
+    KFn pressure;
+    KFn mom[3][3];   // [model][comp]
+    KFn tke;
 };
 
-#define GRAL_BV(NW, MB)                                                                          \
-    BVariant{NW, MB, k_pressure_b<NW, MB>,                                                       \
-             {k_mom_ml_b<COMP_U, NW, MB>, k_mom_ml_b<COMP_V, NW, MB>, k_mom_ml_b<COMP_W, NW, MB>}}
+#define GRAL_BV(NW, MB)                                                                              \
+    BVariant{NW, MB, k_pressure_b<NW, MB>,                                                           \
+             {{k_mom_b<0, COMP_U, NW, MB>, k_mom_b<0, COMP_V, NW, MB>, k_mom_b<0, COMP_W, NW, MB>},  \
+              {k_mom_b<1, COMP_U, NW, MB>, k_mom_b<1, COMP_V, NW, MB>, k_mom_b<1, COMP_W, NW, MB>},  \
+              {k_mom_b<2, COMP_U, NW, MB>, k_mom_b<2, COMP_V, NW, MB>, k_mom_b<2, COMP_W, NW, MB>}}, \
+             k_tke_b<NW, MB>}
 
 const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
-}  // namespace
+const KFn kPlainMom[3][3] = {{k_mom<0, COMP_U>, k_mom<0, COMP_V>, k_mom<0, COMP_W>},
+                             {k_mom<1, COMP_U>, k_mom<1, COMP_V>, k_mom<1, COMP_W>},
+                             {k_mom<2, COMP_U>, k_mom<2, COMP_V>, k_mom<2, COMP_W>}};
 
-int gs_num_variants() { return kNumVariants; }
-
-int gs_block_threads(bool il, int variant) { return il ? kVariants[variant].nw * 32 : GS_WARPS * 32; }
-
-size_t gs_smem_bytes(bool il, int ks, int variant) {
-    (void)variant;
-    return il ? (size_t)5 * ks * 32 * sizeof(float) : 0;
+// Dynamic shared memory of a batched kernel: 5 float rows (momentum, pressure), 9 float rows
+// (TKE), 9 float rows + 2 double rows (model-0 W, whose P/Q are double).
+size_t bsmem(int kind, int model, int ks) {
+    const size_t row = (size_t)ks * 32 * sizeof(float);
+    if (kind == PH_TKE) return 9 * row;
+    if (kind == PH_W && model == 0) return 9 * row + 4 * row;
+    return 5 * row;
 }
 
-cudaError_t gs_prepare(bool il, int ks) {
-    if (!il) return cudaSuccess;
-    const int bytes = (int)gs_smem_bytes(true, ks, 0);
-    for (int v = 0; v < kNumVariants; ++v) {
-        const BVariant &V = kVariants[v];
-        cudaError_t e = cudaFuncSetAttribute(V.pressure, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        for (int q = 0; q < 3 && e == cudaSuccess; ++q)
-            e = cudaFuncSetAttribute(V.mom[q], cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return e;
+KFn batch_kernel(const BVariant &V, int kind, int model) {
+    switch (kind) {
+        case PH_PRESSURE: return V.pressure;
+        case PH_U: return V.mom[model][0];
+        case PH_V: return V.mom[model][1];
+        case PH_W: return V.mom[model][2];
+        default: return V.tke;
     }
-    return cudaSuccess;
 }
 
-cudaError_t gs_occupancy(bool il, int kind, int ks, int variant, int *blocks_per_sm) {
-    const int th = gs_block_threads(il, variant);
-    if (!il) {
-        switch (kind) {
-            case PH_PRESSURE: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_pressure, th, 0);
-            case PH_U: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml<COMP_U>, th, 0);
-            case PH_V: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml<COMP_V>, th, 0);
-            default: return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_mom_ml<COMP_W>, th, 0);
-        }
+KFn plain_kernel(int kind, int model) {
+    switch (kind) {
+        case PH_PRESSURE: return k_pressure;
+        case PH_U: return kPlainMom[model][0];
+        case PH_V: return kPlainMom[model][1];
+        case PH_W: return kPlainMom[model][2];
+        default: return k_tke;
     }
-    const BVariant &V = kVariants[variant];
-    const size_t sm = gs_smem_bytes(true, ks, variant);
-    void (*f)(KArgs, SweepGeom) = (kind == PH_PRESSURE) ? V.pressure : V.mom[kind == PH_U ? 0 : (kind == PH_V ? 1 : 2)];
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, th, sm);
 }
 
 // Group sets of the batched family: a launch sweeps group_set groups at a time (0 = all groups),
@@ -530,27 +782,40 @@ void for_group_sets(const KArgs &a, F &&f) {
     }
 }
 
-void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
-    if (a.il) {
-        const BVariant &V = kVariants[a.variant];
-        for_group_sets(a, [&](const KArgs &b) {
-            V.pressure<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(b, g);
-        });
-    } else {
-        k_pressure<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
-    }
+}  // namespace
+
+int gs_num_variants() { return kNumVariants; }
+
+int gs_block_threads(bool il, int variant) { return il ? kVariants[variant].nw * 32 : GS_WARPS * 32; }
+
+cudaError_t gs_prepare(bool il, int ks, int model) {
+    if (!il) return cudaSuccess;
+    const int kinds[5] = {PH_PRESSURE, PH_U, PH_V, PH_W, PH_TKE};
+    for (int v = 0; v < kNumVariants; ++v)
+        for (int q = 0; q < 5; ++q) {
+            const int bytes = (int)bsmem(kinds[q], model, ks);
+            cudaError_t e = cudaFuncSetAttribute(batch_kernel(kVariants[v], kinds[q], model),
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+            if (e != cudaSuccess) return e;
+        }
+    return cudaSuccess;
 }
 
-void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
+cudaError_t gs_occupancy(bool il, int kind, int model, int ks, int variant, int *blocks_per_sm) {
+    const int th = gs_block_threads(il, variant);
+    if (!il) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, plain_kernel(kind, model), th, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, batch_kernel(kVariants[variant], kind, model),
+                                                         th, bsmem(kind, model, ks));
+}
+
+void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
         const BVariant &V = kVariants[a.variant];
-        for_group_sets(a, [&](const KArgs &b) {
-            V.mom[comp]<<<grid, V.nw * 32, gs_smem_bytes(true, a.ks, a.variant), st>>>(b, g);
-        });
+        KFn f = batch_kernel(V, kind, a.model);
+        const size_t sm = bsmem(kind, a.model, a.ks);
+        for_group_sets(a, [&](const KArgs &b) { f<<<grid, V.nw * 32, sm, st>>>(b, g); });
     } else {
-        if (comp == 0) k_mom_ml<COMP_U><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
-        else if (comp == 1) k_mom_ml<COMP_V><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
-        else k_mom_ml<COMP_W><<<grid, GS_WARPS * 32, 0, st>>>(a, g);
+        plain_kernel(kind, a.model)<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
     }
 }
 

@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -77,7 +79,7 @@ struct gral_ctx {
     Staging sg{};
     BcLists bc{};
     Geom geo_p, geo_u, geo_v;
-    int grid_gs[4] = {0, 0, 0, 0};
+    int grid_gs[6] = {0, 0, 0, 0, 0, 0};   // indexed by PH_* (1..5)
     cudaGraphExec_t graph = nullptr;
     float ms_upload = 0.f;
     float tune_ms[16] = {0};
@@ -87,6 +89,8 @@ struct gral_ctx {
     DevBuf<ColMeta> meta;
     DevBuf<uint32_t> cflags;
     DevBuf<ColF> colf;
+    DevBuf<ColKE> colke;
+    DevBuf<float> varw, z0i;
     DevBuf<SitDev> sit;
     DevBuf<int> flags, misc, diag, bcl, counts;
     DevBuf<unsigned int> counters;
@@ -97,7 +101,8 @@ struct gral_ctx {
         if (graph) cudaGraphExecDestroy(graph);
         DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
         for (auto *b : fb) b->release();
-        meta.release(); cflags.release(); colf.release(); sit.release();
+        meta.release(); cflags.release(); colf.release(); sit.release(); colke.release();
+        varw.release(); z0i.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
@@ -155,12 +160,14 @@ void chunk_levels(int K0, int KEND, int KK, int W, int &kad, int &wlo, int &whi)
 }
 
 int build_meta(gral_ctx *ctx, const gral_params &p, const gral_static &s, std::vector<ColMeta> &meta,
-               std::vector<uint32_t> &cfl, std::vector<ColF> &colf, int &vi_min, int &vi_max) {
+               std::vector<uint32_t> &cfl, std::vector<ColF> &colf, std::vector<ColKE> &colke, int &vi_min,
+               int &vi_max) {
     const int NII = p.nii, NJJ = p.njj, NKK = p.nkk, nj2 = NJJ + 2;
     const int ncols = (NII + 2) * nj2;
     meta.assign(ncols, ColMeta{});
     cfl.assign(ncols, 0u);
     colf.assign(ncols, ColF{});
+    colke.assign(ncols, ColKE{0.0, -1, -1, -1, -1});
     auto adv = [&](int i, int j) { return (i >= 0 && i <= NII + 1 && j >= 0 && j <= NJJ + 1) ? s.advdom[i * nj2 + j] : 0; };
     auto kk = [&](int i, int j) { return (int)s.kkart[i * nj2 + j]; };
     const float *DZK = s.dzk;
@@ -222,6 +229,21 @@ int build_meta(gral_ctx *ctx, const gral_params &p, const gral_static &s, std::v
                     }
                 }
             }
+            // k-eps wall functions of the TKE back-substitution (TKE-prognostic-microscale.cs:278-338)
+            if (p.turbulence_model == 2 && inner) {
+                ColKE &ke = colke[c];
+                const int k = KK + 1;
+                if (k + 1 <= NKK + 1) {
+                    if ((double)z0 >= (double)DZK[k] * 0.5) {
+                        f |= F_GMODE1;
+                        ke.gfac = 0.4 / std::log(((double)DZK[k] + (double)DZK[k + 1] * 0.5) / (double)z0);
+                    } else {
+                        ke.gfac = 0.4 / std::log((double)DZK[k] * 0.5 / (double)z0);
+                    }
+                }
+                auto kwn = [&](int ii, int jj) { return s.cutk[ii * nj2 + jj] > 0 ? (int16_t)(kk(ii, jj) + 1) : (int16_t)-1; };
+                ke.kw_e = kwn(i + 1, j); ke.kw_w = kwn(i - 1, j); ke.kw_n = kwn(i, j + 1); ke.kw_s = kwn(i, j - 1);
+            }
             cfl[c] = f;
             vi_max = std::max(vi_max, VI);
             if ((f & F_ADV) && i >= 2 && i <= NII - 1 && j >= 2 && j <= NJJ - 1) {
@@ -261,8 +283,9 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
     if (p0.nii > 0xffff || p0.njj > 0xffff) return fail(ctx, GRAL_EINVAL, "grid dimension above 65535");
     if (p0.kadvmax < 2 || p0.kadvmax + 2 > KMAX_LEVELS || p0.kadvmax > p0.nkk)
         return fail(ctx, GRAL_EINVAL, "KADVMAX outside 2..62 or above NKK");
-    if (p0.turbulence_model != 1) return fail(ctx, GRAL_EINVAL, "only turbulence_model 1 is built on the GPU yet");
-    if (p0.simd_width != 8) return fail(ctx, GRAL_EINVAL, "simd_width must be 8 (Vector<float> path)");
+    if (p0.turbulence_model < 0 || p0.turbulence_model > 2) return fail(ctx, GRAL_EINVAL, "turbulence_model must be 0, 1 or 2");
+    if (p0.turbulence_model == 1 && p0.simd_width != 8)
+        return fail(ctx, GRAL_EINVAL, "simd_width must be 8 (Vector<float> path)");
     for (int b = 0; b < n; ++b) {
         const gral_params &q = p[b];
         if (q.nii != p0.nii || q.njj != p0.njj || q.nkk != p0.nkk || q.kadvmax != p0.kadvmax ||
@@ -276,6 +299,10 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
         if (q.ref_i < 1 || q.ref_i > q.nii || q.ref_j < 1 || q.ref_j > q.njj)
             return fail(ctx, GRAL_EINVAL, "reference point outside the grid");
         if (!f[b].uk || !f[b].vk || !f[b].wk) return fail(ctx, GRAL_EINVAL, "null field");
+        if (q.turbulence_model != 1 && (!f[b].turb || !f[b].tdiss))
+            return fail(ctx, GRAL_EINVAL, "TURB/TDISS fields are required for turbulence_model 0 and 2");
+        if (q.turbulence_model != 1 && q.turb_init == 0 && (!s->z0_init || !s->ob_init || !s->ust_init))
+            return fail(ctx, GRAL_EINVAL, "z0_init/ob_init/ust_init are required to initialise TURB");
     }
     return GRAL_OK;
 }
@@ -285,19 +312,20 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
     cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
-    launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
+    launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
     launch_velcorr(a, st);
     launch_average(a, st);
-    launch_mom_ml(0, a, ctx->geo_u.g, ctx->grid_gs[1], st);
-    launch_mom_ml(1, a, ctx->geo_v.g, ctx->grid_gs[2], st);
-    launch_mom_ml(2, a, ctx->geo_p.g, ctx->grid_gs[3], st);
+    launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
+    launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
+    launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
+    if (ctx->model == 2) launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st);
     launch_bookkeeping(a, st);
 }
 
 // Grid sizes of the wavefront kernels for the current family and variant: every resident block
 // slot of the GPU (the kernels are persistent and claim tasks).
 int size_grids(gral_ctx *ctx) {
-    const int kinds[4] = {PH_PRESSURE, PH_U, PH_V, PH_W};
+    const int kinds[5] = {PH_PRESSURE, PH_U, PH_V, PH_W, PH_TKE};
     const bool il = ctx->il;
     const int nkv = gs_num_variants();
     const int vv = il ? std::max(ctx->variant, 0) : 0;
@@ -309,12 +337,12 @@ int size_grids(gral_ctx *ctx) {
     ctx->ka.ctr_slot = 0;
     if (il && (ctx->ngroups + std::max(ctx->ka.group_set, 1) - 1) / std::max(ctx->ka.group_set, 1) > kCounterSlots)
         ctx->ka.group_set = 0;
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 5; ++q) {
         int bps = 0;
-        CK(gs_occupancy(il, kinds[q], ctx->ks, v, &bps));
-        ctx->grid_gs[q] = std::max(1, bps) * ctx->num_sms;
+        CK(gs_occupancy(il, kinds[q], ctx->model, ctx->ks, v, &bps));
+        ctx->grid_gs[kinds[q]] = std::max(1, bps) * ctx->num_sms;
     }
-    const int warps = ctx->grid_gs[0] * gs_block_threads(il, v) / 32;
+    const int warps = ctx->grid_gs[PH_PRESSURE] * gs_block_threads(il, v) / 32;
     const long long per_diag = (long long)(il ? ctx->ngroups : ctx->nb) * std::min(ctx->nii, ctx->njj);
     ctx->ka.chunk = il ? 1 : (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
     ctx->ka.variant = v;
@@ -434,8 +462,9 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     std::vector<ColMeta> meta;
     std::vector<uint32_t> cfl;
     std::vector<ColF> colf;
+    std::vector<ColKE> colke;
     int vi_min = 0, vi_max = 0;
-    rc = build_meta(ctx, p0, *s, meta, cfl, colf, vi_min, vi_max);
+    rc = build_meta(ctx, p0, *s, meta, cfl, colf, colke, vi_min, vi_max);
     if (rc != GRAL_OK) return rc;
     if (vi_max + 1 >= ks) return fail(ctx, GRAL_EINVAL, "VerticalIndex above KADVMAX");
 
@@ -482,6 +511,42 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         S.it_max = q.iteration_steps_max;
         S.cadence = q.conv_cadence;
         S.quantise = q.quantise;
+        S.potdtdz = q.potdtdz;
+        S.std_dev_v = q.std_dev_v;
+        S.v0_1 = q.v0_1;
+        S.turb_init = q.turb_init;
+    }
+    // vertical-variance term of the TURB initialisation per situation and column
+    // (PrognosticFlowfield.cs:488-495), float arithmetic with libm powf as the reference
+    std::vector<float> varw;
+    if (ctx->model != 1) {
+        varw.assign((size_t)n * ncols, 0.0f);
+        for (int b = 0; b < n; ++b) {
+            const gral_params &q = p[b];
+            if (q.turb_init) continue;
+            std::map<std::pair<float, float>, float> memo;
+            for (int i = 1; i <= NII; ++i)
+                for (int j = 1; j <= NJJ; ++j) {
+                    const int c = i * nj2 + j;
+                    const float ObLength = s->ob_init[c], ust = s->ust_init[c];
+                    auto key = std::make_pair(ObLength, ust);
+                    auto it = memo.find(key);
+                    float vw;
+                    if (it != memo.end()) {
+                        vw = it->second;
+                    } else {
+                        if (ObLength < 0) {
+                            const float t = 1.15f + 0.1f * powf(q.bd_lay_height / (-ObLength), 0.67f);
+                            vw = (ust * ust) * (t * t) * (q.std_dev_w * q.std_dev_w);
+                        } else {
+                            const float t = ust * q.std_dev_w * 1.25f;
+                            vw = t * t;
+                        }
+                        memo.emplace(key, vw);
+                    }
+                    varw[(size_t)b * ncols + c] = vw;
+                }
+        }
     }
 
     // ---- boundary-condition event lists ----
@@ -525,6 +590,11 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(ctx->meta.ensure(ncols));
     CK(ctx->cflags.ensure(ncols));
     CK(ctx->colf.ensure(ncols));
+    if (ctx->model != 1) {
+        CK(ctx->colke.ensure(ncols));
+        CK(ctx->varw.ensure((size_t)n * ncols));
+        CK(ctx->z0i.ensure(ncols));
+    }
     CK(ctx->tables.ensure(5 * ks));
     CK(ctx->ap0.ensure((size_t)n * ks));
     CK(ctx->sit.ensure(n));
@@ -553,6 +623,10 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     a.relax = p0.relax; a.relaxp = p0.relaxp; a.coriolis = p0.coriolis;
     a.vishmin = (p0.turbulence_model == 2) ? 0.01f : 0.0f;
     a.simd = p0.simd_width;
+    a.model = p0.turbulence_model;
+    a.colke = (ctx->model == 2) ? ctx->colke.p : nullptr;
+    a.building_z0 = p0.building_z0;
+    a.ustern_fx = (float)(0.4 / std::log((double)DXK * 0.5 / (double)p0.building_z0));   // :515
     a.meta = ctx->meta.p; a.cflags = ctx->cflags.p; a.colf = ctx->colf.p;
     a.dzk = ctx->tables.p; a.hokart = ctx->tables.p + ks;
     a.app = ctx->tables.p + 2 * ks; a.abp = ctx->tables.p + 3 * ks; a.atp = ctx->tables.p + 4 * ks;
@@ -608,6 +682,12 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemcpyAsync(ctx->meta.p, meta.data(), ncols * sizeof(ColMeta), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->cflags.p, cfl.data(), ncols * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->colf.p, colf.data(), ncols * sizeof(ColF), cudaMemcpyHostToDevice, st));
+    if (ctx->model != 1) {
+        CK(cudaMemcpyAsync(ctx->colke.p, colke.data(), ncols * sizeof(ColKE), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->varw.p, varw.data(), varw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (s->z0_init) CK(cudaMemcpyAsync(ctx->z0i.p, s->z0_init, ncols * sizeof(float), cudaMemcpyHostToDevice, st));
+        else CK(cudaMemsetAsync(ctx->z0i.p, 0, ncols * sizeof(float), st));
+    }
     CK(cudaMemcpyAsync(ctx->tables.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->ap0.p, ap0.data(), ap0.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->sit.p, ctx->h_sit.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
@@ -633,13 +713,17 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         CK(cudaMemcpyAsync(sg.uk + ssz * b, f[b].uk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(sg.vk + ssz * b, f[b].vk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(sg.wk + ssz * b, f[b].wk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (ctx->model != 1) {
+            CK(cudaMemcpyAsync(sg.turb + ssz * b, f[b].turb, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(sg.tdiss + ssz * b, f[b].tdiss, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        }
     }
-    launch_setup(a, sg, ctx->model, st);
+    launch_setup(a, sg, ctx->model, ctx->model != 1 ? ctx->varw.p : nullptr, ctx->model != 1 ? ctx->z0i.p : nullptr, st);
     launch_gather(a, sg, ctx->model, st);
     CK(cudaGetLastError());
 
     // ---- launch shapes of the wavefront kernels ----
-    CK(gs_prepare(il, ks));
+    CK(gs_prepare(il, ks, ctx->model));
     ctx->it_host = 1;
     ctx->variant = -1;
     int brc = size_grids(ctx);
@@ -709,18 +793,19 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
         CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st));
         launch_bc(a, ctx->bc, st);
         CK(cudaEventRecord(E[GRAL_PHASE_PRESSURE], st));
-        launch_pressure(a, ctx->geo_p.g, ctx->grid_gs[0], st);
+        launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
         CK(cudaEventRecord(E[GRAL_PHASE_VELCORR], st));
         launch_velcorr(a, st);
         CK(cudaEventRecord(E[GRAL_PHASE_AVERAGE], st));
         launch_average(a, st);
         CK(cudaEventRecord(E[GRAL_PHASE_U], st));
-        launch_mom_ml(0, a, ctx->geo_u.g, ctx->grid_gs[1], st);
+        launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
         CK(cudaEventRecord(E[GRAL_PHASE_V], st));
-        launch_mom_ml(1, a, ctx->geo_v.g, ctx->grid_gs[2], st);
+        launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
         CK(cudaEventRecord(E[GRAL_PHASE_W], st));
-        launch_mom_ml(2, a, ctx->geo_p.g, ctx->grid_gs[3], st);
+        launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
         CK(cudaEventRecord(E[GRAL_PHASE_TKE], st));
+        if (ctx->model == 2) launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st);
         CK(cudaEventRecord(E[GRAL_PHASE_BOOKKEEPING], st));
         launch_bookkeeping(a, st);
         CK(cudaEventRecord(E[GRAL_NUM_PHASES], st));
@@ -776,6 +861,10 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
         CK(cudaMemcpyAsync(f[b].uk, ctx->sg.uk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(f[b].vk, ctx->sg.vk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(f[b].wk, ctx->sg.wk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+        if (ctx->model != 1) {
+            CK(cudaMemcpyAsync(f[b].turb, ctx->sg.turb + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(f[b].tdiss, ctx->sg.tdiss + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+        }
     }
     std::vector<int> counts(4 * n);
     CK(cudaMemcpyAsync(counts.data(), ctx->counts.p, 4 * n * sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -285,6 +285,37 @@ __global__ void k_setup_border(KArgs a, Staging sg) {
     }
 }
 
+// k and eps initialisation on every level (:211-227, 410-510): TURB = 0.001, TDISS = 1e-7 on
+// levels 1..NKK+1, then TURB from the velocity and the variances on levels 1..NKK-1.
+__global__ void k_setup_turb(KArgs a, Staging sg, const float *varw, const float *z0_init) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nk2 = a.nkk + 2;
+    const long long per = (long long)a.nii * a.njj * nk2;
+    const long long s = t / per;
+    if (s >= a.nb) return;
+    const SitDev &S = a.sit[s];
+    if (S.turb_init) return;
+    long long r = t - s * per;
+    const int k = (int)(r % nk2);
+    r /= nk2;
+    const int j = 1 + (int)(r % a.njj);
+    const int i = 1 + (int)(r / a.njj);
+    if (k < 1) return;
+    const size_t o = sg.stride * s + sidx3(a, i, j, k);
+    float tk = 0.001f;
+    sg.tdiss[o] = 0.0000001f;
+    if (k <= a.nkk - 1) {
+        const float u = sg.uk[o], v = sg.vk[o];
+        const double wh = net_maxd(sqrt((double)(u * u + v * v)), 0.01);
+        const int col = i * a.nj2 + j;
+        float U0int = (float)(wh * (0.2 * pow(wh, -0.9) + 0.32 * (double)z0_init[col] + 0.18));
+        U0int = (float)net_maxd((double)U0int, 0.3) * S.std_dev_v;
+        const float V0int = S.v0_1;
+        tk = (float)(0.5 * (double)(U0int * U0int + V0int * V0int + varw[(size_t)s * a.ncols + col]));
+    }
+    sg.turb[o] = tk;
+}
+
 // velocities (and k, eps) inside buildings set to zero (:518-575)
 template <bool IL>
 __global__ void k_setup_zero(KArgs a, Staging sg, int model) {
@@ -380,8 +411,13 @@ void launch_bookkeeping(const KArgs &a, cudaStream_t st) {
     k_bookkeeping<<<(a.nb + 127) / 128, 128, 0, st>>>(a);
 }
 
-void launch_setup(const KArgs &a, const Staging &sg, int model, cudaStream_t st) {
+void launch_setup(const KArgs &a, const Staging &sg, int model, const float *varw, const float *z0_init,
+                  cudaStream_t st) {
     GRAL_COL_LAUNCH(k_setup_uks, a, sg);
+    if (model != 1) {
+        const long long n = (long long)a.nb * a.nii * a.njj * (a.nkk + 2);
+        k_setup_turb<<<(int)((n + 255) / 256), 256, 0, st>>>(a, sg, varw, z0_init);
+    }
     const long long nb = (long long)a.nb * (a.njj + a.nii) * (a.nkk - 1);
     k_setup_border<<<(int)((nb + 255) / 256), 256, 0, st>>>(a, sg);
     GRAL_COL_LAUNCH(k_setup_zero, a, sg, model);

@@ -24,19 +24,20 @@ struct Staging {
 
 int gs_num_variants();
 int gs_block_threads(bool il, int variant);
-size_t gs_smem_bytes(bool il, int ks, int variant);
-cudaError_t gs_prepare(bool il, int ks);
-cudaError_t gs_occupancy(bool il, int kind, int ks, int variant, int *blocks_per_sm);
-void launch_pressure(const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
-void launch_mom_ml(int comp, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
+cudaError_t gs_prepare(bool il, int ks, int model);
+cudaError_t gs_occupancy(bool il, int kind, int model, int ks, int variant, int *blocks_per_sm);
+// one Gauss-Seidel phase (kind = PH_PRESSURE, PH_U, PH_V, PH_W or PH_TKE) of the loaded model
+void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
 
 void launch_bc(const KArgs &a, const BcLists &bc, cudaStream_t st);
 void launch_velcorr(const KArgs &a, cudaStream_t st);
 void launch_average(const KArgs &a, cudaStream_t st);
 void launch_bookkeeping(const KArgs &a, cudaStream_t st);
 
-// set-up and tear-down of a batch (PrognosticFlowfield.cs:295-329, 410-579)
-void launch_setup(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
+// set-up and tear-down of a batch (PrognosticFlowfield.cs:295-329, 410-579); varw = per
+// (situation, column) vertical-variance term of the TURB initialisation (model != 1), or null
+void launch_setup(const KArgs &a, const Staging &sg, int model, const float *varw, const float *z0_init,
+                  cudaStream_t st);
 void launch_gather(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
 void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
 // post-checks (PrognosticFlowfield.cs:1193-1243); counts[s*4 + 0..3] = UK, VK, WK, non-finite

@@ -61,7 +61,7 @@ __device__ __forceinline__ ColCtx make_col(const KArgs &a, int i, int j) {
 }
 
 struct SitCtx {
-    float ug, vg, dtime;
+    float ug, vg, dtime, potdtdz;
     double frund;
     int quant;
     const float *ap0;
@@ -70,7 +70,7 @@ struct SitCtx {
 __device__ __forceinline__ SitCtx make_sit(const KArgs &a, int s) {
     SitCtx q;
     const SitDev &S = a.sit[s];
-    q.ug = S.ug; q.vg = S.vg; q.dtime = S.dtime; q.frund = S.frund; q.quant = S.quantise;
+    q.ug = S.ug; q.vg = S.vg; q.dtime = S.dtime; q.potdtdz = S.potdtdz; q.frund = S.frund; q.quant = S.quantise;
     q.ap0 = a.ap0 + (size_t)s * a.ks;
     return q;
 }
@@ -393,6 +393,328 @@ __device__ __forceinline__ float pressure_dim(const KArgs &a, const Acc<IL> &x, 
     const float si = (IS == 1) ? (pi + 0.0f) : (0.0f + pi);    // DPMim + DPMip
     const float sj = (JS == 1) ? (pj - 0.0f) : (0.0f - pj);    // DPMjm - DPMjp
     return DIV / sc.dtime + si / DXK * DYK * dz + sj / DYK * DXK * dz;
+}
+
+}  // namespace gral
+
+namespace gral {
+
+// =============================================================================================
+// k-eps model (TurbulenceModel 2) and no-diffusion model (TurbulenceModel 0): scalar routines of
+// the reference, evaluated per level.  Their power law and source sums are partly in double
+// (U-prognostic-microscale_2.cs:180-203), their recurrences divide twice per level (:247-256).
+// =============================================================================================
+
+// FloatMax(0, (float)Pow5(1 - 0.1*Pe)) * D + FloatMax(F, 0)  (U-prognostic-microscale_2.cs:180-185)
+__device__ __forceinline__ float pl_ke(float D, float Pe, float Fs) {
+    const double x = 1 - 0.1 * (double)Pe;
+    return D * vmaxf(0.0f, (float)(x * x * x * x * x)) + vmaxf(Fs, 0.0f);
+}
+
+// (float)Math.Sqrt(Pow2(0.5*(a1+a2)) + Pow2(0.5*(b1+b2))) with float sums (:207-219)
+__device__ __forceinline__ float wind_half(float a1, float a2, float b1, float b2) {
+    const double x = 0.5 * (double)(a1 + a2), y = 0.5 * (double)(b1 + b2);
+    return (float)sqrt(x * x + y * y);
+}
+
+// U (COMP 0) or V (COMP 1) of models 2 (DIFF) and 0 (no DIFF), one level
+// (U-prognostic-microscale_2.cs:103-257, V-...2.cs, U-...0.cs:103-182, V-...0.cs).
+template <bool DIFF, int COMP, bool IL>
+__device__ __forceinline__ Coef uv_scalar_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
+                                                int k) {
+    const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
+    const float dz = a.dzk[k];
+    const float dxdz = DXK * dz, dydz = DYK * dz;
+    float *PHI = (COMP == 0) ? a.uk : a.vk;
+    const float phi = __ldcg(PHI + x.at(0, k));
+    float VIS = 0.0f, DE = 0.0f, DW = 0.0f, DS = 0.0f, DN = 0.0f, DT = 0.0f, DB = 0.0f;
+    if (DIFF) {
+        const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
+        VIS = (float)sqrt((double)a.turb[x.at(0, k)]) * zs * 0.09f;
+        const float vmx = vmaxf(VIS, a.vishmin);
+        DE = vmx * dydz / DXK; DW = DE;
+        DS = vmx * dxdz / DYK; DN = DS;
+        DT = vmx * AREA / dz;
+        DB = (k > c.KK + 1) ? DT : 0.0f;
+        if (c.fl & F_BS) DS = 0.0f;
+        if (c.fl & F_BN) DN = 0.0f;
+        if (c.fl & F_BW) DW = 0.0f;
+        if (c.fl & F_BE) DE = 0.0f;
+    }
+    const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
+    const float uksW = a.uks[x.at(W, k)], vksW = a.vks[x.at(W, k)];
+    float FE, FW, FS, FN, FT, FB = 0.0f;
+    if (COMP == 0) {
+        const float vksWS = a.vks[x.at(W + S, k)], vksS = a.vks[x.at(S, k)];
+        const float vksWN = a.vks[x.at(W + N, k)], vksN = a.vks[x.at(N, k)];
+        const float wksW = a.wks[x.at(W, k)];
+        FE = uks * dydz;
+        FW = uksW * dydz;
+        FS = 0.25f * (vksW + vks + vksWS + vksS) * dxdz;
+        FN = 0.25f * (vksW + vks + vksWN + vksN) * dxdz;
+        FT = 0.25f * (wksW + wks + a.wks[x.at(W, k + 1)] + a.wks[x.at(0, k + 1)]) * AREA;
+        if (k > c.KK + 1) FB = 0.25f * (wksW + wks + a.wks[x.at(W, k - 1)] + a.wks[x.at(0, k - 1)]) * AREA;
+    } else {
+        const float uksE = a.uks[x.at(E, k)], uksS = a.uks[x.at(S, k)];
+        const float uksES = a.uks[x.at(E + S, k)], uksWS = a.uks[x.at(W + S, k)];
+        const float wksS = a.wks[x.at(S, k)];
+        FE = 0.25f * (uks + uksE + uksS + uksES) * dydz;
+        FW = 0.25f * (uks + uksW + uksS + uksWS) * dydz;
+        FS = a.vks[x.at(S, k)] * dxdz;
+        FN = vks * dxdz;
+        FT = 0.25f * (wksS + wks + a.wks[x.at(S, k + 1)] + a.wks[x.at(0, k + 1)]) * AREA;
+        if (k > c.KK + 1) FB = 0.25f * (wksS + wks + a.wks[x.at(S, k - 1)] + a.wks[x.at(0, k - 1)]) * AREA;
+    }
+    Coef r;
+    float AE1, AW1, AS1, AN1;
+    if (DIFF) {
+        DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
+        DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
+        r.B = pl_ke(DT, fabsf(FT / DT), -FT);
+        r.C = pl_ke(DB, fabsf(FB / DB), FB);
+        AE1 = pl_ke(DE, fabsf(FE / DE), -FE);
+        AW1 = pl_ke(DW, fabsf(FW / DW), FW);
+        AS1 = pl_ke(DS, fabsf(FS / DS), FS);
+        AN1 = pl_ke(DN, fabsf(FN / DN), -FN);
+    } else {                                                  // upwind, U-prognostic-microscale_0.cs:123-128
+        r.B = vmaxf(-FT, 0.0f);
+        r.C = vmaxf(FB, 0.0f);
+        AE1 = vmaxf(-FE, 0.0f);
+        AW1 = vmaxf(FW, 0.0f);
+        AS1 = vmaxf(FS, 0.0f);
+        AN1 = vmaxf(-FN, 0.0f);
+    }
+    const float ap0 = sc.ap0[k];
+    r.A = r.B + r.C + AW1 + AS1 + AE1 + AN1 + ap0;
+    const float pW = __ldcg(PHI + x.at(W, k)), pE = __ldcg(PHI + x.at(E, k));
+    const float pS = __ldcg(PHI + x.at(S, k)), pN = __ldcg(PHI + x.at(N, k));
+    float DIM;
+    if (COMP == 0) {
+        const float DDPX = a.dpmnew[x.at(W, k)] - a.dpmnew[x.at(0, k)];
+        DIM = (float)(AW1 * pW + AS1 * pS + AE1 * pE + AN1 * pN + ap0 * 0.5 * (uksW + uks) + DDPX * dydz +
+                      a.coriolis * (sc.ug - phi) * AREA * dz);
+    } else {
+        const float DDPY = a.dpmnew[x.at(S, k)] - a.dpmnew[x.at(0, k)];
+        DIM = (float)(AW1 * pW + AS1 * pS + AE1 * pE + AN1 * pN + ap0 * 0.5 * (a.vks[x.at(S, k)] + vks) + DDPY * dxdz +
+                      a.coriolis * (sc.vg - phi) * AREA * dz);
+    }
+    if (k == c.KK + 1) {                                      // wall law, U-prognostic-microscale_2.cs:205-231
+        const float windhilf = vmaxf(wind_half(uksW, uks, vksW, vks), 0.01f);
+        float Ust;
+        if (c.fl & F_CUTKLT1) {
+            Ust = c.cf.help_t * windhilf;
+            if (c.fl & F_Z0GED)
+                Ust = c.cf.help_t * wind_half(a.uks[x.at(W, k + 1)], a.uks[x.at(0, k + 1)], a.vks[x.at(W, k + 1)],
+                                              a.vks[x.at(0, k + 1)]);
+        } else {
+            Ust = c.cf.help_o * windhilf;
+        }
+        DIM -= (float)(phi / windhilf * (Ust * Ust) * AREA);
+    }
+    if (DIFF && k > c.KK + 1) {                               // :234-245
+        float ADD;
+        if (COMP == 0) {
+            const float DUDXE = (pE - phi) * dydz;
+            const float DUDXW = (phi - pW) * dydz;
+            const float vksN = a.vks[x.at(N, k)], vksS = a.vks[x.at(S, k)];
+            const float DVDXN = (0.5f * (a.vks[x.at(E + N, k)] + vksN) - 0.5f * (vksN + a.vks[x.at(W + N, k)])) * dxdz;
+            const float DVDXS = (0.5f * (a.vks[x.at(E + S, k)] + vksS) - 0.5f * (vksS + a.vks[x.at(W + S, k)])) * dxdz;
+            const float wksW = a.wks[x.at(W, k)], wksB = a.wks[x.at(0, k - 1)];
+            const float DWDXT = (0.5f * (a.wk[x.at(E, k)] + wks) - 0.5f * (wks + wksW)) * AREA;
+            const float DWDXB = (0.5f * (a.wk[x.at(E, k - 1)] + wksB) - 0.5f * (wksB + a.wks[x.at(W, k - 1)])) * AREA;
+            ADD = VIS / DXK * (DUDXE - DUDXW + DVDXN - DVDXS + DWDXT - DWDXB);
+        } else {
+            const float DVDYN = (pN - phi) * dxdz;
+            const float DVDYS = (phi - pS) * dxdz;
+            const float uksE = a.uks[x.at(E, k)];
+            const float DUDYE = (0.5f * (a.uks[x.at(E + N, k)] + uksE) - 0.5f * (uksE + a.uks[x.at(E + S, k)])) * dxdz;
+            const float DUDYW = (0.5f * (a.uks[x.at(W + N, k)] + uksW) - 0.5f * (uksW + a.uks[x.at(W + S, k)])) * dxdz;
+            const float wksS = a.wks[x.at(S, k)], wksB = a.wks[x.at(0, k - 1)];
+            const float DWDYT = (0.5f * (a.wk[x.at(N, k)] + wks) - 0.5f * (wks + wksS)) * AREA;
+            const float DWDYB = (0.5f * (a.wk[x.at(N, k - 1)] + wksB) - 0.5f * (wksB + a.wks[x.at(S, k - 1)])) * AREA;
+            ADD = VIS / DXK * (DUDYE - DUDYW + DVDYN - DVDYS + DWDYT - DWDYB);
+        }
+        DIM += ADD;
+    }
+    r.D = DIM;
+    r.phi = phi;
+    return r;
+}
+
+// W of models 2 (DIFF) and 0, one level (W-prognostic-microscale_2.cs:84-199, W-...0.cs:84-123).
+template <bool DIFF, bool IL>
+__device__ __forceinline__ Coef w_scalar_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
+                                               int k) {
+    const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
+    const float dz = a.dzk[k];
+    const float dxdz = DXK * dz, dydz = DYK * dz;
+    const float uks = a.uks[x.at(0, k)], uksM = a.uks[x.at(0, k - 1)];
+    const float vks = a.vks[x.at(0, k)], vksM = a.vks[x.at(0, k - 1)];
+    const float wk = __ldcg(a.wk + x.at(0, k));
+    float VIS = 0.0f, DE = 0.0f, DW = 0.0f, DS = 0.0f, DN = 0.0f, DT = 0.0f, DB = 0.0f;
+    if (DIFF) {
+        const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
+        VIS = (float)sqrt((double)a.turb[x.at(0, k)]) * zs * 0.09f;
+        const float vmx = vmaxf(VIS, a.vishmin);
+        DE = vmx * dydz / DXK; DW = DE;
+        DS = vmx * dxdz / DYK; DN = DS;
+        DT = vmx * AREA / dz;
+        DB = (k > c.KK + 1) ? DT : 0.0f;
+        if (c.fl & F_BS) DS = 0.0f;
+        if (c.fl & F_BN) DN = 0.0f;
+        if (c.fl & F_BW) DW = 0.0f;
+        if (c.fl & F_BE) DE = 0.0f;
+    }
+    const float uksE = a.uks[x.at(E, k)], uksW = a.uks[x.at(W, k)];
+    const float vksS = a.vks[x.at(S, k)], vksN = a.vks[x.at(N, k)];
+    const float FE = 0.25f * (uks + uksE + uksM + a.uks[x.at(E, k - 1)]) * dydz;
+    const float FW = 0.25f * (uks + uksW + uksM + a.uks[x.at(W, k - 1)]) * dydz;
+    const float FS = 0.25f * (vks + vksS + vksM + a.vks[x.at(S, k - 1)]) * dxdz;
+    const float FN = 0.25f * (vks + vksN + vksM + a.vks[x.at(N, k - 1)]) * dxdz;
+    const float wks = a.wks[x.at(0, k)], wksB = a.wks[x.at(0, k - 1)];
+    const float FT = wks * AREA;
+    const float FB = (k > c.KK + 1) ? wksB * AREA : 0.0f;
+    Coef r;
+    float AE1, AW1, AS1, AN1;
+    if (DIFF) {
+        DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
+        DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
+        r.B = pl_ke(DT, fabsf(FT / DT), -FT);
+        r.C = pl_ke(DB, fabsf(FB / DB), FB);
+        AE1 = pl_ke(DE, fabsf(FE / DE), -FE);
+        AW1 = pl_ke(DW, fabsf(FW / DW), FW);
+        AS1 = pl_ke(DS, fabsf(FS / DS), FS);
+        AN1 = pl_ke(DN, fabsf(FN / DN), -FN);
+    } else {
+        r.B = vmaxf(-FT, 0.0f);
+        r.C = vmaxf(FB, 0.0f);
+        AE1 = vmaxf(-FE, 0.0f);
+        AW1 = vmaxf(FW, 0.0f);
+        AS1 = vmaxf(FS, 0.0f);
+        AN1 = vmaxf(-FN, 0.0f);
+    }
+    const float ap0 = sc.ap0[k];
+    r.A = r.B + r.C + AW1 + AS1 + AE1 + AN1 + ap0;
+    const float DDPZ = a.dpmnew[x.at(0, k - 1)] - a.dpmnew[x.at(0, k)];
+    const float wW = __ldcg(a.wk + x.at(W, k)), wS = __ldcg(a.wk + x.at(S, k));
+    const float wE = __ldcg(a.wk + x.at(E, k)), wN = __ldcg(a.wk + x.at(N, k));
+    float DIM = (float)(AW1 * wW + AS1 * wS + AE1 * wE + AN1 * wN + ap0 * 0.5 * (wksB + wks) + DDPZ * AREA);
+    if (DIFF && k > c.KK + 1) {                               // W-prognostic-microscale_2.cs:162-172
+        const float DUDZE = (0.5f * (a.uks[x.at(0, k + 1)] + uks) - 0.5f * (uks + uksM)) * dydz;
+        const float DUDZW = (0.5f * (a.uks[x.at(W, k + 1)] + uksW) - 0.5f * (uksW + a.uks[x.at(W, k - 1)])) * dydz;
+        const float DVDZN = (0.5f * (a.vks[x.at(0, k + 1)] + vks) - 0.5f * (vks + vksM)) * dxdz;
+        const float DVDZS = (0.5f * (a.vks[x.at(S, k + 1)] + vksS) - 0.5f * (vksS + a.vks[x.at(S, k - 1)])) * dxdz;
+        const float DWDZT = (__ldcg(a.wk + x.at(0, k + 1)) - wk) * AREA;
+        const float DWDZB = (wk - __ldcg(a.wk + x.at(0, k - 1))) * AREA;
+        DIM += VIS / dz * (DUDZE - DUDZW + DVDZN - DVDZS + DWDZT - DWDZB);
+    }
+    r.D = DIM;
+    r.phi = wk;
+    return r;
+}
+
+// Coefficients of the turbulent kinetic energy k and its dissipation eps at one level
+// (TKE-prognostic-microscale.cs:112-270): shared A, separate (B, C, D) per variable.
+struct CoefKE {
+    float A, B1, C1, D1, B2, C2, D2, k1, e1;
+};
+
+template <bool IL>
+__device__ __forceinline__ CoefKE tke_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
+                                            int k) {
+    const float potdtdz = sc.potdtdz;
+    const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
+    const float DXK_Rez = 1 / DXK, DYK_Rez = 1 / DYK;
+    const float dz = a.dzk[k];
+    const float DXKDZK = DXK * dz, DYKDZK = DYK * dz;
+    const float DZK_Rez = 1 / dz;
+    const float TURB = __ldcg(a.turb + x.at(0, k)), TDISS = __ldcg(a.tdiss + x.at(0, k));
+    const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
+    float VIS = (float)sqrt((double)TURB) * zs * 0.09f;
+    VIS = net_minf(VIS, 15);
+    float DE = net_maxf(VIS, a.vishmin) * DYKDZK * DXK_Rez;
+    float DW = DE;
+    float DS = net_maxf(VIS, a.vishmin) * DXKDZK * DYK_Rez;
+    float DN = DS;
+    float DT = net_maxf(VIS, a.vishmin) * AREA * DZK_Rez;
+    float DB = 0;
+    float DTEPS = net_maxf(VIS / 1.0f, a.vishmin) * AREA * DZK_Rez;   // VIS / Ceps, VISVMIN = VISHMIN
+    float DBEPS = 0;
+    if (k > c.KK + 1) { DB = DT; DBEPS = DTEPS; }
+    if (c.fl & F_BS) DS = 0;
+    if (c.fl & F_BN) DN = 0;
+    if (c.fl & F_BW) DW = 0;
+    if (c.fl & F_BE) DE = 0;
+    const float UK = a.uk[x.at(0, k)], UKip = a.uk[x.at(E, k)];
+    const float VK = a.vk[x.at(0, k)], VKjp = a.vk[x.at(N, k)];
+    const float WK1 = a.wk[x.at(0, k + 1)];
+    const float FE = UKip * DYKDZK;
+    const float FW = UK * DYKDZK;
+    const float FS = VK * DXKDZK;
+    const float FN = VKjp * DXKDZK;
+    const float FT = WK1 * AREA;
+    float FB = 0;
+    if (k > c.KK + 1) FB = a.wk[x.at(0, k)] * AREA;
+    DE = net_maxf(DE, 0.0001f); DB = net_maxf(DB, 0.0001f); DW = net_maxf(DW, 0.0001f);
+    DS = net_maxf(DS, 0.0001f); DN = net_maxf(DN, 0.0001f); DT = net_maxf(DT, 0.0001f);
+    DBEPS = net_maxf(DBEPS, 0.0001f); DTEPS = net_maxf(DTEPS, 0.0001f);
+    const float PE = fabsf(FE / DE), PB = fabsf(FB / DB), PW = fabsf(FW / DW);
+    const float PS = fabsf(FS / DS), PN = fabsf(FN / DN), PT = fabsf(FT / DT);
+    const float PBEPS = fabsf(FN / DBEPS);                      // FN, not FB (:187)
+    const float PTEPS = fabsf(FT / DTEPS);
+    auto p5 = [](float v) { const float q = 1 - 0.1f * v; return q * q * q * q * q; };
+    CoefKE r;
+    r.B1 = DT * net_maxf(0, p5(PT)) + net_maxf(-FT, 0);
+    r.C1 = DB * net_maxf(0, p5(PB)) + net_maxf(FB, 0);
+    const float AE1 = DE * net_maxf(0, p5(PE)) + net_maxf(-FE, 0);
+    const float AW1 = DW * net_maxf(0, p5(PW)) + net_maxf(FW, 0);
+    const float AS1 = DS * net_maxf(0, p5(PS)) + net_maxf(FS, 0);
+    const float AN1 = DN * net_maxf(0, p5(PN)) + net_maxf(-FN, 0);
+    r.B2 = DT * net_maxf(0, p5(PTEPS)) + net_maxf(-FT, 0);
+    r.C2 = DB * net_maxf(0, p5(PBEPS)) + net_maxf(FB, 0);
+    const float ap0 = sc.ap0[k];
+    r.A = r.B1 + r.C1 + AW1 + AS1 + AE1 + AN1 + ap0;
+    // production terms (:213-243)
+    const float UX1 = UKip, UX2 = UK;
+    const float VX1 = 0.5f * (a.vk[x.at(E, k)] + a.vk[x.at(E + N, k)]);
+    const float VX2 = 0.5f * (a.vk[x.at(W, k)] + a.vk[x.at(W + N, k)]);
+    const float WX1 = 0.5f * (a.wk[x.at(E, k)] + a.wk[x.at(E, k + 1)]);
+    const float WX2 = 0.5f * (a.wk[x.at(W, k)] + a.wk[x.at(W, k + 1)]);
+    const float UY1 = 0.5f * (a.uk[x.at(N, k)] + a.uk[x.at(E + N, k)]);
+    const float UY2 = 0.5f * (a.uk[x.at(S, k)] + a.uk[x.at(E + S, k)]);
+    const float VY1 = VKjp, VY2 = VK;
+    const float WY1 = 0.5f * (a.wk[x.at(N, k)] + a.wk[x.at(N, k + 1)]);
+    const float WY2 = 0.5f * (a.wk[x.at(S, k)] + a.wk[x.at(S, k + 1)]);
+    const float DUDX = (UX1 - UX2) * DXK_Rez;
+    const float DVDX = (VX1 - VX2) * DXK_Rez * 0.5f;
+    const float DWDX = (WX1 - WX2) * DXK_Rez * 0.5f;
+    const float DUDY = (UY1 - UY2) * DYK_Rez * 0.5f;
+    const float DVDY = (VY1 - VY2) * DYK_Rez;
+    const float DWDY = (WY1 - WY2) * DYK_Rez * 0.5f;
+    float DUDZ = a.uk[x.at(0, k + 1)] * DZK_Rez * 0.5f;
+    float DVDZ = a.vk[x.at(0, k + 1)] * DZK_Rez * 0.5f;
+    float DWDZ = WK1 * DZK_Rez * 0.5f;
+    if (k > c.KK + 1) {
+        DUDZ = (a.uk[x.at(0, k + 1)] - a.uk[x.at(0, k - 1)]) * DZK_Rez * 0.5f;
+        DVDZ = (a.vk[x.at(0, k + 1)] - a.vk[x.at(0, k - 1)]) * DZK_Rez * 0.5f;
+        DWDZ = (WK1 - a.wk[x.at(0, k - 1)]) * DZK_Rez * 0.5f;
+    }
+    auto sq = [](float v) { return v * v; };
+    const float PROTURB = VIS * AREA * dz *
+        (2 * sq(DUDX) + 2 * sq(DVDY) + 2 * sq(DWDZ) + sq(DUDY + DVDX) + sq(DUDZ + DWDX) + sq(DVDZ + DWDY) - TDISS);
+    const float PROBOU = (float)(-potdtdz * 9.81 / 283 * VIS * 1.35 * AREA * dz);
+    const float tW = __ldcg(a.turb + x.at(W, k)), tS = __ldcg(a.turb + x.at(S, k));
+    const float tE = __ldcg(a.turb + x.at(E, k)), tN = __ldcg(a.turb + x.at(N, k));
+    const float eW = __ldcg(a.tdiss + x.at(W, k)), eS = __ldcg(a.tdiss + x.at(S, k));
+    const float eE = __ldcg(a.tdiss + x.at(E, k)), eN = __ldcg(a.tdiss + x.at(N, k));
+    r.D1 = AW1 * tW + AS1 * tS + AE1 * tE + AN1 * tN + ap0 * TURB + PROTURB + PROBOU;
+    r.D2 = AW1 * eW + AS1 * eS + AE1 * eE + AN1 * eN + ap0 * TDISS + (TDISS / TURB * (1.44f * PROTURB - 1.92f * TDISS));
+    r.k1 = TURB;
+    r.e1 = TDISS;
+    return r;
 }
 
 }  // namespace gral

@@ -125,3 +125,43 @@ def test_quantise_off(gpu_required, layout):
     for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 5, quantise=0):
         np.testing.assert_array_equal(tg, tc)
         check_same(fg, fc)
+
+
+@pytest.mark.parametrize("iterations", [1, 3, 8])
+def test_model2_ke_small(gpu_required, layout, iterations):
+    """k-epsilon closure (TurbulenceModel 2): momentum with TURB-based viscosity, the TKE/TDISS
+    sweep with its wall functions and clamps, and the TURB initialisation."""
+    dom = prep.small_domain(16, 14, seed=6, obukhov=-80.0)      # unstable: the BdLayHeight branch
+    sit = prep.Situation(direction_deg=230.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], iterations, model=2):
+        assert sg["iterations"] == sc["iterations"] == iterations
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc, ("uk", "vk", "wk", "turb", "tdiss"))
+
+
+def test_model2_batch_mixed(gpu_required, layout):
+    dom = prep.small_domain(18, 15, seed=7, n_buildings=4, obukhov=200.0)
+    sits = [prep.Situation(direction_deg=d, speed_10m=v, z0=0.3, ustar=0.25)
+            for d, v in ((20.0, 2.0), (140.0, 4.0), (300.0, 1.5))]
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, sits, 5, model=2):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc, ("uk", "vk", "wk", "turb", "tdiss"))
+
+
+def test_model2_vegetation(gpu_required, layout):
+    dom = prep.small_domain(16, 16, seed=8, with_veg=True)
+    sit = prep.Situation(direction_deg=110.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 5, model=2):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc, ("uk", "vk", "wk", "turb", "tdiss"))
+
+
+@pytest.mark.parametrize("iterations", [1, 4])
+def test_model0_mixing_length(gpu_required, layout, iterations):
+    """TurbulenceModel 0: scalar mixing-length momentum with the double-precision W solve."""
+    dom = prep.small_domain(16, 14, seed=9)
+    sit = prep.Situation(direction_deg=320.0, speed_10m=2.5, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], iterations, model=0):
+        assert sg["iterations"] == sc["iterations"] == iterations
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
