@@ -22,11 +22,14 @@ GRAL_ETIMEDOUT = -4
 GRAL_ENONFINITE = -5
 GRAL_ENODEV = -6
 GRAL_ESTATE = -7
+GRAL_ETOOLARGE = -8
+GRAL_NOALLOC_MAX_ROWS = 4096
 
 STATUS_NAMES = {
     GRAL_OK: "GRAL_OK", GRAL_EINVAL: "GRAL_EINVAL", GRAL_ENOMEM: "GRAL_ENOMEM",
     GRAL_ECUDA: "GRAL_ECUDA", GRAL_ETIMEDOUT: "GRAL_ETIMEDOUT",
     GRAL_ENONFINITE: "GRAL_ENONFINITE", GRAL_ENODEV: "GRAL_ENODEV", GRAL_ESTATE: "GRAL_ESTATE",
+    GRAL_ETOOLARGE: "GRAL_ETOOLARGE",
 }
 
 MAX_HISTORY = 64

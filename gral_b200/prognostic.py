@@ -22,7 +22,7 @@ _lib = None
 
 EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_prog_solve_batch",
            "gral_prog_load", "gral_prog_iterate", "gral_prog_iterate_timed", "gral_prog_store",
-           "gral_prog_last_error", "gral_prog_destroy"]
+           "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc"]
 
 PHASES = ["bc", "pressure", "velcorr", "average", "u", "v", "w", "tke", "bookkeeping"]
 
@@ -70,6 +70,9 @@ def lib(build_if_stale: bool = True):
     L.gral_prog_last_error.restype = C.c_char_p
     L.gral_prog_destroy.argtypes = [C.c_void_p]
     L.gral_prog_destroy.restype = None
+    L.gral_prog_check_speeds_noalloc.argtypes = [C.c_int32] * 4 + [C.c_double] + [C.c_void_p] * 5 + \
+        [C.POINTER(C.c_int32), C.c_void_p]
+    L.gral_prog_check_speeds_noalloc.restype = C.c_int
     _lib = L
     return L
 
@@ -156,3 +159,26 @@ class PrognosticSolver:
         st = self._stats_array(n, traces)
         self._check(self._L.gral_prog_store(self._ctx, fa, st))
         return [stats_to_dict(st[b]) for b in range(n)]
+
+
+def check_speeds_noalloc(nii: int, njj: int, nkk: int, vert_cells_ff: int, geschw_max: float,
+                         uk_ptr: int, vk_ptr: int, wk_ptr: int, advdom_ptr: int, kkart_ptr: int,
+                         stream: int = 0) -> tuple:
+    """Unrealistic-wind-speed counts (U, V, W, non-finite) of a flow field that is already on the
+    GPU, without any device allocation (``gral_prog_check_speeds_noalloc``).
+
+    For callers that hold the solved field in device memory and cannot allocate there: one whose
+    device memory is committed to its own pool, or that must not let cudaMalloc/cudaFree
+    synchronise the device while other streams run.  The pointers are device addresses of
+    [NII+2][NJJ+2][NKK+2] float32 (U, V, W), uint8 ADVDOM and int16 KKART arrays
+    ([NII+2][NJJ+2]); ``stream`` is a cudaStream_t handle (0: the legacy default stream).  Grids
+    with more than ``GRAL_NOALLOC_MAX_ROWS`` (4096) rows are rejected; concurrent calls on one
+    device race on the shared fixed scratch and must be serialised.
+    """
+    L = lib()
+    out = (C.c_int32 * 4)()
+    rc = L.gral_prog_check_speeds_noalloc(nii, njj, nkk, vert_cells_ff, float(geschw_max), uk_ptr, vk_ptr,
+                                          wk_ptr, advdom_ptr, kkart_ptr, out, stream)
+    if rc != GRAL_OK:
+        raise GralError(rc, "gral_prog_check_speeds_noalloc failed")
+    return tuple(int(x) for x in out)

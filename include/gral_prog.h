@@ -43,6 +43,7 @@ extern "C" {
 #define GRAL_ENONFINITE (-5) /* non-finite value in the solved fields */
 #define GRAL_ENODEV (-6)     /* no usable CUDA device */
 #define GRAL_ESTATE (-7)     /* call out of order (e.g. store before load) */
+#define GRAL_ETOOLARGE (-8)  /* grid larger than a fixed-size entry point accepts */
 
 /* Solver scalars.  Defaults in brackets are the reference defaults. */
 typedef struct gral_params {
@@ -170,6 +171,31 @@ const char *gral_prog_last_error(gral_ctx *ctx);
 
 /* Release the context and its device memory. */
 void gral_prog_destroy(gral_ctx *ctx);
+
+/* No counterpart in the reference.  Allocation-free unrealistic-wind-speed check of a solved flow
+ * field that already lives on the GPU: the same counts gral_prog_store reports (uk/vk/wk
+ * _unrealistic: per ADVDOM==1 column, levels 1..min(NKK-1, KKART+vert_cells_ff), |U| or |V| above
+ * 55 m/s, |W| above 20 m/s, or any of them above 10*geschw_max) plus the number of cells holding a
+ * non-finite U, V or W, in counts[0..3].
+ *
+ * For callers that cannot call cudaMalloc when they run the check: a host whose device memory is
+ * committed to its own pool (a cudaMalloc would fail or make that pool give memory back) or that
+ * must not let cudaMalloc/cudaFree synchronise the device while its other streams run.  It needs
+ * no context: uk/vk/wk ([NII+2][NJJ+2][NKK+2]), advdom and kkart ([NII+2][NJJ+2]) are device
+ * pointers in the host layout above, counts is host memory, stream a cudaStream_t (NULL: the
+ * legacy default stream) on the current device.  The call allocates no memory; its scratch is a
+ * fixed static device array of GRAL_NOALLOC_MAX_ROWS rows (64 KiB + 256 B per device that loads
+ * the library, held until the process exits), so nii above GRAL_NOALLOC_MAX_ROWS returns
+ * GRAL_ETOOLARGE.  Host pointers return GRAL_EINVAL.  The first call on a device looks up that
+ * array's device address (with the device current); make that first call before any stream
+ * capture.  All calls on a device share the array, so calls that overlap on the GPU (two host
+ * threads, or two streams) race and may return wrong counts: serialise them.  The call returns
+ * after the counts are on the host. */
+#define GRAL_NOALLOC_MAX_ROWS 4096
+int gral_prog_check_speeds_noalloc(int32_t nii, int32_t njj, int32_t nkk, int32_t vert_cells_ff,
+                                   double geschw_max, const float *uk, const float *vk,
+                                   const float *wk, const uint8_t *advdom, const int16_t *kkart,
+                                   int32_t counts[4], void *stream);
 
 #ifdef __cplusplus
 }
