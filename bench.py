@@ -82,6 +82,33 @@ def batched_situations(n: int = 144, seed: int = 3):
     return out[:n]
 
 
+def rank_situations(base_situation, batch: int, rank: int, world: int):
+    """Situations one rank solves.  A single situation does not shard: every rank solves its own
+    replica.  Batches shard by situation with no exchange during the solve (weak scaling): rank 0
+    solves the 144-situation set itself, rank r the same 36 x 4 grid of directions and speeds turned
+    by r * 10/world degrees, so every rank's situations are distinct and the per-rank work fixed."""
+    from gral_b200 import prep
+    if base_situation is not None:
+        return [base_situation]
+    out = []
+    for x in batched_situations(batch):
+        d = (x.direction_deg + rank * 10.0 / max(world, 1)) % 360.0
+        out.append(prep.Situation(direction_deg=d, speed_10m=x.speed_10m, z0=x.z0, ustar=x.ustar,
+                                  obukhov=x.obukhov, potdtdz=x.potdtdz))
+    return out
+
+
+def max_over_ranks(x: float, device=None) -> float:
+    """Maximum of a per-rank float over the default process group (identity without one)."""
+    import torch
+    import torch.distributed as td
+    if not (td.is_available() and td.is_initialized()) or td.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
 def nominal_cells(dom) -> int:
     adv = dom.static.advdom[1:dom.nii + 1, 1:dom.njj + 1]
     return int((adv == 1).sum()) * dom.vert_cells_ff
@@ -97,16 +124,18 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profile_traffic(kernel: str):
-    """dram bytes per launch of `kernel` from a committed ncu summary, or None."""
+def profile_traffic(layout: str, phase: str, cells: int):
+    """DRAM bytes (read + write) per launch of the phase's kernel from the committed ncu summary
+    ``profiles/dram_traffic.txt`` (lines: layout phase kernel bytes cells_of_capture), scaled to
+    `cells` when the capture ran on a smaller case; None when that kernel was not captured."""
     path = os.path.join(ROOT, "profiles", "dram_traffic.txt")
     try:
         with open(path) as fh:
             for line in fh:
                 parts = line.split()
-                if len(parts) >= 2 and parts[0] == kernel:
-                    return float(parts[1])
-    except OSError:
+                if len(parts) >= 5 and parts[0] == layout and parts[1] == phase:
+                    return round(float(parts[3]) * cells / float(parts[4]))
+    except (OSError, ValueError):
         pass
     return None
 
@@ -227,11 +256,56 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def device_run(dom, sits, steps: int, warmup: int, local: int, model: int = 1):
+    """Load `sits` on one GPU, run `warmup` untimed then `steps` timed SIMPLE iterations (CUDA
+    events on the solver's stream, barrier + synchronize on both sides); returns the max-over-ranks
+    time, the phase split and the store statistics."""
+    import torch
+    import torch.distributed as td
+    from gral_b200 import prep
+    from gral_b200.prognostic import PrognosticSolver
+    dist = td.is_available() and td.is_initialized()
+    total = warmup + steps
+    # room for the autotuner's trial iterations (one per launch variant) before the timed ones
+    ps = [dom.params(x, model=model, iterations=total + 32, iter_min=total + 32) for x in sits]
+    fs = [prep.initial_fields(dom, x, model) for x in sits]
+    solver = PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=len(sits))
+    try:
+        solver.load(ps, dom.static, fs)
+        solver.iterate_timed(warmup)
+        if dist:
+            td.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            tot_ms, phases = solver.iterate_timed(steps)
+        torch.cuda.synchronize()
+        if dist:
+            td.barrier()
+        st = solver.store(fs)[0]
+    finally:
+        solver.close()
+    return max_over_ranks(tot_ms, "cuda"), tot_ms, phases, st, clk.summary()
+
+
+def roofline(cells: int, steps: int, phases: dict, layout: str):
+    cand = {k: v for k, v in phases.items() if k in BYTES_PER_CELL}
+    dom_k = max(cand, key=cand.get)
+    per_launch_s = cand[dom_k] / steps / 1e3
+    alg_bytes = cells * BYTES_PER_CELL[dom_k]
+    achieved = alg_bytes / per_launch_s / 1e9
+    peak, peak_kind = measured_peak()
+    it_ms = sum(phases.values()) / steps
+    it_bytes = cells * sum(BYTES_PER_CELL.values())
+    return {"bound": "hbm", "kernel": dom_k, "achieved": round(achieved, 2), "peak": peak,
+            "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 5),
+            "traffic": profile_traffic(layout, dom_k, cells), "alg_bytes_per_launch": alg_bytes,
+            "hbm_frac_iteration": round(it_bytes / (it_ms / 1e3) / 1e9 / peak, 5)}
+
+
 def run_ours(args, rank, world):
-    import numpy as np
     import torch
     from gral_b200 import prep
-    from gral_b200.prognostic import PHASES, PrognosticSolver
+    from gral_b200.prognostic import PrognosticSolver
 
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
@@ -242,66 +316,52 @@ def run_ours(args, rank, world):
         td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     dom, sit, full_iters, desc = workload(args.workload, args.grid)
-    sits = batched_situations(args.batch) if sit is None else [sit]
+    sits = rank_situations(sit, args.batch, rank, world)
     nsit = len(sits)
     cells = nominal_cells(dom) * nsit
-    total_iters = args.warmup + args.steps
-    # room for the autotuner's trial iterations (one per launch variant) before the timed ones
-    ps = [dom.params(x, model=1, iterations=total_iters + 32, iter_min=total_iters + 32) for x in sits]
-    f0s = [prep.initial_fields(dom, x) for x in sits]
-    solver = PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=nsit)
-    fs = [x.copy() for x in f0s]
-    solver.load(ps, dom.static, fs)
-    solver.iterate_timed(args.warmup)
-    if dist:
-        td.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        tot_ms, phases = solver.iterate_timed(args.steps)
-    torch.cuda.synchronize()
-    t_max = tot_ms
-    if dist:
-        tt = torch.tensor([tot_ms], device="cuda", dtype=torch.float64)
-        td.all_reduce(tt, op=td.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max, _, phases, st_store, clocks = device_run(dom, sits, args.steps, args.warmup, local)
     value = cells * args.steps * world / (t_max / 1e3) / 1e6
     ms_per_step = t_max / args.steps
-
-    # roofline of the dominant kernel
-    cand = {k: v for k, v in phases.items() if k in BYTES_PER_CELL}
-    dom_k = max(cand, key=cand.get)
-    per_launch_s = cand[dom_k] / args.steps / 1e3
-    alg_bytes = cells * BYTES_PER_CELL[dom_k]
-    achieved = alg_bytes / per_launch_s / 1e9
-    peak, peak_kind = measured_peak()
-    traffic = profile_traffic({"pressure": "k_pressure", "u": "k_mom_u1", "v": "k_mom_v1",
-                               "w": "k_mom_w1", "velcorr": "k_velcorr"}[dom_k])
-    it_bytes = cells * sum(BYTES_PER_CELL.values())
-    hbm_frac_iteration = it_bytes / (ms_per_step / 1e3) / 1e9 / peak
-    st_store = solver.store(fs)[0]
-    solver.close()
+    layout = "interleaved" if st_store["layout"] == 1 else "slab"
 
     # end to end through the public ABI: pinned host buffers, full solve, fields back
     e2e = None
     if not args.no_e2e:
         e2e_iters = args.e2e_iters if args.e2e_iters > 0 else full_iters
         pes = [dom.params(x, model=1, iterations=e2e_iters, iter_min=e2e_iters) for x in sits]
-        fps = [pinned_fields(x) for x in f0s]
-        del f0s
+        fps = [pinned_fields(prep.initial_fields(dom, x)) for x in sits]
         with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=nsit) as s2:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             sts = s2.calculate_batch(pes, dom.static, fps)
             dt = time.perf_counter() - t0
-        st = {"iterations": sum(x["iterations"] for x in sts) / nsit}
-        if dist:
-            tt = torch.tensor([dt], device="cuda", dtype=torch.float64)
-            td.all_reduce(tt, op=td.ReduceOp.MAX)
-            dt = float(tt.item())
+        iters = sum(x["iterations"] for x in sts) / nsit
+        dt = max_over_ranks(dt, "cuda")
         nbytes = sum(a.nbytes for fp in fps for a in (fp.uk, fp.vk, fp.wk))
-        e2e = {"value": round(cells * st["iterations"] * world / dt / 1e6, 3), "unit": UNIT,
+        e2e = {"value": round(cells * iters * world / dt / 1e6, 3), "unit": UNIT,
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-               "iterations": st["iterations"], "seconds": round(dt, 4)}
+               "iterations": iters, "seconds": round(dt, 4),
+               "situations_per_hour": round(3600.0 * nsit * world / dt, 1),
+               "note": "one step = one full solve (set-up, all iterations, post-checks, fields back)"}
+
+    # the batched form beside the plain one (same grid, 144 situations), device-timed
+    batched = None
+    if args.workload == "production" and not args.no_batched:
+        bsits = rank_situations(None, args.batch, rank, world)
+        bcells = nominal_cells(dom) * len(bsits)
+        bt, _, bph, bst, bclk = device_run(dom, bsits, args.batched_steps, 3, local)
+        bms = bt / args.batched_steps
+        batched = {"workload": f"batched: {len(bsits)} situations on the same grid", "situations": len(bsits),
+                   "value": round(bcells * args.batched_steps * world / (bt / 1e3) / 1e6, 3), "unit": UNIT,
+                   "steps": args.batched_steps, "warmup": 3, "ms_per_step": round(bms, 4),
+                   "layout": "interleaved" if bst["layout"] == 1 else "slab",
+                   "launch_variant": bst["launch_variant"],
+                   "gpu_launches": bst["launches_per_iteration"] * args.batched_steps,
+                   "situations_per_hour_at_800_iterations": round(3600.0 * len(bsits) * world / (bms * 800 / 1e3), 1),
+                   "roofline": roofline(bcells, args.batched_steps, bph,
+                                        "interleaved" if bst["layout"] == 1 else "slab"),
+                   "phase_ms_per_iteration": {k: round(v / args.batched_steps, 4) for k, v in bph.items() if v > 0},
+                   "clocks": bclk}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -310,25 +370,20 @@ def run_ours(args, rank, world):
                "sample": f"{args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s), "
                          "single-threaded deterministic restatement"}
 
-    launches = {"bc": 3, "pressure": 1, "velcorr": 1, "average": 1, "u": 1, "v": 1, "w": 1, "bookkeeping": 1}
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "description": desc, "cells": cells, "situations": nsit,
                    "grid": [dom.nii, dom.njj, dom.nkk], "kadvmax": dom.kadvmax, "model": 1,
-                   "simd_parity_width": 8, "l2": "working set above L2 (8 fields x 31 MB)",
-                   "parallelism": f"replicas x{world}",
-                   "layout": "interleaved" if st_store["layout"] == 1 else "slab",
-                   "launch_variant": st_store["launch_variant"]},
+                   "simd_parity_width": 8, "l2": "inputs larger than L2 (8 fields x 31 MB per situation)",
+                   "parallelism": (f"replicas x{world}" if sit is not None else f"situations sharded x{world}"),
+                   "layout": layout, "launch_variant": st_store["launch_variant"]},
         "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
-        "roofline": {"bound": "hbm", "kernel": dom_k, "achieved": round(achieved, 2), "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 5),
-                     "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
-                     "hbm_frac_iteration": round(hbm_frac_iteration, 5)},
-        "cpu_baseline": cpu, "e2e": e2e,
-        "gpu_launches": sum(launches.values()) * args.steps,
-        "clocks": clk.summary(),
+        "roofline": roofline(cells, args.steps, phases, layout),
+        "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+        "gpu_launches": st_store["launches_per_iteration"] * args.steps,
+        "clocks": clocks,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -349,6 +404,8 @@ def main():
     ap.add_argument("--cpu-iters", type=int, default=8)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-measurement")
+    ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--ref-iters", type=int, default=4)
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-warmup", action="store_true")

@@ -82,6 +82,7 @@ class GralStats(C.Structure):
         ("ms_total", C.c_double), ("ms_upload", C.c_double),
         ("ms_iterate", C.c_double), ("ms_download", C.c_double),
         ("layout", C.c_int32), ("launch_variant", C.c_int32),
+        ("launches_per_iteration", C.c_int32),
     ]
 
 

@@ -324,6 +324,15 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
 
 // Grid sizes of the wavefront kernels for the current family and variant: every resident block
 // slot of the GPU (the kernels are persistent and claim tasks).
+// kernel launches of one SIMPLE iteration: 3 boundary kernels, one per Gauss-Seidel phase and
+// group set, velocity correction, averages and bookkeeping
+int launches_per_iteration(const gral_ctx *ctx) {
+    const int gs = ctx->ka.group_set <= 0 ? ctx->ngroups : ctx->ka.group_set;
+    const int sets = ctx->il ? (ctx->ngroups + gs - 1) / gs : 1;
+    const int phases = (ctx->model == 2) ? 5 : 4;
+    return 3 + phases * sets + 3;
+}
+
 int size_grids(gral_ctx *ctx) {
     const int kinds[5] = {PH_PRESSURE, PH_U, PH_V, PH_W, PH_TKE};
     const bool il = ctx->il;
@@ -906,6 +915,7 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
         o.ms_download = ms_down;
         o.layout = ctx->il ? 1 : 0;
         o.launch_variant = ctx->il ? ctx->variant : -1;
+        o.launches_per_iteration = launches_per_iteration(ctx);
     }
     if (rc != GRAL_OK) fail(ctx, rc, "non-finite values in the solved fields");
     return rc;

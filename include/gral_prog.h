@@ -115,6 +115,7 @@ typedef struct gral_stats {
     int32_t layout;              /* device layout used: 0 slab (one warp per column), 1 interleaved
                                     (32 situations per group, one block per group-column) */
     int32_t launch_variant;      /* launch variant the autotuner kept (interleaved layout) */
+    int32_t launches_per_iteration; /* kernel launches of one SIMPLE iteration in the kept configuration */
 } gral_stats;
 
 typedef struct gral_ctx gral_ctx;
