@@ -179,20 +179,26 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
     return t;
 }
 
-// Spin (lane 0 only) until *flag >= stamp.  Gives up after limit_ns, or as soon as another warp
-// reported an error; returns false then.  Never waits unboundedly.
+// Spin (lane 0 only) until *flag >= stamp.  The first polls follow each other directly (the
+// predecessor is usually about to publish), later ones back off with __nanosleep up to 256 ns.
+// Gives up after limit_ns, or as soon as another warp reported an error; returns false then.
+// Never waits unboundedly.
 __device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned long long limit_ns) {
     if (ld_acquire(flag) >= stamp) return true;
     const unsigned long long t0 = globaltimer_ns();
-    unsigned ns = 20;
-    for (;;) {
-        __nanosleep(ns);
-        if (ns < 200) ns += ns;
+    unsigned ns = 16;
+    for (unsigned n = 1;; ++n) {
+        if (n > 4) {
+            __nanosleep(ns);
+            if (ns < 256) ns += ns;
+        }
         if (ld_acquire(flag) >= stamp) return true;
-        if (*(volatile int *)err != ERR_NONE) return false;
-        if (globaltimer_ns() - t0 > limit_ns) {
-            atomicCAS(err, ERR_NONE, ERR_TIMEOUT);
-            return false;
+        if ((n & 7) == 0) {
+            if (*(volatile int *)err != ERR_NONE) return false;
+            if (globaltimer_ns() - t0 > limit_ns) {
+                atomicCAS(err, ERR_NONE, ERR_TIMEOUT);
+                return false;
+            }
         }
     }
 }

@@ -104,36 +104,6 @@ __device__ __forceinline__ void gs_tasks(const KArgs &a, const SweepGeom &g, Bod
     }
 }
 
-// Serial vertical Thomas recurrence and relaxed back-substitution of one column, run by lane 0
-// on the warp's shared rows (U-prognostic-microscale_1.cs:485-524): rows A, B, C, D, phi.
-__device__ __forceinline__ void thomas_relax(float (*S)[KMAX_LEVELS], int K0, int KK, int VI, int kkm,
-                                             float relax) {
-    float P = 0.0f, Q = 0.0f;
-    for (int k = K0; k <= VI; ++k) {
-        const float A = S[0][k], B = S[1][k], C = S[2][k], D = S[3][k];
-        if (k > KK + 1) {
-            const float T = 1.0f / (A - C * P);
-            P = B * T;
-            Q = (D + C * Q) * T;
-        } else {
-            const float T = 1.0f / A;
-            P = B * T;
-            Q = D * T;
-        }
-        S[1][k] = P;
-        S[3][k] = Q;
-    }
-    float up = S[4][VI + 1];
-    for (int k = VI; k >= K0; --k) {
-        float u = S[4][k];
-        if (kkm < k) {
-            u += relax * (S[1][k] * up + S[3][k] - u);
-            S[4][k] = u;
-        }
-        up = u;
-    }
-}
-
 enum { COMP_U = 0, COMP_V = 1, COMP_W = 2 };
 
 template <int COMP, bool IL>
@@ -388,72 +358,6 @@ __device__ void plain_tke_column(const KArgs &a, int s, int i, int j, float (*S)
     }
 }
 
-// Pressure correction (PrognosticFlowfield.cs:804-901).  The reference's PIMP/QIMP buffer lives
-// per sweep row and is not cleared between columns, so the top level reads P/Q at
-// VerticalIndex+1 left by an earlier column of the same row (:865-868); the row carry buffer
-// reproduces that.  Row carry of the plain family: [s][j][2][KS].
-__device__ void plain_pressure_column(const KArgs &a, int s, int i, int j, int IS, int JS, bool first,
-                                      float (*S)[KMAX_LEVELS]) {
-    const int lane = threadIdx.x & 31;
-    const int ks = a.ks;
-    float *rc = a.rowcarry + ((size_t)s * a.nj2 + j) * 2 * ks;
-    if (first) {
-        for (int k = lane; k < 2 * ks; k += 32) __stcg(rc + k, 0.0f);
-        __threadfence_block();
-        __syncwarp();
-    }
-    const ColCtx c = make_col(a, i, j);
-    if (!(c.fl & F_ADV) || !a.sit[s].active) return;
-    const SitCtx sc = make_sit(a, s);
-    const Acc<false> x = make_acc<false>(a, s, c.col);
-    for (int r = 0; r < 2; ++r) {
-        const int k = lane + 32 * r;
-        if (k <= c.KK || k > c.VI) continue;
-        S[3][k] = pressure_dim<false>(a, x, c, sc, k, IS, JS);
-    }
-    __syncwarp();
-    if (lane == 0) {
-        float P = __ldcg(rc + c.VI + 1), Q = __ldcg(rc + ks + c.VI + 1);
-        for (int k = c.VI; k > c.KK; --k) {
-            const float T = 1.0f / (a.app[k] - a.atp[k] * P);
-            P = a.abp[k] * T;
-            Q = (a.atp[k] * Q + S[3][k]) * T;
-            S[1][k] = P;
-            S[2][k] = Q;
-        }
-        float prev = 0.0f;                                         // DPM[KKART] is always 0
-        for (int k = c.KK + 1; k <= c.VI; ++k) {
-            prev = S[1][k] * prev + S[2][k];
-            S[4][k] = prev;
-        }
-    }
-    __syncwarp();
-    unsigned dmax = 0;
-    const int klo = max(c.KK, a.vi_min);
-    for (int r = 0; r < 2; ++r) {
-        const int k = lane + 32 * r;
-        if (k <= c.KK || k > c.VI) continue;
-        const float temp = S[4][k];
-        dmax = max(dmax, residual_key(temp, sc));
-        __stcg(a.dpm + x.at(0, k), temp);
-        a.dpmnew[x.at(0, k)] += a.relaxp * temp;
-        if (k > klo) {
-            __stcg(rc + k, S[1][k]);
-            __stcg(rc + ks + k, S[2][k]);
-        }
-    }
-    for (int d = 16; d > 0; d >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
-    if (lane == 0 && dmax > 0) atomicMax(&a.sit[s].dumax_bits, dmax);
-}
-
-__global__ void __launch_bounds__(GS_WARPS * 32) k_pressure(KArgs a, SweepGeom g) {
-    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
-    float (*S)[KMAX_LEVELS] = sm[threadIdx.x >> 5];
-    gs_tasks<PH_PRESSURE, false, false>(a, g, [&](int s, int i, int j, int IS, int JS, bool first) {
-        plain_pressure_column(a, s, i, j, IS, JS, first, S);
-    });
-}
-
 template <int MODEL, int COMP>
 __global__ void __launch_bounds__(GS_WARPS * 32) k_mom(KArgs a, SweepGeom g) {
     __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
@@ -474,6 +378,273 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_tke(KArgs a, SweepGeom g) {
     gs_tasks<PH_TKE, false, false>(a, g, [&](int s, int i, int j, int, int, bool) {
         plain_tke_column(a, s, i, j, S);
     });
+}
+
+// ---------------------------- plain family, split tasks ------------------------------------
+// Model-1 momentum and the pressure correction run each column task in two halves around the
+// wait: `pre` does everything that does not read values the column's Gauss-Seidel predecessors
+// write (coefficients, sources, the Thomas forward elimination of the momentum equations), `post`
+// reads the predecessors' results and finishes the column.  Only `post` sits on the wavefront's
+// critical path; `pre` overlaps the predecessors' work.  Results are bit-identical to the unsplit
+// evaluation (the operations and their order are the same).
+
+template <int PHASE, bool REVERSE, class Job>
+__device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &g, Job &job) {
+    const int lane = threadIdx.x & 31;
+    const unsigned units = (unsigned)*a.nact;
+    const unsigned total = (unsigned)g.diag_start[g.ndiag] * units;
+    unsigned int *ctr = a.counters + PHASE;
+    const int it = *a.it_global;
+    int IS, JS;
+    sweep_dir(it, IS, JS);
+    if (REVERSE) { IS = -IS; JS = -JS; }
+    const int stamp = it * 8 + PHASE;
+    for (;;) {
+        unsigned base = 0;
+        if (lane == 0) base = atomicAdd(ctr, (unsigned)a.chunk);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= total) break;
+        if (*(volatile int *)a.err != ERR_NONE) break;
+        const unsigned end = min(total, base + (unsigned)a.chunk);
+        for (unsigned t = base; t < end; ++t) {
+            int u, i1, j1;
+            decode_task(t, g, units, u, i1, j1);
+            u = a.act[u];
+            const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+            const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+            int *fl = a.flags + (size_t)u * a.ncols;
+            job.pre(u, i, j, IS, JS, i1 == g.ia);
+            int ok = 1;
+            if (lane == 0) {
+                if (i1 > g.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, stamp, a.err, a.wait_limit_ns);
+                if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            if (ok) job.post(u, IS, JS);
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence();
+                st_release(fl + i * a.nj2 + j, stamp);
+            }
+        }
+    }
+}
+
+// Model-1 Thomas recurrence split at the wait (U-prognostic-microscale_1.cs:485-524): before it,
+// rows A, B become T = 1/(A - C*P) and P; after it, D becomes Q and the relaxed back-substitution
+// updates phi.
+__device__ __forceinline__ void ml_forward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI) {
+    float P = 0.0f;
+#pragma unroll 4
+    for (int k = K0; k <= VI; ++k) {
+        const float A = S[0][k], B = S[1][k], C = S[2][k];
+        const float T = (k > KK + 1) ? 1.0f / (A - C * P) : 1.0f / A;
+        P = B * T;
+        S[0][k] = T;
+        S[1][k] = P;
+    }
+}
+
+__device__ __forceinline__ void ml_backward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI, int kkm, float relax,
+                                            float top) {
+    float Q = 0.0f;
+#pragma unroll 4
+    for (int k = K0; k <= VI; ++k) {
+        const float T = S[0][k], D = S[3][k];
+        Q = (k > KK + 1) ? (D + S[2][k] * Q) * T : D * T;
+        S[3][k] = Q;
+    }
+    float up = top;
+#pragma unroll 4
+    for (int k = VI; k >= K0; --k) {
+        float u = S[4][k];
+        if (kkm < k) {
+            u += relax * (S[1][k] * up + S[3][k] - u);
+            S[4][k] = u;
+        }
+        up = u;
+    }
+}
+
+template <int COMP>
+struct Mom1Job {
+    const KArgs &a;
+    float (*S)[KMAX_LEVELS];
+    ColCtx c;
+    Acc<false> x;
+    bool act;
+    float top;          // the column's value at VerticalIndex+1 (not swept)
+    MomPre p[2];
+
+    __device__ void pre(int s, int i, int j, int, int, bool) {
+        const int lane = threadIdx.x & 31;
+        c = make_col(a, i, j);
+        act = (c.fl & F_ADV) && a.sit[s].active;
+        if (!act) return;
+        const SitCtx sc = make_sit(a, s);
+        x = make_acc<false>(a, s, c.col);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            if (COMP == COMP_U) p[r] = u1_pre<false>(a, x, c, sc, k);
+            else if (COMP == COMP_V) p[r] = v1_pre<false>(a, x, c, sc, k);
+            else p[r] = w1_pre<false>(a, x, c, sc, k);
+            S[0][k] = p[r].A; S[1][k] = p[r].B; S[2][k] = p[r].C; S[4][k] = p[r].phi;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            top = __ldcg(comp_field<COMP>(a) + x.at(0, c.VI + 1));
+            ml_forward(S, c.K0, c.KK, c.VI);
+        }
+    }
+
+    __device__ void post(int, int, int) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        float *F = comp_field<COMP>(a);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            float nW, nS, nE, nN;
+            nbr4(F, x, c, k, nW, nS, nE, nN);
+            if (COMP == COMP_U) S[3][k] = u1_post(p[r], c, k, nW, nS, nE, nN);
+            else if (COMP == COMP_V) S[3][k] = v1_post(p[r], c, k, nW, nS, nE, nN);
+            else S[3][k] = w1_post(p[r], c, k, nW, nS, nE, nN);
+        }
+        __syncwarp();
+        const int kkm = back_limit<COMP>(c);
+        if (lane == 0) ml_backward(S, c.K0, c.KK, c.VI, kkm, a.relax, top);
+        __syncwarp();
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k >= c.K0 && k <= c.VI && kkm < k) __stcg(F + x.at(0, k), S[4][k]);
+        }
+    }
+};
+
+template <int COMP>
+__global__ void __launch_bounds__(GS_WARPS * 32) k_mom1s(KArgs a, SweepGeom g) {
+    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    Mom1Job<COMP> job{a, sm[threadIdx.x >> 5]};
+    constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
+    gs_tasks_split<PH, COMP == COMP_V>(a, g, job);     // model-1 V sweeps with (-IS,-JS)
+}
+
+// Pressure correction (PrognosticFlowfield.cs:804-901).  The reference's PIMP/QIMP buffer lives per
+// sweep row and is not cleared between columns, so the top level reads P/Q at VerticalIndex+1 left
+// by an earlier column of the same row (:865-868); the row carry buffer [s][j][2][KS] reproduces
+// that, zeroed by the first column of each row.
+// Split at the wait.  Before it: the divergence terms and, speculatively, the
+// downward Thomas elimination started from the row carry's current P at VerticalIndex+1; after
+// it: the swept neighbours' DPM, the carry re-read (the elimination is redone when the
+// predecessor changed it), Q, the back-substitution, the residual and the stores.
+struct PressJob {
+    const KArgs &a;
+    float (*S)[KMAX_LEVELS];
+    ColCtx c;
+    Acc<false> x;
+    SitCtx sc;
+    float *rc;
+    bool act;
+    float t0[2];
+    float dn[2];        // DPMNEW of the column (only this task updates it)
+    float P0;
+
+    __device__ void forward(float P) {
+#pragma unroll 4
+        for (int k = c.VI; k > c.KK; --k) {
+            const float T = 1.0f / (a.app[k] - a.atp[k] * P);
+            P = a.abp[k] * T;
+            S[0][k] = T;
+            S[1][k] = P;
+        }
+    }
+
+    __device__ void pre(int s, int i, int j, int, int, bool first) {
+        const int lane = threadIdx.x & 31;
+        const int ks = a.ks;
+        rc = a.rowcarry + ((size_t)s * a.nj2 + j) * 2 * ks;
+        if (first) {
+            for (int k = lane; k < 2 * ks; k += 32) __stcg(rc + k, 0.0f);
+            __threadfence_block();
+            __syncwarp();
+        }
+        c = make_col(a, i, j);
+        act = (c.fl & F_ADV) && a.sit[s].active;
+        if (!act) return;
+        sc = make_sit(a, s);
+        x = make_acc<false>(a, s, c.col);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k <= c.KK || k > c.VI) continue;
+            t0[r] = pressure_pre<false>(a, x, c, sc, k);
+            dn[r] = a.dpmnew[x.at(0, k)];
+        }
+        if (lane == 0) {
+            P0 = __ldcg(rc + c.VI + 1);
+            forward(P0);
+        }
+    }
+
+    __device__ void post(int s, int IS, int JS) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        const int ks = a.ks;
+        float P = 0.0f, Q = 0.0f;
+        if (lane == 0) {
+            P = __ldcg(rc + c.VI + 1);
+            Q = __ldcg(rc + ks + c.VI + 1);
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k <= c.KK || k > c.VI) continue;
+            S[3][k] = pressure_post<false>(a, x, c, t0[r], k, IS, JS);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            if (__float_as_uint(P) != __float_as_uint(P0)) forward(P);
+#pragma unroll 4
+            for (int k = c.VI; k > c.KK; --k) {
+                Q = (a.atp[k] * Q + S[3][k]) * S[0][k];
+                S[2][k] = Q;
+            }
+            float prev = 0.0f;                                     // DPM[KKART] is always 0
+#pragma unroll 4
+            for (int k = c.KK + 1; k <= c.VI; ++k) {
+                prev = S[1][k] * prev + S[2][k];
+                S[4][k] = prev;
+            }
+        }
+        __syncwarp();
+        unsigned dmax = 0;
+        const int klo = max(c.KK, a.vi_min);
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k <= c.KK || k > c.VI) continue;
+            const float temp = S[4][k];
+            dmax = max(dmax, residual_key(temp, sc));
+            __stcg(a.dpm + x.at(0, k), temp);
+            a.dpmnew[x.at(0, k)] = dn[r] + a.relaxp * temp;
+            if (k > klo) {
+                __stcg(rc + k, S[1][k]);
+                __stcg(rc + ks + k, S[2][k]);
+            }
+        }
+        for (int d = 16; d > 0; d >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
+        if (lane == 0 && dmax > 0) atomicMax(&a.sit[s].dumax_bits, dmax);
+    }
+};
+
+__global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom g) {
+    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    PressJob job{a, sm[threadIdx.x >> 5]};
+    gs_tasks_split<PH_PRESSURE, false>(a, g, job);
 }
 
 // ---------------------------- batched family -----------------------------------------------
@@ -735,7 +906,7 @@ const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 const KFn kPlainMom[3][3] = {{k_mom<0, COMP_U>, k_mom<0, COMP_V>, k_mom<0, COMP_W>},
-                             {k_mom<1, COMP_U>, k_mom<1, COMP_V>, k_mom<1, COMP_W>},
+                             {k_mom1s<COMP_U>, k_mom1s<COMP_V>, k_mom1s<COMP_W>},
                              {k_mom<2, COMP_U>, k_mom<2, COMP_V>, k_mom<2, COMP_W>}};
 
 // Dynamic shared memory of a batched kernel: 5 float rows (momentum, pressure), 9 float rows
@@ -759,7 +930,7 @@ KFn batch_kernel(const BVariant &V, int kind, int model) {
 
 KFn plain_kernel(int kind, int model) {
     switch (kind) {
-        case PH_PRESSURE: return k_pressure;
+        case PH_PRESSURE: return k_pressure_s;
         case PH_U: return kPlainMom[model][0];
         case PH_V: return kPlainMom[model][1];
         case PH_W: return kPlainMom[model][2];

@@ -136,10 +136,27 @@ __device__ __forceinline__ float ml_ustern(const KArgs &a, const Acc<IL> &x, con
 }
 
 // ---------------------------------------------------------------------------------------------
-// U momentum, mixing-length model, one level (U-prognostic-microscale_1.cs:205-470).
+// Model-1 momentum, one level, split in two for the wavefront:
+//   *_pre   everything that does not read the swept field's four horizontal neighbours at level k
+//           (coefficients, viscosity, source terms, wall law, extra viscous pieces) -- safe to
+//           evaluate before the column's Gauss-Seidel predecessors have finished;
+//   *_post  reads those four neighbours and completes DIM in the reference's association order.
+// pre + post evaluate exactly the operations of the reference expression, so the split changes
+// no bit of the result (every product and partial sum is rounded as in the unsplit expression).
 // ---------------------------------------------------------------------------------------------
+struct MomPre {
+    float A, B, C, phi;          // matrix row and the level's old value
+    float aw, as, ae, an;        // AW1, AS1, AE1, AN1
+    float t1, t2, t3;            // source terms following the neighbour products, in order
+    float w;                     // wall term of the wall chunk (U, V)
+    float vdx;                   // VIS/DXK (U, V)
+    float e0, e1, e2, e3;        // extra viscous pieces (component specific)
+    float hz;                    // DYK*DZK (U) or DXK*DZK (V)
+};
+
+// U momentum (U-prognostic-microscale_1.cs:205-470).
 template <bool IL>
-__device__ __forceinline__ Coef u1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+__device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
@@ -170,54 +187,60 @@ __device__ __forceinline__ Coef u1_level(const KArgs &a, const Acc<IL> &x, const
     const float FB = (k > c.KK + 1) ? 0.25f * (wksW + wks + wksWB + wksB) * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
-    Coef r;
+    MomPre r;
     r.B = pl_coef(DT, fabsf(FT / DT), -FT);
     r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    const float AE1 = pl_coef(DE, fabsf(FE / DE), -FE);
-    const float AW1 = pl_coef(DW, fabsf(FW / DW), FW);
-    const float AS1 = pl_coef(DS, fabsf(FS / DS), FS);
-    const float AN1 = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
+    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
+    r.as = pl_coef(DS, fabsf(FS / DS), FS);
+    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
     const float ap0 = sc.ap0[k];
-    r.A = r.B + r.C + AW1 + AS1 + AE1 + AN1 + ap0;
+    r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPX = a.dpmnew[x.at(W, k)] - a.dpmnew[x.at(0, k)];
-    const float ukW = __ldcg(a.uk + x.at(W, k)), ukE = __ldcg(a.uk + x.at(E, k));
-    const float ukS = __ldcg(a.uk + x.at(S, k)), ukN = __ldcg(a.uk + x.at(N, k));
-    float DIM;
+    r.t1 = ap0 * 0.5f * (uksW + uks);
+    r.t2 = DDPX * dydz;
     if (c.fl & F_VEG) {
         const float in2 = 0.5f * (vksW + vks), in = 0.5f * (uksW + uks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.01f);
-        DIM = AW1 * ukW + AS1 * ukS + AE1 * ukE + AN1 * ukN + ap0 * 0.5f * (uksW + uks) + DDPX * dydz +
-              (a.coriolis * (sc.ug - uk) - a.veg[(size_t)c.col * a.ks + k - 1] * uk * wh) * AREA * dz;
+        r.t3 = (a.coriolis * (sc.ug - uk) - a.veg[(size_t)c.col * a.ks + k - 1] * uk * wh) * AREA * dz;
     } else {
-        DIM = AW1 * ukW + AS1 * ukS + AE1 * ukE + AN1 * ukN + ap0 * 0.5f * (uksW + uks) + DDPX * dydz +
-              a.coriolis * (sc.ug - uk) * AREA * dz;
+        r.t3 = a.coriolis * (sc.ug - uk) * AREA * dz;
     }
+    r.w = 0.0f;
     if (k >= c.wlo && k <= c.whi) {                       // masked wall term of the chunk, :419-450
         const float in = 0.5f * (uksW + uks), in2 = 0.5f * (vksW + vks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.1f);
         const float Ust = ml_ustern(a, x, c);
         const float m2 = (k == c.KK + 1) ? 1.0f : 0.0f;
-        DIM -= uk / wh * (Ust * Ust) * AREA * m2;
+        r.w = uk / wh * (Ust * Ust) * AREA * m2;
     }
+    r.vdx = VIS / DXK;
+    r.hz = dydz;
     if (k >= c.kad) {                                      // extra eddy-viscosity terms, :453-470
-        const float DUDXE = (ukE - uk) * dydz;
-        const float DUDXW = (uk - ukW) * dydz;
-        const float DVDXN = (0.5f * (a.vks[x.at(E + N, k)] + vksN) - 0.5f * (vksN + vksWN)) * dxdz;
-        const float DVDXS = (0.5f * (a.vks[x.at(E + S, k)] + vksS) - 0.5f * (vksS + vksWS)) * dxdz;
-        const float DWDXT = (0.5f * (a.wk[x.at(E, k)] + wks) - 0.5f * (wks + wksW)) * AREA;
-        const float DWDXB = (0.5f * (a.wk[x.at(E, k - 1)] + wksB) - 0.5f * (wksB + wksWB)) * AREA;
-        DIM += VIS / DXK * (DUDXE - DUDXW + DVDXN - DVDXS + DWDXT - DWDXB);
+        r.e0 = (0.5f * (a.vks[x.at(E + N, k)] + vksN) - 0.5f * (vksN + vksWN)) * dxdz;        // DVDXN
+        r.e1 = (0.5f * (a.vks[x.at(E + S, k)] + vksS) - 0.5f * (vksS + vksWS)) * dxdz;        // DVDXS
+        r.e2 = (0.5f * (a.wk[x.at(E, k)] + wks) - 0.5f * (wks + wksW)) * AREA;                // DWDXT
+        r.e3 = (0.5f * (a.wk[x.at(E, k - 1)] + wksB) - 0.5f * (wksB + wksWB)) * AREA;         // DWDXB
     }
-    r.D = DIM;
     r.phi = uk;
     return r;
 }
 
-// ---------------------------------------------------------------------------------------------
-// V momentum, mixing-length model, one level (V-prognostic-microscale_1.cs:205-488).
-// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float u1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
+                                         float nN) {
+    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
+    if (k >= c.wlo && k <= c.whi) DIM -= p.w;
+    if (k >= c.kad) {
+        const float DUDXE = (nE - p.phi) * p.hz;
+        const float DUDXW = (p.phi - nW) * p.hz;
+        DIM += p.vdx * (DUDXE - DUDXW + p.e0 - p.e1 + p.e2 - p.e3);
+    }
+    return DIM;
+}
+
+// V momentum (V-prognostic-microscale_1.cs:205-488).
 template <bool IL>
-__device__ __forceinline__ Coef v1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+__device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
@@ -257,54 +280,62 @@ __device__ __forceinline__ Coef v1_level(const KArgs &a, const Acc<IL> &x, const
     const float FB = (k > c.KK + 1) ? 0.25f * (wksS + wks + a.wks[x.at(S, k - 1)] + wksB) * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
-    Coef r;
+    MomPre r;
     r.B = pl_coef(DT, fabsf(FT / DT), -FT);
     r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    const float AE1 = pl_coef(DE, fabsf(FE / DE), -FE);
-    const float AW1 = pl_coef(DW, fabsf(FW / DW), FW);
-    const float AS1 = pl_coef(DS, fabsf(FS / DS), FS);
-    const float AN1 = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
+    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
+    r.as = pl_coef(DS, fabsf(FS / DS), FS);
+    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
     const float ap0 = sc.ap0[k];
-    r.A = r.B + r.C + AW1 + AS1 + AE1 + AN1 + ap0;
+    r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPY = a.dpmnew[x.at(S, k)] - a.dpmnew[x.at(0, k)];
-    const float vkN = __ldcg(a.vk + x.at(N, k)), vkS = __ldcg(a.vk + x.at(S, k));
-    const float vkW = __ldcg(a.vk + x.at(W, k)), vkE = __ldcg(a.vk + x.at(E, k));
-    float DIM;
+    r.t1 = ap0 * 0.5f * (vksS + vks);
+    r.t2 = DDPY * dxdz;
     if (c.fl & F_VEG) {
         const float in2 = 0.5f * (vksW + vks), in = 0.5f * (uksW + uks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.01f);
-        DIM = AW1 * vkW + AS1 * vkS + AE1 * vkE + AN1 * vkN + ap0 * 0.5f * (vksS + vks) + DDPY * dxdz +
-              (a.coriolis * (sc.vg - vk) - a.veg[(size_t)c.col * a.ks + k - 1] * vk * wh) * AREA * dz;
+        r.t3 = (a.coriolis * (sc.vg - vk) - a.veg[(size_t)c.col * a.ks + k - 1] * vk * wh) * AREA * dz;
     } else {
-        DIM = AW1 * vkW + AS1 * vkS + AE1 * vkE + AN1 * vkN + ap0 * 0.5f * (vksS + vks) + DDPY * dxdz +
-              a.coriolis * (sc.vg - vk) * AREA * dz;
+        r.t3 = a.coriolis * (sc.vg - vk) * AREA * dz;
     }
+    r.w = 0.0f;
     if (k >= c.wlo && k <= c.whi) {                       // :437-467
         const float in = 0.5f * (uksW + uks), in2 = 0.5f * (vksW + vks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.1f);
         const float Ust = ml_ustern(a, x, c);
         const float m2 = (k == c.KK + 1) ? 1.0f : 0.0f;
-        DIM -= vk / wh * (Ust * Ust) * AREA * m2;
+        r.w = vk / wh * (Ust * Ust) * AREA * m2;
     }
+    r.vdx = VIS / DXK;
+    r.hz = dxdz;
     if (k >= c.kad) {                                      // :470-488
-        const float DVDYN = (vkN - vk) * dxdz;
-        const float DVDYS = (vk - vkS) * dxdz;
         const float DUDYE = (0.5f * (a.uks[x.at(E + N, k)] + uksE) - 0.5f * (uksE + uksES)) * dxdz;
         const float DUDYW = (0.5f * (a.uks[x.at(W + N, k)] + uksW) - 0.5f * (uksW + uksWS)) * dxdz;
-        const float DWDYT = (0.5f * (a.wk[x.at(N, k)] + wks) - 0.5f * (wks + wksS)) * AREA;
-        const float DWDYB = (0.5f * (a.wk[x.at(N, k - 1)] + wksB) - 0.5f * (wksB + wksS)) * AREA;
-        DIM += VIS / DXK * (DUDYE - DUDYW + DVDYN - DVDYS + DWDYT - DWDYB);
+        r.e0 = DUDYE - DUDYW;
+        r.e1 = (0.5f * (a.wk[x.at(N, k)] + wks) - 0.5f * (wks + wksS)) * AREA;                // DWDYT
+        r.e2 = (0.5f * (a.wk[x.at(N, k - 1)] + wksB) - 0.5f * (wksB + wksS)) * AREA;          // DWDYB
     }
-    r.D = DIM;
     r.phi = vk;
     return r;
 }
 
-// ---------------------------------------------------------------------------------------------
-// W momentum, mixing-length model, one level (W-prognostic-microscale_1.cs:205-402).
-// ---------------------------------------------------------------------------------------------
+__device__ __forceinline__ float v1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
+                                         float nN) {
+    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
+    if (k >= c.wlo && k <= c.whi) DIM -= p.w;
+    if (k >= c.kad) {
+        const float DVDYN = (nN - p.phi) * p.hz;
+        const float DVDYS = (p.phi - nS) * p.hz;
+        DIM += p.vdx * (p.e0 + DVDYN - DVDYS + p.e1 - p.e2);
+    }
+    return DIM;
+}
+
+// W momentum (W-prognostic-microscale_1.cs:205-402); its extra viscous term reads only the own
+// column, so it is complete before the wait (e0 = the whole increment).
 template <bool IL>
-__device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+__device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
@@ -335,26 +366,23 @@ __device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const
     const float FB = (k > c.KK + 1) ? wksB * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
-    Coef r;
+    MomPre r;
     r.B = pl_coef(DT, fabsf(FT / DT), -FT);
     r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    const float AE1 = pl_coef(DE, fabsf(FE / DE), -FE);
-    const float AW1 = pl_coef(DW, fabsf(FW / DW), FW);
-    const float AS1 = pl_coef(DS, fabsf(FS / DS), FS);
-    const float AN1 = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
+    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
+    r.as = pl_coef(DS, fabsf(FS / DS), FS);
+    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
     const float ap0 = sc.ap0[k];
-    r.A = r.B + r.C + AW1 + AS1 + AE1 + AN1 + ap0;
+    r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPZ = a.dpmnew[x.at(0, k - 1)] - a.dpmnew[x.at(0, k)];
-    const float wkW = __ldcg(a.wk + x.at(W, k)), wkS = __ldcg(a.wk + x.at(S, k));
-    const float wkE = __ldcg(a.wk + x.at(E, k)), wkN = __ldcg(a.wk + x.at(N, k));
-    float DIM;
+    r.t1 = ap0 * 0.5f * (wksB + wks);
+    r.t2 = DDPZ * AREA;
+    r.t3 = 0.0f;
     if (c.fl & F_VEG) {
         const float in2 = 0.5f * (vksS + vks), in = 0.5f * (uksW + uks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.01f);
-        DIM = AW1 * wkW + AS1 * wkS + AE1 * wkE + AN1 * wkN + ap0 * 0.5f * (wksB + wks) + DDPZ * AREA -
-              a.veg[(size_t)c.col * a.ks + k - 1] * wk * wh * AREA * dz;
-    } else {
-        DIM = AW1 * wkW + AS1 * wkS + AE1 * wkE + AN1 * wkN + ap0 * 0.5f * (wksB + wks) + DDPZ * AREA;
+        r.t3 = a.veg[(size_t)c.col * a.ks + k - 1] * wk * wh * AREA * dz;     // subtracted
     }
     if (k >= c.kad) {                                      // :376-402
         const float DUDZE = (0.5f * (a.uks[x.at(0, k + 1)] + uks) - 0.5f * (uks + uksM)) * dydz;
@@ -363,21 +391,64 @@ __device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const
         const float DVDZS = (0.5f * (a.vks[x.at(S, k + 1)] + vksS) - 0.5f * (vksS + vksSB)) * dxdz;
         const float DWDZT = (__ldcg(a.wk + x.at(0, k + 1)) - wk) * AREA;
         const float DWDZB = (wk - __ldcg(a.wk + x.at(0, k - 1))) * AREA;
-        DIM += VIS / dz * (DUDZE - DUDZW + DVDZN - DVDZS + DWDZT - DWDZB);
+        r.e0 = VIS / dz * (DUDZE - DUDZW + DVDZN - DVDZS + DWDZT - DWDZB);
     }
-    r.D = DIM;
     r.phi = wk;
     return r;
+}
+
+__device__ __forceinline__ float w1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
+                                         float nN) {
+    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2;
+    if (c.fl & F_VEG) DIM = DIM - p.t3;
+    if (k >= c.kad) DIM += p.e0;
+    return DIM;
+}
+
+// The swept field's four horizontal neighbours of level k: W, S, E, N (read through L2: other
+// warps of the same launch write them).
+template <bool IL>
+__device__ __forceinline__ void nbr4(const float *F, const Acc<IL> &x, const ColCtx &c, int k, float &nW, float &nS,
+                                     float &nE, float &nN) {
+    nW = __ldcg(F + x.at(-(long long)c.nj2, k));
+    nS = __ldcg(F + x.at(-1, k));
+    nE = __ldcg(F + x.at(c.nj2, k));
+    nN = __ldcg(F + x.at(1, k));
+}
+
+template <bool IL>
+__device__ __forceinline__ Coef u1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+    const MomPre p = u1_pre(a, x, c, sc, k);
+    float nW, nS, nE, nN;
+    nbr4(a.uk, x, c, k, nW, nS, nE, nN);
+    return Coef{p.A, p.B, p.C, u1_post(p, c, k, nW, nS, nE, nN), p.phi};
+}
+
+template <bool IL>
+__device__ __forceinline__ Coef v1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+    const MomPre p = v1_pre(a, x, c, sc, k);
+    float nW, nS, nE, nN;
+    nbr4(a.vk, x, c, k, nW, nS, nE, nN);
+    return Coef{p.A, p.B, p.C, v1_post(p, c, k, nW, nS, nE, nN), p.phi};
+}
+
+template <bool IL>
+__device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
+    const MomPre p = w1_pre(a, x, c, sc, k);
+    float nW, nS, nE, nN;
+    nbr4(a.wk, x, c, k, nW, nS, nE, nN);
+    return Coef{p.A, p.B, p.C, w1_post(p, c, k, nW, nS, nE, nN), p.phi};
 }
 
 // ---------------------------------------------------------------------------------------------
 // Pressure correction, right-hand side of level k (PrognosticFlowfield.cs:739-748, 853-855): the
 // divergence on the fly, the already-swept neighbours (i-IS, j) and (i, j-JS); the reference
 // zeroed the other two neighbours' DPM before the sweep, so they enter as literal zeros.
+// pressure_pre is the divergence term (no pressure read), pressure_post adds the neighbours.
 // ---------------------------------------------------------------------------------------------
 template <bool IL>
-__device__ __forceinline__ float pressure_dim(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
-                                              int k, int IS, int JS) {
+__device__ __forceinline__ float pressure_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
+                                              int k) {
     const long long E = c.nj2, N = 1;
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
@@ -388,12 +459,27 @@ __device__ __forceinline__ float pressure_dim(const KArgs &a, const Acc<IL> &x, 
     else
         DIV = (a.uk[x.at(0, k)] - a.uk[x.at(E, k)]) * DYK * dz + (a.vk[x.at(0, k)] - a.vk[x.at(N, k)]) * DXK * dz -
               a.wk[x.at(0, k + 1)] * AREA;
+    return DIV / sc.dtime;
+}
+
+template <bool IL>
+__device__ __forceinline__ float pressure_post(const KArgs &a, const Acc<IL> &x, const ColCtx &c, float t0, int k,
+                                               int IS, int JS) {
+    const float DXK = a.dxk, DYK = a.dyk;
+    const float dz = a.dzk[k];
     const float pi = __ldcg(a.dpm + x.at(-(long long)IS * c.nj2, k));
     const float pj = __ldcg(a.dpm + x.at(-(long long)JS, k));
     const float si = (IS == 1) ? (pi + 0.0f) : (0.0f + pi);    // DPMim + DPMip
     const float sj = (JS == 1) ? (pj - 0.0f) : (0.0f - pj);    // DPMjm - DPMjp
-    return DIV / sc.dtime + si / DXK * DYK * dz + sj / DYK * DXK * dz;
+    return t0 + si / DXK * DYK * dz + sj / DYK * DXK * dz;
 }
+
+template <bool IL>
+__device__ __forceinline__ float pressure_dim(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
+                                              int k, int IS, int JS) {
+    return pressure_post(a, x, c, pressure_pre(a, x, c, sc, k), k, IS, JS);
+}
+
 
 }  // namespace gral
 
