@@ -109,6 +109,9 @@ struct KArgs {
     int *flags;                          // [nb][ncols] stamps
     unsigned int *counters;              // task counters, one per GS phase kind
     float *rowcarry;                     // [nb][nj2][2][ks] pressure row carry (P, Q)
+    const short2 *rcw;                   // per column: i of the last column before it in its sweep row
+                                         // that writes the row carry at VerticalIndex+1 (x: IS=+1,
+                                         // y: IS=-1), -1 if none
     int *err;                            // device error word (0 = ok)
     const int *act;                      // active situation list (slab layout)
     const int *nact;                     // number of active situations

@@ -94,12 +94,10 @@ __device__ __forceinline__ void gs_tasks(const KArgs &a, const SweepGeom &g, Bod
                 if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);
+            __syncwarp();
             if (ok) body(u, i, j, IS, JS, i1 == g.ia);
             __syncwarp();
-            if (lane == 0) {
-                __threadfence();
-                st_release(fl + i * a.nj2 + j, stamp);
-            }
+            if (lane == 0) st_release(fl + i * a.nj2 + j, stamp);
         }
     }
 }
@@ -399,6 +397,7 @@ __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &
     sweep_dir(it, IS, JS);
     if (REVERSE) { IS = -IS; JS = -JS; }
     const int stamp = it * 8 + PHASE;
+    job.stamp = stamp;
     for (;;) {
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(ctr, (unsigned)a.chunk);
@@ -420,23 +419,39 @@ __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &
                 if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
             }
             ok = __shfl_sync(0xffffffffu, ok, 0);
+            __syncwarp();
             if (ok) job.post(u, IS, JS);
             __syncwarp();
-            if (lane == 0) {
-                __threadfence();
-                st_release(fl + i * a.nj2 + j, stamp);
-            }
+            if (lane == 0) st_release(fl + i * a.nj2 + j, stamp);
         }
     }
+    job.finish();
 }
 
 // Model-1 Thomas recurrence split at the wait (U-prognostic-microscale_1.cs:485-524): before it,
 // rows A, B become T = 1/(A - C*P) and P; after it, D becomes Q and the relaxed back-substitution
-// updates phi.
+// updates phi.  Lane 0 runs the recurrences eight levels at a time: the eight levels' operands are
+// loaded from shared memory together, so only the arithmetic chain is serial.
+constexpr int TCH = 8;
+
 __device__ __forceinline__ void ml_forward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI) {
     float P = 0.0f;
-#pragma unroll 4
-    for (int k = K0; k <= VI; ++k) {
+    int k = K0;
+    for (; k + TCH - 1 <= VI; k += TCH) {
+        float A[TCH], B[TCH], C[TCH];
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) { A[q] = S[0][k + q]; B[q] = S[1][k + q]; C[q] = S[2][k + q]; }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) {
+            const float T = (k + q > KK + 1) ? 1.0f / (A[q] - C[q] * P) : 1.0f / A[q];
+            P = B[q] * T;
+            A[q] = T;
+            B[q] = P;
+        }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) { S[0][k + q] = A[q]; S[1][k + q] = B[q]; }
+    }
+    for (; k <= VI; ++k) {
         const float A = S[0][k], B = S[1][k], C = S[2][k];
         const float T = (k > KK + 1) ? 1.0f / (A - C * P) : 1.0f / A;
         P = B * T;
@@ -448,15 +463,41 @@ __device__ __forceinline__ void ml_forward(float (*S)[KMAX_LEVELS], int K0, int 
 __device__ __forceinline__ void ml_backward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI, int kkm, float relax,
                                             float top) {
     float Q = 0.0f;
-#pragma unroll 4
-    for (int k = K0; k <= VI; ++k) {
+    int k = K0;
+    for (; k + TCH - 1 <= VI; k += TCH) {
+        float T[TCH], D[TCH], C[TCH];
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) { T[q] = S[0][k + q]; D[q] = S[3][k + q]; C[q] = S[2][k + q]; }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) {
+            Q = (k + q > KK + 1) ? (D[q] + C[q] * Q) * T[q] : D[q] * T[q];
+            D[q] = Q;
+        }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) S[3][k + q] = D[q];
+    }
+    for (; k <= VI; ++k) {
         const float T = S[0][k], D = S[3][k];
         Q = (k > KK + 1) ? (D + S[2][k] * Q) * T : D * T;
         S[3][k] = Q;
     }
     float up = top;
-#pragma unroll 4
-    for (int k = VI; k >= K0; --k) {
+    k = VI;
+    for (; k - (TCH - 1) >= K0; k -= TCH) {
+        float P[TCH], Qv[TCH], U[TCH];
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) { P[q] = S[1][k - q]; Qv[q] = S[3][k - q]; U[q] = S[4][k - q]; }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) {
+            float u = U[q];
+            if (kkm < k - q) u += relax * (P[q] * up + Qv[q] - u);
+            U[q] = u;
+            up = u;
+        }
+#pragma unroll
+        for (int q = 0; q < TCH; ++q) S[4][k - q] = U[q];
+    }
+    for (; k >= K0; --k) {
         float u = S[4][k];
         if (kkm < k) {
             u += relax * (S[1][k] * up + S[3][k] - u);
@@ -470,6 +511,7 @@ template <int COMP>
 struct Mom1Job {
     const KArgs &a;
     float (*S)[KMAX_LEVELS];
+    int stamp;
     ColCtx c;
     Acc<false> x;
     bool act;
@@ -523,12 +565,14 @@ struct Mom1Job {
             if (k >= c.K0 && k <= c.VI && kkm < k) __stcg(F + x.at(0, k), S[4][k]);
         }
     }
+
+    __device__ void finish() {}
 };
 
 template <int COMP>
 __global__ void __launch_bounds__(GS_WARPS * 32) k_mom1s(KArgs a, SweepGeom g) {
     __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
-    Mom1Job<COMP> job{a, sm[threadIdx.x >> 5]};
+    Mom1Job<COMP> job{a, sm[threadIdx.x >> 5], 0};
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
     gs_tasks_split<PH, COMP == COMP_V>(a, g, job);     // model-1 V sweeps with (-IS,-JS)
 }
@@ -537,13 +581,16 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_mom1s(KArgs a, SweepGeom g) {
 // sweep row and is not cleared between columns, so the top level reads P/Q at VerticalIndex+1 left
 // by an earlier column of the same row (:865-868); the row carry buffer [s][j][2][KS] reproduces
 // that, zeroed by the first column of each row.
-// Split at the wait.  Before it: the divergence terms and, speculatively, the
-// downward Thomas elimination started from the row carry's current P at VerticalIndex+1; after
-// it: the swept neighbours' DPM, the carry re-read (the elimination is redone when the
-// predecessor changed it), Q, the back-substitution, the residual and the stores.
+// Split at the wait.  Before it: the divergence terms and the downward Thomas elimination, which
+// starts from the carry's P at VerticalIndex+1: zero when no earlier column of the row writes that
+// level (a host-built table names the last writer), else read after waiting for that writer --
+// an ancestor of this column in the wavefront, usually finished long before.  After the wait: the
+// swept neighbours' DPM, Q (started from the carry's Q, which the predecessor may have written),
+// the back-substitution, the residual and the stores.
 struct PressJob {
     const KArgs &a;
     float (*S)[KMAX_LEVELS];
+    int stamp;
     ColCtx c;
     Acc<false> x;
     SitCtx sc;
@@ -551,11 +598,35 @@ struct PressJob {
     bool act;
     float t0[2];
     float dn[2];        // DPMNEW of the column (only this task updates it)
-    float P0;
+    unsigned run_max;   // residual key maximum of this warp's tasks of situation run_s so far
+    int run_s;
 
+    // The residual maximum is only read after the phase (k_bookkeeping), so each warp keeps a
+    // running maximum and publishes it once per situation instead of once per column.
+    __device__ void flush() {
+        if ((threadIdx.x & 31) == 0 && run_s >= 0 && run_max > 0) atomicMax(&a.sit[run_s].dumax_bits, run_max);
+        run_max = 0;
+    }
+    __device__ void finish() { flush(); }
+
+    // T = 1/(APP - ATP*P), P = ABP*T from level VI down to KKART+1, eight levels per step.
     __device__ void forward(float P) {
-#pragma unroll 4
-        for (int k = c.VI; k > c.KK; --k) {
+        int k = c.VI;
+        for (; k - (TCH - 1) > c.KK; k -= TCH) {
+            float ap[TCH], at[TCH], ab[TCH];
+#pragma unroll
+            for (int q = 0; q < TCH; ++q) { ap[q] = a.app[k - q]; at[q] = a.atp[k - q]; ab[q] = a.abp[k - q]; }
+#pragma unroll
+            for (int q = 0; q < TCH; ++q) {
+                const float T = 1.0f / (ap[q] - at[q] * P);
+                P = ab[q] * T;
+                ap[q] = T;
+                ab[q] = P;
+            }
+#pragma unroll
+            for (int q = 0; q < TCH; ++q) { S[0][k - q] = ap[q]; S[1][k - q] = ab[q]; }
+        }
+        for (; k > c.KK; --k) {
             const float T = 1.0f / (a.app[k] - a.atp[k] * P);
             P = a.abp[k] * T;
             S[0][k] = T;
@@ -563,7 +634,7 @@ struct PressJob {
         }
     }
 
-    __device__ void pre(int s, int i, int j, int, int, bool first) {
+    __device__ void pre(int s, int i, int j, int IS, int, bool first) {
         const int lane = threadIdx.x & 31;
         const int ks = a.ks;
         rc = a.rowcarry + ((size_t)s * a.nj2 + j) * 2 * ks;
@@ -585,7 +656,13 @@ struct PressJob {
             dn[r] = a.dpmnew[x.at(0, k)];
         }
         if (lane == 0) {
-            P0 = __ldcg(rc + c.VI + 1);
+            const short2 w = a.rcw[c.col];
+            const int wi = (IS == 1) ? w.x : w.y;
+            float P0 = 0.0f;
+            if (wi >= 0) {
+                const int *fl = a.flags + (size_t)s * a.ncols;
+                if (wait_stamp(fl + wi * a.nj2 + j, stamp, a.err, a.wait_limit_ns)) P0 = __ldcg(rc + c.VI + 1);
+            }
             forward(P0);
         }
     }
@@ -594,11 +671,8 @@ struct PressJob {
         if (!act) return;
         const int lane = threadIdx.x & 31;
         const int ks = a.ks;
-        float P = 0.0f, Q = 0.0f;
-        if (lane == 0) {
-            P = __ldcg(rc + c.VI + 1);
-            Q = __ldcg(rc + ks + c.VI + 1);
-        }
+        float Q = 0.0f;
+        if (lane == 0) Q = __ldcg(rc + ks + c.VI + 1);
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int k = lane + 32 * r;
@@ -607,15 +681,38 @@ struct PressJob {
         }
         __syncwarp();
         if (lane == 0) {
-            if (__float_as_uint(P) != __float_as_uint(P0)) forward(P);
-#pragma unroll 4
-            for (int k = c.VI; k > c.KK; --k) {
+            int k = c.VI;
+            for (; k - (TCH - 1) > c.KK; k -= TCH) {
+                float at[TCH], d[TCH], t[TCH];
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) { at[q] = a.atp[k - q]; d[q] = S[3][k - q]; t[q] = S[0][k - q]; }
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) {
+                    Q = (at[q] * Q + d[q]) * t[q];
+                    d[q] = Q;
+                }
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) S[2][k - q] = d[q];
+            }
+            for (; k > c.KK; --k) {
                 Q = (a.atp[k] * Q + S[3][k]) * S[0][k];
                 S[2][k] = Q;
             }
             float prev = 0.0f;                                     // DPM[KKART] is always 0
-#pragma unroll 4
-            for (int k = c.KK + 1; k <= c.VI; ++k) {
+            k = c.KK + 1;
+            for (; k + TCH - 1 <= c.VI; k += TCH) {
+                float pp[TCH], qq[TCH];
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) { pp[q] = S[1][k + q]; qq[q] = S[2][k + q]; }
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) {
+                    prev = pp[q] * prev + qq[q];
+                    qq[q] = prev;
+                }
+#pragma unroll
+                for (int q = 0; q < TCH; ++q) S[4][k + q] = qq[q];
+            }
+            for (; k <= c.VI; ++k) {
                 prev = S[1][k] * prev + S[2][k];
                 S[4][k] = prev;
             }
@@ -637,13 +734,19 @@ struct PressJob {
             }
         }
         for (int d = 16; d > 0; d >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
-        if (lane == 0 && dmax > 0) atomicMax(&a.sit[s].dumax_bits, dmax);
+        if (s != run_s) {
+            flush();
+            run_s = s;
+        }
+        run_max = max(run_max, dmax);
     }
 };
 
 __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom g) {
     __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
-    PressJob job{a, sm[threadIdx.x >> 5]};
+    PressJob job{a, sm[threadIdx.x >> 5], 0};
+    job.run_max = 0;
+    job.run_s = -1;
     gs_tasks_split<PH_PRESSURE, false>(a, g, job);
 }
 
@@ -690,10 +793,7 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
             __syncthreads();
             if (s_ok) body(grp, i, j, IS, JS, i1 == g.ia);
             __syncthreads();
-            if (threadIdx.x == 0) {
-                __threadfence();
-                st_release(fl + i * a.nj2 + j, stamp);
-            }
+            if (threadIdx.x == 0) st_release(fl + i * a.nj2 + j, stamp);
         }
     }
 }

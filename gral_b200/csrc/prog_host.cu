@@ -64,6 +64,7 @@ struct gral_ctx {
     int cap_nii = 0, cap_njj = 0, cap_nkk = 0, cap_kadv = 0, cap_batch = 0;
     int il_min_batch = 32;
     int forced_variant = -1;   // GRAL_PROG_BATCH_VARIANT
+    int lookahead = 8;         // GRAL_PROG_LOOKAHEAD: plain-family warps per average diagonal width
     int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
     std::string err = "no error";
 
@@ -90,6 +91,7 @@ struct gral_ctx {
     DevBuf<uint32_t> cflags;
     DevBuf<ColF> colf;
     DevBuf<ColKE> colke;
+    DevBuf<short2> rcw;
     DevBuf<float> varw, z0i;
     DevBuf<SitDev> sit;
     DevBuf<int> flags, misc, diag, bcl, counts;
@@ -101,7 +103,7 @@ struct gral_ctx {
         if (graph) cudaGraphExecDestroy(graph);
         DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
         for (auto *b : fb) b->release();
-        meta.release(); cflags.release(); colf.release(); sit.release(); colke.release();
+        meta.release(); cflags.release(); colf.release(); sit.release(); colke.release(); rcw.release();
         varw.release(); z0i.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
@@ -346,10 +348,22 @@ int size_grids(gral_ctx *ctx) {
     ctx->ka.ctr_slot = 0;
     if (il && (ctx->ngroups + std::max(ctx->ka.group_set, 1) - 1) / std::max(ctx->ka.group_set, 1) > kCounterSlots)
         ctx->ka.group_set = 0;
+    // Plain family: enough warps for `lookahead` diagonals of the average wavefront width, so a
+    // warp's pre-wait work runs a few diagonals ahead of the front without thousands of warps
+    // polling far-future flags (0 = as many as fit).
+    const double diag_width = (double)ctx->nb * (double)(ctx->nii - 3) * (double)(ctx->njj - 3) /
+                              (double)std::max(1, ctx->nii + ctx->njj - 7);
+    // The pressure sweep reads the row carry speculatively before its wait; a shallower lookahead
+    // keeps that read fresh (3 of the momentum's 8 diagonals measured best on the 400x400 grid).
+    const int warps_per_block = gs_block_threads(false, 0) / 32;
     for (int q = 0; q < 5; ++q) {
         int bps = 0;
         CK(gs_occupancy(il, kinds[q], ctx->model, ctx->ks, v, &bps));
-        ctx->grid_gs[kinds[q]] = std::max(1, bps) * ctx->num_sms;
+        long long blocks = (long long)std::max(1, bps) * ctx->num_sms;
+        const int la = (kinds[q] == PH_PRESSURE) ? std::max(1, ctx->lookahead * 3 / 8) : ctx->lookahead;
+        const long long want_blocks = (long long)std::ceil(la * diag_width / (double)warps_per_block);
+        if (!il && ctx->lookahead > 0) blocks = std::max<long long>(ctx->num_sms, std::min(blocks, want_blocks));
+        ctx->grid_gs[kinds[q]] = (int)blocks;
     }
     const int warps = ctx->grid_gs[PH_PRESSURE] * gs_block_threads(il, v) / 32;
     const long long per_diag = (long long)(il ? ctx->ngroups : ctx->nb) * std::min(ctx->nii, ctx->njj);
@@ -429,6 +443,7 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
         else if (std::strcmp(lay, "slab") == 0) ctx->il_min_batch = 1 << 30;
     }
     if (const char *v = std::getenv("GRAL_PROG_BATCH_VARIANT")) ctx->forced_variant = std::atoi(v);
+    if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD")) ctx->lookahead = std::max(0, std::atoi(v));
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
     for (auto &e : ctx->ev)
@@ -476,6 +491,28 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     rc = build_meta(ctx, p0, *s, meta, cfl, colf, colke, vi_min, vi_max);
     if (rc != GRAL_OK) return rc;
     if (vi_max + 1 >= ks) return fail(ctx, GRAL_EINVAL, "VerticalIndex above KADVMAX");
+
+    // ---- row-carry writers of the pressure sweep ----
+    // A column of the pressure sweep row j writes the carry at levels max(KKART, vi_min) < k <= VI
+    // (PrognosticFlowfield.cs:865-880); the column reading level VI+1 gets it from the last such
+    // writer before it in sweep order, or the zeroed buffer when there is none.
+    std::vector<short2> rcw(ncols, make_short2(-1, -1));
+    {
+        std::vector<int> last(ks + 1);
+        for (int dir = 0; dir < 2; ++dir)
+            for (int j = 2; j <= NJJ - 1; ++j) {
+                std::fill(last.begin(), last.end(), -1);
+                for (int q = 2; q <= NII - 1; ++q) {
+                    const int i = (dir == 0) ? q : NII + 1 - q;
+                    const int c = i * nj2 + j;
+                    const int VI = meta[c].vi, KK = meta[c].kkart;
+                    const short w = (short)((VI + 1 <= ks) ? last[VI + 1] : -1);
+                    if (dir == 0) rcw[c].x = w; else rcw[c].y = w;
+                    if (cfl[c] & F_ADV)
+                        for (int k = std::max(KK, vi_min) + 1; k <= VI && k <= ks; ++k) last[k] = i;
+                }
+            }
+    }
 
     // ---- level tables (float, reference expressions) ----
     const float DXK = p0.dxk, DYK = p0.dyk, AREA = DXK * DYK;
@@ -599,6 +636,7 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(ctx->meta.ensure(ncols));
     CK(ctx->cflags.ensure(ncols));
     CK(ctx->colf.ensure(ncols));
+    CK(ctx->rcw.ensure(ncols));
     if (ctx->model != 1) {
         CK(ctx->colke.ensure(ncols));
         CK(ctx->varw.ensure((size_t)n * ncols));
@@ -647,6 +685,7 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     a.flags = ctx->flags.p;
     a.counters = ctx->counters.p;
     a.rowcarry = ctx->rowcarry.p;
+    a.rcw = ctx->rcw.p;
     a.err = ctx->misc.p;
     a.nact = ctx->misc.p + 1;
     a.it_global = ctx->misc.p + 2;
@@ -691,6 +730,7 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemcpyAsync(ctx->meta.p, meta.data(), ncols * sizeof(ColMeta), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->cflags.p, cfl.data(), ncols * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->colf.p, colf.data(), ncols * sizeof(ColF), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->rcw.p, rcw.data(), ncols * sizeof(short2), cudaMemcpyHostToDevice, st));
     if (ctx->model != 1) {
         CK(cudaMemcpyAsync(ctx->colke.p, colke.data(), ncols * sizeof(ColKE), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->varw.p, varw.data(), varw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
