@@ -163,9 +163,9 @@ __device__ __forceinline__ void mom_sweep(Rows &R, int K0, int KK, int VI, int k
         }
         return;
     }
-    float P = 0.0f, Q = 0.0f;
-    for (int k = K0; k <= VI; ++k) {
-        const float A = R.a(k), B = R.b(k), C = R.c(k), D = R.d(k);
+    // float recurrences, eight levels per step (operands loaded together, arithmetic chain serial)
+    constexpr int CH = 8;
+    auto level = [&](int k, float A, float B, float C, float D, float &P, float &Q) {
         if (k > KK + 1) {
             if (MODEL == 1) {
                 const float T = 1.0f / (A - C * P);
@@ -186,11 +186,44 @@ __device__ __forceinline__ void mom_sweep(Rows &R, int K0, int KK, int VI, int k
                 Q = D / A;
             }
         }
+    };
+    float P = 0.0f, Q = 0.0f;
+    int k = K0;
+    for (; k + CH - 1 <= VI; k += CH) {
+        float A[CH], B[CH], C[CH], D[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) { A[q] = R.a(k + q); B[q] = R.b(k + q); C[q] = R.c(k + q); D[q] = R.d(k + q); }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            level(k + q, A[q], B[q], C[q], D[q], P, Q);
+            B[q] = P;
+            D[q] = Q;
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) { R.b(k + q) = B[q]; R.d(k + q) = D[q]; }
+    }
+    for (; k <= VI; ++k) {
+        level(k, R.a(k), R.b(k), R.c(k), R.d(k), P, Q);
         R.b(k) = P;
         R.d(k) = Q;
     }
     float up = top;
-    for (int k = VI; k >= K0; --k) {
+    k = VI;
+    for (; k - (CH - 1) >= K0; k -= CH) {
+        float Pv[CH], Qv[CH], U[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) { Pv[q] = R.b(k - q); Qv[q] = R.d(k - q); U[q] = R.p(k - q); }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            float u = U[q];
+            if (kkm < k - q) u += relax * (Pv[q] * up + Qv[q] - u);
+            U[q] = u;
+            up = u;
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) R.p(k - q) = U[q];
+    }
+    for (; k >= K0; --k) {
         float u = R.p(k);
         if (kkm < k) {
             u += relax * (R.b(k) * up + R.d(k) - u);

@@ -65,6 +65,7 @@ struct gral_ctx {
     int il_min_batch = 32;
     int forced_variant = -1;   // GRAL_PROG_BATCH_VARIANT
     int lookahead = 8;         // GRAL_PROG_LOOKAHEAD: plain-family warps per average diagonal width
+    int lookahead_p = 3;       // GRAL_PROG_LOOKAHEAD_P: the same for the pressure sweep
     int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
     std::string err = "no error";
 
@@ -353,16 +354,14 @@ int size_grids(gral_ctx *ctx) {
     // polling far-future flags (0 = as many as fit).
     const double diag_width = (double)ctx->nb * (double)(ctx->nii - 3) * (double)(ctx->njj - 3) /
                               (double)std::max(1, ctx->nii + ctx->njj - 7);
-    // The pressure sweep reads the row carry speculatively before its wait; a shallower lookahead
-    // keeps that read fresh (3 of the momentum's 8 diagonals measured best on the 400x400 grid).
     const int warps_per_block = gs_block_threads(false, 0) / 32;
     for (int q = 0; q < 5; ++q) {
         int bps = 0;
         CK(gs_occupancy(il, kinds[q], ctx->model, ctx->ks, v, &bps));
         long long blocks = (long long)std::max(1, bps) * ctx->num_sms;
-        const int la = (kinds[q] == PH_PRESSURE) ? std::max(1, ctx->lookahead * 3 / 8) : ctx->lookahead;
+        const int la = (kinds[q] == PH_PRESSURE) ? ctx->lookahead_p : ctx->lookahead;
         const long long want_blocks = (long long)std::ceil(la * diag_width / (double)warps_per_block);
-        if (!il && ctx->lookahead > 0) blocks = std::max<long long>(ctx->num_sms, std::min(blocks, want_blocks));
+        if (!il && la > 0) blocks = std::max<long long>(ctx->num_sms, std::min(blocks, want_blocks));
         ctx->grid_gs[kinds[q]] = (int)blocks;
     }
     const int warps = ctx->grid_gs[PH_PRESSURE] * gs_block_threads(il, v) / 32;
@@ -444,6 +443,7 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
     }
     if (const char *v = std::getenv("GRAL_PROG_BATCH_VARIANT")) ctx->forced_variant = std::atoi(v);
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD")) ctx->lookahead = std::max(0, std::atoi(v));
+    if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD_P")) ctx->lookahead_p = std::max(0, std::atoi(v));
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
     for (auto &e : ctx->ev)

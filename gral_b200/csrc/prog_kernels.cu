@@ -16,34 +16,49 @@ namespace {
 
 constexpr int COL_WARPS = 8;   // warps per block of the column kernels
 
-template <bool IL>
+// Slab layout: one warp per (situation, column), lanes over levels.  Interleaved layout: one warp
+// per (group, column), lane = situation, looping over the levels -- or, with WIDE, one block per
+// (group, column) whose warps share the levels (more loads in flight for bandwidth-bound bodies).
+template <bool IL, bool WIDE = false>
 inline int col_grid(const KArgs &a) {
-    const long long units = IL ? a.ngroups : a.nb;
-    const long long warps = units * a.ncols;
+    if (IL && WIDE) return a.ngroups * a.ncols;
+    const long long warps = (long long)(IL ? a.ngroups : a.nb) * a.ncols;
     return (int)((warps + COL_WARPS - 1) / COL_WARPS);
 }
 
 // Calls body(s, col, i, j, x, kbeg, kstep) for every active (situation, column): the body loops
 // `for (k = kbeg; k <= hi; k += kstep)` over the levels it needs.
-template <bool IL, class Body>
+template <bool IL, bool WIDE = false, class Body>
 __device__ __forceinline__ void col_loop(const KArgs &a, bool need_active, Body &&body) {
-    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const long long unit = gw / a.ncols;
-    const int col = (int)(gw - unit * a.ncols);
-    int s;
-    if (IL) {
-        if (unit >= a.ngroups) return;
-        s = (int)unit * 32 + lane;
-        if (s >= a.nb) return;
+    int s, col, kbeg, kstep;
+    if (IL && WIDE) {
+        const int unit = blockIdx.x / a.ncols;
+        col = blockIdx.x - unit * a.ncols;
+        s = unit * 32 + lane;
+        if (unit >= a.ngroups || s >= a.nb) return;
+        kbeg = threadIdx.x >> 5;
+        kstep = COL_WARPS;
     } else {
-        if (unit >= *a.nact) return;
-        s = a.act[unit];
+        const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+        const long long unit = gw / a.ncols;
+        col = (int)(gw - unit * a.ncols);
+        if (IL) {
+            s = (int)unit * 32 + lane;
+            if (unit >= a.ngroups || s >= a.nb) return;
+            kbeg = 0;
+            kstep = 1;
+        } else {
+            if (unit >= *a.nact) return;
+            s = a.act[unit];
+            kbeg = lane;
+            kstep = 32;
+        }
     }
     if (need_active && !a.sit[s].active) return;
     const int i = col / a.nj2, j = col - (col / a.nj2) * a.nj2;
     const Acc<IL> x = make_acc<IL>(a, s, col);
-    body(s, col, i, j, x, IL ? 0 : lane, IL ? 1 : 32);
+    body(s, col, i, j, x, kbeg, kstep);
 }
 
 // ---- boundary conditions (PrognosticFlowfield.cs:595-714) ----
@@ -155,7 +170,7 @@ __global__ void k_velcorr(KArgs a) {
         const int q = sd.quantise;
         const long long dW = -(long long)a.nj2;
 #pragma unroll 4
-        for (int k = kbeg; k <= m.vi; k += (IL ? 1 : 32)) {
+        for (int k = kbeg; k <= m.vi; k += kstep) {
             if (k < 1) continue;
             const float d = a.dpm[x.at(0, k)];
             if (i > 2 && m.kkm_u < k)
@@ -174,7 +189,7 @@ __global__ void k_velcorr(KArgs a) {
 // ---- staggered -> cell-centre averages and the border copies (:958-1039) ----
 template <bool IL>
 __global__ void k_average(KArgs a) {
-    col_loop<IL>(a, true, [&](int, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
+    auto body = [&](int, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
         if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
         if (!(a.cflags[col] & F_VC)) return;
         const ColMeta m = a.meta[col];
@@ -184,7 +199,7 @@ __global__ void k_average(KArgs a) {
         const bool cpS = (j == 2);
         const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
 #pragma unroll 4
-        for (int k = kbeg; k <= m.vi; k += (IL ? 1 : 32)) {
+        for (int k = kbeg; k <= m.vi; k += kstep) {
             if (k < m.kstart) continue;
             if (KK < k) {
                 a.uks[x.at(0, k)] = 0.5f * (a.uk[x.at(0, k)] + a.uk[x.at(dE, k)]);
@@ -200,9 +215,10 @@ __global__ void k_average(KArgs a) {
         if (west || east) {
             const long long dd = west ? -(long long)nj2 : dE;
 #pragma unroll 4
-            for (int k = kbeg; k < a.ks; k += (IL ? 1 : 32)) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
+            for (int k = kbeg; k < a.ks; k += kstep) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
         }
-    });
+    };
+    col_loop<IL, true>(a, true, body);
 }
 
 // ---- convergence bookkeeping (:1144-1178), one thread per situation ----
@@ -405,7 +421,10 @@ void launch_bc(const KArgs &a, const BcLists &bc, cudaStream_t st) {
 
 void launch_velcorr(const KArgs &a, cudaStream_t st) { GRAL_COL_LAUNCH(k_velcorr, a); }
 
-void launch_average(const KArgs &a, cudaStream_t st) { GRAL_COL_LAUNCH(k_average, a); }
+void launch_average(const KArgs &a, cudaStream_t st) {
+    if (a.il) k_average<true><<<col_grid<true, true>(a), COL_WARPS * 32, 0, st>>>(a);
+    else k_average<false><<<col_grid<false>(a), COL_WARPS * 32, 0, st>>>(a);
+}
 
 void launch_bookkeeping(const KArgs &a, cudaStream_t st) {
     k_bookkeeping<<<(a.nb + 127) / 128, 128, 0, st>>>(a);

@@ -98,18 +98,17 @@ __device__ __forceinline__ float pl_coef(float D, float Pe, float Fs) {
     return D * vmaxf(0.0f, in * in * in * in * in) + vmaxf(Fs, 0.0f);
 }
 
-// Mixing-length eddy viscosity of level k (U-prognostic-microscale_1.cs:239-268); zero at and
-// below KKART+1 (the reference masks those lanes).
-template <bool IL>
-__device__ __forceinline__ float ml_vis(const KArgs &a, const Acc<IL> &x, const ColCtx &c, int k, float dz,
-                                        float ukp, float ukm) {
+// Mixing-length eddy viscosity of level k (U-prognostic-microscale_1.cs:239-268) from the column's
+// U and V at k+1 and k-1; zero at and below KKART+1 (the reference masks those lanes).
+__device__ __forceinline__ float ml_vis(const KArgs &a, const ColCtx &c, int k, float dz, float ukp, float ukm,
+                                        float vkp, float vkm) {
     if (k <= c.KK + 1) return 0.0f;
     const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
     float mixL = vminf(0.071f * zs, 100.0f);
     if (c.cf.cov > 0) mixL *= (1.0f - 0.99f * c.cf.cov);
     float in = (ukp - ukm) / (2.0f * dz);
     const float DUDZ = in * in;
-    in = (a.vk[x.at(0, k + 1)] - a.vk[x.at(0, k - 1)]) / (2.0f * dz);
+    in = (vkp - vkm) / (2.0f * dz);
     const float DVDZ = in * in;
     return vminf(mixL * mixL * sqrtf(0.5f * (DUDZ + DVDZ)), 15.0f);
 }
@@ -154,15 +153,28 @@ struct MomPre {
     float hz;                    // DYK*DZK (U) or DXK*DZK (V)
 };
 
-// U momentum (U-prognostic-microscale_1.cs:205-470).
+// U momentum (U-prognostic-microscale_1.cs:205-470).  All operands of the level are loaded first,
+// unconditionally (every address lies inside the padded grid and levels 0..KS-1), so a level costs
+// one memory round trip; the arithmetic follows in the reference's order.
 template <bool IL>
 __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const float uk = __ldcg(a.uk + x.at(0, k));
+    const float ukp = __ldcg(a.uk + x.at(0, k + 1)), ukm = __ldcg(a.uk + x.at(0, k - 1));
+    const float vkp = a.vk[x.at(0, k + 1)], vkm = a.vk[x.at(0, k - 1)];
+    const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
+    const float uksW = a.uks[x.at(W, k)], vksW = a.vks[x.at(W, k)], vksWS = a.vks[x.at(W + S, k)];
+    const float vksS = a.vks[x.at(S, k)], vksWN = a.vks[x.at(W + N, k)], vksN = a.vks[x.at(N, k)];
+    const float wksW = a.wks[x.at(W, k)], wksWT = a.wks[x.at(W, k + 1)], wksT = a.wks[x.at(0, k + 1)];
+    const float wksB = a.wks[x.at(0, k - 1)], wksWB = a.wks[x.at(W, k - 1)];
+    const float dpW = a.dpmnew[x.at(W, k)], dp0 = a.dpmnew[x.at(0, k)];
+    const float vksEN = a.vks[x.at(E + N, k)], vksES = a.vks[x.at(E + S, k)];
+    const float wkE = a.wk[x.at(E, k)], wkEB = a.wk[x.at(E, k - 1)];
+    const float ap0 = sc.ap0[k];
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     const float dxdz = DXK * dz, dydz = DYK * dz;
-    const float uk = __ldcg(a.uk + x.at(0, k));
-    const float VIS = ml_vis(a, x, c, k, dz, __ldcg(a.uk + x.at(0, k + 1)), __ldcg(a.uk + x.at(0, k - 1)));
+    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -174,16 +186,11 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
     if (c.fl & F_BN) DN = 0.0f;
     if (c.fl & F_BW) DW = 0.0f;
     if (c.fl & F_BE) DE = 0.0f;
-    const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
-    const float uksW = a.uks[x.at(W, k)], vksW = a.vks[x.at(W, k)], vksWS = a.vks[x.at(W + S, k)];
-    const float vksS = a.vks[x.at(S, k)], vksWN = a.vks[x.at(W + N, k)], vksN = a.vks[x.at(N, k)];
-    const float wksW = a.wks[x.at(W, k)];
     const float FE = uks * dydz;
     const float FW = uksW * dydz;
     const float FS = 0.25f * (vksW + vks + vksWS + vksS) * dxdz;
     const float FN = 0.25f * (vksW + vks + vksWN + vksN) * dxdz;
-    const float FT = 0.25f * (wksW + wks + a.wks[x.at(W, k + 1)] + a.wks[x.at(0, k + 1)]) * AREA;
-    const float wksB = a.wks[x.at(0, k - 1)], wksWB = a.wks[x.at(W, k - 1)];
+    const float FT = 0.25f * (wksW + wks + wksWT + wksT) * AREA;
     const float FB = (k > c.KK + 1) ? 0.25f * (wksW + wks + wksWB + wksB) * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
@@ -194,9 +201,8 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
     r.aw = pl_coef(DW, fabsf(FW / DW), FW);
     r.as = pl_coef(DS, fabsf(FS / DS), FS);
     r.an = pl_coef(DN, fabsf(FN / DN), -FN);
-    const float ap0 = sc.ap0[k];
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
-    const float DDPX = a.dpmnew[x.at(W, k)] - a.dpmnew[x.at(0, k)];
+    const float DDPX = dpW - dp0;
     r.t1 = ap0 * 0.5f * (uksW + uks);
     r.t2 = DDPX * dydz;
     if (c.fl & F_VEG) {
@@ -217,10 +223,10 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
     r.vdx = VIS / DXK;
     r.hz = dydz;
     if (k >= c.kad) {                                      // extra eddy-viscosity terms, :453-470
-        r.e0 = (0.5f * (a.vks[x.at(E + N, k)] + vksN) - 0.5f * (vksN + vksWN)) * dxdz;        // DVDXN
-        r.e1 = (0.5f * (a.vks[x.at(E + S, k)] + vksS) - 0.5f * (vksS + vksWS)) * dxdz;        // DVDXS
-        r.e2 = (0.5f * (a.wk[x.at(E, k)] + wks) - 0.5f * (wks + wksW)) * AREA;                // DWDXT
-        r.e3 = (0.5f * (a.wk[x.at(E, k - 1)] + wksB) - 0.5f * (wksB + wksWB)) * AREA;         // DWDXB
+        r.e0 = (0.5f * (vksEN + vksN) - 0.5f * (vksN + vksWN)) * dxdz;        // DVDXN
+        r.e1 = (0.5f * (vksES + vksS) - 0.5f * (vksS + vksWS)) * dxdz;        // DVDXS
+        r.e2 = (0.5f * (wkE + wks) - 0.5f * (wks + wksW)) * AREA;             // DWDXT
+        r.e3 = (0.5f * (wkEB + wksB) - 0.5f * (wksB + wksWB)) * AREA;         // DWDXB
     }
     r.phi = uk;
     return r;
@@ -238,25 +244,26 @@ __device__ __forceinline__ float u1_post(const MomPre &p, const ColCtx &c, int k
     return DIM;
 }
 
-// V momentum (V-prognostic-microscale_1.cs:205-488).
+// V momentum (V-prognostic-microscale_1.cs:205-488); operands first, as u1_pre.
 template <bool IL>
 __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const float vk = __ldcg(a.vk + x.at(0, k));
+    const float ukp = a.uk[x.at(0, k + 1)], ukm = a.uk[x.at(0, k - 1)];
+    const float vkp = __ldcg(a.vk + x.at(0, k + 1)), vkm = __ldcg(a.vk + x.at(0, k - 1));
+    const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
+    const float uksE = a.uks[x.at(E, k)], uksS = a.uks[x.at(S, k)], uksES = a.uks[x.at(E + S, k)];
+    const float uksW = a.uks[x.at(W, k)], vksW = a.vks[x.at(W, k)], uksWS = a.uks[x.at(W + S, k)];
+    const float vksS = a.vks[x.at(S, k)], wksS = a.wks[x.at(S, k)], wksB = a.wks[x.at(0, k - 1)];
+    const float wksST = a.wks[x.at(S, k + 1)], wksT = a.wks[x.at(0, k + 1)], wksSB = a.wks[x.at(S, k - 1)];
+    const float dpS = a.dpmnew[x.at(S, k)], dp0 = a.dpmnew[x.at(0, k)];
+    const float uksEN = a.uks[x.at(E + N, k)], uksWN = a.uks[x.at(W + N, k)];
+    const float wkN = a.wk[x.at(N, k)], wkNB = a.wk[x.at(N, k - 1)];
+    const float ap0 = sc.ap0[k];
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     const float dxdz = DXK * dz, dydz = DYK * dz;
-    const float vk = __ldcg(a.vk + x.at(0, k));
-    float VIS = 0.0f;
-    if (k > c.KK + 1) {
-        const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
-        float mixL = vminf(0.071f * zs, 100.0f);
-        if (c.cf.cov > 0) mixL *= (1.0f - 0.99f * c.cf.cov);
-        float in = (a.uk[x.at(0, k + 1)] - a.uk[x.at(0, k - 1)]) / (2.0f * dz);
-        const float DUDZ = in * in;
-        in = (__ldcg(a.vk + x.at(0, k + 1)) - __ldcg(a.vk + x.at(0, k - 1))) / (2.0f * dz);
-        const float DVDZ = in * in;
-        VIS = vminf(mixL * mixL * sqrtf(0.5f * (DUDZ + DVDZ)), 15.0f);
-    }
+    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -268,16 +275,12 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
     if (c.fl & F_BN) DN = 0.0f;
     if (c.fl & F_BW) DW = 0.0f;
     if (c.fl & F_BE) DE = 0.0f;
-    const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
-    const float uksE = a.uks[x.at(E, k)], uksS = a.uks[x.at(S, k)], uksES = a.uks[x.at(E + S, k)];
-    const float uksW = a.uks[x.at(W, k)], vksW = a.vks[x.at(W, k)], uksWS = a.uks[x.at(W + S, k)];
-    const float vksS = a.vks[x.at(S, k)], wksS = a.wks[x.at(S, k)], wksB = a.wks[x.at(0, k - 1)];
     const float FE = 0.25f * (uks + uksE + uksS + uksES) * dydz;
     const float FW = 0.25f * (uks + uksW + uksS + uksWS) * dydz;
     const float FS = vksS * dxdz;
     const float FN = vks * dxdz;
-    const float FT = 0.25f * (wksS + wks + a.wks[x.at(S, k + 1)] + a.wks[x.at(0, k + 1)]) * AREA;
-    const float FB = (k > c.KK + 1) ? 0.25f * (wksS + wks + a.wks[x.at(S, k - 1)] + wksB) * AREA : 0.0f;
+    const float FT = 0.25f * (wksS + wks + wksST + wksT) * AREA;
+    const float FB = (k > c.KK + 1) ? 0.25f * (wksS + wks + wksSB + wksB) * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
     MomPre r;
@@ -287,9 +290,8 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
     r.aw = pl_coef(DW, fabsf(FW / DW), FW);
     r.as = pl_coef(DS, fabsf(FS / DS), FS);
     r.an = pl_coef(DN, fabsf(FN / DN), -FN);
-    const float ap0 = sc.ap0[k];
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
-    const float DDPY = a.dpmnew[x.at(S, k)] - a.dpmnew[x.at(0, k)];
+    const float DDPY = dpS - dp0;
     r.t1 = ap0 * 0.5f * (vksS + vks);
     r.t2 = DDPY * dxdz;
     if (c.fl & F_VEG) {
@@ -310,11 +312,11 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
     r.vdx = VIS / DXK;
     r.hz = dxdz;
     if (k >= c.kad) {                                      // :470-488
-        const float DUDYE = (0.5f * (a.uks[x.at(E + N, k)] + uksE) - 0.5f * (uksE + uksES)) * dxdz;
-        const float DUDYW = (0.5f * (a.uks[x.at(W + N, k)] + uksW) - 0.5f * (uksW + uksWS)) * dxdz;
+        const float DUDYE = (0.5f * (uksEN + uksE) - 0.5f * (uksE + uksES)) * dxdz;
+        const float DUDYW = (0.5f * (uksWN + uksW) - 0.5f * (uksW + uksWS)) * dxdz;
         r.e0 = DUDYE - DUDYW;
-        r.e1 = (0.5f * (a.wk[x.at(N, k)] + wks) - 0.5f * (wks + wksS)) * AREA;                // DWDYT
-        r.e2 = (0.5f * (a.wk[x.at(N, k - 1)] + wksB) - 0.5f * (wksB + wksS)) * AREA;          // DWDYB
+        r.e1 = (0.5f * (wkN + wks) - 0.5f * (wks + wksS)) * AREA;                // DWDYT
+        r.e2 = (0.5f * (wkNB + wksB) - 0.5f * (wksB + wksS)) * AREA;             // DWDYB
     }
     r.phi = vk;
     return r;
@@ -333,17 +335,29 @@ __device__ __forceinline__ float v1_post(const MomPre &p, const ColCtx &c, int k
 }
 
 // W momentum (W-prognostic-microscale_1.cs:205-402); its extra viscous term reads only the own
-// column, so it is complete before the wait (e0 = the whole increment).
+// column, so it is complete before the wait (e0 = the whole increment).  Operands first.
 template <bool IL>
 __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
-    const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
-    const float dz = a.dzk[k];
-    const float dxdz = DXK * dz, dydz = DYK * dz;
     const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
     const float uksM = a.uks[x.at(0, k - 1)], vksM = a.vks[x.at(0, k - 1)];
     const float wk = __ldcg(a.wk + x.at(0, k));
-    const float VIS = ml_vis(a, x, c, k, dz, a.uk[x.at(0, k + 1)], a.uk[x.at(0, k - 1)]);
+    const float ukp = a.uk[x.at(0, k + 1)], ukm = a.uk[x.at(0, k - 1)];
+    const float vkp = a.vk[x.at(0, k + 1)], vkm = a.vk[x.at(0, k - 1)];
+    const float uksW = a.uks[x.at(W, k)], uksWB = a.uks[x.at(W, k - 1)];
+    const float vksS = a.vks[x.at(S, k)], vksSB = a.vks[x.at(S, k - 1)];
+    const float uksE = a.uks[x.at(E, k)], uksEB = a.uks[x.at(E, k - 1)];
+    const float vksN = a.vks[x.at(N, k)], vksNB = a.vks[x.at(N, k - 1)];
+    const float wksB = a.wks[x.at(0, k - 1)];
+    const float dpB = a.dpmnew[x.at(0, k - 1)], dp0 = a.dpmnew[x.at(0, k)];
+    const float uksT = a.uks[x.at(0, k + 1)], uksWT = a.uks[x.at(W, k + 1)];
+    const float vksT = a.vks[x.at(0, k + 1)], vksST = a.vks[x.at(S, k + 1)];
+    const float wkT = __ldcg(a.wk + x.at(0, k + 1)), wkB = __ldcg(a.wk + x.at(0, k - 1));
+    const float ap0 = sc.ap0[k];
+    const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
+    const float dz = a.dzk[k];
+    const float dxdz = DXK * dz, dydz = DYK * dz;
+    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -355,14 +369,11 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
     if (c.fl & F_BN) DN = 0.0f;
     if (c.fl & F_BW) DW = 0.0f;
     if (c.fl & F_BE) DE = 0.0f;
-    const float uksW = a.uks[x.at(W, k)], uksWB = a.uks[x.at(W, k - 1)];
-    const float vksS = a.vks[x.at(S, k)], vksSB = a.vks[x.at(S, k - 1)];
-    const float FE = 0.25f * (uks + a.uks[x.at(E, k)] + uksM + a.uks[x.at(E, k - 1)]) * dydz;
+    const float FE = 0.25f * (uks + uksE + uksM + uksEB) * dydz;
     const float FW = 0.25f * (uks + uksW + uksM + uksWB) * dydz;
     const float FS = 0.25f * (vks + vksS + vksM + vksSB) * dxdz;
-    const float FN = 0.25f * (vks + a.vks[x.at(N, k)] + vksM + a.vks[x.at(N, k - 1)]) * dxdz;
+    const float FN = 0.25f * (vks + vksN + vksM + vksNB) * dxdz;
     const float FT = wks * AREA;
-    const float wksB = a.wks[x.at(0, k - 1)];
     const float FB = (k > c.KK + 1) ? wksB * AREA : 0.0f;
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
@@ -373,9 +384,8 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
     r.aw = pl_coef(DW, fabsf(FW / DW), FW);
     r.as = pl_coef(DS, fabsf(FS / DS), FS);
     r.an = pl_coef(DN, fabsf(FN / DN), -FN);
-    const float ap0 = sc.ap0[k];
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
-    const float DDPZ = a.dpmnew[x.at(0, k - 1)] - a.dpmnew[x.at(0, k)];
+    const float DDPZ = dpB - dp0;
     r.t1 = ap0 * 0.5f * (wksB + wks);
     r.t2 = DDPZ * AREA;
     r.t3 = 0.0f;
@@ -385,12 +395,12 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
         r.t3 = a.veg[(size_t)c.col * a.ks + k - 1] * wk * wh * AREA * dz;     // subtracted
     }
     if (k >= c.kad) {                                      // :376-402
-        const float DUDZE = (0.5f * (a.uks[x.at(0, k + 1)] + uks) - 0.5f * (uks + uksM)) * dydz;
-        const float DUDZW = (0.5f * (a.uks[x.at(W, k + 1)] + uksW) - 0.5f * (uksW + uksWB)) * dydz;
-        const float DVDZN = (0.5f * (a.vks[x.at(0, k + 1)] + vks) - 0.5f * (vks + vksM)) * dxdz;
-        const float DVDZS = (0.5f * (a.vks[x.at(S, k + 1)] + vksS) - 0.5f * (vksS + vksSB)) * dxdz;
-        const float DWDZT = (__ldcg(a.wk + x.at(0, k + 1)) - wk) * AREA;
-        const float DWDZB = (wk - __ldcg(a.wk + x.at(0, k - 1))) * AREA;
+        const float DUDZE = (0.5f * (uksT + uks) - 0.5f * (uks + uksM)) * dydz;
+        const float DUDZW = (0.5f * (uksWT + uksW) - 0.5f * (uksW + uksWB)) * dydz;
+        const float DVDZN = (0.5f * (vksT + vks) - 0.5f * (vks + vksM)) * dxdz;
+        const float DVDZS = (0.5f * (vksST + vksS) - 0.5f * (vksS + vksSB)) * dxdz;
+        const float DWDZT = (wkT - wk) * AREA;
+        const float DWDZB = (wk - wkB) * AREA;
         r.e0 = VIS / dz * (DUDZE - DUDZW + DVDZN - DVDZS + DWDZT - DWDZB);
     }
     r.phi = wk;
@@ -450,15 +460,15 @@ template <bool IL>
 __device__ __forceinline__ float pressure_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc,
                                               int k) {
     const long long E = c.nj2, N = 1;
+    const float u0 = a.uk[x.at(0, k)], uE = a.uk[x.at(E, k)], v0 = a.vk[x.at(0, k)], vN = a.vk[x.at(N, k)];
+    const float w0 = a.wk[x.at(0, k)], wT = a.wk[x.at(0, k + 1)];
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     float DIV;
     if (k > c.KK + 1)
-        DIV = (a.uk[x.at(0, k)] - a.uk[x.at(E, k)]) * DYK * dz + (a.vk[x.at(0, k)] - a.vk[x.at(N, k)]) * DXK * dz +
-              (a.wk[x.at(0, k)] - a.wk[x.at(0, k + 1)]) * AREA;
+        DIV = (u0 - uE) * DYK * dz + (v0 - vN) * DXK * dz + (w0 - wT) * AREA;
     else
-        DIV = (a.uk[x.at(0, k)] - a.uk[x.at(E, k)]) * DYK * dz + (a.vk[x.at(0, k)] - a.vk[x.at(N, k)]) * DXK * dz -
-              a.wk[x.at(0, k + 1)] * AREA;
+        DIV = (u0 - uE) * DYK * dz + (v0 - vN) * DXK * dz - wT * AREA;
     return DIV / sc.dtime;
 }
 
