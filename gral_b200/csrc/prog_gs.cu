@@ -584,9 +584,9 @@ struct Mom1Job {
             if (k < c.K0 || k > c.VI) continue;
             float nW, nS, nE, nN;
             nbr4(F, x, c, k, nW, nS, nE, nN);
-            if (COMP == COMP_U) S[3][k] = u1_post(p[r], c, k, nW, nS, nE, nN);
-            else if (COMP == COMP_V) S[3][k] = v1_post(p[r], c, k, nW, nS, nE, nN);
-            else S[3][k] = w1_post(p[r], c, k, nW, nS, nE, nN);
+            if (COMP == COMP_U) S[3][k] = u1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
+            else if (COMP == COMP_V) S[3][k] = v1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
+            else S[3][k] = w1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
         }
         __syncwarp();
         const int kkm = back_limit<COMP>(c);

@@ -287,8 +287,8 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
     if (p0.kadvmax < 2 || p0.kadvmax + 2 > KMAX_LEVELS || p0.kadvmax > p0.nkk)
         return fail(ctx, GRAL_EINVAL, "KADVMAX outside 2..62 or above NKK");
     if (p0.turbulence_model < 0 || p0.turbulence_model > 2) return fail(ctx, GRAL_EINVAL, "turbulence_model must be 0, 1 or 2");
-    if (p0.turbulence_model == 1 && p0.simd_width != 8)
-        return fail(ctx, GRAL_EINVAL, "simd_width must be 8 (Vector<float> path)");
+    if (p0.turbulence_model == 1 && p0.simd_width != 8 && p0.simd_width != 16)
+        return fail(ctx, GRAL_EINVAL, "simd_width must be 8 (Vector<float> path) or 16 (Vector512 path)");
     for (int b = 0; b < n; ++b) {
         const gral_params &q = p[b];
         if (q.nii != p0.nii || q.njj != p0.njj || q.nkk != p0.nkk || q.kadvmax != p0.kadvmax ||

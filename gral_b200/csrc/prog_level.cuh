@@ -92,18 +92,29 @@ struct Coef {
     float A, B, C, D, phi;
 };
 
-// Patankar power law of one face, Vector<float> association order (U-prognostic-microscale_1.cs:348-370).
+// Patankar power law of one face, Vector<float> association order (U-prognostic-microscale_1.cs:348-370);
+// the Vector512 twins fuse the outer multiply-add and square twice
+// (U-prognostic-microscale_1_Vec512.cs:355-377).
 __device__ __forceinline__ float pl_coef(float D, float Pe, float Fs) {
     const float in = 1.0f - 0.1f * Pe;
     return D * vmaxf(0.0f, in * in * in * in * in) + vmaxf(Fs, 0.0f);
 }
+__device__ __forceinline__ float pl_coef512(float D, float Pe, float Fs) {
+    const float in = 1.0f - 0.1f * Pe;
+    return fmaf(D, vmaxf(0.0f, in * ((in * in) * (in * in))), vmaxf(Fs, 0.0f));
+}
+__device__ __forceinline__ float pl1(bool v512, float D, float Pe, float Fs) {
+    return v512 ? pl_coef512(D, Pe, Fs) : pl_coef(D, Pe, Fs);
+}
 
 // Mixing-length eddy viscosity of level k (U-prognostic-microscale_1.cs:239-268) from the column's
 // U and V at k+1 and k-1; zero at and below KKART+1 (the reference masks those lanes).
+// The Vector512 twins take the height above KKART as HOKART[k] - fma(DZK, 0.5, HOKART[KKART])
+// (U-prognostic-microscale_1_Vec512.cs:218).
 __device__ __forceinline__ float ml_vis(const KArgs &a, const ColCtx &c, int k, float dz, float ukp, float ukm,
                                         float vkp, float vkm) {
     if (k <= c.KK + 1) return 0.0f;
-    const float zs = a.hokart[k] - c.hokK - dz * 0.5f;
+    const float zs = (a.simd == 16) ? a.hokart[k] - fmaf(dz, 0.5f, c.hokK) : a.hokart[k] - c.hokK - dz * 0.5f;
     float mixL = vminf(0.071f * zs, 100.0f);
     if (c.cf.cov > 0) mixL *= (1.0f - 0.99f * c.cf.cov);
     float in = (ukp - ukm) / (2.0f * dz);
@@ -159,6 +170,7 @@ struct MomPre {
 template <bool IL>
 __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const bool v512 = (a.simd == 16);
     const float uk = __ldcg(a.uk + x.at(0, k));
     const float ukp = __ldcg(a.uk + x.at(0, k + 1)), ukm = __ldcg(a.uk + x.at(0, k - 1));
     const float vkp = a.vk[x.at(0, k + 1)], vkm = a.vk[x.at(0, k - 1)];
@@ -195,16 +207,16 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
     MomPre r;
-    r.B = pl_coef(DT, fabsf(FT / DT), -FT);
-    r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
-    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
-    r.as = pl_coef(DS, fabsf(FS / DS), FS);
-    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.B = pl1(v512, DT, fabsf(FT / DT), -FT);
+    r.C = pl1(v512, DB, fabsf(FB / DB), FB);
+    r.ae = pl1(v512, DE, fabsf(FE / DE), -FE);
+    r.aw = pl1(v512, DW, fabsf(FW / DW), FW);
+    r.as = pl1(v512, DS, fabsf(FS / DS), FS);
+    r.an = pl1(v512, DN, fabsf(FN / DN), -FN);
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPX = dpW - dp0;
     r.t1 = ap0 * 0.5f * (uksW + uks);
-    r.t2 = DDPX * dydz;
+    r.t2 = (v512 && !(c.fl & F_VEG)) ? DDPX : DDPX * dydz;     // Vector512: fma(DDPX, DYKDZK, ...)
     if (c.fl & F_VEG) {
         const float in2 = 0.5f * (vksW + vks), in = 0.5f * (uksW + uks);
         const float wh = vmaxf(sqrtf(in * in + in2 * in2), 0.01f);
@@ -233,8 +245,14 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
 }
 
 __device__ __forceinline__ float u1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
-                                         float nN) {
-    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
+                                         float nN, bool v512) {
+    float DIM;
+    if (v512) {   // U-prognostic-microscale_1_Vec512.cs:399-421
+        const float S1 = fmaf(p.aw, nW, p.as * nS), S2 = fmaf(p.ae, nE, p.an * nN);
+        DIM = (c.fl & F_VEG) ? S1 + S2 + p.t1 + p.t2 + p.t3 : S1 + S2 + p.t1 + fmaf(p.t2, p.hz, p.t3);
+    } else {
+        DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
+    }
     if (k >= c.wlo && k <= c.whi) DIM -= p.w;
     if (k >= c.kad) {
         const float DUDXE = (nE - p.phi) * p.hz;
@@ -248,6 +266,7 @@ __device__ __forceinline__ float u1_post(const MomPre &p, const ColCtx &c, int k
 template <bool IL>
 __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const bool v512 = (a.simd == 16);
     const float vk = __ldcg(a.vk + x.at(0, k));
     const float ukp = a.uk[x.at(0, k + 1)], ukm = a.uk[x.at(0, k - 1)];
     const float vkp = __ldcg(a.vk + x.at(0, k + 1)), vkm = __ldcg(a.vk + x.at(0, k - 1));
@@ -284,12 +303,12 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
     MomPre r;
-    r.B = pl_coef(DT, fabsf(FT / DT), -FT);
-    r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
-    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
-    r.as = pl_coef(DS, fabsf(FS / DS), FS);
-    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.B = pl1(v512, DT, fabsf(FT / DT), -FT);
+    r.C = pl1(v512, DB, fabsf(FB / DB), FB);
+    r.ae = pl1(v512, DE, fabsf(FE / DE), -FE);
+    r.aw = pl1(v512, DW, fabsf(FW / DW), FW);
+    r.as = pl1(v512, DS, fabsf(FS / DS), FS);
+    r.an = pl1(v512, DN, fabsf(FN / DN), -FN);
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPY = dpS - dp0;
     r.t1 = ap0 * 0.5f * (vksS + vks);
@@ -323,8 +342,12 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
 }
 
 __device__ __forceinline__ float v1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
-                                         float nN) {
-    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
+                                         float nN, bool v512) {
+    float DIM;
+    if (v512 && (c.fl & F_VEG))   // V-prognostic-microscale_1_Vec512.cs:404-410 (plain sums without vegetation)
+        DIM = fmaf(p.aw, nW, p.as * nS) + fmaf(p.ae, nE, p.an * nN) + p.t1 + p.t2 + p.t3;
+    else
+        DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2 + p.t3;
     if (k >= c.wlo && k <= c.whi) DIM -= p.w;
     if (k >= c.kad) {
         const float DVDYN = (nN - p.phi) * p.hz;
@@ -339,6 +362,7 @@ __device__ __forceinline__ float v1_post(const MomPre &p, const ColCtx &c, int k
 template <bool IL>
 __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
+    const bool v512 = (a.simd == 16);
     const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
     const float uksM = a.uks[x.at(0, k - 1)], vksM = a.vks[x.at(0, k - 1)];
     const float wk = __ldcg(a.wk + x.at(0, k));
@@ -378,12 +402,12 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
     DE = vmaxf(DE, 0.0001f); DB = vmaxf(DB, 0.0001f); DW = vmaxf(DW, 0.0001f);
     DS = vmaxf(DS, 0.0001f); DN = vmaxf(DN, 0.0001f); DT = vmaxf(DT, 0.0001f);
     MomPre r;
-    r.B = pl_coef(DT, fabsf(FT / DT), -FT);
-    r.C = pl_coef(DB, fabsf(FB / DB), FB);
-    r.ae = pl_coef(DE, fabsf(FE / DE), -FE);
-    r.aw = pl_coef(DW, fabsf(FW / DW), FW);
-    r.as = pl_coef(DS, fabsf(FS / DS), FS);
-    r.an = pl_coef(DN, fabsf(FN / DN), -FN);
+    r.B = pl1(v512, DT, fabsf(FT / DT), -FT);
+    r.C = pl1(v512, DB, fabsf(FB / DB), FB);
+    r.ae = pl1(v512, DE, fabsf(FE / DE), -FE);
+    r.aw = pl1(v512, DW, fabsf(FW / DW), FW);
+    r.as = pl1(v512, DS, fabsf(FS / DS), FS);
+    r.an = pl1(v512, DN, fabsf(FN / DN), -FN);
     r.A = r.B + r.C + r.aw + r.as + r.ae + r.an + ap0;
     const float DDPZ = dpB - dp0;
     r.t1 = ap0 * 0.5f * (wksB + wks);
@@ -408,8 +432,9 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
 }
 
 __device__ __forceinline__ float w1_post(const MomPre &p, const ColCtx &c, int k, float nW, float nS, float nE,
-                                         float nN) {
-    float DIM = p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2;
+                                         float nN, bool v512) {
+    float DIM = v512 ? fmaf(p.aw, nW, p.as * nS) + fmaf(p.ae, nE, p.an * nN) + p.t1 + p.t2   // W-..._Vec512.cs:367-382
+                     : p.aw * nW + p.as * nS + p.ae * nE + p.an * nN + p.t1 + p.t2;
     if (c.fl & F_VEG) DIM = DIM - p.t3;
     if (k >= c.kad) DIM += p.e0;
     return DIM;
@@ -431,7 +456,7 @@ __device__ __forceinline__ Coef u1_level(const KArgs &a, const Acc<IL> &x, const
     const MomPre p = u1_pre(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.uk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, u1_post(p, c, k, nW, nS, nE, nN), p.phi};
+    return Coef{p.A, p.B, p.C, u1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
 }
 
 template <bool IL>
@@ -439,7 +464,7 @@ __device__ __forceinline__ Coef v1_level(const KArgs &a, const Acc<IL> &x, const
     const MomPre p = v1_pre(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.vk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, v1_post(p, c, k, nW, nS, nE, nN), p.phi};
+    return Coef{p.A, p.B, p.C, v1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
 }
 
 template <bool IL>
@@ -447,7 +472,7 @@ __device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const
     const MomPre p = w1_pre(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.wk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, w1_post(p, c, k, nW, nS, nE, nN), p.phi};
+    return Coef{p.A, p.B, p.C, w1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
 }
 
 // ---------------------------------------------------------------------------------------------

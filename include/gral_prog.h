@@ -52,7 +52,8 @@ typedef struct gral_params {
     int32_t vert_cells_ff;        /* Program.VertCellsFF (micro_vert_layers.txt) */
     float dxk, dyk;               /* Program.DXK/DYK */
     int32_t turbulence_model;     /* 0 no diffusion, 1 mixing length [1], 2 k-eps */
-    int32_t simd_width;           /* model-1 parity width: 8 = Vector<float> path [8] */
+    int32_t simd_width;           /* model-1 parity width: 8 = Vector<float> path [8], 16 = the
+                                     Vector512 routines (Program.UseVector512Class) */
     int32_t iteration_steps_min;  /* [100] Integrationtime.txt line 1 */
     int32_t iteration_steps_max;  /* [500] Integrationtime.txt line 2 */
     int32_t conv_cadence;         /* [100] convergence test every this many iterations */

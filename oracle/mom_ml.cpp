@@ -8,8 +8,12 @@
  * eddy-viscosity term) use the chunk's base index, and the last chunk is pulled back to
  * KEND-SIMD (U-prognostic-microscale_1.cs:194-202).  This file keeps that chunk structure
  * literally, lane by lane, so the per-lane reformulation of the CUDA kernels is checked against
- * the reference's own loop shape.  Only the Vector<float> path (SIMD = 8 on .NET 8 x64) is
- * restated; the Vector512 twins use fused multiply-adds in places and are not covered here.
+ * the reference's own loop shape.  SIMD = 8 is the Vector<float> path (.NET 8 x64, AVX2);
+ * SIMD = 16 is the Vector512 twins (U/V/W-prognostic-microscale_1_Vec512.cs, chosen with
+ * Program.UseVector512Class, PrognosticFlowfield.cs:1072), which keep the same loop but evaluate
+ * a few expressions with fused multiply-adds and another association: the height above KKART
+ * (zs), the power law, and the neighbour sums of DIM (pairs fma(A, x, B*y)); std::fma restates
+ * Avx512F.FusedMultiplyAdd (one rounding).
  */
 #include <algorithm>
 #include <cmath>
@@ -28,11 +32,29 @@ static inline float pl_coef(float D, float Pe, float Fsigned) {
     return D * vmax(0.0f, in * in * in * in * in) + vmax(Fsigned, 0.0f);
 }
 
+/* Vector512 power law: FusedMultiplyAdd(D, Max(0, i*((i*i)*(i*i))), Max(sign*F, 0))
+ * (U-prognostic-microscale_1_Vec512.cs:355-377). */
+static inline float pl_coef512(float D, float Pe, float Fsigned) {
+    float in = 1.0f - 0.1f * Pe;
+    return std::fma(D, vmax(0.0f, in * ((in * in) * (in * in))), vmax(Fsigned, 0.0f));
+}
+
+static inline float pl(bool v512, float D, float Pe, float Fsigned) {
+    return v512 ? pl_coef512(D, Pe, Fsigned) : pl_coef(D, Pe, Fsigned);
+}
+
+/* height of level k above the KKART surface: Vector512 uses HOKART[k] - fma(DZK, 0.5, HOKART[KKART])
+ * (U-prognostic-microscale_1_Vec512.cs:218) */
+static inline float zs_of(bool v512, float hok, float hokK, float dz) {
+    return v512 ? hok - std::fma(dz, 0.5f, hokK) : hok - hokK - dz * 0.5f;
+}
+
 /* ------------------------------------------------------------------------------------------ */
 /* U component, U-prognostic-microscale_1.cs:50-529                                           */
 /* ------------------------------------------------------------------------------------------ */
 void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AREAxy, float UG,
               float relax) {
+    const bool v512 = (SIMD == 16);
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
@@ -86,7 +108,7 @@ void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const int kk = k + l;
                     const float DZK_V = DZK[kk];
                     const float DXKDZK = DXK * DZK_V, DYKDZK = DYK * DZK_V;
-                    const float zs = HOKART[kk] - HOKART_KKART - DZK_V * 0.5f;
+                    const float zs = zs_of(v512, HOKART[kk], HOKART_KKART, DZK_V);
                     float VIS = 0.0f;
                     if ((k + SIMD) > KKART_LL_P1) {
                         float mixL = vmin(0.071f * zs, 100.0f);
@@ -131,19 +153,32 @@ void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const float PE = std::fabs(FE / DE), PB = std::fabs(FB / DB);
                     const float PW = std::fabs(FW / DW), PS = std::fabs(FS / DS);
                     const float PN = std::fabs(FN / DN), PT = std::fabs(FT / DT);
-                    const float BIM = pl_coef(DT, PT, -FT);
-                    const float CIM = pl_coef(DB, PB, FB);
-                    const float AE1 = pl_coef(DE, PE, -FE);
-                    const float AW1 = pl_coef(DW, PW, FW);
-                    const float AS1 = pl_coef(DS, PS, FS);
-                    const float AN1 = pl_coef(DN, PN, -FN);
+                    const float BIM = pl(v512, DT, PT, -FT);
+                    const float CIM = pl(v512, DB, PB, FB);
+                    const float AE1 = pl(v512, DE, PE, -FE);
+                    const float AW1 = pl(v512, DW, PW, FW);
+                    const float AS1 = pl(v512, DS, PS, FS);
+                    const float AN1 = pl(v512, DN, PN, -FN);
                     const float AP0_V = st.ap0[kk];
                     const float AIM = BIM + CIM + AW1 + AS1 + AE1 + AN1 + AP0_V;
 
                     const float DDPX = DPMNEW_W_L[kk] - DPMNEW_L[kk];
                     const float UK_W = UK_W_L[kk], UK_E = UK_E_L[kk], UK_LV = UK_L[kk];
                     float DIM_U;
-                    if (veg) {
+                    if (v512) {   /* U-prognostic-microscale_1_Vec512.cs:399-421 */
+                        const float S1 = std::fma(AW1, UK_W, AS1 * UK_S_L[kk]);
+                        const float S2 = std::fma(AE1, UK_E, AN1 * UK_N_L[kk]);
+                        if (veg) {
+                            float in2 = 0.5f * (VKS_W + VKS_V);
+                            float in = 0.5f * (UKS_W + UKS_V);
+                            float windhilf = vmax(std::sqrt(in * in + in2 * in2), 0.01f);
+                            DIM_U = S1 + S2 + AP0_V * 0.5f * (UKS_W + UKS_V) + DDPX * DYKDZK +
+                                    (Cor * (UG - UK_LV) - VEG_L[kk - 1] * UK_LV * windhilf) * AREAxy * DZK_V;
+                        } else {
+                            DIM_U = S1 + S2 + AP0_V * 0.5f * (UKS_W + UKS_V) +
+                                    std::fma(DDPX, DYKDZK, Cor * (UG - UK_LV) * AREAxy * DZK_V);
+                        }
+                    } else if (veg) {
                         float in2 = 0.5f * (VKS_W + VKS_V);
                         float in = 0.5f * (UKS_W + UKS_V);
                         float windhilf = vmax(std::sqrt(in * in + in2 * in2), 0.01f);
@@ -240,6 +275,7 @@ void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
 /* ------------------------------------------------------------------------------------------ */
 void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AREAxy, float VG,
               float relax) {
+    const bool v512 = (SIMD == 16);
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
@@ -295,7 +331,7 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const float DZK_V = DZK[kk];
                     const float DXKDZK = DXK * DZK_V, DYKDZK = DYK * DZK_V;
                     const float VK_LV = VK_L[kk];
-                    const float zs = HOKART[kk] - HOKART_KKART - DZK_V * 0.5f;
+                    const float zs = zs_of(v512, HOKART[kk], HOKART_KKART, DZK_V);
                     float VIS = 0.0f;
                     if ((k + SIMD) > KKART_LL_P1) {
                         float mixL = vmin(0.071f * zs, 100.0f);
@@ -340,12 +376,12 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const float PE = std::fabs(FE / DE), PB = std::fabs(FB / DB);
                     const float PW = std::fabs(FW / DW), PS = std::fabs(FS / DS);
                     const float PN = std::fabs(FN / DN), PT = std::fabs(FT / DT);
-                    const float BIM = pl_coef(DT, PT, -FT);
-                    const float CIM = pl_coef(DB, PB, FB);
-                    const float AE1 = pl_coef(DE, PE, -FE);
-                    const float AW1 = pl_coef(DW, PW, FW);
-                    const float AS1 = pl_coef(DS, PS, FS);
-                    const float AN1 = pl_coef(DN, PN, -FN);
+                    const float BIM = pl(v512, DT, PT, -FT);
+                    const float CIM = pl(v512, DB, PB, FB);
+                    const float AE1 = pl(v512, DE, PE, -FE);
+                    const float AW1 = pl(v512, DW, PW, FW);
+                    const float AS1 = pl(v512, DS, PS, FS);
+                    const float AN1 = pl(v512, DN, PN, -FN);
                     const float AP0_V = st.ap0[kk];
                     const float AIM = BIM + CIM + AW1 + AS1 + AE1 + AN1 + AP0_V;
 
@@ -356,9 +392,14 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                         float in2 = 0.5f * (VKS_W + VKS_V);
                         float in = 0.5f * (UKS_W + UKS_V);
                         float windhilf = vmax(std::sqrt(in * in + in2 * in2), 0.01f);
-                        DIMV = AW1 * VK_W_L[kk] + AS1 * VK_S + AE1 * VK_E_L[kk] + AN1 * VK_N +
-                               AP0_V * 0.5f * (VKS_S + VKS_V) + DDPY * DXKDZK +
-                               (Cor * (VG - VK_LV) - VEG_L[kk - 1] * VK_LV * windhilf) * AREAxy * DZK_V;
+                        if (v512)   /* V-prognostic-microscale_1_Vec512.cs:404-410; no vegetation: plain sums */
+                            DIMV = std::fma(AW1, VK_W_L[kk], AS1 * VK_S) + std::fma(AE1, VK_E_L[kk], AN1 * VK_N) +
+                                   AP0_V * 0.5f * (VKS_S + VKS_V) + DDPY * DXKDZK +
+                                   (Cor * (VG - VK_LV) - VEG_L[kk - 1] * VK_LV * windhilf) * AREAxy * DZK_V;
+                        else
+                            DIMV = AW1 * VK_W_L[kk] + AS1 * VK_S + AE1 * VK_E_L[kk] + AN1 * VK_N +
+                                   AP0_V * 0.5f * (VKS_S + VKS_V) + DDPY * DXKDZK +
+                                   (Cor * (VG - VK_LV) - VEG_L[kk - 1] * VK_LV * windhilf) * AREAxy * DZK_V;
                     } else {
                         DIMV = AW1 * VK_W_L[kk] + AS1 * VK_S + AE1 * VK_E_L[kk] + AN1 * VK_N +
                                AP0_V * 0.5f * (VKS_S + VKS_V) + DDPY * DXKDZK +
@@ -444,6 +485,7 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
 /* W component, W-prognostic-microscale_1.cs:51-453                                           */
 /* ------------------------------------------------------------------------------------------ */
 void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AREAxy, float relax) {
+    const bool v512 = (SIMD == 16);
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
@@ -492,7 +534,7 @@ void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const float DXKDZK = DXK * DZK_V, DYKDZK = DYK * DZK_V;
                     const float UKS_V = UKS_L[kk], VKS_V = VKS_L[kk], WKS_V = WKS_L[kk];
                     const float UKS_M = UKS_L[kk - 1], VKS_M = VKS_L[kk - 1];
-                    const float zs = HOKART[kk] - HOKART_KKART - DZK_V * 0.5f;
+                    const float zs = zs_of(v512, HOKART[kk], HOKART_KKART, DZK_V);
                     float VIS = 0.0f;
                     if ((k + SIMD) > KKART_LL_P1) {
                         float mixL = vmin(0.071f * zs, 100.0f);
@@ -534,12 +576,12 @@ void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                     const float PE = std::fabs(FE / DE), PB = std::fabs(FB / DB);
                     const float PW = std::fabs(FW / DW), PS = std::fabs(FS / DS);
                     const float PN = std::fabs(FN / DN), PT = std::fabs(FT / DT);
-                    const float BIM = pl_coef(DT, PT, -FT);
-                    const float CIM = pl_coef(DB, PB, FB);
-                    const float AE1 = pl_coef(DE, PE, -FE);
-                    const float AW1 = pl_coef(DW, PW, FW);
-                    const float AS1 = pl_coef(DS, PS, FS);
-                    const float AN1 = pl_coef(DN, PN, -FN);
+                    const float BIM = pl(v512, DT, PT, -FT);
+                    const float CIM = pl(v512, DB, PB, FB);
+                    const float AE1 = pl(v512, DE, PE, -FE);
+                    const float AW1 = pl(v512, DW, PW, FW);
+                    const float AS1 = pl(v512, DS, PS, FS);
+                    const float AN1 = pl(v512, DN, PN, -FN);
                     const float AP0_V = st.ap0[kk];
                     const float AIM = BIM + CIM + AW1 + AS1 + AE1 + AN1 + AP0_V;
 
@@ -550,9 +592,17 @@ void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
                         float in2 = 0.5f * (VKS_S + VKS_V);
                         float in = 0.5f * (UKS_W + UKS_V);
                         float windhilf = vmax(std::sqrt(in * in + in2 * in2), 0.01f);
-                        DIMW = AW1 * WK_W_L[kk] + AS1 * WK_S_L[kk] + AE1 * WK_E_L[kk] + AN1 * WK_N_L[kk] +
-                               AP0_V * 0.5f * (WKS_L[kk - 1] + WKS_V) + DDPZ * AREAxy -
-                               VEG_L[kk - 1] * WK_LV * windhilf * AREAxy * DZK_V;
+                        if (v512)   /* W-prognostic-microscale_1_Vec512.cs:367-372 */
+                            DIMW = std::fma(AW1, WK_W_L[kk], AS1 * WK_S_L[kk]) + std::fma(AE1, WK_E_L[kk], AN1 * WK_N_L[kk]) +
+                                   AP0_V * 0.5f * (WKS_L[kk - 1] + WKS_V) + DDPZ * AREAxy -
+                                   VEG_L[kk - 1] * WK_LV * windhilf * AREAxy * DZK_V;
+                        else
+                            DIMW = AW1 * WK_W_L[kk] + AS1 * WK_S_L[kk] + AE1 * WK_E_L[kk] + AN1 * WK_N_L[kk] +
+                                   AP0_V * 0.5f * (WKS_L[kk - 1] + WKS_V) + DDPZ * AREAxy -
+                                   VEG_L[kk - 1] * WK_LV * windhilf * AREAxy * DZK_V;
+                    } else if (v512) {   /* :377-382 */
+                        DIMW = std::fma(AW1, WK_W_L[kk], AS1 * WK_S_L[kk]) + std::fma(AE1, WK_E_L[kk], AN1 * WK_N_L[kk]) +
+                               AP0_V * 0.5f * (WKS_L[kk - 1] + WKS_V) + DDPZ * AREAxy;
                     } else {
                         DIMW = AW1 * WK_W_L[kk] + AS1 * WK_S_L[kk] + AE1 * WK_E_L[kk] + AN1 * WK_N_L[kk] +
                                AP0_V * 0.5f * (WKS_L[kk - 1] + WKS_V) + DDPZ * AREAxy;

@@ -22,7 +22,7 @@ int validate(const gral_params *p, const gral_static *s, const gral_fields *f) {
     if (p->nii < 4 || p->njj < 4 || p->nkk < 3) return GRAL_EINVAL;
     if (!s->kkart || !s->advdom || !s->cutk || !s->z0 || !s->dzk || !s->hokart) return GRAL_EINVAL;
     if (p->turbulence_model < 0 || p->turbulence_model > 2) return GRAL_EINVAL;
-    if (p->turbulence_model == 1 && p->simd_width != 8) return GRAL_EINVAL;
+    if (p->turbulence_model == 1 && p->simd_width != 8 && p->simd_width != 16) return GRAL_EINVAL;
     if (p->turbulence_model != 1 && (!f->turb || !f->tdiss)) return GRAL_EINVAL;
     if (p->turbulence_model != 1 && p->turb_init == 0 &&
         (!s->z0_init || !s->ob_init || !s->ust_init)) return GRAL_EINVAL;

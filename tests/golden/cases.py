@@ -1,4 +1,5 @@
-"""Golden cases of the prognostic solve (turbulence models 0, 1 and 2).
+"""Golden cases of the prognostic solve (turbulence models 0, 1 and 2; model 1 with the
+Vector<float> width 8 and the Vector512 width 16).
 
 Inputs are rebuilt from ``gral_b200.prep`` with the seeds stated here, so only outputs are stored:
 ``<name>.npz`` (fields, DeltaUMax trace, statistics) for the small grids and SHA-256 digests in
@@ -34,7 +35,12 @@ CASES: Dict[str, tuple] = {
                    [(20.0, 2.0, 0.3, 0.25), (140.0, 4.0, 0.3, 0.25), (300.0, 1.5, 0.3, 0.25)], 2, 5, {}, "npz"),
     "m2_veg_s8": ("small", dict(nii=16, njj=16, seed=8, with_veg=True), [(110.0, 3.0, 0.2, 0.3)], 2, 5, {}, "npz"),
     "m0_small_s9": ("small", dict(nii=16, njj=14, seed=9), [(320.0, 2.5, 0.2, 0.3)], 0, 4, {}, "npz"),
+    "m1w16_small_s12": ("small", dict(nii=16, njj=14, seed=12, vert_cells_ff=20), [(250.0, 3.0, 0.2, 0.3)], 1, 6,
+                        dict(simd_width=16), "npz"),
+    "m1w16_veg_s13": ("small", dict(nii=16, njj=16, seed=13, vert_cells_ff=20, with_veg=True),
+                      [(160.0, 3.0, 0.2, 0.3), (20.0, 2.0, 0.2, 0.3)], 1, 5, dict(simd_width=16), "npz"),
     "m1_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, {}, "sha"),
+    "m1w16_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, dict(simd_width=16), "sha"),
     "m1_city_400": ("city", dict(), [(225.0, 2.0, 0.5, 0.3)], 1, 2, {}, "sha"),
 }
 

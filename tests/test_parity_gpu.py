@@ -165,3 +165,24 @@ def test_model0_mixing_length(gpu_required, layout, iterations):
         assert sg["iterations"] == sc["iterations"] == iterations
         np.testing.assert_array_equal(tg, tc)
         check_same(fg, fc)
+
+
+@pytest.mark.parametrize("with_veg", [False, True])
+def test_model1_vector512_width(gpu_required, layout, with_veg):
+    """simd_width 16: the reference's Vector512 routines (chunks of 16 levels, fused multiply-adds
+    in the power law, the height above KKART and the neighbour sums)."""
+    dom = prep.small_domain(16, 16, seed=14, vert_cells_ff=20, with_veg=with_veg)
+    sits = [prep.Situation(direction_deg=d, speed_10m=3.0, z0=0.2, ustar=0.3) for d in (75.0, 300.0)]
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, sits, 6, simd_width=16):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc)
+
+
+def test_vector512_width_rejects_short_columns(gpu_required):
+    """A column whose prognostic levels are fewer than 16 has no Vector512 chunk (the reference
+    would index below level 0): rejected with GRAL_EINVAL."""
+    from gral_b200.prognostic import GralError
+    dom = prep.small_domain(16, 14, seed=0)        # VertCellsFF 12
+    sit = prep.Situation()
+    with pytest.raises(GralError):
+        solve_gpu(dom, [dom.params(sit, iterations=2, simd_width=16)], [prep.initial_fields(dom, sit)])
