@@ -53,6 +53,7 @@ class GralParams(C.Structure):
         ("quantise", C.c_int32), ("turb_init", C.c_int32),
         ("std_dev_v", C.c_float), ("std_dev_w", C.c_float),
         ("bd_lay_height", C.c_float), ("v0_1", C.c_float),
+        ("post_diagnostic", C.c_int32),
     ]
 
 

@@ -121,6 +121,7 @@ struct KArgs {
     float *trace;                        // [nb][trace_cap] DeltaUMax per iteration, or null
     int trace_cap;
     int vi_min;                          // smallest VerticalIndex of an active column
+    int diag_iter;                       // iteration (1..10) of a DiagnosticFlowfield sweep launch
 };
 
 // Geometry of a Gauss-Seidel sweep: sweep coordinates i1 in [ia, ia+ni), j1 in [ja, ja+nj);
@@ -132,7 +133,7 @@ struct SweepGeom {
 
 enum : int { ERR_NONE = 0, ERR_TIMEOUT = 1, ERR_NONFINITE = 2 };
 
-enum : int { PH_PRESSURE = 1, PH_U = 2, PH_V = 3, PH_W = 4, PH_TKE = 5 };
+enum : int { PH_PRESSURE = 1, PH_U = 2, PH_V = 3, PH_W = 4, PH_TKE = 5, PH_DIAG = 6 };
 enum : int { F_GMODE1 = 1 << 13 };   // ColKE ground law uses level k+1 (Z0 >= DZK/2)
 
 __host__ __device__ inline size_t fidx(int s, int col, int ncols, int ks) {
@@ -205,5 +206,12 @@ __device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned
         }
     }
 }
+
+// Full-height level tables of the diagnostic pressure solve (DiagnosticFlowfield.cs:124-138):
+// APP, ATP, ABP with KKART < k-1 (abp1) and at KKART+1 (abp0), DZK; and the per-situation DTIME.
+struct DiagTabs {
+    const float *dzk, *app, *atp, *abp0, *abp1;
+    const float *dtime;
+};
 
 }  // namespace gral

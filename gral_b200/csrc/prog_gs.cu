@@ -419,15 +419,24 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_tke(KArgs a, SweepGeom g) {
 // critical path; `pre` overlaps the predecessors' work.  Results are bit-identical to the unsplit
 // evaluation (the operations and their order are the same).
 
+// Sweep orders of the diagnostic pressure solve by IterationLoops % 4 (DiagnosticFlowfield.cs:94-
+// 315): 0 rows and columns ascending, 1 rows descending, 2 both descending, 3 columns descending.
+__device__ __forceinline__ void diag_dir(int it, int &IS, int &JS) {
+    const int m = it % 4;
+    IS = (m == 2 || m == 3) ? -1 : 1;
+    JS = (m == 1 || m == 2) ? -1 : 1;
+}
+
 template <int PHASE, bool REVERSE, class Job>
 __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &g, Job &job) {
     const int lane = threadIdx.x & 31;
     const unsigned units = (unsigned)*a.nact;
     const unsigned total = (unsigned)g.diag_start[g.ndiag] * units;
     unsigned int *ctr = a.counters + PHASE;
-    const int it = *a.it_global;
+    const int it = (PHASE == PH_DIAG) ? a.diag_iter : *a.it_global;
     int IS, JS;
-    sweep_dir(it, IS, JS);
+    if (PHASE == PH_DIAG) diag_dir(it, IS, JS);
+    else sweep_dir(it, IS, JS);
     if (REVERSE) { IS = -IS; JS = -JS; }
     const int stamp = it * 8 + PHASE;
     job.stamp = stamp;
@@ -783,6 +792,88 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom
     gs_tasks_split<PH_PRESSURE, false>(a, g, job);
 }
 
+// DiagnosticFlowfield.Calculate's pressure sweep (DiagnosticFlowfield.cs:86-315) on the full-height
+// fields after a prognostic solve: every column of the sweep range, levels KKART+1..NKK-1, the four
+// neighbours' DPM of this sweep or the last one (plain Gauss-Seidel, DPM zeroed once before the
+// first iteration), PIMP/QIMP at NKK zero, no quantisation and no residual.  Split at the wait
+// like the prognostic pressure: divergence and forward elimination before it, the neighbours'
+// DPM, Q and the back-substitution after.  Rows per warp (dynamic shared memory, KS = NKK+2):
+// T, P, Q, D, DPM, DIV/DTIME.
+struct DiagJob {
+    const KArgs &a;
+    float *R;
+    int stamp;
+    const DiagTabs &t;
+    int col, KK, top;
+    Acc<false> x;
+    float DT;
+
+    __device__ float &row(int r, int k) { return R[r * a.ks + k]; }
+
+    __device__ void pre(int s, int i, int j, int, int, bool) {
+        const int lane = threadIdx.x & 31;
+        const long long E = a.nj2, N = 1;
+        const float DXK = a.dxk, DYK = a.dyk;
+        col = i * a.nj2 + j;
+        KK = a.meta[col].kkart;
+        top = a.nkk - 1;
+        x = make_acc<false>(a, s, col);
+        DT = t.dtime[s];
+        for (int k = KK + 1 + lane; k <= top; k += 32) {
+            const float u0 = a.uk[x.at(0, k)], uE = a.uk[x.at(E, k)], v0 = a.vk[x.at(0, k)], vN = a.vk[x.at(N, k)];
+            const float w0 = a.wk[x.at(0, k)], wT = a.wk[x.at(0, k + 1)];
+            const float dz = t.dzk[k];
+            const float DIV = (k > KK + 1) ? (u0 - uE) * DYK * dz + (v0 - vN) * DXK * dz + (w0 - wT) * DXK * DYK
+                                           : (u0 - uE) * DYK * dz + (v0 - vN) * DXK * dz - wT * DXK * DYK;
+            row(5, k) = DIV / DT;
+        }
+        if (lane == 0) {
+            float P = 0.0f;
+            for (int k = top; k > KK; --k) {
+                const float T = 1.0f / (t.app[k] - t.atp[k] * P);
+                P = ((k > KK + 1) ? t.abp1[k] : t.abp0[k]) * T;
+                row(0, k) = T;
+                row(1, k) = P;
+            }
+        }
+    }
+
+    __device__ void post(int, int, int) {
+        const int lane = threadIdx.x & 31;
+        const float DXK = a.dxk, DYK = a.dyk;
+        const long long E = a.nj2, N = 1;
+        for (int k = KK + 1 + lane; k <= top; k += 32) {
+            const float dz = t.dzk[k];
+            const float im = __ldcg(a.dpm + x.at(-E, k)), ip = __ldcg(a.dpm + x.at(E, k));
+            const float jm = __ldcg(a.dpm + x.at(-N, k)), jp = __ldcg(a.dpm + x.at(N, k));
+            row(3, k) = row(5, k) + (im + ip) / DXK * DYK * dz + (jm - jp) / DYK * DXK * dz;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            float Q = 0.0f;
+            for (int k = top; k > KK; --k) {
+                Q = (t.atp[k] * Q + row(3, k)) * row(0, k);
+                row(2, k) = Q;
+            }
+            float prev = 0.0f;                                     // DPM[KKART] = 0
+            for (int k = KK + 1; k <= top; ++k) {
+                prev = row(1, k) * prev + row(2, k);
+                row(4, k) = prev;
+            }
+        }
+        __syncwarp();
+        for (int k = 1 + lane; k <= top; k += 32) __stcg(a.dpm + x.at(0, k), (k > KK) ? row(4, k) : 0.0f);
+    }
+
+    __device__ void finish() {}
+};
+
+__global__ void __launch_bounds__(GS_WARPS * 32) k_diag_pressure(KArgs a, SweepGeom g, DiagTabs t) {
+    extern __shared__ float dsm[];
+    DiagJob job{a, dsm + (size_t)(threadIdx.x >> 5) * 6 * a.ks, 0, t};
+    gs_tasks_split<PH_DIAG, false>(a, g, job);
+}
+
 // ---------------------------- batched family -----------------------------------------------
 // One block per task = (group of 32 situations, column).  The block's warps split the levels for
 // the coefficient assembly (lane = situation, contiguous 128-byte loads in the interleaved layout)
@@ -1121,6 +1212,20 @@ void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStrea
     } else {
         plain_kernel(kind, a.model)<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
     }
+}
+
+size_t diag_smem(int ks) { return (size_t)GS_WARPS * 6 * ks * sizeof(float); }
+
+cudaError_t diag_prepare(int ks) {
+    return cudaFuncSetAttribute(k_diag_pressure, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem(ks));
+}
+
+cudaError_t diag_occupancy(int ks, int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_diag_pressure, GS_WARPS * 32, diag_smem(ks));
+}
+
+void launch_diag_pressure(const KArgs &a, const SweepGeom &g, const DiagTabs &t, int grid, cudaStream_t st) {
+    k_diag_pressure<<<grid, GS_WARPS * 32, diag_smem(a.ks), st>>>(a, g, t);
 }
 
 }  // namespace gral

@@ -93,6 +93,11 @@ struct gral_ctx {
     DevBuf<ColF> colf;
     DevBuf<ColKE> colke;
     DevBuf<short2> rcw;
+    // DiagnosticFlowfield after the solve (gral_params.post_diagnostic)
+    bool post_diag = false;
+    int diag_grid = 0;
+    DevBuf<float> ddpm, dtab, ddt;
+    DevBuf<int> dflags;
     DevBuf<float> varw, z0i;
     DevBuf<SitDev> sit;
     DevBuf<int> flags, misc, diag, bcl, counts;
@@ -105,6 +110,7 @@ struct gral_ctx {
         DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
         for (auto *b : fb) b->release();
         meta.release(); cflags.release(); colf.release(); sit.release(); colke.release(); rcw.release();
+        ddpm.release(); dtab.release(); ddt.release(); dflags.release();
         varw.release(); z0i.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
@@ -126,6 +132,12 @@ int fail(gral_ctx *c, int code, const std::string &msg) {
         if (e_ != cudaSuccess)                                                                        \
             return fail(ctx, e_ == cudaErrorMemoryAllocation ? GRAL_ENOMEM : GRAL_ECUDA,              \
                         std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+    } while (0)
+
+#define CK_RC(call)                \
+    do {                           \
+        const int rc_ = (call);    \
+        if (rc_ != GRAL_OK) return rc_; \
     } while (0)
 
 inline float f32(float x) { return x; }
@@ -298,6 +310,8 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
             q.conv_cadence != p0.conv_cadence || q.relax != p0.relax || q.relaxp != p0.relaxp ||
             q.building_z0 != p0.building_z0 || q.coriolis != p0.coriolis)
             return fail(ctx, GRAL_EINVAL, "situations of a batch must share grid and solver controls");
+        if (q.post_diagnostic != p0.post_diagnostic)
+            return fail(ctx, GRAL_EINVAL, "post_diagnostic must be the same for every situation of a batch");
         if (q.conv_cadence < 1 || q.iteration_steps_max < 1) return fail(ctx, GRAL_EINVAL, "bad iteration controls");
         if (q.ref_i < 1 || q.ref_i > q.nii || q.ref_j < 1 || q.ref_j > q.njj)
             return fail(ctx, GRAL_EINVAL, "reference point outside the grid");
@@ -423,6 +437,36 @@ int tune_variants(gral_ctx *ctx) {
 }
 
 }  // namespace
+
+// DiagnosticFlowfield.Calculate and the final vertical velocity (MicroscaleFlat.cs:383-462) on the
+// full-height staging fields of every situation, after the scatter of the prognostic result.
+int run_diagnostic(gral_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int nk2 = ctx->nkk + 2;
+    KArgs kd = ctx->ka;
+    kd.il = 0;
+    kd.ks = nk2;
+    kd.uk = ctx->sg.uk; kd.vk = ctx->sg.vk; kd.wk = ctx->sg.wk;
+    kd.dpm = ctx->ddpm.p;
+    kd.flags = ctx->dflags.p;
+    kd.chunk = 1;
+    DiagTabs t;
+    t.dzk = ctx->dtab.p; t.app = ctx->dtab.p + nk2; t.atp = ctx->dtab.p + 2 * nk2;
+    t.abp0 = ctx->dtab.p + 3 * nk2; t.abp1 = ctx->dtab.p + 4 * nk2;
+    t.dtime = ctx->ddt.p;
+    launch_diag_dtime(kd, ctx->params[0].kadvmax, ctx->ddt.p, st);
+    CK(cudaMemsetAsync(ctx->ddpm.p, 0, (size_t)ctx->nb * ctx->ncols * nk2 * sizeof(float), st));
+    CK(cudaMemsetAsync(ctx->dflags.p, 0, (size_t)ctx->nb * ctx->ncols * sizeof(int), st));
+    for (int d = 1; d <= 10; ++d) {                    // Iterations = 10 after a prognostic solve (:33-37)
+        kd.diag_iter = d;
+        CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * sizeof(unsigned int), st));
+        launch_diag_pressure(kd, ctx->geo_p.g, t, ctx->diag_grid, st);
+        launch_diag_velcorr(kd, t, st);
+    }
+    launch_diag_wfinal(kd, t, st);
+    CK(cudaGetLastError());
+    return GRAL_OK;
+}
 
 extern "C" {
 
@@ -731,6 +775,31 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemcpyAsync(ctx->cflags.p, cfl.data(), ncols * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->colf.p, colf.data(), ncols * sizeof(ColF), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->rcw.p, rcw.data(), ncols * sizeof(short2), cudaMemcpyHostToDevice, st));
+    ctx->post_diag = p0.post_diagnostic != 0;
+    if (ctx->post_diag) {
+        // full-height level tables of DiagnosticFlowfield.cs:124-138 (float, the reference's
+        // expressions): dzk, app, atp, abp0 (k = KKART+1), abp1 (k > KKART+1)
+        const float *DZK = s->dzk;
+        std::vector<float> dt(5 * (size_t)nk2, 0.0f);
+        for (int k = 0; k < nk2; ++k) dt[k] = DZK[k];
+        for (int k = 1; k <= NKK - 1; ++k) {
+            dt[nk2 + k] = 2 * (DYK * DZK[k] / DXK + DXK * DZK[k] / DYK + DXK * DYK / DZK[k]);
+            dt[2 * nk2 + k] = (DXK * DYK) / (0.5F * (DZK[k + 1] + DZK[k]));
+            dt[3 * nk2 + k] = DXK * DYK / DZK[k];
+            dt[4 * nk2 + k] = DXK * DYK / (0.5F * (DZK[k - 1] + DZK[k]));
+        }
+        CK(ctx->dtab.ensure(dt.size()));
+        CK(ctx->ddpm.ensure((size_t)n * ncols * nk2));
+        CK(ctx->dflags.ensure((size_t)n * ncols));
+        CK(ctx->ddt.ensure(n));
+        CK(cudaMemcpyAsync(ctx->dtab.p, dt.data(), dt.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        CK(diag_prepare(nk2));
+        int bps = 0;
+        CK(diag_occupancy(nk2, &bps));
+        const double width = (double)n * (NII - 3) * (NJJ - 3) / std::max(1, NII + NJJ - 7);
+        ctx->diag_grid = (int)std::max<long long>(ctx->num_sms, std::min<long long>((long long)std::max(1, bps) * ctx->num_sms,
+                                                  (long long)std::ceil(8 * width / 4)));
+    }
     if (ctx->model != 1) {
         CK(cudaMemcpyAsync(ctx->colke.p, colke.data(), ncols * sizeof(ColKE), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->varw.p, varw.data(), varw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -905,6 +974,7 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
     launch_postcheck(ctx->ka, ctx->counts.p, st);
     launch_scatter(ctx->ka, ctx->sg, ctx->model, st);
     CK(cudaGetLastError());
+    if (ctx->post_diag) CK_RC(run_diagnostic(ctx));
     const size_t ssz = ctx->sg.stride;
     for (int b = 0; b < n; ++b) {
         CK(cudaMemcpyAsync(f[b].uk, ctx->sg.uk + ssz * b, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
@@ -916,10 +986,13 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
         }
     }
     std::vector<int> counts(4 * n);
+    int herr = 0;
     CK(cudaMemcpyAsync(counts.data(), ctx->counts.p, 4 * n * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(ctx->sit.p, hs.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
     CK(cudaEventRecord(ctx->ev[3], st));
     CK(cudaStreamSynchronize(st));
+    if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "a wavefront wait exceeded its time limit");
     float ms_down = 0.f;
     cudaEventElapsedTime(&ms_down, ctx->ev[2], ctx->ev[3]);
     int rc = GRAL_OK;

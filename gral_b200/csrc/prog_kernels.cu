@@ -398,6 +398,64 @@ __global__ void k_postcheck(KArgs a, int *counts) {
     });
 }
 
+// ---- DiagnosticFlowfield after the prognostic solve (DiagnosticFlowfield.cs:24-436) ----
+// time step from the corner column's wind at KADVMAX (:30-31), one thread per situation
+__global__ void k_diag_dtime(KArgs a, int kadvmax, float *dtime) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= a.nb) return;
+    const Acc<false> x = make_acc<false>(a, s, 1 * a.nj2 + 1);
+    const float u = a.uk[x.at(0, kadvmax)], v = a.vk[x.at(0, kadvmax)];
+    float DT = (float)(0.5 * (double)net_minf(a.dxk, a.dyk) / sqrt((double)(u * u + v * v)));
+    dtime[s] = net_minf(DT, 5.0f);
+}
+
+// velocity correction without quantisation on levels 1..NKK-1 (:320-382)
+__global__ void k_diag_velcorr(KArgs a, DiagTabs t) {
+    col_loop<false>(a, false, [&](int s, int col, int i, int j, const Acc<false> &x, int kbeg, int kstep) {
+        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+        const int KK = a.meta[col].kkart, KKW = a.meta[col - a.nj2].kkart, KKS = a.meta[col - 1].kkart;
+        const float DXK = a.dxk, DYK = a.dyk, DT = t.dtime[s];
+        const long long W = -(long long)a.nj2;
+        for (int k = 1 + kbeg; k <= a.nkk - 1; k += kstep) {
+            const float d = a.dpm[x.at(0, k)];
+            const float DDPX = a.dpm[x.at(W, k)] - d, DDPY = a.dpm[x.at(-1, k)] - d;
+            const float DDPZ = (k > KK + 1) ? a.dpm[x.at(0, k - 1)] - d : 0.0f;
+            float &u = a.uk[x.at(0, k)], &v = a.vk[x.at(0, k)], &w = a.wk[x.at(0, k)];
+            u = ((KK < k) && (KKW < k)) ? u + (DDPX / DXK * DT) : 0.0f;
+            v = ((KK < k) && (KKS < k)) ? v + (DDPY / DYK * DT) : 0.0f;
+            w = (KK + 1 < k) ? w + (DDPZ * 2 / (t.dzk[k] + t.dzk[k - 1]) * DT) : 0.0f;
+        }
+    });
+}
+
+// final vertical velocity of the columns outside the prognostic sub-domains, bottom-up
+// (MicroscaleFlat.cs:389-462); one thread per (situation, column)
+__global__ void k_diag_wfinal(KArgs a, DiagTabs t) {
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long s = g / a.ncols;
+    if (s >= a.nb) return;
+    const int col = (int)(g - s * a.ncols);
+    const int i = col / a.nj2, j = col - i * a.nj2;
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+    if (a.cflags[col] & F_ADV) return;
+    const Acc<false> x = make_acc<false>(a, (int)s, col);
+    const long long E = a.nj2, N = 1;
+    const int KK = a.meta[col].kkart;
+    const int KKW = a.meta[col - a.nj2].kkart, KKE = a.meta[col + a.nj2].kkart;
+    const int KKS = a.meta[col - 1].kkart, KKN = a.meta[col + 1].kkart;
+    const float DXK = a.dxk, DYK = a.dyk;
+    for (int k = 1; k < a.nkk; ++k) {
+        if (!(k > KK)) continue;
+        const float dz = t.dzk[k];
+        const float fwo1 = (k <= KKW) ? 0.0f : dz * DYK * a.uk[x.at(0, k)];
+        const float fwo2 = (k <= KKE) ? 0.0f : dz * DYK * a.uk[x.at(E, k)];
+        const float fsn1 = (k <= KKS) ? 0.0f : dz * DXK * a.vk[x.at(0, k)];
+        const float fsn2 = (k <= KKN) ? 0.0f : dz * DXK * a.vk[x.at(N, k)];
+        const float fbt1 = ((k <= KK + 1) || (k == 1)) ? 0.0f : DXK * DYK * a.wk[x.at(0, k)];
+        a.wk[x.at(0, k + 1)] = (fwo1 - fwo2 + fsn1 - fsn2 + fbt1) / (DXK * DYK);
+    }
+}
+
 }  // namespace
 
 #define GRAL_COL_LAUNCH(kern, ...)                                                        \
@@ -448,6 +506,19 @@ void launch_gather(const KArgs &a, const Staging &sg, int model, cudaStream_t st
 
 void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t st) {
     GRAL_COL_LAUNCH(k_gather, a, sg, model, 0);
+}
+
+void launch_diag_dtime(const KArgs &a, int kadvmax, float *dtime, cudaStream_t st) {
+    k_diag_dtime<<<(a.nb + 127) / 128, 128, 0, st>>>(a, kadvmax, dtime);
+}
+
+void launch_diag_velcorr(const KArgs &a, const DiagTabs &t, cudaStream_t st) {
+    k_diag_velcorr<<<col_grid<false>(a), COL_WARPS * 32, 0, st>>>(a, t);
+}
+
+void launch_diag_wfinal(const KArgs &a, const DiagTabs &t, cudaStream_t st) {
+    const long long n = (long long)a.nb * a.ncols;
+    k_diag_wfinal<<<(int)((n + 255) / 256), 256, 0, st>>>(a, t);
 }
 
 void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st) {

@@ -43,4 +43,14 @@ void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t s
 // post-checks (PrognosticFlowfield.cs:1193-1243); counts[s*4 + 0..3] = UK, VK, WK, non-finite
 void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st);
 
+// DiagnosticFlowfield.Calculate (DiagnosticFlowfield.cs:24-436) and the final vertical velocity of
+// the columns outside the prognostic sub-domains (MicroscaleFlat.cs:389-462), on full-height
+// fields: `a` describes them as a slab layout with KS = NKK+2 and a.dpm the diagnostic DPM.
+cudaError_t diag_prepare(int ks);
+cudaError_t diag_occupancy(int ks, int *blocks_per_sm);
+void launch_diag_dtime(const KArgs &a, int kadvmax, float *dtime, cudaStream_t st);
+void launch_diag_pressure(const KArgs &a, const SweepGeom &g, const DiagTabs &t, int grid, cudaStream_t st);
+void launch_diag_velcorr(const KArgs &a, const DiagTabs &t, cudaStream_t st);
+void launch_diag_wfinal(const KArgs &a, const DiagTabs &t, cudaStream_t st);
+
 }  // namespace gral

@@ -87,7 +87,8 @@ class Domain:
     def params(self, situation: Optional[Situation] = None, *, model: int = 1, iterations: int = 100,
                iter_min: Optional[int] = None, simd_width: int = 8, quantise: int = 1,
                conv_cadence: int = 100, conv_threshold: float = 0.012, latitude: float = 47.0,
-               relax: float = 0.1, relaxp: float = 1.0, building_z0: float = 0.001) -> dict:
+               relax: float = 0.1, relaxp: float = 1.0, building_z0: float = 0.001,
+               post_diagnostic: int = 0) -> dict:
         sit = situation or Situation()
         cor = float(F32(2 * 7.29 * 0.00001 * math.sin(abs(latitude) * 3.1415 / 180)))
         return dict(
@@ -99,7 +100,8 @@ class Domain:
             conv_threshold=conv_threshold, relax=relax, relaxp=relaxp,
             building_z0=building_z0, coriolis=cor, potdtdz=sit.potdtdz,
             ref_i=self.ref[0], ref_j=self.ref[1], quantise=quantise, turb_init=0,
-            std_dev_v=1.0, std_dev_w=1.0, bd_lay_height=1000.0, v0_1=float(F32(2.0 * sit.ustar)))
+            std_dev_v=1.0, std_dev_w=1.0, bd_lay_height=1000.0, v0_1=float(F32(2.0 * sit.ustar)),
+            post_diagnostic=post_diagnostic)
 
 
 def rasterise(nii: int, njj: int, buildings: List[Building]) -> np.ndarray:

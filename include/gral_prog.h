@@ -70,6 +70,12 @@ typedef struct gral_params {
     float std_dev_v, std_dev_w;   /* Program.StdDeviationV/W [1, 1] */
     float bd_lay_height;          /* Program.BdLayHeight */
     float v0_1;                   /* Program.V0[1] (sigma_v used by the TURB initialisation) */
+    int32_t post_diagnostic;      /* [0] 1: after the prognostic solve, run what the flat-terrain
+                                     caller runs next on the same fields: DiagnosticFlowfield.
+                                     Calculate (10 pressure iterations over the full height,
+                                     DiagnosticFlowfield.cs:24-436) and the final vertical
+                                     velocity of the columns outside the prognostic sub-domains
+                                     (MicroscaleFlat.cs:389-462) */
 } gral_params;
 
 /* Per-grid inputs; shared by all situations of a batch. */

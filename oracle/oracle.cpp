@@ -101,6 +101,95 @@ inline double quant(double x, double Frund, bool on) {
 
 }  // namespace
 
+/* DiagnosticFlowfield.Calculate after a prognostic solve (DiagnosticFlowfield.cs:24-436), in the
+ * deterministic order (UseFixedRndSeedVal: one worker, rows j outer, columns i inner), then the
+ * final vertical velocity of the columns outside the prognostic sub-domains
+ * (MicroscaleFlat.cs:389-462, FlowFieldLevel = prognostic). */
+static void diagnostic_post(State &st) {
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    const float DXK = st.dxk, DYK = st.dyk;
+    const float *DZK = st.dzk();
+    const float u11 = st.uk[st.i3(1, 1, st.kadvmax)], v11 = st.vk[st.i3(1, 1, st.kadvmax)];
+    float DTIME = (float)(0.5 * (double)net_min(DXK, DYK) / std::sqrt((double)(pow2f(u11) + pow2f(v11))));
+    DTIME = net_min(DTIME, 5.0f);
+    const int Iterations = 10;
+    for (int i = 1; i <= NII; ++i)                                   /* :39-49 */
+        for (int j = 1; j <= NJJ; ++j)
+            for (int k = 1; k <= NKK + 1; ++k) st.dpm[st.i3(i, j, k)] = 0;
+    std::vector<float> PIMP(st.nk2 + 1, 0.0f), QIMP(st.nk2 + 1, 0.0f);
+    for (int IterationLoops = 1; IterationLoops <= Iterations; ++IterationLoops) {
+        for (int i = 2; i < NII; ++i)                                /* divergence, :54-81 */
+            for (int j = 2; j < NJJ; ++j) {
+                const int KK = st.kkart(i, j);
+                for (int k = 1; k <= NKK - 1; ++k) {
+                    if (!(KK < k)) continue;
+                    const float u0 = st.uk[st.i3(i, j, k)], uE = st.uk[st.i3(i + 1, j, k)];
+                    const float v0 = st.vk[st.i3(i, j, k)], vN = st.vk[st.i3(i, j + 1, k)];
+                    if (k > KK + 1)
+                        st.div[st.i3(i, j, k)] = (u0 - uE) * DYK * DZK[k] + (v0 - vN) * DXK * DZK[k] +
+                                                 (st.wk[st.i3(i, j, k)] - st.wk[st.i3(i, j, k + 1)]) * DXK * DYK;
+                    else
+                        st.div[st.i3(i, j, k)] = (u0 - uE) * DYK * DZK[k] + (v0 - vN) * DXK * DZK[k] -
+                                                 st.wk[st.i3(i, j, k + 1)] * DXK * DYK;
+                }
+            }
+        /* pressure-correction TDMA, :86-315; the four sweep orders of IterationLoops % 4 */
+        const int m = IterationLoops % 4;
+        const bool jdesc = (m == 1 || m == 2), idesc = (m == 2 || m == 3);
+        for (int j1 = 2; j1 < NJJ; ++j1) {
+            const int j = jdesc ? NJJ - j1 + 1 : j1;
+            for (int i1 = 2; i1 < NII; ++i1) {
+                const int i = idesc ? NII - i1 + 1 : i1;
+                const int KK = st.kkart(i, j);
+                for (int k = NKK - 1; k >= 1; k--) {
+                    if (!(KK < k)) continue;
+                    const float DIM = st.div[st.i3(i, j, k)] / DTIME +
+                                      (st.dpm[st.i3(i - 1, j, k)] + st.dpm[st.i3(i + 1, j, k)]) / DXK * DYK * DZK[k] +
+                                      (st.dpm[st.i3(i, j - 1, k)] - st.dpm[st.i3(i, j + 1, k)]) / DYK * DXK * DZK[k];
+                    const float APP = 2 * (DYK * DZK[k] / DXK + DXK * DZK[k] / DYK + DXK * DYK / DZK[k]);
+                    const float ABP = (k > KK + 1) ? DXK * DYK / (0.5f * (DZK[k - 1] + DZK[k])) : DXK * DYK / DZK[k];
+                    const float ATP = (DXK * DYK) / (0.5f * (DZK[k + 1] + DZK[k]));
+                    const float TERMP = 1 / (APP - ATP * PIMP[k + 1]);
+                    PIMP[k] = ABP * TERMP;
+                    QIMP[k] = (ATP * QIMP[k + 1] + DIM) * TERMP;
+                }
+                float *DPM_L = st.col(st.dpm, i, j);
+                DPM_L[0] = 0;
+                for (int k = 1; k <= NKK - 1; ++k) DPM_L[k] = (KK < k) ? PIMP[k] * DPM_L[k - 1] + QIMP[k] : 0;
+            }
+        }
+        for (int i = 2; i < NII; ++i)                                /* velocity correction, :320-382 */
+            for (int j = 2; j < NJJ; ++j) {
+                const int KK = st.kkart(i, j);
+                const float *DPM_L = st.col(st.dpm, i, j);
+                const float *DPMim = st.col(st.dpm, i - 1, j), *DPMjm = st.col(st.dpm, i, j - 1);
+                for (int k = 1; k < NKK; ++k) {
+                    const float DDPX = DPMim[k] - DPM_L[k], DDPY = DPMjm[k] - DPM_L[k];
+                    const float DDPZ = (k > KK + 1) ? DPM_L[k - 1] - DPM_L[k] : 0.0f;
+                    float &u = st.uk[st.i3(i, j, k)], &v = st.vk[st.i3(i, j, k)], &w = st.wk[st.i3(i, j, k)];
+                    u = ((KK < k) && (st.kkart(i - 1, j) < k)) ? u + (DDPX / DXK * DTIME) : 0.0f;
+                    v = ((KK < k) && (st.kkart(i, j - 1) < k)) ? v + (DDPY / DYK * DTIME) : 0.0f;
+                    w = (KK + 1 < k) ? w + (DDPZ * 2 / (DZK[k] + DZK[k - 1]) * DTIME) : 0.0f;
+                }
+            }
+    }
+    /* final vertical velocity outside the prognostic sub-domains (MicroscaleFlat.cs:389-462) */
+    for (int i = 2; i < NII; ++i)
+        for (int j = 2; j < NJJ; ++j) {
+            if (st.advdom(i, j) != 0) continue;
+            const int KK = st.kkart(i, j);
+            for (int k = 1; k < NKK; ++k) {
+                if (!(k > KK)) continue;
+                const float fwo1 = (k <= st.kkart(i - 1, j)) ? 0.0f : DZK[k] * DYK * st.uk[st.i3(i, j, k)];
+                const float fwo2 = (k <= st.kkart(i + 1, j)) ? 0.0f : DZK[k] * DYK * st.uk[st.i3(i + 1, j, k)];
+                const float fsn1 = (k <= st.kkart(i, j - 1)) ? 0.0f : DZK[k] * DXK * st.vk[st.i3(i, j, k)];
+                const float fsn2 = (k <= st.kkart(i, j + 1)) ? 0.0f : DZK[k] * DXK * st.vk[st.i3(i, j + 1, k)];
+                const float fbt1 = ((k <= KK + 1) || (k == 1)) ? 0.0f : DXK * DYK * st.wk[st.i3(i, j, k)];
+                st.wk[st.i3(i, j, k + 1)] = (fwo1 - fwo2 + fsn1 - fsn2 + fbt1) / (DXK * DYK);
+            }
+        }
+}
+
 extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fields *f,
                             gral_stats *stats) {
     int rc = validate(p, s, f);
@@ -459,6 +548,8 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
             }
         }
     }
+
+    if (p->post_diagnostic) diagnostic_post(st);
 
     if (stats) {
         stats->iterations = iterations;

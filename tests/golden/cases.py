@@ -39,7 +39,10 @@ CASES: Dict[str, tuple] = {
                         dict(simd_width=16), "npz"),
     "m1w16_veg_s13": ("small", dict(nii=16, njj=16, seed=13, vert_cells_ff=20, with_veg=True),
                       [(160.0, 3.0, 0.2, 0.3), (20.0, 2.0, 0.2, 0.3)], 1, 5, dict(simd_width=16), "npz"),
+    "m1_diag_s15": ("small", dict(nii=20, njj=18, seed=15, n_buildings=3, subdomain_factor=1),
+                    [(240.0, 3.0, 0.2, 0.3)], 1, 4, dict(post_diagnostic=1), "npz"),
     "m1_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, {}, "sha"),
+    "m1_diag_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, dict(post_diagnostic=1), "sha"),
     "m1w16_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, dict(simd_width=16), "sha"),
     "m1_city_400": ("city", dict(), [(225.0, 2.0, 0.5, 0.3)], 1, 2, {}, "sha"),
 }

@@ -186,3 +186,24 @@ def test_vector512_width_rejects_short_columns(gpu_required):
     sit = prep.Situation()
     with pytest.raises(GralError):
         solve_gpu(dom, [dom.params(sit, iterations=2, simd_width=16)], [prep.initial_fields(dom, sit)])
+
+
+@pytest.mark.parametrize("model", [1, 2])
+def test_post_diagnostic(gpu_required, layout, model):
+    """post_diagnostic: DiagnosticFlowfield.Calculate (10 full-height pressure iterations) and the
+    final vertical velocity of the columns outside the prognostic sub-domains, after the solve."""
+    dom = prep.small_domain(20, 18, seed=15, n_buildings=3, subdomain_factor=1)
+    assert (dom.static.advdom[2:-2, 2:-2] == 0).any()
+    sits = [prep.Situation(direction_deg=d, speed_10m=3.0, z0=0.2, ustar=0.3) for d in (240.0, 40.0)]
+    names = ("uk", "vk", "wk") + (("turb", "tdiss") if model == 2 else ())
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, sits, 4, model=model, post_diagnostic=1):
+        np.testing.assert_array_equal(tg, tc)
+        check_same(fg, fc, names)
+
+
+def test_post_diagnostic_full_height_cube(gpu_required, layout):
+    """The cube grid: NKK 162, so the diagnostic sweep covers 161 levels per column."""
+    dom = prep.cube_domain()
+    sit = prep.Situation(direction_deg=270.0, speed_10m=3.0, z0=0.2, ustar=0.3)
+    for fg, fc, sg, sc, tg, tc in run_pair(dom, [sit], 2, post_diagnostic=1):
+        check_same(fg, fc)
