@@ -880,7 +880,56 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_diag_pressure(KArgs a, SweepG
 // and write rows [k][32] to shared memory; warp 0 then runs the 32 situations' Thomas
 // recurrences and back-substitutions side by side.
 
+// L2 prefetch of one contiguous run (the interleaved layout keeps a (field, column) block of a
+// group contiguous over levels); 16-byte aligned, size a multiple of 16.
+__device__ __forceinline__ void l2_prefetch(const float *p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Operand blocks of a batched task, prefetched into L2 while the block still works on the task
+// before it: for each field the columns (offsets in columns) the phase's level function reads,
+// levels KSTART-1..VerticalIndex+1 (pressure: KKART..VerticalIndex+1).
+template <int PHASE>
+__device__ void prefetch_task(const KArgs &a, const SweepGeom &g, unsigned t, unsigned units, int IS, int JS) {
+    int grp, i1, j1;
+    decode_task(t, g, units, grp, i1, j1);
+    grp += a.group_lo;
+    const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+    const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+    const int col = i * a.nj2 + j;
+    if (!(a.cflags[col] & F_ADV)) return;
+    const ColMeta m = a.meta[col];
+    const int klo = (PHASE == PH_PRESSURE) ? (int)m.kkart : max(0, (int)m.kstart - 1);
+    const int khi = m.vi + 1;
+    const unsigned bytes = (unsigned)(khi - klo + 1) * 32u * sizeof(float);
+    const long long W = -(long long)a.nj2, E = a.nj2, S = -1, N = 1;
+    auto pf = [&](const float *F, long long dc) {
+        l2_prefetch(F + (((size_t)grp * a.ncols + (size_t)((long long)col + dc)) * a.ks + klo) * 32, bytes);
+    };
+    if (PHASE == PH_U) {
+        pf(a.uk, 0); pf(a.uk, W); pf(a.uk, S); pf(a.uk, E); pf(a.uk, N); pf(a.vk, 0);
+        pf(a.uks, 0); pf(a.uks, W); pf(a.wks, 0); pf(a.wks, W); pf(a.wk, E); pf(a.dpmnew, 0); pf(a.dpmnew, W);
+        pf(a.vks, 0); pf(a.vks, W); pf(a.vks, W + S); pf(a.vks, S); pf(a.vks, W + N); pf(a.vks, N);
+        pf(a.vks, E + N); pf(a.vks, E + S);
+    } else if (PHASE == PH_V) {
+        pf(a.vk, 0); pf(a.vk, W); pf(a.vk, S); pf(a.vk, E); pf(a.vk, N); pf(a.uk, 0);
+        pf(a.vks, 0); pf(a.vks, W); pf(a.vks, S); pf(a.wks, 0); pf(a.wks, S); pf(a.wk, N); pf(a.dpmnew, 0);
+        pf(a.dpmnew, S); pf(a.uks, 0); pf(a.uks, E); pf(a.uks, S); pf(a.uks, E + S); pf(a.uks, W);
+        pf(a.uks, W + S); pf(a.uks, E + N); pf(a.uks, W + N);
+    } else if (PHASE == PH_W) {
+        pf(a.wk, 0); pf(a.wk, W); pf(a.wk, S); pf(a.wk, E); pf(a.wk, N); pf(a.uk, 0); pf(a.vk, 0);
+        pf(a.uks, 0); pf(a.uks, W); pf(a.uks, E); pf(a.vks, 0); pf(a.vks, S); pf(a.vks, N); pf(a.wks, 0);
+        pf(a.dpmnew, 0);
+    } else if (PHASE == PH_PRESSURE) {
+        pf(a.uk, 0); pf(a.uk, E); pf(a.vk, 0); pf(a.vk, N); pf(a.wk, 0); pf(a.dpmnew, 0);
+        pf(a.dpm, -(long long)IS * a.nj2); pf(a.dpm, -(long long)JS);
+    }
+}
+
 // Block-wide variant of gs_tasks: thread 0 claims and waits, the block works, thread 0 publishes.
+// While warp 0 runs the serial recurrences, the body calls `ahead` from one idle thread, which
+// prefetches into L2 the operands of the task one round of blocks further in claim order (task
+// t + gridDim.x): some block claims it about one task duration later.
 template <int PHASE, bool REVERSE, class Body>
 __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &g, Body &&body) {
     __shared__ unsigned s_base;
@@ -915,7 +964,11 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
                 s_ok = ok;
             }
             __syncthreads();
-            if (s_ok) body(grp, i, j, IS, JS, i1 == g.ia);
+            auto ahead = [&]() {
+                const unsigned pt = t + gridDim.x;
+                if (pt < total) prefetch_task<PHASE>(a, g, pt, units, IS, JS);
+            };
+            if (s_ok) body(grp, i, j, IS, JS, i1 == g.ia, ahead);
             __syncthreads();
             if (threadIdx.x == 0) st_release(fl + i * a.nj2 + j, stamp);
         }
@@ -955,8 +1008,8 @@ __device__ __forceinline__ BLane blane(float *smem, int ks) {
     return R;
 }
 
-template <int MODEL, int COMP, int NW>
-__device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *smem) {
+template <int MODEL, int COMP, int NW, class Ahead>
+__device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *smem, Ahead &&ahead) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
@@ -973,6 +1026,7 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
         }
     }
     __syncthreads();
+    if (threadIdx.x == 32) ahead();
     if (warp != 0 || !act) return;
     float *F = comp_field<COMP>(a);
     const int kkm = back_limit<COMP>(c);
@@ -981,8 +1035,8 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
         if (kkm < k) __stcg(F + x.at(0, k), R.p(k));
 }
 
-template <int NW>
-__device__ void batch_tke_column(const KArgs &a, int grp, int i, int j, float *smem) {
+template <int NW, class Ahead>
+__device__ void batch_tke_column(const KArgs &a, int grp, int i, int j, float *smem, Ahead &&ahead) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
@@ -999,6 +1053,7 @@ __device__ void batch_tke_column(const KArgs &a, int grp, int i, int j, float *s
         }
     }
     __syncthreads();
+    if (threadIdx.x == 32) ahead();
     if (warp != 0 || !act) return;
     const ColKE ke = a.colke[c.col];
     const float *vf[3] = {a.uk, a.vk, a.wk};
@@ -1012,9 +1067,9 @@ __device__ void batch_tke_column(const KArgs &a, int grp, int i, int j, float *s
 }
 
 // Row carry of the batched family: [group][j][2][KS][32].
-template <int NW>
+template <int NW, class Ahead>
 __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int IS, int JS, bool first,
-                                      float *smem, unsigned &nmax_acc) {
+                                      float *smem, unsigned &nmax_acc, Ahead &&ahead) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
     const int ks = a.ks;
@@ -1032,6 +1087,7 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
         for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.d(k) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
     }
     __syncthreads();
+    if (threadIdx.x == 32) ahead();
     if (warp == 0 && act) {
         float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
         for (int k = c.VI; k > c.KK; --k) {
@@ -1084,9 +1140,9 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_pressure_b(KArgs a, SweepGeom
         __syncthreads();
         nmax = 0;
     };
-    gs_tasks_block<PH_PRESSURE, false>(a, g, [&](int grp, int i, int j, int IS, int JS, bool first) {
+    gs_tasks_block<PH_PRESSURE, false>(a, g, [&](int grp, int i, int j, int IS, int JS, bool first, auto &&ahead) {
         if (grp != cur) { flush(); cur = grp; }
-        batch_pressure_column<NW>(a, grp, i, j, IS, JS, first, smem, nmax);
+        batch_pressure_column<NW>(a, grp, i, j, IS, JS, first, smem, nmax, ahead);
     });
     flush();
 }
@@ -1096,16 +1152,16 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_mom_b(KArgs a, SweepGeom g) {
     extern __shared__ float smem[];
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
     constexpr bool REV = (MODEL == 1 && COMP == COMP_V);
-    gs_tasks_block<PH, REV>(a, g, [&](int grp, int i, int j, int, int, bool) {
-        batch_mom_column<MODEL, COMP, NW>(a, grp, i, j, smem);
+    gs_tasks_block<PH, REV>(a, g, [&](int grp, int i, int j, int, int, bool, auto &&ahead) {
+        batch_mom_column<MODEL, COMP, NW>(a, grp, i, j, smem, ahead);
     });
 }
 
 template <int NW, int MINB>
 __global__ void __launch_bounds__(NW * 32, MINB) k_tke_b(KArgs a, SweepGeom g) {
     extern __shared__ float smem[];
-    gs_tasks_block<PH_TKE, false>(a, g, [&](int grp, int i, int j, int, int, bool) {
-        batch_tke_column<NW>(a, grp, i, j, smem);
+    gs_tasks_block<PH_TKE, false>(a, g, [&](int grp, int i, int j, int, int, bool, auto &&ahead) {
+        batch_tke_column<NW>(a, grp, i, j, smem, ahead);
     });
 }
 
