@@ -36,7 +36,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mcell-iterations/s on 1 B200 (batched vs plain, ≤1e-4 rel err); HBM fraction"
 UNIT = "Mcell-iterations/s"
-BYTES_PER_CELL = {"pressure": 24, "velcorr": 28, "u": 20, "v": 20, "w": 20}   # model 1
+BYTES_PER_CELL = {"pressure": 24, "velcorr": 28, "u": 20, "v": 20, "w": 20,   # model 1
+                  "pvau": 24 + 28 + 20}   # fused pressure + velocity correction + averages + U
 
 
 def workload(name: str, grid: int = 400):
@@ -288,14 +289,14 @@ def device_run(dom, sits, steps: int, warmup: int, local: int, model: int = 1):
 
 
 def roofline(cells: int, steps: int, phases: dict, layout: str):
-    cand = {k: v for k, v in phases.items() if k in BYTES_PER_CELL}
+    cand = {k: v for k, v in phases.items() if k in BYTES_PER_CELL and v > 0}
     dom_k = max(cand, key=cand.get)
     per_launch_s = cand[dom_k] / steps / 1e3
     alg_bytes = cells * BYTES_PER_CELL[dom_k]
     achieved = alg_bytes / per_launch_s / 1e9
     peak, peak_kind = measured_peak()
     it_ms = sum(phases.values()) / steps
-    it_bytes = cells * sum(BYTES_PER_CELL.values())
+    it_bytes = cells * 112   # pressure 24 + velocity correction 28 + U, V, W 20 each
     return {"bound": "hbm", "kernel": dom_k, "achieved": round(achieved, 2), "peak": peak,
             "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 5),
             "traffic": profile_traffic(layout, dom_k, cells), "alg_bytes_per_launch": alg_bytes,

@@ -131,9 +131,24 @@ struct SweepGeom {
     const int *diag_start;   // [ndiag+1] cells on diagonals < d (device)
 };
 
+// Task list of the fused pressure -> velocity correction -> averages -> U wavefront (slab family,
+// model 1): steps of segments (kind, diagonal); segment q holds seg_start[q+1]-seg_start[q] tasks,
+// its code = kind | diagonal << 3.  Pressure, velocity correction and averages use geometry gp
+// (the pressure sweep range), U uses gu.
+struct FusedGeom {
+    const int *seg_start;     // [nseg+1]
+    const int *seg_code;      // [nseg]
+    int nseg;
+    SweepGeom gp, gu;
+};
+
 enum : int { ERR_NONE = 0, ERR_TIMEOUT = 1, ERR_NONFINITE = 2 };
 
-enum : int { PH_PRESSURE = 1, PH_U = 2, PH_V = 3, PH_W = 4, PH_TKE = 5, PH_DIAG = 6 };
+// Gauss-Seidel task kinds.  A column's flag carries stamp = IterationLoops*8 + kind; within an
+// iteration a column completes its kinds in increasing order (pressure, velocity correction,
+// averages, U, V, W, TKE), so one monotonic flag per column serves every kind.  The value also
+// indexes the task counters.  The diagnostic sweep has flags of its own.
+enum : int { PH_DIAG = 0, PH_PRESSURE = 1, PH_VC = 2, PH_AV = 3, PH_U = 4, PH_V = 5, PH_W = 6, PH_TKE = 7 };
 enum : int { F_GMODE1 = 1 << 13 };   // ColKE ground law uses level k+1 (Z0 >= DZK/2)
 
 __host__ __device__ inline size_t fidx(int s, int col, int ncols, int ks) {

@@ -792,6 +792,122 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom
     gs_tasks_split<PH_PRESSURE, false>(a, g, job);
 }
 
+// ---------------------------- fused wavefront, slab family --------------------------------
+// Pressure, velocity correction, averages and the model-1 U sweep of one iteration in one launch.
+// U sweeps in the pressure's direction and reads only the averages of its 3x3 neighbourhood, so
+// its front can trail the pressure front by a few diagonals instead of a whole phase.  Step s of
+// the task list holds the pressure tasks of diagonal s, the velocity corrections of diagonal s-1,
+// the averages of s-2 and the U tasks of U-diagonal s-5 (P-diagonal s-4): every dependency of a
+// task lies in an earlier step or an earlier segment of its step, so claiming in list order stays
+// deadlock-free.  Dependencies (actual coordinates, stamps it*8 + kind):
+//   velocity correction (i,j) after pressure at (i,j), (i-1,j), (i,j-1)  -- it reads their DPM and
+//                         overwrites U/V/W that pressure tasks (i-1,j), (i,j-1) read for DIV;
+//   averages (i,j) after the velocity corrections at (i,j), (i+1,j), (i,j+1);
+//   U (i,j) after the averages of the 3x3 neighbourhood (which also covers the corrected U/V/W and
+//   final DPMNEW it reads) and its two U sweep predecessors.
+
+// Lanes 0..n-1 each wait on one flag; true if all flags reached their stamp.
+__device__ __forceinline__ bool wait_lanes(const KArgs &a, const int *flag, int stamp, bool mine) {
+    bool ok = true;
+    if (mine) ok = wait_stamp(flag, stamp, a.err, a.wait_limit_ns);
+    return __all_sync(0xffffffffu, ok);
+}
+
+__global__ void __launch_bounds__(GS_WARPS * 32) k_fused_pvau(KArgs a, FusedGeom fg) {
+    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    float (*S)[KMAX_LEVELS] = sm[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int it = *a.it_global;
+    int IS, JS;
+    sweep_dir(it, IS, JS);
+    const int sP = it * 8 + PH_PRESSURE, sVC = it * 8 + PH_VC, sAV = it * 8 + PH_AV, sU = it * 8 + PH_U;
+    PressJob pj{a, S, sP};
+    pj.run_max = 0;
+    pj.run_s = -1;
+    Mom1Job<COMP_U> uj{a, S, sU};
+    const unsigned units = (unsigned)*a.nact;
+    const unsigned total = (unsigned)fg.seg_start[fg.nseg] * units;
+    unsigned int *ctr = a.counters + PH_PRESSURE;
+    const int ilo = 2, ihi = a.nii - 1, jlo = 2, jhi = a.njj - 1;   // velocity correction / averages range
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(ctr, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) break;
+        if (*(volatile int *)a.err != ERR_NONE) break;
+        int kind, uu, i1, j1;
+        {   // segment by binary search over the starts (in columns, times the number of units)
+            int lo = 0, hi = fg.nseg;
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if ((unsigned)fg.seg_start[mid] * units <= t) lo = mid; else hi = mid;
+            }
+            const int code = fg.seg_code[lo];
+            kind = code & 7;
+            const int d = code >> 3;
+            const SweepGeom &g = (kind == PH_U) ? fg.gu : fg.gp;
+            const unsigned len = (unsigned)(g.diag_start[d + 1] - g.diag_start[d]);
+            const unsigned r = t - (unsigned)fg.seg_start[lo] * units;
+            uu = (int)(r / len);
+            const int pos = (int)(r % len);
+            const int ioff = max(0, d - (g.nj - 1)) + pos;
+            i1 = g.ia + ioff;
+            j1 = g.ja + d - ioff;
+        }
+        const int s = a.act[uu];
+        const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+        const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+        int *fl = a.flags + (size_t)s * a.ncols;
+        const int col = i * a.nj2 + j;
+        int stamp;
+        if (kind == PH_PRESSURE) {
+            stamp = sP;
+            pj.pre(s, i, j, IS, JS, i1 == fg.gp.ia);
+            bool ok = true;
+            if (lane == 0) {
+                if (i1 > fg.gp.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, sP, a.err, a.wait_limit_ns);
+                if (ok && j1 > fg.gp.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), sP, a.err, a.wait_limit_ns);
+            }
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            __syncwarp();
+            if (ok) pj.post(s, IS, JS);
+        } else if (kind == PH_VC) {
+            stamp = sVC;
+            const int wi = (lane == 1) ? i - 1 : i, wj = (lane == 2) ? j - 1 : j;
+            const bool mine = lane < 3 && wi >= ilo && wj >= jlo;
+            const bool ok = wait_lanes(a, fl + wi * a.nj2 + wj, sP, mine);
+            __syncwarp();
+            if (ok && a.sit[s].active) velcorr_col<false>(a, s, col, i, j, make_acc<false>(a, s, col), lane, 32);
+        } else if (kind == PH_AV) {
+            stamp = sAV;
+            const int wi = (lane == 1) ? i + 1 : i, wj = (lane == 2) ? j + 1 : j;
+            const bool mine = lane < 3 && wi <= ihi && wj <= jhi;
+            const bool ok = wait_lanes(a, fl + wi * a.nj2 + wj, sVC, mine);
+            __syncwarp();
+            if (ok && a.sit[s].active) average_col<false>(a, col, i, j, make_acc<false>(a, s, col), lane, 32);
+        } else {
+            stamp = sU;
+            const int wi = i + (lane % 3) - 1, wj = j + (lane / 3) - 1;
+            const bool mine = lane < 9 && wi >= ilo && wi <= ihi && wj >= jlo && wj <= jhi;
+            bool ok = wait_lanes(a, fl + wi * a.nj2 + wj, sAV, mine);
+            __syncwarp();
+            if (ok) {
+                uj.pre(s, i, j, IS, JS, false);
+                if (lane == 0) {
+                    if (i1 > fg.gu.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, sU, a.err, a.wait_limit_ns);
+                    if (ok && j1 > fg.gu.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), sU, a.err, a.wait_limit_ns);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                if (ok) uj.post(s, IS, JS);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) st_release(fl + col, stamp);
+    }
+    pj.finish();
+}
+
 // DiagnosticFlowfield.Calculate's pressure sweep (DiagnosticFlowfield.cs:86-315) on the full-height
 // fields after a prognostic solve: every column of the sweep range, levels KKART+1..NKK-1, the four
 // neighbours' DPM of this sweep or the last one (plain Gauss-Seidel, DPM zeroed once before the
@@ -1282,6 +1398,14 @@ cudaError_t diag_occupancy(int ks, int *blocks_per_sm) {
 
 void launch_diag_pressure(const KArgs &a, const SweepGeom &g, const DiagTabs &t, int grid, cudaStream_t st) {
     k_diag_pressure<<<grid, GS_WARPS * 32, diag_smem(a.ks), st>>>(a, g, t);
+}
+
+cudaError_t fused_occupancy(int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_fused_pvau, GS_WARPS * 32, 0);
+}
+
+void launch_fused_pvau(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st) {
+    k_fused_pvau<<<grid, GS_WARPS * 32, 0, st>>>(a, fg);
 }
 
 }  // namespace gral

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <utility>
 #include <string>
@@ -81,7 +82,12 @@ struct gral_ctx {
     Staging sg{};
     BcLists bc{};
     Geom geo_p, geo_u, geo_v;
-    int grid_gs[6] = {0, 0, 0, 0, 0, 0};   // indexed by PH_* (1..5)
+    bool fused = false;        // fused pressure/velcorr/average/U wavefront (slab family, model 1)
+    int fused_grid = 0;
+    int lookahead_f = 6;       // GRAL_PROG_LOOKAHEAD_F: fused-kernel warps per average diagonal width
+    FusedGeom fgeo{};
+    DevBuf<int> fseg;
+    int grid_gs[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // indexed by PH_*
     cudaGraphExec_t graph = nullptr;
     float ms_upload = 0.f;
     float tune_ms[16] = {0};
@@ -110,7 +116,7 @@ struct gral_ctx {
         DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
         for (auto *b : fb) b->release();
         meta.release(); cflags.release(); colf.release(); sit.release(); colke.release(); rcw.release();
-        ddpm.release(); dtab.release(); ddt.release(); dflags.release();
+        ddpm.release(); dtab.release(); ddt.release(); dflags.release(); fseg.release();
         varw.release(); z0i.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
@@ -329,10 +335,14 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
     cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
-    launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
-    launch_velcorr(a, st);
-    launch_average(a, st);
-    launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
+    if (ctx->fused) {
+        launch_fused_pvau(a, ctx->fgeo, ctx->fused_grid, st);
+    } else {
+        launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
+        launch_velcorr(a, st);
+        launch_average(a, st);
+        launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
+    }
     launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
     launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
     if (ctx->model == 2) launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st);
@@ -346,6 +356,7 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
 int launches_per_iteration(const gral_ctx *ctx) {
     const int gs = ctx->ka.group_set <= 0 ? ctx->ngroups : ctx->ka.group_set;
     const int sets = ctx->il ? (ctx->ngroups + gs - 1) / gs : 1;
+    if (ctx->fused) return 3 + 1 + 2 + 1;
     const int phases = (ctx->model == 2) ? 5 : 4;
     return 3 + phases * sets + 3;
 }
@@ -488,6 +499,7 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
     if (const char *v = std::getenv("GRAL_PROG_BATCH_VARIANT")) ctx->forced_variant = std::atoi(v);
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD")) ctx->lookahead = std::max(0, std::atoi(v));
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD_P")) ctx->lookahead_p = std::max(0, std::atoi(v));
+    if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD_F")) ctx->lookahead_f = std::max(0, std::atoi(v));
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return GRAL_ECUDA; }
     for (auto &e : ctx->ev)
@@ -759,6 +771,49 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     put_geom(ctx->geo_p);
     put_geom(ctx->geo_u);
     put_geom(ctx->geo_v);
+
+    // task list of the fused pressure/velcorr/average/U wavefront: step s holds pressure diagonal
+    // s, velocity-correction diagonal s-1, averages s-2 and U-diagonal s-5 (P-diagonal s-4)
+    {
+        const char *fz = std::getenv("GRAL_PROG_FUSE");
+        ctx->fused = !il && ctx->model == 1 && !(fz && std::atoi(fz) == 0);
+        if (ctx->fused) {
+            const Geom &gp = ctx->geo_p, &gu = ctx->geo_u;
+            const int DP = gp.g.ndiag, DU = gu.g.ndiag;
+            std::vector<int> start(1, 0), code;
+            auto add = [&](int kind, const Geom &G, int d) {
+                code.push_back(kind | (d << 3));
+                start.push_back(start.back() + (G.ds[d + 1] - G.ds[d]));
+            };
+            // U trails the pressure by lag_u >= 4 P-diagonals (its averages' neighbourhood must be
+            // complete); more lag lets its pre-wait work start before its U predecessors finish
+            int lag_u = 16;
+            if (const char *v = std::getenv("GRAL_PROG_FUSE_LAG")) lag_u = std::max(4, std::atoi(v));
+            const int steps = std::max(DP + 2, DU + lag_u + 1);
+            for (int q = 0; q < steps; ++q) {
+                if (q < DP) add(PH_PRESSURE, gp, q);
+                if (q - 1 >= 0 && q - 1 < DP) add(PH_VC, gp, q - 1);
+                if (q - 2 >= 0 && q - 2 < DP) add(PH_AV, gp, q - 2);
+                const int du = q - lag_u - 1;               // U-diagonal du is P-diagonal du + 1
+                if (du >= 0 && du < DU) add(PH_U, gu, du);
+            }
+            CK(ctx->fseg.ensure(start.size() + code.size()));
+            CK(cudaMemcpyAsync(ctx->fseg.p, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(ctx->fseg.p + start.size(), code.data(), code.size() * sizeof(int),
+                               cudaMemcpyHostToDevice, st));
+            ctx->fgeo.seg_start = ctx->fseg.p;
+            ctx->fgeo.seg_code = ctx->fseg.p + start.size();
+            ctx->fgeo.nseg = (int)code.size();
+            ctx->fgeo.gp = gp.g;
+            ctx->fgeo.gu = gu.g;
+            int bps = 0;
+            CK(fused_occupancy(&bps));
+            const double width = (double)n * (NII - 3) * (NJJ - 3) / std::max(1, NII + NJJ - 7);
+            const long long want = (long long)std::ceil(ctx->lookahead_f * 2.0 * width / 4.0);
+            ctx->fused_grid = (int)std::max<long long>(ctx->num_sms,
+                                                       std::min<long long>((long long)std::max(1, bps) * ctx->num_sms, want));
+        }
+    }
     int *bp = ctx->bcl.p;
     auto put_ints = [&](const std::vector<int> &v) {
         int *dst = bp;
@@ -902,31 +957,35 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
     int trc = tune_variants(ctx);
     if (trc != GRAL_OK) return trc;
     const KArgs &a = ctx->ka;
-    const int marks = GRAL_NUM_PHASES + 1;
+    // the iteration's launches in order, each tagged with the phase it is timed under
+    std::vector<std::pair<int, std::function<void()>>> seq;
+    seq.push_back({GRAL_PHASE_BC, [&] {
+        cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
+        launch_bc(a, ctx->bc, st);
+    }});
+    if (ctx->fused) {
+        seq.push_back({GRAL_PHASE_FUSED, [&] { launch_fused_pvau(a, ctx->fgeo, ctx->fused_grid, st); }});
+    } else {
+        seq.push_back({GRAL_PHASE_PRESSURE, [&] { launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st); }});
+        seq.push_back({GRAL_PHASE_VELCORR, [&] { launch_velcorr(a, st); }});
+        seq.push_back({GRAL_PHASE_AVERAGE, [&] { launch_average(a, st); }});
+        seq.push_back({GRAL_PHASE_U, [&] { launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st); }});
+    }
+    seq.push_back({GRAL_PHASE_V, [&] { launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st); }});
+    seq.push_back({GRAL_PHASE_W, [&] { launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st); }});
+    if (ctx->model == 2)
+        seq.push_back({GRAL_PHASE_TKE, [&] { launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st); }});
+    seq.push_back({GRAL_PHASE_BOOKKEEPING, [&] { launch_bookkeeping(a, st); }});
+    const int marks = (int)seq.size() + 1;
     std::vector<cudaEvent_t> ev((size_t)iterations * marks, nullptr);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     for (int it = 0; it < iterations; ++it) {
         cudaEvent_t *E = ev.data() + (size_t)it * marks;
-        CK(cudaEventRecord(E[GRAL_PHASE_BC], st));
-        CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st));
-        launch_bc(a, ctx->bc, st);
-        CK(cudaEventRecord(E[GRAL_PHASE_PRESSURE], st));
-        launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
-        CK(cudaEventRecord(E[GRAL_PHASE_VELCORR], st));
-        launch_velcorr(a, st);
-        CK(cudaEventRecord(E[GRAL_PHASE_AVERAGE], st));
-        launch_average(a, st);
-        CK(cudaEventRecord(E[GRAL_PHASE_U], st));
-        launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
-        CK(cudaEventRecord(E[GRAL_PHASE_V], st));
-        launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
-        CK(cudaEventRecord(E[GRAL_PHASE_W], st));
-        launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
-        CK(cudaEventRecord(E[GRAL_PHASE_TKE], st));
-        if (ctx->model == 2) launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st);
-        CK(cudaEventRecord(E[GRAL_PHASE_BOOKKEEPING], st));
-        launch_bookkeeping(a, st);
-        CK(cudaEventRecord(E[GRAL_NUM_PHASES], st));
+        for (size_t q = 0; q < seq.size(); ++q) {
+            CK(cudaEventRecord(E[q], st));
+            seq[q].second();
+        }
+        CK(cudaEventRecord(E[seq.size()], st));
     }
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(st));
@@ -935,10 +994,10 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
     double ph[GRAL_NUM_PHASES] = {0};
     for (int it = 0; it < iterations; ++it) {
         cudaEvent_t *E = ev.data() + (size_t)it * marks;
-        for (int q = 0; q < GRAL_NUM_PHASES; ++q) {
+        for (size_t q = 0; q < seq.size(); ++q) {
             float ms = 0.f;
             CK(cudaEventElapsedTime(&ms, E[q], E[q + 1]));
-            ph[q] += ms;
+            ph[seq[q].first] += ms;
         }
     }
     float tot = 0.f;

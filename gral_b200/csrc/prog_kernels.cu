@@ -161,28 +161,7 @@ __global__ void k_bc_top(KArgs a) {
 template <bool IL>
 __global__ void k_velcorr(KArgs a) {
     col_loop<IL>(a, true, [&](int s, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
-        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
-        if (!(a.cflags[col] & F_VC)) return;
-        const ColMeta m = a.meta[col];
-        const SitDev &sd = a.sit[s];
-        const float DT = sd.dtime, DXK = a.dxk, DYK = a.dyk;
-        const double fr = sd.frund;
-        const int q = sd.quantise;
-        const long long dW = -(long long)a.nj2;
-#pragma unroll 4
-        for (int k = kbeg; k <= m.vi; k += kstep) {
-            if (k < 1) continue;
-            const float d = a.dpm[x.at(0, k)];
-            if (i > 2 && m.kkm_u < k)
-                a.uk[x.at(0, k)] = (float)quantd((double)(a.uk[x.at(0, k)] + (a.dpm[x.at(dW, k)] - d) / DXK * DT), fr, q);
-            if (j > 2 && m.kkm_v < k)
-                a.vk[x.at(0, k)] = (float)quantd((double)(a.vk[x.at(0, k)] + (a.dpm[x.at(-1, k)] - d) / DYK * DT), fr, q);
-            if (m.kkart + 1 < k)
-                a.wk[x.at(0, k)] = (float)quantd(
-                    (double)(a.wk[x.at(0, k)] + (a.dpm[x.at(0, k - 1)] - d) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, q);
-            else
-                a.wk[x.at(0, k)] = 0;
-        }
+        velcorr_col<IL>(a, s, col, i, j, x, kbeg, kstep);
     });
 }
 
@@ -190,33 +169,7 @@ __global__ void k_velcorr(KArgs a) {
 template <bool IL>
 __global__ void k_average(KArgs a) {
     auto body = [&](int, int col, int i, int j, const Acc<IL> &x, int kbeg, int kstep) {
-        if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
-        if (!(a.cflags[col] & F_VC)) return;
-        const ColMeta m = a.meta[col];
-        const int nj2 = a.nj2;
-        const long long dE = nj2;
-        const int KK = m.kkart;
-        const bool cpS = (j == 2);
-        const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
-#pragma unroll 4
-        for (int k = kbeg; k <= m.vi; k += kstep) {
-            if (k < m.kstart) continue;
-            if (KK < k) {
-                a.uks[x.at(0, k)] = 0.5f * (a.uk[x.at(0, k)] + a.uk[x.at(dE, k)]);
-                a.vks[x.at(0, k)] = 0.5f * (a.vk[x.at(0, k)] + a.vk[x.at(1, k)]);
-            }
-            if (KK + 1 < k) a.wks[x.at(0, k)] = 0.5f * (a.wk[x.at(0, k)] + a.wk[x.at(0, k + 1)]);
-            if (cpS) a.uks[x.at(-1, k)] = a.uks[x.at(0, k)];
-            if (cpN) a.uks[x.at(1, k)] = a.uks[x.at(0, k)];
-        }
-        // VKS[1][j] = VKS[2][j] and VKS[NII][j] = VKS[NII-1][j] on every level (:1018-1036)
-        const bool west = (i == 2) && (a.cflags[1 * nj2 + j] & F_ADV);
-        const bool east = (i == a.nii - 1) && (a.cflags[col] & F_ADV);
-        if (west || east) {
-            const long long dd = west ? -(long long)nj2 : dE;
-#pragma unroll 4
-            for (int k = kbeg; k < a.ks; k += kstep) a.vks[x.at(dd, k)] = a.vks[x.at(0, k)];
-        }
+        average_col<IL>(a, col, i, j, x, kbeg, kstep);
     };
     col_loop<IL, true>(a, true, body);
 }

@@ -28,6 +28,9 @@ cudaError_t gs_prepare(bool il, int ks, int model);
 cudaError_t gs_occupancy(bool il, int kind, int model, int ks, int variant, int *blocks_per_sm);
 // one Gauss-Seidel phase (kind = PH_PRESSURE, PH_U, PH_V, PH_W or PH_TKE) of the loaded model
 void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
+// pressure + velocity correction + averages + model-1 U in one wavefront launch (slab family)
+cudaError_t fused_occupancy(int *blocks_per_sm);
+void launch_fused_pvau(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st);
 
 void launch_bc(const KArgs &a, const BcLists &bc, cudaStream_t st);
 void launch_velcorr(const KArgs &a, cudaStream_t st);

@@ -24,7 +24,7 @@ EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_pro
            "gral_prog_load", "gral_prog_iterate", "gral_prog_iterate_timed", "gral_prog_store",
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc"]
 
-PHASES = ["bc", "pressure", "velcorr", "average", "u", "v", "w", "tke", "bookkeeping"]
+PHASES = ["bc", "pressure", "velcorr", "average", "u", "v", "w", "tke", "bookkeeping", "pvau"]
 
 
 class GralError(RuntimeError):

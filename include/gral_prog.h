@@ -156,7 +156,7 @@ int gral_prog_iterate(gral_ctx *ctx);
 int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats);
 
 /* Phases of one SIMPLE iteration, in launch order, as reported by gral_prog_iterate_timed. */
-#define GRAL_NUM_PHASES 9
+#define GRAL_NUM_PHASES 10
 #define GRAL_PHASE_BC 0          /* lateral and top boundary conditions, PrognosticFlowfield.cs:595-714 */
 #define GRAL_PHASE_PRESSURE 1    /* divergence + pressure-correction TDMA sweep, :723-901 */
 #define GRAL_PHASE_VELCORR 2     /* velocity correction with Frund rounding, :904-949 */
@@ -166,6 +166,8 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats);
 #define GRAL_PHASE_W 6           /* W momentum */
 #define GRAL_PHASE_TKE 7         /* k and eps transport (model 2) */
 #define GRAL_PHASE_BOOKKEEPING 8 /* convergence bookkeeping, :1144-1178 */
+#define GRAL_PHASE_FUSED 9       /* pressure, velocity correction, averages and U in one wavefront
+                                    launch (slab layout, model 1); phases 1-4 then read 0 */
 
 /* Instrumentation: runs exactly `iterations` SIMPLE iterations on the loaded situations (the
  * convergence bookkeeping still runs, so a situation that meets the reference's stop rule stops
