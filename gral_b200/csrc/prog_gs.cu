@@ -1150,12 +1150,12 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
     }
     __syncthreads();
     if (threadIdx.x == 32) ahead();
-    if (warp != 0 || !act) return;
     float *F = comp_field<COMP>(a);
     const int kkm = back_limit<COMP>(c);
-    mom_sweep<MODEL, COMP>(R, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x.at(0, c.VI + 1)));
-    for (int k = c.K0; k <= c.VI; ++k)
-        if (kkm < k) __stcg(F + x.at(0, k), R.p(k));
+    if (warp == 0 && act) mom_sweep<MODEL, COMP>(R, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x.at(0, c.VI + 1)));
+    __syncthreads();
+    if (!act) return;
+    for (int k = max(c.K0, kkm + 1) + warp; k <= c.VI; k += NW) __stcg(F + x.at(0, k), R.p(k));
 }
 
 template <int NW, class Ahead>
