@@ -746,7 +746,10 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     a.nact = ctx->misc.p + 1;
     a.it_global = ctx->misc.p + 2;
     a.act = ctx->misc.p + 3;
+    // bound of every device-side spin wait (GRAL_PROG_WAIT_NS overrides it, e.g. to exercise the
+    // timeout path: the waiting kernel sets the error word and returns, the context stays usable)
     a.wait_limit_ns = 2000000000ull;
+    if (const char *v = std::getenv("GRAL_PROG_WAIT_NS")) a.wait_limit_ns = std::strtoull(v, nullptr, 10);
     a.trace = ctx->trace.p;
     a.trace_cap = tcap;
     a.vi_min = vi_min;

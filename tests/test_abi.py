@@ -96,3 +96,12 @@ def test_create_without_gpu_fails_cleanly():
 def test_params_mirror_rejects_missing_keys():
     with pytest.raises(KeyError):
         abi.params_to_c({"nii": 4})
+
+
+def test_phase_names_match_header():
+    from gral_b200.prognostic import PHASES
+    text = open(HEADER).read()
+    n = int(re.search(r"#define GRAL_NUM_PHASES (\d+)", text).group(1))
+    assert len(PHASES) == n
+    ids = {int(v): k for k, v in re.findall(r"#define GRAL_PHASE_(\w+) (\d+)", text)}
+    assert sorted(ids) == list(range(n))
