@@ -14,6 +14,10 @@ model; synthetic, seeded inputs.
              against the measured HBM copy bandwidth.
   cpu_baseline  the CPU oracle (a single-threaded restatement of the reference's deterministic
              solver) on a bounded sample of the same workload.
+  gff        the flow-field cache writer/reader (GFFWrite.cs / GFFRead.cs formats) on the same
+             grid: device pack kernel per format (CUDA events, L2 flushed before each launch)
+             against HBM bandwidth, the host-timed pack into pinned memory and read back, and
+             the numpy restatement of the writer timed on one core.
 
 `--impl reference` times that CPU restatement on all host cores (one independent situation per
 worker process) on the same workload and prints the same metric.
@@ -303,6 +307,57 @@ def roofline(cells: int, steps: int, phases: dict, layout: str):
             "hbm_frac_iteration": round(it_bytes / (it_ms / 1e3) / 1e9 / peak, 5)}
 
 
+def gff_measure(dom, sit, repeats: int = 10):
+    """Flow-field cache payloads of one solved situation of `dom` (rank 0 only)."""
+    import torch
+    from gral_b200 import prep
+    from gral_b200.abi import FieldArrays
+    from gral_b200.prognostic import GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, PrognosticSolver
+    from oracle import gff as O
+
+    f = prep.initial_fields(dom, sit)
+    peak, peak_kind = measured_peak()
+    out = {"workload": f"one situation, {dom.nii}x{dom.njj}x{dom.nkk} grid, fields resident after a store",
+           "formats": {}}
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
+        s.load([dom.params(sit, iterations=1)], dom.static, [f])
+        s.store([f])
+        for mode, name in ((GFF_COLUMNS, "columns_-1"), (GFF_LEVELS, "levels_-2"), (GFF_TERRAIN, "terrain_-3")):
+            nbytes = s.gff_size(mode)
+            words = (nbytes - 32) // 2
+            kk_words = dom.nii * dom.njj if mode == GFF_TERRAIN else 0
+            # per value word: one float read (4 B) and one int16 written (2 B); KKART words 2 B each way
+            alg = 6 * (words - kk_words) + 4 * kk_words
+            s.gff_pack_timed(0, mode, 3)
+            ms = s.gff_pack_timed(0, mode, repeats)
+            buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True).numpy()
+            s.gff_pack(0, mode, 225.0, 2.0, 4, out=buf)
+            t0 = time.perf_counter()
+            for _ in range(repeats):
+                s.gff_pack(0, mode, 225.0, 2.0, 4, out=buf)
+            pack_ms = (time.perf_counter() - t0) / repeats * 1e3
+            uk, vk, wk = (torch.empty(f.uk.shape, dtype=torch.float32, pin_memory=True).numpy() for _ in range(3))
+            tgt = FieldArrays(uk, vk, wk)
+            s.gff_unpack(buf, dom.nii, dom.njj, dom.nkk, dom.dxk, kkart=dom.static.kkart, out=tgt)
+            t0 = time.perf_counter()
+            for _ in range(repeats):
+                s.gff_unpack(buf, dom.nii, dom.njj, dom.nkk, dom.dxk, kkart=dom.static.kkart, out=tgt)
+            unpack_ms = (time.perf_counter() - t0) / repeats * 1e3
+            ent = {"payload_bytes": nbytes, "alg_bytes_per_launch": alg,
+                   "kernel_us": round(ms * 1e3, 2),
+                   "roofline": {"bound": "hbm", "achieved": round(alg / (ms / 1e3) / 1e9, 1), "peak": peak,
+                                "unit": "GB/s", "frac": round(alg / (ms / 1e3) / 1e9 / peak, 4),
+                                "peak_kind": peak_kind},
+                   "pack_e2e_ms": round(pack_ms, 3), "unpack_e2e_ms": round(unpack_ms, 3)}
+            if mode != GFF_TERRAIN:
+                t0 = time.perf_counter()
+                O.pack(mode, f.uk, f.vk, f.wk, kkart=dom.static.kkart, dxk=dom.dxk)
+                ent["cpu_pack_ms"] = round((time.perf_counter() - t0) * 1e3, 2)
+                ent["cpu_kind"] = "numpy restatement, 1 core"
+            out["formats"][name] = ent
+    return out
+
+
 def run_ours(args, rank, world):
     import torch
     from gral_b200 import prep
@@ -364,6 +419,10 @@ def run_ours(args, rank, world):
                    "phase_ms_per_iteration": {k: round(v / args.batched_steps, 4) for k, v in bph.items() if v > 0},
                    "clocks": bclk}
 
+    gffm = None
+    if rank == 0 and args.workload == "production" and not args.no_gff:
+        gffm = gff_measure(dom, sit)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, dt = cpu_sample("production" if args.workload == "batched" else args.workload, args.cpu_iters)
@@ -382,7 +441,7 @@ def run_ours(args, rank, world):
                    "layout": layout, "launch_variant": st_store["launch_variant"]},
         "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
         "roofline": roofline(cells, args.steps, phases, layout),
-        "cpu_baseline": cpu, "e2e": e2e, "batched": batched,
+        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm,
         "gpu_launches": st_store["launches_per_iteration"] * args.steps,
         "clocks": clocks,
     }
@@ -407,6 +466,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-measurement")
     ap.add_argument("--batched-steps", type=int, default=10)
+    ap.add_argument("--no-gff", action="store_true", help="skip the flow-field cache payload measurement")
     ap.add_argument("--ref-iters", type=int, default=4)
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-warmup", action="store_true")

@@ -22,7 +22,12 @@ _lib = None
 
 EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_prog_solve_batch",
            "gral_prog_load", "gral_prog_iterate", "gral_prog_iterate_timed", "gral_prog_store",
-           "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc"]
+           "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
+           "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack"]
+
+# payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
+GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, GFF_TKE = 0, 1, 2, 3
+GFF_HEADER_BYTES = 32
 
 PHASES = ["bc", "pressure", "velcorr", "average", "u", "v", "w", "tke", "bookkeeping", "pvau"]
 
@@ -73,6 +78,18 @@ def lib(build_if_stale: bool = True):
     L.gral_prog_check_speeds_noalloc.argtypes = [C.c_int32] * 4 + [C.c_double] + [C.c_void_p] * 5 + \
         [C.POINTER(C.c_int32), C.c_void_p]
     L.gral_prog_check_speeds_noalloc.restype = C.c_int
+    L.gral_prog_gff_size.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_uint64)]
+    L.gral_prog_gff_size.restype = C.c_int
+    L.gral_prog_gff_pack.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32,
+                                     C.c_void_p, C.c_uint64]
+    L.gral_prog_gff_pack.restype = C.c_int
+    L.gral_prog_gff_pack_timed.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]
+    L.gral_prog_gff_pack_timed.restype = C.c_int
+    L.gral_prog_gff_unpack.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_int32, C.c_int32,
+                                       C.c_float, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32)]
+    L.gral_prog_gff_unpack.restype = C.c_int
     _lib = L
     return L
 
@@ -159,6 +176,50 @@ class PrognosticSolver:
         st = self._stats_array(n, traces)
         self._check(self._L.gral_prog_store(self._ctx, fa, st))
         return [stats_to_dict(st[b]) for b in range(n)]
+
+    # flow-field cache payloads (GFFWrite.cs / GFFRead.cs); the zip container stays with the caller
+    def gff_size(self, mode: int) -> int:
+        n = C.c_uint64()
+        self._check(self._L.gral_prog_gff_size(self._ctx, mode, C.byref(n)))
+        return n.value
+
+    def gff_pack(self, situation: int, mode: int, wind_dir: float = 0.0, wind_speed: float = 0.0,
+                 stability_class: int = 0, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Payload bytes (header + data) of one situation of the last store, packed on the GPU."""
+        n = self.gff_size(mode)
+        if out is None:
+            out = np.empty(n, np.uint8)
+        self._check(self._L.gral_prog_gff_pack(self._ctx, situation, mode, wind_dir, wind_speed, stability_class,
+                                               out.ctypes.data, out.nbytes))
+        return out[:n]
+
+    def gff_pack_timed(self, situation: int, mode: int, repeats: int) -> float:
+        """Mean device ms of one pack launch (L2 flushed before each), no copy to the host."""
+        ms = C.c_double()
+        self._check(self._L.gral_prog_gff_pack_timed(self._ctx, situation, mode, repeats, C.byref(ms)))
+        return ms.value
+
+    def gff_unpack(self, payload, nii: int, njj: int, nkk: int, dxk: float,
+                   kkart: Optional[np.ndarray] = None, out: Optional[FieldArrays] = None):
+        """Read a flow-field payload on the GPU into flat [NII+2][NJJ+2][NKK+2] arrays.
+
+        Returns ``(uk, vk, wk, (wind_dir, wind_speed, stability_class, flag))``; with a format flag
+        the reference's reader skips (not -1, -2, -3) the arrays come back untouched.
+        """
+        buf = payload if isinstance(payload, np.ndarray) else np.frombuffer(bytes(payload), np.uint8)
+        buf = np.ascontiguousarray(buf, np.uint8)
+        shape = (nii + 2, njj + 2, nkk + 2)
+        if out is None:
+            uk, vk, wk = (np.zeros(shape, np.float32) for _ in range(3))
+        else:
+            uk, vk, wk = out.uk, out.vk, out.wk
+        kk = None if kkart is None else np.ascontiguousarray(kkart, np.int16)
+        d, v, st, fl = C.c_float(), C.c_float(), C.c_int32(), C.c_int32()
+        self._check(self._L.gral_prog_gff_unpack(self._ctx, buf.ctypes.data, buf.nbytes, nii, njj, nkk, dxk,
+                                                 None if kk is None else kk.ctypes.data, uk.ctypes.data,
+                                                 vk.ctypes.data, wk.ctypes.data, C.byref(d), C.byref(v),
+                                                 C.byref(st), C.byref(fl)))
+        return uk, vk, wk, (d.value, v.value, st.value, fl.value)
 
 
 def check_speeds_noalloc(nii: int, njj: int, nkk: int, vert_cells_ff: int, geschw_max: float,

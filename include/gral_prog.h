@@ -176,6 +176,54 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats);
  * each phase, total_ms the device time of the whole run.  Either pointer may be NULL. */
 int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms, double *total_ms);
 
+/* GRAL flow-field and turbulence cache files (GFFWrite.cs, GFFRead.cs).  The reference writes
+ * each as a zip archive holding one entry; these calls produce and consume that entry's bytes
+ * (the host does the zip step).  Every payload starts with the same 32-byte little-endian header:
+ * int32 NKK (negated in modes 1 and 2), int32 NJJ, int32 NII, float wind direction, float wind
+ * speed, int32 stability class, float DXK, int32 format flag (-1, -2, -3; -1 for the .tke file).
+ * Values are int16 of 100 x the field value, clamped to the int16 range.
+ *   GRAL_GFF_COLUMNS  flag -1 (GFFWrite.cs:167-254): i = 1..NII+1, j = 1..NJJ+1, k = 1..NKK+1,
+ *                     U[k-1], V[k-1], W[k] interleaved per level; truncating conversion.
+ *   GRAL_GFF_LEVELS   flag -2 (:256-386): k outer, then rows i, each row U, V, W over j.
+ *   GRAL_GFF_TERRAIN  flag -3 (:388-520): KKART of i = 1..NII, j = 1..NJJ, then per column the
+ *                     levels k = max(KKART,1)..NKK+1 of U, then V, then W; round-half-even.
+ *   GRAL_GFF_TKE      the .tke file of model 2 (:83-133): TURB of i = 1..NII, j = 1..NJJ,
+ *                     k = 1..NKK, round-half-even; a non-finite value fails (GRAL_ENONFINITE),
+ *                     where the reference's conversion throws and the file is deleted. */
+#define GRAL_GFF_COLUMNS 0
+#define GRAL_GFF_LEVELS 1
+#define GRAL_GFF_TERRAIN 2
+#define GRAL_GFF_TKE 3
+#define GRAL_GFF_HEADER_BYTES 32
+
+/* Size in bytes of the payload `mode` gives for the loaded grid (mode 2 depends on its KKART). */
+int gral_prog_gff_size(gral_ctx *ctx, int32_t mode, uint64_t *bytes);
+
+/* Packs the payload of situation `situation` of the last gral_prog_store on the device from the
+ * fields that stay resident there until the next load (the values gral_prog_store returned,
+ * after the diagnostic step when post_diagnostic is set), into host memory `out` of `capacity`
+ * bytes (at least gral_prog_gff_size). */
+int gral_prog_gff_pack(gral_ctx *ctx, int32_t situation, int32_t mode, float wind_dir, float wind_speed,
+                       int32_t stability_class, uint8_t *out, uint64_t capacity);
+
+/* Instrumentation: runs the device pack of gral_prog_gff_pack `repeats` times on the stored
+ * situation (no copy to the host), with L2 flushed by a 256 MiB device write before each launch,
+ * and returns the mean device time of one pack launch in *kernel_ms. */
+int gral_prog_gff_pack_timed(gral_ctx *ctx, int32_t situation, int32_t mode, int32_t repeats, double *kernel_ms);
+
+/* Reads a flow-field payload of any of the three formats (GFFRead.cs:181-320) on the device into
+ * flat [NII+2][NJJ+2][NKK+2] host arrays uk, vk, wk (the layout of gral_fields): the entries the
+ * file holds are set from it (value int16 * 0.01f), those of the terrain format below KKART to 0,
+ * all other entries to 0.  The header must match nii, njj, |nkk| and dxk, and in the terrain
+ * format the file's KKART must equal `kkart` ([NII+2][NJJ+2], needed only for that format), else
+ * GRAL_EINVAL, as the reference rejects such a file.  A format flag other than -1, -2, -3 makes
+ * the reference read nothing further and succeed: then the arrays are left untouched and
+ * *format is set to that flag.  wind_dir, wind_speed, stability_class and format may be NULL.
+ * The context needs no load; the grid must fit its capacity. */
+int gral_prog_gff_unpack(gral_ctx *ctx, const uint8_t *payload, uint64_t bytes, int32_t nii, int32_t njj,
+                         int32_t nkk, float dxk, const int16_t *kkart, float *uk, float *vk, float *wk,
+                         float *wind_dir, float *wind_speed, int32_t *stability_class, int32_t *format);
+
 /* Text of the last error on this context (never NULL). */
 const char *gral_prog_last_error(gral_ctx *ctx);
 
