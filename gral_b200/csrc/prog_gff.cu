@@ -17,18 +17,15 @@ constexpr int kThreads = 256;
 // and the clamp-then-cast of :296-309, which give the same result for every input: the product
 // is clamped to [-32768, 32767] and truncated toward zero; NaN converts to 0 (the x64 JIT's
 // truncating conversion of NaN is 0x80000000, whose low 16 bits are 0; newer runtimes saturate
-// NaN to 0 as well).
+// NaN to 0 as well).  The float-to-int32 conversion saturates and maps NaN to 0, so an integer
+// clamp after it gives exactly that.
 __device__ __forceinline__ short to_i16_trunc(float x) {
-    const float v = x * 100.0f;
-    if (v != v) return 0;
-    return (short)__float2int_rz(fminf(fmaxf(v, -32768.0f), 32767.0f));
+    return (short)max(-32768, min(32767, __float2int_rz(x * 100.0f)));
 }
 
 // MathF.Round(x * 100) (round half to even), then the clamp and cast of GFFWrite.cs:446-458.
 __device__ __forceinline__ short to_i16_round(float x) {
-    const float v = rintf(x * 100.0f);
-    if (v != v) return 0;
-    return (short)__float2int_rz(fminf(fmaxf(v, -32768.0f), 32767.0f));
+    return (short)max(-32768, min(32767, __float2int_rn(x * 100.0f)));
 }
 
 // (float)(int16 * 0.01F) of GFFRead.cs:223-227, 249-253 and 298-308: one float multiply.
@@ -39,45 +36,60 @@ __device__ __forceinline__ size_t col_base(const GffGrid &g, int i, int j) {
 }
 
 // ---- flag -1: i, j outer, k inner, U[k-1], V[k-1], W[k] interleaved (GFFWrite.cs:189-220) ----
-// One thread per (column, level); the warp's 32 levels are consecutive floats of one or two
-// columns and 192 consecutive payload bytes.
-__global__ void __launch_bounds__(kThreads) k_pack_columns(GffGrid g, const float *__restrict__ uk,
-                                                           const float *__restrict__ vk,
-                                                           const float *__restrict__ wk, short *__restrict__ out) {
+// Block 32 x 8: warp y takes one column, its lanes the levels (two passes of 32 levels unrolled,
+// so each thread has six loads in flight).  A warp's 32 levels are 128 consecutive bytes of
+// each field and 192 consecutive payload bytes; the (i, j) decode happens once per thread.
+constexpr int kColsPerBlock = 8;
+
+__global__ void __launch_bounds__(32 * kColsPerBlock) k_pack_columns(GffGrid g, const float *__restrict__ uk,
+                                                                     const float *__restrict__ vk,
+                                                                     const float *__restrict__ wk,
+                                                                     short *__restrict__ out) {
     const int nk = g.nkk + 1, nj = g.njj + 1;
-    const long long n = (long long)(g.nii + 1) * nj * nk;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int k = (int)(t % nk) + 1;
-    const long long c = t / nk;
-    const int j = (int)(c % nj) + 1, i = (int)(c / nj) + 1;
-    const size_t b = col_base(g, i, j);
-    short *o = out + 3 * t;
-    o[0] = to_i16_trunc(uk[b + k - 1]);
-    o[1] = to_i16_trunc(vk[b + k - 1]);
-    o[2] = to_i16_trunc(wk[b + k]);
+    const unsigned c = blockIdx.x * kColsPerBlock + threadIdx.y;   // payload column (i-1)*nj + (j-1)
+    if (c >= (unsigned)(g.nii + 1) * nj) return;
+    const int i = c / nj + 1, j = c % nj + 1;
+    const float *u = uk + col_base(g, i, j), *v = vk + col_base(g, i, j), *w = wk + col_base(g, i, j) + 1;
+    short *o = out + (size_t)c * nk * 3;
+    for (int k = threadIdx.x; k < nk; k += 64) {
+        const int k2 = k + 32;
+        const bool two = k2 < nk;
+        const float u0 = u[k], v0 = v[k], w0 = w[k];
+        float u1 = 0.f, v1 = 0.f, w1 = 0.f;
+        if (two) { u1 = u[k2]; v1 = v[k2]; w1 = w[k2]; }
+        o[3 * k] = to_i16_trunc(u0);
+        o[3 * k + 1] = to_i16_trunc(v0);
+        o[3 * k + 2] = to_i16_trunc(w0);
+        if (two) {
+            o[3 * k2] = to_i16_trunc(u1);
+            o[3 * k2 + 1] = to_i16_trunc(v1);
+            o[3 * k2 + 2] = to_i16_trunc(w1);
+        }
+    }
 }
 
-__global__ void __launch_bounds__(kThreads) k_unpack_columns(GffGrid g, const short *__restrict__ in,
-                                                             float *__restrict__ uk, float *__restrict__ vk,
-                                                             float *__restrict__ wk) {
+__global__ void __launch_bounds__(32 * kColsPerBlock) k_unpack_columns(GffGrid g, const short *__restrict__ in,
+                                                                       float *__restrict__ uk,
+                                                                       float *__restrict__ vk,
+                                                                       float *__restrict__ wk) {
     const int nk = g.nkk + 1, nj = g.njj + 1;
-    const long long n = (long long)(g.nii + 1) * nj * nk;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int k = (int)(t % nk) + 1;
-    const long long c = t / nk;
-    const int j = (int)(c % nj) + 1, i = (int)(c / nj) + 1;
-    const size_t b = col_base(g, i, j);
-    const short *p = in + 3 * t;
-    uk[b + k - 1] = from_i16(p[0]);
-    vk[b + k - 1] = from_i16(p[1]);
-    wk[b + k] = from_i16(p[2]);
+    const unsigned c = blockIdx.x * kColsPerBlock + threadIdx.y;
+    if (c >= (unsigned)(g.nii + 1) * nj) return;
+    const int i = c / nj + 1, j = c % nj + 1;
+    float *u = uk + col_base(g, i, j), *v = vk + col_base(g, i, j), *w = wk + col_base(g, i, j) + 1;
+    const short *p = in + (size_t)c * nk * 3;
+    for (int k = threadIdx.x; k < nk; k += 32) {
+        const short a = p[3 * k], b = p[3 * k + 1], d = p[3 * k + 2];
+        u[k] = from_i16(a);
+        v[k] = from_i16(b);
+        w[k] = from_i16(d);
+    }
 }
 
 // ---- flag -2: k outer, rows i, each row U, V, W over j (GFFWrite.cs:277-328) ----
 // The fields are k-fastest and the payload j-fastest: a 32x32 (j, k) tile per block goes through
-// shared memory, read along k and written along j.  Block 32x8, grid (j tiles, k tiles, rows).
+// shared memory, read along k and written along j.  Block 32x8 (32x4 measured slower), grid
+// (j tiles, k tiles, rows).
 constexpr int kTile = 32, kRowsPerPass = 8;
 
 __global__ void __launch_bounds__(kTile * kRowsPerPass) k_pack_levels(GffGrid g, const float *__restrict__ uk,
@@ -156,12 +168,22 @@ __global__ void __launch_bounds__(kThreads) k_pack_terrain(GffGrid g, const floa
     if (lane == 0 && i <= g.nii && j <= g.njj) out[(size_t)(i - 1) * g.njj + (j - 1)] = (short)kkart;
     const int k0 = max(kkart, 1), n = g.nkk + 2 - k0;
     short *o = out + (size_t)g.nii * g.njj + off[w];
-    const size_t b = col_base(g, i, j);
-    for (int m = lane; m < n; m += 32) {
-        const int k = k0 + m;
-        o[m] = to_i16_round(uk[b + k - 1]);
-        o[n + m] = to_i16_round(vk[b + k - 1]);
-        o[2 * n + m] = to_i16_round(wk[b + k]);
+    const size_t b = col_base(g, i, j) + k0;
+    const float *u = uk + b - 1, *v = vk + b - 1, *wz = wk + b;
+    for (int m = lane; m < n; m += 64) {      // two passes of 32 levels with their loads in flight
+        const int m2 = m + 32;
+        const bool two = m2 < n;
+        const float u0 = u[m], v0 = v[m], w0 = wz[m];
+        float u1 = 0.f, v1 = 0.f, w1 = 0.f;
+        if (two) { u1 = u[m2]; v1 = v[m2]; w1 = wz[m2]; }
+        o[m] = to_i16_round(u0);
+        o[n + m] = to_i16_round(v0);
+        o[2 * n + m] = to_i16_round(w0);
+        if (two) {
+            o[m2] = to_i16_round(u1);
+            o[n + m2] = to_i16_round(v1);
+            o[2 * n + m2] = to_i16_round(w1);
+        }
     }
 }
 
@@ -198,13 +220,9 @@ __global__ void __launch_bounds__(kThreads) k_pack_tke(GffGrid g, const float *_
     const int k = (int)(t % g.nkk) + 1;
     const long long c = t / g.nkk;
     const int j = (int)(c % g.njj) + 1, i = (int)(c / g.njj) + 1;
-    const float v = turb[col_base(g, i, j) + k] * 100.0f;
-    if (v != v) {
-        *bad = 1;
-        out[t] = 0;
-        return;
-    }
-    out[t] = (short)__float2int_rn(fminf(fmaxf(v, -32768.0f), 32767.0f));
+    const float x = turb[col_base(g, i, j) + k];
+    if (x != x) *bad = 1;
+    out[t] = to_i16_round(x);
 }
 
 int blocks_for(long long threads) { return (int)((threads + kThreads - 1) / kThreads); }
@@ -242,7 +260,10 @@ void launch_gff_pack(const GffGrid &g, int mode, const float *uk, const float *v
                      int *bad, cudaStream_t st) {
     const long long cols = (long long)(g.nii + 1) * (g.njj + 1);
     switch (mode) {
-        case 0: k_pack_columns<<<blocks_for(cols * (g.nkk + 1)), kThreads, 0, st>>>(g, uk, vk, wk, out); break;
+        case 0:
+            k_pack_columns<<<(int)((cols + kColsPerBlock - 1) / kColsPerBlock), dim3(32, kColsPerBlock), 0, st>>>(
+                g, uk, vk, wk, out);
+            break;
         case 1: {
             const dim3 grid((g.njj + 1 + kTile - 1) / kTile, (g.nkk + 1 + kTile - 1) / kTile, g.nii + 1);
             k_pack_levels<<<grid, dim3(kTile, kRowsPerPass), 0, st>>>(g, uk, vk, wk, out);
@@ -258,7 +279,8 @@ void launch_gff_unpack(const GffGrid &g, int flag, const short *in, const int16_
                        float *uk, float *vk, float *wk, cudaStream_t st) {
     const long long cols = (long long)(g.nii + 1) * (g.njj + 1);
     if (flag == -1) {
-        k_unpack_columns<<<blocks_for(cols * (g.nkk + 1)), kThreads, 0, st>>>(g, in, uk, vk, wk);
+        k_unpack_columns<<<(int)((cols + kColsPerBlock - 1) / kColsPerBlock), dim3(32, kColsPerBlock), 0, st>>>(
+            g, in, uk, vk, wk);
     } else if (flag == -2) {
         const dim3 grid((g.njj + 1 + kTile - 1) / kTile, (g.nkk + 1 + kTile - 1) / kTile, g.nii + 1);
         k_unpack_levels<<<grid, dim3(kTile, kRowsPerPass), 0, st>>>(g, in, uk, vk, wk);
