@@ -22,139 +22,14 @@
 
 #include "gral_prog.h"
 #include "prog_common.cuh"
+#include "prog_ctx.cuh"
 #include "prog_gff.cuh"
 #include "prog_kernels.cuh"
 
 using namespace gral;
 
-namespace {
-
-template <class T>
-struct DevBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    cudaError_t ensure(size_t count) {
-        if (count <= n) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        cudaError_t e = cudaMalloc((void **)&p, std::max<size_t>(count, 1) * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        return e;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
-
-constexpr int kCounterSlots = 64;   // wavefront launches per phase (group sets) with own counters
-
-struct Geom {
-    SweepGeom g;
-    std::vector<int> ds;
-};
-
-}  // namespace
-
-struct gral_ctx {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {};
-    int cap_nii = 0, cap_njj = 0, cap_nkk = 0, cap_kadv = 0, cap_batch = 0;
-    int il_min_batch = 32;
-    int forced_variant = -1;   // GRAL_PROG_BATCH_VARIANT
-    int lookahead = 8;         // GRAL_PROG_LOOKAHEAD: plain-family warps per average diagonal width
-    int lookahead_p = 3;       // GRAL_PROG_LOOKAHEAD_P: the same for the pressure sweep
-    int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
-    std::string err = "no error";
-
-    // current load
-    bool loaded = false;
-    int nii = 0, njj = 0, nkk = 0, ks = 0, nb = 0, ncols = 0, nj2 = 0, model = 1;
-    bool il = false;     // interleaved layout + batched kernel family
-    int ngroups = 0;
-    int it_host = 1, it_max = 0, it_min = 0, cadence = 100;
-    std::vector<gral_params> params;
-    std::vector<gral_fields> fields;
-    KArgs ka{};
-    Staging sg{};
-    BcLists bc{};
-    Geom geo_p, geo_u, geo_v;
-    bool fused = false;        // fused pressure/velcorr/average/U wavefront (slab family, model 1)
-    int fused_grid = 0;
-    int lookahead_f = 6;       // GRAL_PROG_LOOKAHEAD_F: fused-kernel warps per average diagonal width
-    FusedGeom fgeo{};
-    DevBuf<int> fseg;
-    int grid_gs[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // indexed by PH_*
-    cudaGraphExec_t graph = nullptr;
-    float ms_upload = 0.f;
-    float tune_ms[16] = {0};
-
-    // device buffers
-    DevBuf<float> slab, stage, veg, tables, ap0, rowcarry, trace;
-    DevBuf<ColMeta> meta;
-    DevBuf<uint32_t> cflags;
-    DevBuf<ColF> colf;
-    DevBuf<ColKE> colke;
-    DevBuf<short2> rcw;
-    // DiagnosticFlowfield after the solve (gral_params.post_diagnostic)
-    bool post_diag = false;
-    int diag_grid = 0;
-    DevBuf<float> ddpm, dtab, ddt;
-    DevBuf<int> dflags;
-    DevBuf<float> varw, z0i;
-    // flow-field cache payloads (gral_prog_gff_*)
-    bool stored = false;                 // the staging fields hold the last store's results
-    std::vector<int16_t> h_kkart;        // KKART of the load, flat [NII+2][NJJ+2]
-    DevBuf<short> gff;                   // packed or uploaded payload words
-    DevBuf<uint32_t> gffoff;             // terrain-format record offsets
-    DevBuf<int16_t> gffkk;               // KKART of an unpack
-    DevBuf<float> gffu;                  // unpacked fields, 3 x [NII+2][NJJ+2][NKK+2]
-    DevBuf<char> l2flush;                // written before each timed pack launch
-    DevBuf<SitDev> sit;
-    DevBuf<int> flags, misc, diag, bcl, counts;
-    DevBuf<unsigned int> counters;
-    std::vector<SitDev> h_sit;
-    std::vector<int> h_act;
-
-    ~gral_ctx() {
-        if (graph) cudaGraphExecDestroy(graph);
-        DevBuf<float> *fb[] = {&slab, &stage, &veg, &tables, &ap0, &rowcarry, &trace};
-        for (auto *b : fb) b->release();
-        meta.release(); cflags.release(); colf.release(); sit.release(); colke.release(); rcw.release();
-        ddpm.release(); dtab.release(); ddt.release(); dflags.release(); fseg.release();
-        varw.release(); z0i.release();
-        gff.release(); gffoff.release(); gffkk.release(); gffu.release(); l2flush.release();
-        flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
-        counters.release();
-        for (auto &e : ev) if (e) cudaEventDestroy(e);
-        if (stream) cudaStreamDestroy(stream);
-    }
-};
 
 namespace {
-
-int fail(gral_ctx *c, int code, const std::string &msg) {
-    if (c) c->err = msg;
-    return code;
-}
-
-#define CK(call)                                                                                      \
-    do {                                                                                              \
-        cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess)                                                                        \
-            return fail(ctx, e_ == cudaErrorMemoryAllocation ? GRAL_ENOMEM : GRAL_ECUDA,              \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                          \
-    } while (0)
-
-#define CK_RC(call)                \
-    do {                           \
-        const int rc_ = (call);    \
-        if (rc_ != GRAL_OK) return rc_; \
-    } while (0)
 
 inline float f32(float x) { return x; }
 
@@ -1132,219 +1007,6 @@ int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const 
 
 int gral_prog_solve(gral_ctx *ctx, const gral_params *p, const gral_static *s, gral_fields *f, gral_stats *stats) {
     return gral_prog_solve_batch(ctx, 1, p, s, f, stats);
-}
-
-// ---- flow-field cache payloads (GFFWrite.cs, GFFRead.cs) ----
-
-}  // extern "C"
-
-namespace {
-
-void put_header(uint8_t *out, int32_t nkk, int32_t njj, int32_t nii, float dir, float speed, int32_t stab,
-                float dxk, int32_t flag) {
-    const int32_t a[3] = {nkk, njj, nii};
-    std::memcpy(out, a, 12);
-    std::memcpy(out + 12, &dir, 4);
-    std::memcpy(out + 16, &speed, 4);
-    std::memcpy(out + 20, &stab, 4);
-    std::memcpy(out + 24, &dxk, 4);
-    std::memcpy(out + 28, &flag, 4);
-}
-
-int *gff_bad_flag(gral_ctx *ctx, long long words) {
-    return reinterpret_cast<int *>(ctx->gff.p + words + (words & 1));
-}
-
-int gff_words(gral_ctx *ctx, int mode, long long *words, std::vector<uint32_t> *off) {
-    const GffGrid g{ctx->nii, ctx->njj, ctx->nkk};
-    long long terrain = 0;
-    if (mode == GRAL_GFF_TERRAIN) {
-        std::vector<uint32_t> tmp;
-        terrain = gff_terrain_offsets(g, ctx->h_kkart.data(), 1, off ? *off : tmp);
-        if (terrain < 0) return fail(ctx, GRAL_EINVAL, "KKART above NKK+1 leaves no room for a terrain-format record");
-    }
-    *words = gff_data_words(g, mode, terrain);
-    return GRAL_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-int gral_prog_gff_size(gral_ctx *ctx, int32_t mode, uint64_t *bytes) {
-    if (!ctx || !bytes) return GRAL_EINVAL;
-    if (mode < GRAL_GFF_COLUMNS || mode > GRAL_GFF_TKE) return fail(ctx, GRAL_EINVAL, "unknown payload mode");
-    if (!ctx->loaded) return fail(ctx, GRAL_ESTATE, "payload size before load");
-    long long words = 0;
-    const int rc = gff_words(ctx, mode, &words, nullptr);
-    if (rc != GRAL_OK) return rc;
-    *bytes = GRAL_GFF_HEADER_BYTES + 2 * (uint64_t)words;
-    return GRAL_OK;
-}
-
-}  // extern "C"
-
-namespace {
-
-// Checks a pack request and prepares its device buffers (payload words, terrain offsets, the
-// cleared TKE error flag); *words receives the payload words after the header.
-int gff_pack_prepare(gral_ctx *ctx, int32_t situation, int32_t mode, long long *words) {
-    if (mode < GRAL_GFF_COLUMNS || mode > GRAL_GFF_TKE) return fail(ctx, GRAL_EINVAL, "unknown payload mode");
-    if (!ctx->loaded || !ctx->stored) return fail(ctx, GRAL_ESTATE, "payload pack before store");
-    if (situation < 0 || situation >= ctx->nb) return fail(ctx, GRAL_EINVAL, "situation index out of range");
-    if (mode == GRAL_GFF_TKE && ctx->model != 2)
-        return fail(ctx, GRAL_EINVAL, "the turbulence payload needs turbulence model 2");
-    if (mode == GRAL_GFF_LEVELS && ctx->nii + 1 > 65535) return fail(ctx, GRAL_ETOOLARGE, "more than 65534 rows");
-    CK(cudaSetDevice(ctx->device));
-    std::vector<uint32_t> off;
-    int rc = gff_words(ctx, mode, words, &off);
-    if (rc != GRAL_OK) return rc;
-    cudaStream_t st = ctx->stream;
-    CK(ctx->gff.ensure((size_t)*words + 3));   // spare words: the mode-3 error flag, 4-byte aligned
-    if (mode == GRAL_GFF_TERRAIN) {
-        CK(ctx->gffoff.ensure(off.size()));
-        CK(cudaMemcpyAsync(ctx->gffoff.p, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-    }
-    if (mode == GRAL_GFF_TKE) CK(cudaMemsetAsync(gff_bad_flag(ctx, *words), 0, sizeof(int), st));
-    return GRAL_OK;
-}
-
-void gff_pack_launch(gral_ctx *ctx, int32_t situation, int32_t mode, long long words) {
-    const GffGrid g{ctx->nii, ctx->njj, ctx->nkk};
-    const size_t o = ctx->sg.stride * (size_t)situation;
-    launch_gff_pack(g, mode, ctx->sg.uk + o, ctx->sg.vk + o, ctx->sg.wk + o,
-                    ctx->model == 2 ? ctx->sg.turb + o : nullptr,
-                    reinterpret_cast<const int16_t *>(ctx->meta.p), (int)(sizeof(ColMeta) / sizeof(int16_t)),
-                    ctx->gffoff.p, ctx->gff.p, gff_bad_flag(ctx, words), ctx->stream);
-}
-
-}  // namespace
-
-extern "C" {
-
-int gral_prog_gff_pack(gral_ctx *ctx, int32_t situation, int32_t mode, float wind_dir, float wind_speed,
-                       int32_t stability_class, uint8_t *out, uint64_t capacity) {
-    if (!ctx) return GRAL_EINVAL;
-    if (!out) return fail(ctx, GRAL_EINVAL, "null output buffer");
-    long long words = 0;
-    int rc = gff_pack_prepare(ctx, situation, mode, &words);
-    if (rc != GRAL_OK) return rc;
-    if (capacity < GRAL_GFF_HEADER_BYTES + 2 * (uint64_t)words)
-        return fail(ctx, GRAL_EINVAL, "output buffer smaller than the payload");
-    cudaStream_t st = ctx->stream;
-    int *bad = gff_bad_flag(ctx, words);
-    gff_pack_launch(ctx, situation, mode, words);
-    CK(cudaGetLastError());
-    int hbad = 0;
-    if (mode == GRAL_GFF_TKE) CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(out + GRAL_GFF_HEADER_BYTES, ctx->gff.p, 2 * (size_t)words, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (hbad) return fail(ctx, GRAL_ENONFINITE, "non-finite TKE value: the reference's conversion fails there");
-    const int32_t nkk_word = (mode == GRAL_GFF_LEVELS || mode == GRAL_GFF_TERRAIN) ? -ctx->nkk : ctx->nkk;
-    const int32_t flag = (mode == GRAL_GFF_TKE) ? -1 : -1 - mode;
-    put_header(out, nkk_word, ctx->njj, ctx->nii, wind_dir, wind_speed, stability_class, ctx->params[0].dxk, flag);
-    return GRAL_OK;
-}
-
-int gral_prog_gff_pack_timed(gral_ctx *ctx, int32_t situation, int32_t mode, int32_t repeats, double *kernel_ms) {
-    if (!ctx) return GRAL_EINVAL;
-    if (repeats < 1 || !kernel_ms) return fail(ctx, GRAL_EINVAL, "repeats must be positive and kernel_ms set");
-    long long words = 0;
-    int rc = gff_pack_prepare(ctx, situation, mode, &words);
-    if (rc != GRAL_OK) return rc;
-    cudaStream_t st = ctx->stream;
-    const size_t flush = 256u << 20;
-    CK(ctx->l2flush.ensure(flush));
-    double sum = 0.0;
-    for (int r = 0; r < repeats; ++r) {
-        CK(cudaMemsetAsync(ctx->l2flush.p, r & 0xff, flush, st));
-        CK(cudaEventRecord(ctx->ev[0], st));
-        gff_pack_launch(ctx, situation, mode, words);
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ctx->ev[1], st));
-        CK(cudaEventSynchronize(ctx->ev[1]));
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-        sum += ms;
-    }
-    *kernel_ms = sum / repeats;
-    return GRAL_OK;
-}
-
-int gral_prog_gff_unpack(gral_ctx *ctx, const uint8_t *payload, uint64_t bytes, int32_t nii, int32_t njj,
-                         int32_t nkk, float dxk, const int16_t *kkart, float *uk, float *vk, float *wk,
-                         float *wind_dir, float *wind_speed, int32_t *stability_class, int32_t *format) {
-    if (!ctx) return GRAL_EINVAL;
-    if (!payload || !uk || !vk || !wk) return fail(ctx, GRAL_EINVAL, "null pointer");
-    if (nii < 1 || njj < 1 || nkk < 1) return fail(ctx, GRAL_EINVAL, "bad grid dimensions");
-    if (nii > ctx->cap_nii || njj > ctx->cap_njj || nkk > ctx->cap_nkk)
-        return fail(ctx, GRAL_EINVAL, "grid exceeds the context's capacity");
-    if (bytes < GRAL_GFF_HEADER_BYTES) return fail(ctx, GRAL_EINVAL, "payload shorter than its header");
-    int32_t h[8];
-    std::memcpy(h, payload, sizeof(h));
-    float dir, speed, cell;
-    std::memcpy(&dir, payload + 12, 4);
-    std::memcpy(&speed, payload + 16, 4);
-    std::memcpy(&cell, payload + 24, 4);
-    // GFFRead.cs:185-208: Math.Abs of the first word (which throws for int.MinValue), then the
-    // grid and the cell size must equal the model's
-    if (h[0] == INT32_MIN || std::abs(h[0]) != nkk)
-        return fail(ctx, GRAL_EINVAL, "field dimension in z-direction does not match");
-    if (h[1] != njj) return fail(ctx, GRAL_EINVAL, "field dimension in y-direction does not match");
-    if (h[2] != nii) return fail(ctx, GRAL_EINVAL, "field dimension in x-direction does not match");
-    if (cell != dxk) return fail(ctx, GRAL_EINVAL, "horizontal grid size does not match");
-    const int32_t flag = h[7];
-    if (wind_dir) *wind_dir = dir;
-    if (wind_speed) *wind_speed = speed;
-    if (stability_class) *stability_class = h[5];
-    if (format) *format = flag;
-    if (flag != -1 && flag != -2 && flag != -3) return GRAL_OK;   // the reference reads nothing more
-    if (flag == -2 && nii + 1 > 65535) return fail(ctx, GRAL_ETOOLARGE, "more than 65534 rows");
-    const GffGrid g{nii, njj, nkk};
-    const size_t ncols = (size_t)(nii + 2) * (njj + 2), cells = ncols * (nkk + 2);
-    std::vector<uint32_t> off;
-    long long words;
-    if (flag == -3) {
-        if (!kkart) return fail(ctx, GRAL_EINVAL, "the terrain format needs the domain's KKART");
-        const long long terrain = gff_terrain_offsets(g, kkart, 1, off);
-        if (terrain < 0) return fail(ctx, GRAL_EINVAL, "KKART above NKK+1 leaves no room for a terrain-format record");
-        words = gff_data_words(g, 2, terrain);
-        if (bytes - GRAL_GFF_HEADER_BYTES < 2 * (uint64_t)words)
-            return fail(ctx, GRAL_EINVAL, "payload shorter than its grid");
-        // GFFRead.cs:260-272: the file's KKART must be the model's
-        const uint8_t *kb = payload + GRAL_GFF_HEADER_BYTES;
-        for (int i = 1; i <= nii; ++i)
-            for (int j = 1; j <= njj; ++j) {
-                int16_t v;
-                std::memcpy(&v, kb + 2 * ((size_t)(i - 1) * njj + (j - 1)), 2);
-                if (v != kkart[(size_t)i * (njj + 2) + j])
-                    return fail(ctx, GRAL_EINVAL, "building or terrain of flow field does not match");
-            }
-    } else {
-        words = gff_data_words(g, 0, 0);
-        if (bytes - GRAL_GFF_HEADER_BYTES < 2 * (uint64_t)words)
-            return fail(ctx, GRAL_EINVAL, "payload shorter than its grid");
-    }
-    CK(cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
-    CK(ctx->gff.ensure((size_t)words + 2));
-    CK(ctx->gffu.ensure(3 * cells));
-    CK(cudaMemcpyAsync(ctx->gff.p, payload + GRAL_GFF_HEADER_BYTES, 2 * (size_t)words, cudaMemcpyHostToDevice, st));
-    if (flag == -3) {
-        CK(ctx->gffoff.ensure(off.size()));
-        CK(ctx->gffkk.ensure(ncols));
-        CK(cudaMemcpyAsync(ctx->gffoff.p, off.data(), off.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(ctx->gffkk.p, kkart, ncols * sizeof(int16_t), cudaMemcpyHostToDevice, st));
-    }
-    float *du = ctx->gffu.p, *dv = du + cells, *dw = dv + cells;
-    CK(cudaMemsetAsync(du, 0, 3 * cells * sizeof(float), st));
-    launch_gff_unpack(g, flag, ctx->gff.p, ctx->gffkk.p, ctx->gffoff.p, du, dv, dw, st);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(uk, du, cells * sizeof(float), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(vk, dv, cells * sizeof(float), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(wk, dw, cells * sizeof(float), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return GRAL_OK;
 }
 
 }  // extern "C"
