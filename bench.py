@@ -14,6 +14,12 @@ model; synthetic, seeded inputs.
              against the measured HBM copy bandwidth.
   cpu_baseline  the CPU oracle (a single-threaded restatement of the reference's deterministic
              solver) on a bounded sample of the same workload.
+  prep       the flow-field set-up before the solve (sub-domains, flat-terrain initial field,
+             vegetation) on the same grid: device kernel time (CUDA events) against HBM bandwidth,
+             host-timed calls including the copies, and the oracle restatement on one core.
+  wind       the wind at 2^20 random particle positions interpolated from the solved field
+             (IntWindCalculate): device kernel time, the call with the host copies, the oracle on
+             one core.
   gff        the flow-field cache writer/reader (GFFWrite.cs / GFFRead.cs formats) on the same
              grid: device pack kernel per format (CUDA events, L2 flushed before each launch)
              against HBM bandwidth, the host-timed pack into pinned memory and read back, and
@@ -358,6 +364,115 @@ def gff_measure(dom, sit, repeats: int = 10):
     return out
 
 
+def prep_measure(dom, repeats: int = 5):
+    """Set-up entry points on the grid of `dom` (rank 0 only)."""
+    import numpy as np
+    from gral_b200.abi import MetProfile
+    from gral_b200.prognostic import PrognosticSolver
+    from oracle import prep as OP
+
+    F32 = np.float32
+    st = dom.static
+    th = math.radians(225.0)                 # the production situation: 225 deg, 2 m/s at 10 m, neutral
+    met = MetProfile(np.array([0, 10.0], F32), np.array([0, -2.0 * math.sin(th)], F32),
+                     np.array([0, -2.0 * math.cos(th)], F32), 1000.0)
+    grid = dict(nii=dom.nii, njj=dom.njj, nkk=dom.nkk, vert_cells_ff=dom.vert_cells_ff, dxk=dom.dxk,
+                dyk=dom.dyk, near_wall=0, igeb=max(int(20 / dom.dxk), 1))
+    rng = np.random.default_rng(2)
+    lines = [dict(crown_height=float(rng.uniform(2, 25)), trunk_height=float(rng.uniform(0, 8)),
+                  trunk_lad=float(rng.uniform(0.05, 0.5)), crown_lad=float(rng.uniform(0.1, 1.5)),
+                  cov=float(rng.uniform(0.1, 1.0)), i=int(rng.integers(1, dom.nii + 1)),
+                  j=int(rng.integers(1, dom.njj + 1)), drag=1) for _ in range(20000)]
+    cov0 = np.zeros((dom.nii + 2, dom.njj + 2), F32)
+    peak, peak_kind = measured_peak()
+    cols = dom.nii * dom.njj
+    cells = cols * dom.nkk
+    calls = {
+        "subdomains": (lambda s: s.subdomains(st.cutk, dom.nii, dom.njj, dom.dxk, dom.dyk, 15),
+                       lambda: OP.subdomains(st.cutk, dom.nii, dom.njj, dom.dxk, dom.dyk, 15), None),
+        # per column: CUTK read, KKART and AHK written; per level: U and V written
+        "flat_init": (lambda s: s.flat_init(grid, st.cutk, st.dzk, st.hokart, met),
+                      lambda: OP.flat_init(grid, st.cutk, st.dzk, st.hokart, met), 10 * cols + 8 * cells),
+        "flat_init_near_wall": (lambda s: s.flat_init(dict(grid, near_wall=1), st.cutk, st.dzk, st.hokart, met,
+                                                      st.advdom),
+                                lambda: OP.flat_init(dict(grid, near_wall=1), st.cutk, st.dzk, st.hokart, met,
+                                                     st.advdom), None),
+        "vegetation_20k_lines": (lambda s: s.vegetation(dom.nii, dom.njj, dom.nkk, st.kkart, st.dzk, st.hokart,
+                                                        lines, cov0),
+                                 lambda: OP.vegetation(dom.nii, dom.njj, dom.nkk, st.kkart, st.dzk, st.hokart,
+                                                       lines, cov0), None),
+    }
+    out = {"workload": f"{dom.nii}x{dom.njj}x{dom.nkk} city grid, production situation (225 deg, 2 m/s at 10 m)",
+           "calls": {}}
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
+        for name, (dev, cpu, alg) in calls.items():
+            dev(s)
+            ks, ts = [], []
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                dev(s)
+                ts.append(time.perf_counter() - t0)
+                ks.append(s.prep_last_ms())
+            t0 = time.perf_counter()
+            cpu()
+            cpu_ms = (time.perf_counter() - t0) * 1e3
+            kms = statistics.median(ks)
+            ent = {"kernel_ms": round(kms, 4), "call_ms": round(statistics.median(ts) * 1e3, 3),
+                   "cpu_oracle_ms": round(cpu_ms, 1), "cpu_kind": "oracle restatement, 1 core"}
+            if alg:
+                ach = alg / (kms / 1e3) / 1e9
+                ent["roofline"] = {"bound": "hbm", "alg_bytes_per_launch": alg, "achieved": round(ach, 1),
+                                   "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": peak_kind}
+            out["calls"][name] = ent
+    return out
+
+
+def wind_measure(dom, sit, n: int = 1 << 20, repeats: int = 5):
+    """Wind interpolation at n particles after a store (rank 0 only)."""
+    import numpy as np
+    from gral_b200 import prep
+    from gral_b200.abi import PARTICLE_DTYPE
+    from gral_b200.prognostic import PrognosticSolver
+    from oracle import prep as OP
+
+    f = prep.initial_fields(dom, sit)
+    rng = np.random.default_rng(9)
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["i"] = rng.integers(1, dom.nii + 1, n)
+    p["j"] = rng.integers(1, dom.njj + 1, n)
+    p["x"] = (p["i"] - 1) * dom.dxk + rng.uniform(0, dom.dxk, n)
+    p["y"] = (p["j"] - 1) * dom.dyk + rng.uniform(0, dom.dyk, n)
+    p["z"] = rng.uniform(0.0, 200.0, n).astype(np.float32)
+    g = dict(terrain=0, buildings=1, ikooa=0, jkooa=0, dxk=dom.dxk, dyk=dom.dyk)
+    st = dom.static
+    peak, peak_kind = measured_peak()
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
+        s.load([dom.params(sit, iterations=1)], st, [f])
+        s.store([f])
+        s.wind_at(0, g, st.dzk, st.hokart, p)
+        ks, ts = [], []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            s.wind_at(0, g, st.dzk, st.hokart, p)
+            ts.append(time.perf_counter() - t0)
+            ks.append(s.prep_last_ms())
+    t0 = time.perf_counter()
+    OP.wind_at(g, dom.nii, dom.njj, dom.nkk, st.dzk, st.hokart, f, p)
+    cpu_s = time.perf_counter() - t0
+    kms = statistics.median(ks)
+    # per particle: its 32 B record, 16 B of results and six field values from random cells, each
+    # of which moves a whole 32 B sector
+    alg = (32 + 16 + 6 * 32) * n
+    ach = alg / (kms / 1e3) / 1e9
+    return {"workload": f"{n} random particles below 200 m on the {dom.nii}x{dom.njj}x{dom.nkk} field (flat, buildings)",
+            "kernel_ms": round(kms, 4), "particles_per_s_kernel": round(n / (kms / 1e3), 0),
+            "call_ms": round(statistics.median(ts) * 1e3, 3),
+            "particles_per_s_call": round(n / statistics.median(ts), 0),
+            "roofline": {"bound": "hbm", "alg_bytes_per_launch": alg, "achieved": round(ach, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(ach / peak, 4), "peak_kind": peak_kind},
+            "cpu_oracle_particles_per_s": round(n / cpu_s, 0), "cpu_kind": "oracle restatement, 1 core"}
+
+
 def run_ours(args, rank, world):
     import torch
     from gral_b200 import prep
@@ -422,6 +537,12 @@ def run_ours(args, rank, world):
     gffm = None
     if rank == 0 and args.workload == "production" and not args.no_gff:
         gffm = gff_measure(dom, sit)
+    prepm = None
+    if rank == 0 and args.workload == "production" and not args.no_prep:
+        prepm = prep_measure(dom)
+    windm = None
+    if rank == 0 and args.workload == "production" and not args.no_wind:
+        windm = wind_measure(dom, sit)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -441,7 +562,7 @@ def run_ours(args, rank, world):
                    "layout": layout, "launch_variant": st_store["launch_variant"]},
         "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
         "roofline": roofline(cells, args.steps, phases, layout),
-        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm,
+        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm, "prep": prepm, "wind": windm,
         "gpu_launches": st_store["launches_per_iteration"] * args.steps,
         "clocks": clocks,
     }
@@ -467,6 +588,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-measurement")
     ap.add_argument("--batched-steps", type=int, default=10)
     ap.add_argument("--no-gff", action="store_true", help="skip the flow-field cache payload measurement")
+    ap.add_argument("--no-prep", action="store_true", help="skip the set-up (sub-domains, initial field) measurement")
+    ap.add_argument("--no-wind", action="store_true", help="skip the particle wind interpolation measurement")
     ap.add_argument("--ref-iters", type=int, default=4)
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-warmup", action="store_true")

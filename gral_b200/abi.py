@@ -69,6 +69,30 @@ class GralFields(C.Structure):
     _fields_ = [("uk", _fp), ("vk", _fp), ("wk", _fp), ("turb", _fp), ("tdiss", _fp)]
 
 
+class GralMet(C.Structure):
+    _fields_ = [("n_heights", C.c_int32), ("measurement_height", _fp), ("obs_u", _fp), ("obs_v", _fp),
+                ("ob_length", C.c_float), ("ol_column", _fp)]
+
+
+class GralFlatGrid(C.Structure):
+    _fields_ = [("nii", C.c_int32), ("njj", C.c_int32), ("nkk", C.c_int32), ("vert_cells_ff", C.c_int32),
+                ("dxk", C.c_float), ("dyk", C.c_float), ("near_wall", C.c_int32), ("igeb", C.c_int32)]
+
+
+class GralVegPoint(C.Structure):
+    _fields_ = [("crown_height", C.c_double), ("trunk_height", C.c_double), ("trunk_lad", C.c_double),
+                ("crown_lad", C.c_double), ("cov", C.c_double), ("i", C.c_int32), ("j", C.c_int32),
+                ("drag", C.c_int32), ("reserved", C.c_int32)]
+
+
+class GralWindGrid(C.Structure):
+    _fields_ = [("terrain", C.c_int32), ("buildings", C.c_int32), ("ikooa", C.c_int32), ("jkooa", C.c_int32),
+                ("dxk", C.c_float), ("dyk", C.c_float), ("ahmin", C.c_float), ("met", C.POINTER(GralMet))]
+
+
+PARTICLE_DTYPE = np.dtype([("x", "<f8"), ("y", "<f8"), ("z", "<f4"), ("ahint", "<f4"), ("i", "<i4"), ("j", "<i4")])
+
+
 class GralStats(C.Structure):
     _fields_ = [
         ("iterations", C.c_int32), ("iteration_loops", C.c_int32),
@@ -154,3 +178,34 @@ def stats_to_dict(s: GralStats) -> dict:
          if name not in ("delta_history", "trace_delta_umax")}
     d["delta_history"] = [s.delta_history[i] for i in range(min(s.n_history, MAX_HISTORY))]
     return d
+
+
+@dataclass
+class MetProfile:
+    """Met input of one situation (``gral_met``): heights, wind components at them (index 0
+    unused, as in the reference's arrays), the profile's Obukhov length and optionally one per
+    column (adaptive roughness)."""
+    heights: np.ndarray
+    obs_u: np.ndarray
+    obs_v: np.ndarray
+    ob_length: float
+    ol_column: Optional[np.ndarray] = None
+
+    def to_c(self) -> GralMet:
+        self._keep = [np.ascontiguousarray(a, dtype=np.float32) for a in (self.heights, self.obs_u, self.obs_v)]
+        self._ol = None if self.ol_column is None else np.ascontiguousarray(self.ol_column, dtype=np.float32)
+        h, u, v = self._keep
+        return GralMet(n_heights=h.size - 1, measurement_height=_ptr(h, C.c_float), obs_u=_ptr(u, C.c_float),
+                       obs_v=_ptr(v, C.c_float), ob_length=float(self.ob_length),
+                       ol_column=_ptr(self._ol, C.c_float))
+
+
+def veg_points_to_c(points) -> "C.Array":
+    """``gral_veg_point`` array from dicts with crown_height, trunk_height, trunk_lad, crown_lad,
+    cov, i, j and drag."""
+    arr = (GralVegPoint * max(len(points), 1))()
+    for q, p in enumerate(points):
+        arr[q] = GralVegPoint(p["crown_height"], p["trunk_height"], p["trunk_lad"], p["crown_lad"], p["cov"],
+                              p["i"], p["j"], int(p.get("drag", 1)), 0)
+    return arr
+

@@ -34,6 +34,19 @@ struct DevBuf {
     }
 };
 
+// Device buffers of the set-up entry points (gral_prog_subdomains, _flat_init, _vegetation).
+struct PrepBufs {
+    DevBuf<float> cutk, ahk, tab, fields, veg, cov;
+    DevBuf<int> ints;
+    DevBuf<int16_t> kkart;
+    DevBuf<uint8_t> adv, mask;
+    DevBuf<unsigned char> points;
+    void release() {
+        cutk.release(); ahk.release(); tab.release(); fields.release(); veg.release(); cov.release();
+        ints.release(); kkart.release(); adv.release(); mask.release(); points.release();
+    }
+};
+
 constexpr int kCounterSlots = 64;   // wavefront launches per phase (group sets) with own counters
 
 struct Geom {
@@ -103,6 +116,8 @@ struct gral_ctx {
     DevBuf<int16_t> gffkk;               // KKART of an unpack
     DevBuf<float> gffu;                  // unpacked fields, 3 x [NII+2][NJJ+2][NKK+2]
     DevBuf<char> l2flush;                // written before each timed pack launch
+    PrepBufs prep;                       // set-up entry points
+    double prep_ms = 0.0;                // device time of the last set-up call's kernels
     DevBuf<SitDev> sit;
     DevBuf<int> flags, misc, diag, bcl, counts;
     DevBuf<unsigned int> counters;
@@ -117,6 +132,7 @@ struct gral_ctx {
         ddpm.release(); dtab.release(); ddt.release(); dflags.release(); fseg.release();
         varw.release(); z0i.release();
         gff.release(); gffoff.release(); gffkk.release(); gffu.release(); l2flush.release();
+        prep.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);

@@ -15,15 +15,18 @@ from typing import List, Optional, Sequence
 import numpy as np
 
 from . import build as _build
-from .abi import (GRAL_OK, STATUS_NAMES, FieldArrays, GralFields, GralParams, GralStatic, GralStats,
-                  StaticArrays, params_to_c, stats_to_dict)
+from .abi import (GRAL_OK, PARTICLE_DTYPE, STATUS_NAMES, FieldArrays, GralFields, GralFlatGrid, GralMet,
+                  GralParams, GralStatic, GralStats, GralVegPoint, GralWindGrid, MetProfile, StaticArrays,
+                  params_to_c, stats_to_dict, veg_points_to_c)
 
 _lib = None
 
 EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_prog_solve_batch",
            "gral_prog_load", "gral_prog_iterate", "gral_prog_iterate_timed", "gral_prog_store",
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
-           "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack"]
+           "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack",
+           "gral_prog_subdomains", "gral_prog_flat_init", "gral_prog_vegetation", "gral_prog_prep_last_ms",
+           "gral_prog_wind_at"]
 
 # payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
 GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, GFF_TKE = 0, 1, 2, 3
@@ -90,6 +93,19 @@ def lib(build_if_stale: bool = True):
                                        C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_int32),
                                        C.POINTER(C.c_int32)]
     L.gral_prog_gff_unpack.restype = C.c_int
+    vp = C.c_void_p
+    L.gral_prog_subdomains.argtypes = [vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_int32, vp, vp]
+    L.gral_prog_subdomains.restype = C.c_int
+    L.gral_prog_flat_init.argtypes = [vp, C.POINTER(GralFlatGrid), vp, vp, vp, vp, C.POINTER(GralMet), vp, vp,
+                                      C.POINTER(C.c_int32), C.POINTER(GralFields)]
+    L.gral_prog_flat_init.restype = C.c_int
+    L.gral_prog_vegetation.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, C.c_int32,
+                                       C.POINTER(GralVegPoint), vp, vp, vp]
+    L.gral_prog_vegetation.restype = C.c_int
+    L.gral_prog_prep_last_ms.argtypes = [vp, C.POINTER(C.c_double)]
+    L.gral_prog_prep_last_ms.restype = C.c_int
+    L.gral_prog_wind_at.argtypes = [vp, C.c_int32, C.POINTER(GralWindGrid), vp, vp, C.c_int32, vp, vp, vp, vp, vp]
+    L.gral_prog_wind_at.restype = C.c_int
     _lib = L
     return L
 
@@ -192,6 +208,75 @@ class PrognosticSolver:
         self._check(self._L.gral_prog_gff_pack(self._ctx, situation, mode, wind_dir, wind_speed, stability_class,
                                                out.ctypes.data, out.nbytes))
         return out[:n]
+
+    # flow-field set-up before the solve (ReadGeometryAndDomains.cs, MicroscaleFlat.cs, ReadVegetation.cs)
+    def subdomains(self, cutk: np.ndarray, nii: int, njj: int, dxk: float, dyk: float, factor: int = 15) -> np.ndarray:
+        """ADVDOM [NII+2][NJJ+2] of the prognostic sub-domains around the buildings."""
+        cutk = np.ascontiguousarray(cutk, np.float32)
+        adv = np.zeros((nii + 2, njj + 2), np.uint8)
+        self._check(self._L.gral_prog_subdomains(self._ctx, nii, njj, dxk, dyk, factor, cutk.ctypes.data,
+                                                 adv.ctypes.data))
+        return adv
+
+    def flat_init(self, grid: dict, cutk: np.ndarray, dzk: np.ndarray, hokart: np.ndarray, met: MetProfile,
+                  advdom: Optional[np.ndarray] = None):
+        """Flat-terrain set-up of one situation; returns (kkart, ahk, kadvmax, FieldArrays)."""
+        nii, njj, nkk = grid["nii"], grid["njj"], grid["nkk"]
+        g = GralFlatGrid(**grid)
+        cutk, dzk, hokart = (np.ascontiguousarray(a, np.float32) for a in (cutk, dzk, hokart))
+        adv = None if advdom is None else np.ascontiguousarray(advdom, np.uint8)
+        shape = (nii + 2, njj + 2, nkk + 2)
+        f = FieldArrays(*(np.empty(shape, np.float32) for _ in range(3)))
+        kk = np.empty((nii + 2, njj + 2), np.int16)
+        ahk = np.empty((nii + 2, njj + 2), np.float32)
+        kadv = C.c_int32()
+        m = met.to_c()
+        fc = f.to_c()
+        self._check(self._L.gral_prog_flat_init(self._ctx, C.byref(g), cutk.ctypes.data, dzk.ctypes.data,
+                                                hokart.ctypes.data, None if adv is None else adv.ctypes.data,
+                                                C.byref(m), kk.ctypes.data, ahk.ctypes.data, C.byref(kadv),
+                                                C.byref(fc)))
+        return kk, ahk, kadv.value, f
+
+    def vegetation(self, nii: int, njj: int, nkk: int, kkart: np.ndarray, dzk: np.ndarray, hokart: np.ndarray,
+                   points: Sequence[dict], cov: np.ndarray):
+        """VEG [NII+2][NJJ+2][NKK+2], its mask and COV after rasterising the vegetation lines."""
+        kk = np.ascontiguousarray(kkart, np.int16)
+        dz, ho = (np.ascontiguousarray(a, np.float32) for a in (dzk, hokart))
+        cov = np.array(cov, dtype=np.float32, copy=True, order="C")
+        veg = np.empty((nii + 2, njj + 2, nkk + 2), np.float32)
+        mask = np.empty((nii + 2, njj + 2), np.uint8)
+        pts = veg_points_to_c(points)
+        self._check(self._L.gral_prog_vegetation(self._ctx, nii, njj, nkk, kk.ctypes.data, dz.ctypes.data,
+                                                 ho.ctypes.data, len(points), pts, veg.ctypes.data,
+                                                 mask.ctypes.data, cov.ctypes.data))
+        return veg, mask, cov
+
+    def wind_at(self, situation: int, grid: dict, dzk: Optional[np.ndarray], hokart: Optional[np.ndarray],
+                particles: np.ndarray, met: Optional[MetProfile] = None):
+        """U, V, W and IndexK at particle positions (``PARTICLE_DTYPE`` records), interpolated from
+        the stored fields of `situation` as Zeitschleife.IntWindCalculate does."""
+        p = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        n = p.size
+        ux, uy, uz = (np.empty(n, np.float32) for _ in range(3))
+        kk = np.empty(n, np.int32)
+        m = None if met is None else met.to_c()
+        g = GralWindGrid(grid.get("terrain", 0), grid.get("buildings", 1), grid.get("ikooa", 0), grid.get("jkooa", 0),
+                         grid["dxk"], grid["dyk"], grid.get("ahmin", 0.0),
+                         C.pointer(m) if m is not None else C.POINTER(GralMet)())
+        dz = None if dzk is None else np.ascontiguousarray(dzk, np.float32)
+        ho = None if hokart is None else np.ascontiguousarray(hokart, np.float32)
+        self._check(self._L.gral_prog_wind_at(self._ctx, situation, C.byref(g),
+                                              None if dz is None else dz.ctypes.data,
+                                              None if ho is None else ho.ctypes.data, n, p.ctypes.data,
+                                              ux.ctypes.data, uy.ctypes.data, uz.ctypes.data, kk.ctypes.data))
+        return ux, uy, uz, kk
+
+    def prep_last_ms(self) -> float:
+        """Device ms of the kernels of the last subdomains/flat_init/vegetation call."""
+        ms = C.c_double()
+        self._check(self._L.gral_prog_prep_last_ms(self._ctx, C.byref(ms)))
+        return ms.value
 
     def gff_pack_timed(self, situation: int, mode: int, repeats: int) -> float:
         """Mean device ms of one pack launch (L2 flushed before each), no copy to the host."""

@@ -224,6 +224,107 @@ int gral_prog_gff_unpack(gral_ctx *ctx, const uint8_t *payload, uint64_t bytes, 
                          int32_t nkk, float dxk, const int16_t *kkart, float *uk, float *vk, float *wk,
                          float *wind_dir, float *wind_speed, int32_t *stability_class, int32_t *format);
 
+/* ---- Flow-field set-up of the callers (MicroscaleFlat.cs, ReadGeometryAndDomains.cs,
+ * ReadVegetation.cs), computed on the device.  The context needs no load; grids must fit its
+ * capacity.  Arrays are flat in the layout of gral_static / gral_fields. ---- */
+
+/* Prognostic sub-domains (ReadGeometryAndDomains.cs:321-347): ADVDOM = 1 in the rectangle
+ * i +- (int)(factor*CUTK/DXK), j +- (int)(factor*CUTK/DYK) around every cell with CUTK > 0,
+ * clipped to 1..NII x 1..NJJ, 0 elsewhere.  factor = Program.PrognosticSubDomainFactor. */
+int gral_prog_subdomains(gral_ctx *ctx, int32_t nii, int32_t njj, float dxk, float dyk, int32_t factor,
+                         const float *cutk, uint8_t *advdom);
+
+/* Met input of one weather situation as MicroscaleFlat.Calculate reads it. */
+typedef struct {
+    int32_t n_heights;               /* Program.MetProfileNumb (>= 1) */
+    const float *measurement_height; /* Program.MeasurementHeight, entries 1..n_heights */
+    const float *obs_u, *obs_v;      /* Program.ObsWindU/V, entries 1..n_heights */
+    float ob_length;                 /* Program.Ob[1][1] */
+    const float *ol_column;          /* Program.OLGral [NII+2][NJJ+2] when AdaptiveRoughnessMax > 0,
+                                        else NULL (every column uses ob_length) */
+} gral_met;
+
+typedef struct {
+    int32_t nii, njj, nkk, vert_cells_ff;
+    float dxk, dyk;
+    int32_t near_wall; /* damping near obstacle walls (MicroscaleFlat.cs:201-357): 0 none; 1 on columns
+                          with ADVDOM == 0 (prognostic approach, SubDomainDistance < 10000); 2 on
+                          every column (diagnostic approach) */
+    int32_t igeb;      /* Program.IGEB (max((int)(20/DXK), 1)): search range of the damping in cells */
+} gral_flat_grid;
+
+/* Flat-terrain set-up of one weather situation before the flow-field solve (MicroscaleFlat.cs:
+ * 29-357): KKART, AHK (= BUI_HEIGHT) and KADVMAX from CUTK, the initial U and V from the met
+ * profile (power law below the first measurement height and, with one height, above it; linear
+ * interpolation between heights), zero inside and on the faces of obstacles, W = 0, the copies
+ * to the east and north edge columns, then the optional near-wall damping.  Outputs: kkart, ahk
+ * [NII+2][NJJ+2]; *kadvmax; f->uk, vk, wk [NII+2][NJJ+2][NKK+2] (levels 1..NKK of columns 1..NII+1
+ * x 1..NJJ+1 as the reference sets them, every other entry 0, which the solve leaves at 0).
+ * The order is the reference's sequential one (its parallel loop races on the edge copy).
+ * advdom is read only for near_wall == 1.  MathF.Pow/Log values are tabulated on the host with
+ * the C library, as .NET evaluates them. */
+int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cutk, const float *dzk,
+                        const float *hokart, const uint8_t *advdom, const gral_met *met, int16_t *kkart,
+                        float *ahk, int32_t *kadvmax, gral_fields *f);
+
+/* One coordinate line of vegetation.dat with the parameters of its area (ReadVegetation.cs:66-82). */
+typedef struct {
+    double crown_height;  /* m */
+    double trunk_height;  /* m: trunk percentage x crown height x 0.01 */
+    double trunk_lad, crown_lad;  /* leaf-area densities */
+    double cov;           /* cover: percentage x 0.01 */
+    int32_t i, j;         /* IXCUT, IYCUT; lines outside 1..NII x 1..NJJ are skipped */
+    int32_t drag;         /* 1: rasterised into VEG (isCloser); 0: sets COV only */
+    int32_t reserved;
+} gral_veg_point;
+
+/* Vegetation rasterisation (ReadVegetation.cs:83-118), the points applied in file order: per
+ * point with drag, VEG[i][j][k] for k = KKART-1..NKK-1 by the crown/trunk rule, then COV[i][j].
+ * Outputs veg [NII+2][NJJ+2][NKK+2] (0 where no point sets it), veg_mask (1 where the reference
+ * allocates VEG[i][j]), cov (in/out: cells without a point keep their value). */
+int gral_prog_vegetation(gral_ctx *ctx, int32_t nii, int32_t njj, int32_t nkk, const int16_t *kkart,
+                         const float *dzk, const float *hokart, int32_t n_points, const gral_veg_point *points,
+                         float *veg, uint8_t *veg_mask, float *cov);
+
+/* ---- Wind at particle positions (Zeitschleife.IntWindCalculate, Intwind.cs:31-152) ---- */
+
+/* Grid constants of the interpolation. */
+typedef struct {
+    int32_t terrain;    /* 1: Program.Topo == TerrainAvailable (binary search of the level above
+                           AHMIN); 0: flat terrain */
+    int32_t buildings;  /* flat terrain: Program.BuildingsExist (1: interpolate the flow field;
+                           0: the met profile, no flow field) */
+    int32_t ikooa, jkooa; /* Program.IKOOAGRAL, JKOOAGRAL: south-west corner of the grid (m) */
+    float dxk, dyk;
+    float ahmin;        /* Program.AHMIN (terrain) */
+    const gral_met *met; /* flat terrain without buildings: the met profile (ol_column unused) */
+} gral_wind_grid;
+
+/* One particle: its cell (FFCellX/Y, 1..NII x 1..NJJ), surface height AHint and position. */
+typedef struct {
+    double x, y;        /* xcoord_nteil, ycoord_nteil (m) */
+    float z;            /* zcoord_nteil (m) */
+    float ahint;        /* AHint */
+    int32_t i, j;       /* IndexI, IndexJ */
+} gral_particle;
+
+/* U, V, W and the level index IndexK at n particles, interpolated from the fields of situation
+ * `situation` of the last gral_prog_store (resident on the device until the next load), exactly
+ * as IntWindCalculate does; dzk and hokart are DZK and HOKART [NKK+2].  A particle whose cell lies
+ * outside 1..NII x 1..NJJ gets NaN and the call returns GRAL_EINVAL (the reference would index
+ * outside its arrays).  In the profile branch (flat, no buildings) the power law is evaluated
+ * with a double-precision pow rounded to float, which can differ from the C library's powf by one
+ * unit in the last place (U and V then by up to two); every other result is bit-identical to the
+ * reference's float/double evaluation. */
+int gral_prog_wind_at(gral_ctx *ctx, int32_t situation, const gral_wind_grid *g, const float *dzk,
+                      const float *hokart, int32_t n, const gral_particle *particles, float *ux, float *uy,
+                      float *uz, int32_t *index_k);
+
+/* Instrumentation: device time in ms of the kernels of the last gral_prog_subdomains,
+ * gral_prog_flat_init, gral_prog_vegetation or gral_prog_wind_at call on this context (CUDA
+ * events around its launches, host copies excluded). */
+int gral_prog_prep_last_ms(gral_ctx *ctx, double *kernel_ms);
+
 /* Text of the last error on this context (never NULL). */
 const char *gral_prog_last_error(gral_ctx *ctx);
 

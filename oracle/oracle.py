@@ -23,7 +23,7 @@ _lib = None
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the committed Makefile (g++, no FP contraction)."""
-    srcs = [os.path.join(_HERE, f) for f in ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "oracle_common.h",
+    srcs = [os.path.join(_HERE, f) for f in ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "prep.cpp", "wind.cpp", "oracle_common.h",
                                               os.path.join("..", "include", "gral_prog.h"))]
     if force or not os.path.exists(_LIB) or any(os.path.getmtime(s) > os.path.getmtime(_LIB) for s in srcs):
         subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
