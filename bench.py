@@ -20,6 +20,9 @@ model; synthetic, seeded inputs.
   wind       the wind at 2^20 random particle positions interpolated from the solved field
              (IntWindCalculate): device kernel time, the call with the host copies, the oracle on
              one core.
+  instances  independent situations on grids of different sizes (the uneven-domain batch: grids
+             log-uniform 128x128x20 .. 512x512x40 at 2-4 m, hills and buildings, random inflow),
+             solved one at a time and side by side (gral_prog_solve_instances), host-timed.
   gff        the flow-field cache writer/reader (GFFWrite.cs / GFFRead.cs formats) on the same
              grid: device pack kernel per format (CUDA events, L2 flushed before each launch)
              against HBM bandwidth, the host-timed pack into pinned memory and read back, and
@@ -473,6 +476,40 @@ def wind_measure(dom, sit, n: int = 1 << 20, repeats: int = 5):
             "cpu_oracle_particles_per_s": round(n / cpu_s, 0), "cpu_kind": "oracle restatement, 1 core"}
 
 
+def instances_measure(n: int = 16, iterations: int = 100, concurrent: int = 16, seed: int = 0):
+    """Uneven-domain instances, sequential against side by side (rank 0 only)."""
+    import numpy as np
+    from gral_b200 import prep
+    from gral_b200.prognostic import solve_instances
+
+    rng = np.random.default_rng(seed)
+    doms, ps, fs = [], [], []
+    for q in range(n):
+        side = int(round(math.exp(rng.uniform(math.log(128), math.log(512)))))
+        nj = int(round(side * rng.uniform(0.8, 1.0)))
+        vc = int(round(20 + (side - 128) / (512 - 128) * 20))
+        dx = float(rng.choice([2.0, 3.0, 4.0]))
+        d = prep.hilly_domain(side, nj, dx, vc, seed=100 + q)
+        sit = prep.random_situation(100 + q)
+        doms.append(d)
+        ps.append(d.params(sit, model=1, iterations=iterations))
+        fs.append(prep.initial_fields(d, sit))
+    statics = [d.static for d in doms]
+    cells = sum(int((d.static.advdom[1:d.nii + 1, 1:d.njj + 1] == 1).sum()) * d.vert_cells_ff for d in doms)
+    out = {"workload": f"{n} instances, grids {min(d.nii for d in doms)}..{max(d.nii for d in doms)} columns a side, "
+                       f"{iterations} iterations each, model 1", "cells": cells}
+    for name, k in (("sequential", 1), ("side_by_side", concurrent)):
+        f2 = [f.copy() for f in fs]
+        t0 = time.perf_counter()
+        _, status, rc = solve_instances(ps, statics, f2, max_concurrent=k)
+        dt = time.perf_counter() - t0
+        out[name] = {"max_concurrent": k, "seconds": round(dt, 3), "status_ok": rc == 0,
+                     "value": round(cells * iterations / dt / 1e6, 3), "unit": UNIT,
+                     "instances_per_hour_at_800_iterations": round(3600.0 * n / (dt * 800 / iterations), 1)}
+    out["speedup"] = round(out["sequential"]["seconds"] / out["side_by_side"]["seconds"], 3)
+    return out
+
+
 def run_ours(args, rank, world):
     import torch
     from gral_b200 import prep
@@ -543,6 +580,9 @@ def run_ours(args, rank, world):
     windm = None
     if rank == 0 and args.workload == "production" and not args.no_wind:
         windm = wind_measure(dom, sit)
+    instm = None
+    if rank == 0 and args.workload == "production" and not args.no_instances:
+        instm = instances_measure()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -562,7 +602,7 @@ def run_ours(args, rank, world):
                    "layout": layout, "launch_variant": st_store["launch_variant"]},
         "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
         "roofline": roofline(cells, args.steps, phases, layout),
-        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm, "prep": prepm, "wind": windm,
+        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm, "prep": prepm, "wind": windm, "instances": instm,
         "gpu_launches": st_store["launches_per_iteration"] * args.steps,
         "clocks": clocks,
     }
@@ -590,6 +630,7 @@ def main():
     ap.add_argument("--no-gff", action="store_true", help="skip the flow-field cache payload measurement")
     ap.add_argument("--no-prep", action="store_true", help="skip the set-up (sub-domains, initial field) measurement")
     ap.add_argument("--no-wind", action="store_true", help="skip the particle wind interpolation measurement")
+    ap.add_argument("--no-instances", action="store_true", help="skip the uneven-domain instances measurement")
     ap.add_argument("--ref-iters", type=int, default=4)
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--ref-warmup", action="store_true")

@@ -172,10 +172,12 @@ def make_domain(nii: int, njj: int, dxk: float, dz1: float, stretch: float, vert
                 buildings: List[Building], *, dyk: Optional[float] = None, z0: float = 0.2,
                 ustar: float = 0.3, obukhov: float = 1000.0, subdomain_factor: int = 15,
                 veg: Optional[np.ndarray] = None, cov: Optional[np.ndarray] = None,
-                top: float = 800.0) -> Domain:
+                top: float = 800.0, surface: Optional[np.ndarray] = None) -> Domain:
     dyk = dxk if dyk is None else dyk
     nkk, dzk, hok = vertical_grid_flat(dz1, stretch, top=top)
     cutk = rasterise(nii, njj, buildings)
+    if surface is not None:   # blocked cells below a terrain surface, buildings standing on it
+        cutk = (cutk + surface.astype(F32)).astype(F32)
     kkart = kkart_from_cutk(cutk, dzk, hok, nkk)
     kmax_b = int(kkart[cutk > 0].max()) if (cutk > 0).any() else 1
     kadvmax = min(nkk, max(1, kmax_b) + vert_cells_ff)
@@ -281,6 +283,38 @@ def city_domain(n: int = 400, dx: float = 2.0, dz1: float = 2.0, stretch: float 
     """Production-size grid: 400x400 cells at 2 m, 64 seeded buildings, 10-30 m tall."""
     bl = random_buildings(n, n, dx, n_buildings, seed)
     return make_domain(n, n, dx, dz1, stretch, vert_cells_ff, bl, **kw)
+
+
+def hilly_domain(nii: int, njj: int, dx: float, vert_cells_ff: int, seed: int, n_hills: Optional[int] = None,
+                 n_buildings: Optional[int] = None, dz1: float = 2.0, stretch: float = 1.05) -> Domain:
+    """Instance of the uneven-domain set: 1-5 Gaussian hills (5-50 m high, sigma 30-150 m) and
+    0-80 buildings (counts seeded unless given), the hill surface blocked like buildings (CUTK =
+    surface + building height) so that the flat-terrain solver sees the terrain through KKART."""
+    rng = np.random.default_rng(5000 + seed)
+    nh = int(rng.integers(1, 6)) if n_hills is None else n_hills
+    nb = int(rng.integers(0, 81)) if n_buildings is None else n_buildings
+    xs = (np.arange(nii + 2, dtype=np.float64) - 0.5) * dx
+    ys = (np.arange(njj + 2, dtype=np.float64) - 0.5) * dx
+    surf = np.zeros((nii + 2, njj + 2))
+    for _ in range(nh):
+        h, sg = rng.uniform(5.0, 50.0), rng.uniform(30.0, 150.0)
+        cx, cy = rng.uniform(0, nii * dx), rng.uniform(0, njj * dx)
+        surf += h * np.exp(-((xs[:, None] - cx) ** 2 + (ys[None, :] - cy) ** 2) / (2 * sg * sg))
+    surf[0, :] = surf[:, 0] = 0
+    surf[nii + 1, :] = surf[:, njj + 1] = 0
+    # footprints 10-40 m, narrowed to what fits the grid between its margins
+    fmax = min(40.0, (min(nii, njj) - 2 * 3 - 2) * dx / 2)
+    bl = random_buildings(nii, njj, dx, nb, seed, foot_m=(min(10.0, fmax), fmax), margin_cells=3,
+                          gap_cells=1) if nb and fmax >= dx else []
+    top = max(800.0, float(surf.max()) + 400.0)
+    return make_domain(nii, njj, dx, dz1, stretch, vert_cells_ff, bl, surface=surf.astype(F32), top=top)
+
+
+def random_situation(seed: int) -> "Situation":
+    """Random inflow direction, 10 m speed and roughness (z0 0.05-1 m), neutral."""
+    rng = np.random.default_rng(7000 + seed)
+    return Situation(direction_deg=float(rng.uniform(0, 360)), speed_10m=float(rng.uniform(0.5, 4.0)),
+                     z0=float(rng.uniform(0.05, 1.0)))
 
 
 def small_domain(nii: int = 16, njj: int = 14, seed: int = 0, n_buildings: int = 3,

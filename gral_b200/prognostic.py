@@ -26,7 +26,7 @@ EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_pro
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
            "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack",
            "gral_prog_subdomains", "gral_prog_flat_init", "gral_prog_vegetation", "gral_prog_prep_last_ms",
-           "gral_prog_wind_at"]
+           "gral_prog_wind_at", "gral_prog_solve_instances"]
 
 # payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
 GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, GFF_TKE = 0, 1, 2, 3
@@ -106,6 +106,10 @@ def lib(build_if_stale: bool = True):
     L.gral_prog_prep_last_ms.restype = C.c_int
     L.gral_prog_wind_at.argtypes = [vp, C.c_int32, C.POINTER(GralWindGrid), vp, vp, C.c_int32, vp, vp, vp, vp, vp]
     L.gral_prog_wind_at.restype = C.c_int
+    L.gral_prog_solve_instances.argtypes = [C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic),
+                                            C.POINTER(GralFields), C.POINTER(GralStats), C.POINTER(C.c_int32),
+                                            C.c_int32, C.c_uint64]
+    L.gral_prog_solve_instances.restype = C.c_int
     _lib = L
     return L
 
@@ -328,3 +332,20 @@ def check_speeds_noalloc(nii: int, njj: int, nkk: int, vert_cells_ff: int, gesch
     if rc != GRAL_OK:
         raise GralError(rc, "gral_prog_check_speeds_noalloc failed")
     return tuple(int(x) for x in out)
+
+
+def solve_instances(params: Sequence[dict], statics: Sequence[StaticArrays], fields: Sequence[FieldArrays],
+                    max_concurrent: int = 8, hbm_bytes: int = 0):
+    """Independent situations on grids of different sizes, several at once on one GPU
+    (``gral_prog_solve_instances``); fields are updated in place.  Returns (stats, status, rc)."""
+    L = lib()
+    n = len(params)
+    pa = (GralParams * n)(*[params_to_c(p) for p in params])
+    sa = (GralStatic * n)(*[st.to_c() for st in statics])
+    fa = (GralFields * n)(*[f.to_c() for f in fields])
+    st = (GralStats * n)()
+    status = (C.c_int32 * n)()
+    rc = L.gral_prog_solve_instances(n, pa, sa, fa, st, status, max_concurrent, hbm_bytes)
+    stats = [stats_to_dict(st[b]) for b in range(n)]
+    return stats, [int(x) for x in status], rc
+

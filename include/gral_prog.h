@@ -147,6 +147,19 @@ int gral_prog_solve(gral_ctx *ctx, const gral_params *p, const gral_static *s,
 int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s,
                           gral_fields *f, gral_stats *stats);
 
+/* Independent situations whose grids differ (one gral_params, gral_static and gral_fields per
+ * instance; GRAL solves such sets one after the other), several at once, each exactly as
+ * gral_prog_solve does (results are identical to n single calls): largest first, in waves of K
+ * instances, whose loads run one after the other and whose iterations and stores then run side
+ * by side, each in its own context, stream and host thread.  K is max_concurrent, further limited
+ * to what fits in hbm_bytes of device memory (0: 90 % of the free memory at the call), judged from
+ * the footprint of the largest instance, which is loaded first.  status[b] receives
+ * instance b's return code (the error text of a failed instance is not kept); the call returns
+ * GRAL_OK when every instance succeeded, else the code of the first failed instance in index
+ * order.  stats may be NULL. */
+int gral_prog_solve_instances(int32_t n, const gral_params *p, const gral_static *s, gral_fields *f,
+                              gral_stats *stats, int32_t *status, int32_t max_concurrent, uint64_t hbm_bytes);
+
 /* Split form of gral_prog_solve_batch for callers that keep fields resident on the device:
  * load copies inputs to HBM and runs the set-up, iterate runs the SIMPLE loop on the loaded
  * situations, store copies results back.  solve_batch = load + iterate + store. */

@@ -87,3 +87,15 @@ def test_params_reference_scalars():
     assert p["v0_1"] == np.float32(0.5)
     # CorolisParam of the reference for 47 deg latitude, float32
     assert abs(p["coriolis"] - 2 * 7.29e-5 * np.sin(47 * 3.1415 / 180)) < 1e-9
+
+
+def test_hilly_domains_build():
+    """The uneven-domain instances build for small and large grids: hills raise KKART, every
+    column of a hilly grid is prognostic, KADVMAX follows KKART + VertCellsFF."""
+    for q, (ni, nj, dx, vc) in enumerate([(20, 20, 2.0, 8), (24, 20, 2.0, 8), (48, 28, 4.0, 9), (128, 112, 2.0, 20),
+                                          (192, 176, 2.5, 30)]):
+        d = prep.hilly_domain(ni, nj, dx, vc, seed=q)
+        st = d.static
+        assert d.kadvmax == min(d.nkk, max(1, int(st.kkart[st.cutk > 0].max())) + vc)
+        assert st.kkart.max() > 0
+        assert (st.cutk[1:ni + 1, 1:nj + 1] > 0).all()
