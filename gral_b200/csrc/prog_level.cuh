@@ -852,21 +852,37 @@ __device__ __forceinline__ void velcorr_col(const KArgs &a, int s, int col, int 
     const SitDev &sd = a.sit[s];
     const float DT = sd.dtime, DXK = a.dxk, DYK = a.dyk;
     const double fr = sd.frund;
-    const int q = sd.quantise;
+    const int qz = sd.quantise;
     const long long dW = -(long long)a.nj2;
-#pragma unroll 4
-    for (int k = kbeg; k <= m.vi; k += kstep) {
-        if (k < 1) continue;
-        const float d = a.dpm[x.at(0, k)];
-        if (i > 2 && m.kkm_u < k)
-            a.uk[x.at(0, k)] = (float)quantd((double)(a.uk[x.at(0, k)] + (a.dpm[x.at(dW, k)] - d) / DXK * DT), fr, q);
-        if (j > 2 && m.kkm_v < k)
-            a.vk[x.at(0, k)] = (float)quantd((double)(a.vk[x.at(0, k)] + (a.dpm[x.at(-1, k)] - d) / DYK * DT), fr, q);
-        if (m.kkart + 1 < k)
-            a.wk[x.at(0, k)] = (float)quantd(
-                (double)(a.wk[x.at(0, k)] + (a.dpm[x.at(0, k - 1)] - d) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, q);
-        else
-            a.wk[x.at(0, k)] = 0;
+    const bool du = i > 2, dv = j > 2;
+    // Chunks of CH levels: every load of the chunk is issued before its stores.  No level reads
+    // what another level writes (DPM is read only; U, V, W are read and written at the same cell),
+    // so this only lets the loads overlap instead of queuing behind the previous level's stores.
+    constexpr int CH = 4;
+    for (int kb = kbeg; kb <= m.vi; kb += CH * kstep) {
+        float d[CH], dw[CH], ds[CH], dk[CH], u[CH], v[CH], w[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = kb + q * kstep;
+            d[q] = dw[q] = ds[q] = dk[q] = u[q] = v[q] = w[q] = 0.f;
+            if (k < 1 || k > m.vi) continue;
+            d[q] = a.dpm[x.at(0, k)];
+            if (du && m.kkm_u < k) { u[q] = a.uk[x.at(0, k)]; dw[q] = a.dpm[x.at(dW, k)]; }
+            if (dv && m.kkm_v < k) { v[q] = a.vk[x.at(0, k)]; ds[q] = a.dpm[x.at(-1, k)]; }
+            if (m.kkart + 1 < k) { w[q] = a.wk[x.at(0, k)]; dk[q] = a.dpm[x.at(0, k - 1)]; }
+        }
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = kb + q * kstep;
+            if (k < 1 || k > m.vi) continue;
+            if (du && m.kkm_u < k) a.uk[x.at(0, k)] = (float)quantd((double)(u[q] + (dw[q] - d[q]) / DXK * DT), fr, qz);
+            if (dv && m.kkm_v < k) a.vk[x.at(0, k)] = (float)quantd((double)(v[q] + (ds[q] - d[q]) / DYK * DT), fr, qz);
+            if (m.kkart + 1 < k)
+                a.wk[x.at(0, k)] =
+                    (float)quantd((double)(w[q] + (dk[q] - d[q]) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, qz);
+            else
+                a.wk[x.at(0, k)] = 0;
+        }
     }
 }
 
@@ -882,16 +898,38 @@ __device__ __forceinline__ void average_col(const KArgs &a, int col, int i, int 
     const int KK = m.kkart;
     const bool cpS = (j == 2);
     const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
-#pragma unroll 4
-    for (int k = kbeg; k <= m.vi; k += kstep) {
-        if (k < m.kstart) continue;
-        if (KK < k) {
-            a.uks[x.at(0, k)] = 0.5f * (a.uk[x.at(0, k)] + a.uk[x.at(dE, k)]);
-            a.vks[x.at(0, k)] = 0.5f * (a.vk[x.at(0, k)] + a.vk[x.at(1, k)]);
+    // chunks of CH levels with their loads first, as in velcorr_col (UK, VK, WK are only read
+    // here; the border copies take this column's UKS, new or, inside the obstacle, the old value)
+    constexpr int CH = 4;
+    for (int kb = kbeg; kb <= m.vi; kb += CH * kstep) {
+        float u0[CH], u1[CH], v0[CH], v1[CH], w0[CH], w1[CH], uo[CH];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = kb + q * kstep;
+            u0[q] = u1[q] = v0[q] = v1[q] = w0[q] = w1[q] = uo[q] = 0.f;
+            if (k < m.kstart || k > m.vi) continue;
+            if (KK < k) {
+                u0[q] = a.uk[x.at(0, k)]; u1[q] = a.uk[x.at(dE, k)];
+                v0[q] = a.vk[x.at(0, k)]; v1[q] = a.vk[x.at(1, k)];
+            } else if (cpS || cpN) {
+                uo[q] = a.uks[x.at(0, k)];
+            }
+            if (KK + 1 < k) { w0[q] = a.wk[x.at(0, k)]; w1[q] = a.wk[x.at(0, k + 1)]; }
         }
-        if (KK + 1 < k) a.wks[x.at(0, k)] = 0.5f * (a.wk[x.at(0, k)] + a.wk[x.at(0, k + 1)]);
-        if (cpS) a.uks[x.at(-1, k)] = a.uks[x.at(0, k)];
-        if (cpN) a.uks[x.at(1, k)] = a.uks[x.at(0, k)];
+#pragma unroll
+        for (int q = 0; q < CH; ++q) {
+            const int k = kb + q * kstep;
+            if (k < m.kstart || k > m.vi) continue;
+            float us = uo[q];
+            if (KK < k) {
+                us = 0.5f * (u0[q] + u1[q]);
+                a.uks[x.at(0, k)] = us;
+                a.vks[x.at(0, k)] = 0.5f * (v0[q] + v1[q]);
+            }
+            if (KK + 1 < k) a.wks[x.at(0, k)] = 0.5f * (w0[q] + w1[q]);
+            if (cpS) a.uks[x.at(-1, k)] = us;
+            if (cpN) a.uks[x.at(1, k)] = us;
+        }
     }
     // VKS[1][j] = VKS[2][j] and VKS[NII][j] = VKS[NII-1][j] on every level (:1018-1036)
     const bool west = (i == 2) && (a.cflags[1 * nj2 + j] & F_ADV);
