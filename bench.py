@@ -430,6 +430,44 @@ def prep_measure(dom, repeats: int = 5):
     return out
 
 
+def batch_setup_measure(dom, n: int = 144, sample: int = 4):
+    """Loading a batch of n situations: initial fields built on the device from met profiles
+    (gral_prog_load_flat) against host-built fields copied in (gral_prog_load) (rank 0 only)."""
+    import numpy as np
+    from gral_b200.abi import FieldArrays, MetProfile
+    from gral_b200.prognostic import PrognosticSolver
+    from oracle import prep as OP
+
+    F32 = np.float32
+    st = dom.static
+    grid = dict(nii=dom.nii, njj=dom.njj, nkk=dom.nkk, vert_cells_ff=dom.vert_cells_ff, dxk=dom.dxk,
+                dyk=dom.dyk, near_wall=0, igeb=max(int(20 / dom.dxk), 1))
+    mets = []
+    for q in range(n):
+        th = math.radians(10.0 * (q % 36))
+        sp = (0.5, 1.0, 2.0, 4.0)[(q // 36) % 4]
+        mets.append(MetProfile(np.array([0, 10.0], F32), np.array([0, -sp * math.sin(th)], F32),
+                               np.array([0, -sp * math.cos(th)], F32), (250.0, 1000.0, -60.0)[q % 3]))
+    ps = [dom.params(None, iterations=1) for _ in range(n)]
+    shape = (dom.nii + 2, dom.njj + 2, dom.nkk + 2)
+    out = FieldArrays(np.zeros(shape, F32), np.zeros(shape, F32), np.zeros(shape, F32))
+    t0 = time.perf_counter()
+    host = [OP.flat_init(grid, st.cutk, st.dzk, st.hokart, mets[q])[3] for q in range(sample)]
+    host_s = (time.perf_counter() - t0) / sample * n
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=n) as s:
+        s.load_flat(ps[:2], st, mets[:2], grid, [out, out])
+        t0 = time.perf_counter()
+        s.load_flat(ps, st, mets, grid, [out] * n)
+        flat_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        s.load(ps, st, [host[q % sample] for q in range(n)])
+        load_s = time.perf_counter() - t0
+    return {"workload": f"{n} situations on the {dom.nii}x{dom.njj}x{dom.nkk} grid (met profiles of the batched set)",
+            "load_flat_s": round(flat_s, 3), "load_host_fields_s": round(load_s, 3),
+            "host_setup_s_estimate": round(host_s, 1),
+            "host_setup_kind": f"oracle restatement of MicroscaleFlat.cs on 1 core, {sample} situations timed, scaled to {n}"}
+
+
 def wind_measure(dom, sit, n: int = 1 << 20, repeats: int = 5):
     """Wind interpolation at n particles after a store (rank 0 only)."""
     import numpy as np
@@ -577,6 +615,7 @@ def run_ours(args, rank, world):
     prepm = None
     if rank == 0 and args.workload == "production" and not args.no_prep:
         prepm = prep_measure(dom)
+        prepm["batch_setup"] = batch_setup_measure(dom)
     windm = None
     if rank == 0 and args.workload == "production" and not args.no_wind:
         windm = wind_measure(dom, sit)

@@ -117,6 +117,10 @@ struct gral_ctx {
     DevBuf<float> gffu;                  // unpacked fields, 3 x [NII+2][NJJ+2][NKK+2]
     DevBuf<char> l2flush;                // written before each timed pack launch
     PrepBufs prep;                       // set-up entry points
+    // gral_prog_load_flat: initial fields built on the device during the load (else null)
+    const gral_met *flat_met = nullptr;
+    const gral_flat_grid *flat_grid = nullptr;
+    std::vector<float> h_ref;            // per situation: the six reference-column values of the set-up
     double prep_ms = 0.0;                // device time of the last set-up call's kernels
     DevBuf<SitDev> sit;
     DevBuf<int> flags, misc, diag, bcl, counts;

@@ -25,6 +25,7 @@
 #include "prog_ctx.cuh"
 #include "prog_gff.cuh"
 #include "prog_kernels.cuh"
+#include "prog_prep.cuh"
 
 using namespace gral;
 
@@ -471,6 +472,38 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         tab[4 * ks + k] = AREA / (0.5f * (DZ[k + 1] + DZ[k]));
     }
 
+    // ---- initial fields built on the device (gral_prog_load_flat) ----
+    // The staging of every situation is filled by the flat-terrain set-up kernels; the six values
+    // of the reference column that the scalars below need come back to the host.
+    if (ctx->flat_met) {
+        const size_t ssz0 = (size_t)ncols * nk2;
+        CK(ctx->stage.ensure(ssz0 * ((ctx->model != 1) ? 5 : 3) * n));
+        cudaStream_t st0 = ctx->stream;
+        PrepBufs &pb = ctx->prep;
+        CK(pb.cutk.ensure(ncols));
+        CK(cudaMemcpyAsync(pb.cutk.p, s->cutk, ncols * sizeof(float), cudaMemcpyHostToDevice, st0));
+        if (ctx->flat_grid->near_wall == 1) {
+            CK(pb.adv.ensure(ncols));
+            CK(cudaMemcpyAsync(pb.adv.p, s->advdom, ncols, cudaMemcpyHostToDevice, st0));
+        }
+        float *u0 = ctx->stage.p, *v0 = u0 + ssz0 * n, *w0 = v0 + ssz0 * n;
+        ctx->h_ref.assign(6 * (size_t)n, 0.0f);
+        for (int b = 0; b < n; ++b) {
+            int *dk = nullptr;
+            const int frc = flat_fill(ctx, ctx->flat_grid, pb.cutk.p, pb.adv.p, s->dzk, s->hokart, &ctx->flat_met[b],
+                                      u0 + ssz0 * b, v0 + ssz0 * b, w0 + ssz0 * b, &dk, false);
+            if (frc != GRAL_OK) return frc;
+            const int rx = p[b].ref_i, ry = p[b].ref_j;
+            auto at = [&](int i, int j, int k) { return ((size_t)i * nj2 + j) * nk2 + k; };
+            const float *src[6] = {u0 + ssz0 * b + at(rx, ry, NKK - 1), v0 + ssz0 * b + at(rx, ry, NKK - 1),
+                                   u0 + ssz0 * b + at(rx, ry, p[b].kadvmax), v0 + ssz0 * b + at(rx, ry, p[b].kadvmax),
+                                   u0 + ssz0 * b + at(rx + 1, ry, NKK - 1), v0 + ssz0 * b + at(rx, ry + 1, NKK - 1)};
+            for (int q = 0; q < 6; ++q)
+                CK(cudaMemcpyAsync(&ctx->h_ref[6 * (size_t)b + q], src[q], sizeof(float), cudaMemcpyDeviceToHost, st0));
+        }
+        CK(cudaStreamSynchronize(st0));
+    }
+
     // ---- per-situation scalars (:146-163, 231-240, 406-407) ----
     ctx->h_sit.assign(n, SitDev{});
     std::vector<float> ap0((size_t)n * ks, 0.0f);
@@ -478,11 +511,23 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         const gral_params &q = p[b];
         const int rx = q.ref_i, ry = q.ref_j;
         auto I3 = [&](int i, int j, int k) { return ((size_t)i * nj2 + j) * nk2 + k; };
-        const float *UK = f[b].uk, *VK = f[b].vk;
-        const float u1 = UK[I3(rx, ry, NKK - 1)], v1 = VK[I3(rx, ry, NKK - 1)];
+        // U, V of the reference column at NKK-1 and KADVMAX, U east and V north of it at NKK-1
+        float rv[6];
+        if (ctx->flat_met) {
+            for (int r = 0; r < 6; ++r) rv[r] = ctx->h_ref[6 * (size_t)b + r];
+        } else {
+            const float *UK = f[b].uk, *VK = f[b].vk;
+            rv[0] = UK[I3(rx, ry, NKK - 1)];
+            rv[1] = VK[I3(rx, ry, NKK - 1)];
+            rv[2] = UK[I3(rx, ry, q.kadvmax)];
+            rv[3] = VK[I3(rx, ry, q.kadvmax)];
+            rv[4] = UK[I3(rx + 1, ry, NKK - 1)];
+            rv[5] = VK[I3(rx, ry + 1, NKK - 1)];
+        }
+        const float u1 = rv[0], v1 = rv[1];
         float topwind = (float)std::sqrt((double)(u1 * u1 + v1 * v1));
         topwind = net_max(topwind, 0.01f);
-        const float u2 = UK[I3(rx, ry, q.kadvmax)], v2 = VK[I3(rx, ry, q.kadvmax)];
+        const float u2 = rv[2], v2 = rv[3];
         float DT = 0.5f * net_min(DXK, s->dzk[1]) / net_max(0.01f, sqrtf(u2 * u2 + v2 * v2));
         DT = net_min(DT, 5.0f);
         for (int k = 1; k <= q.kadvmax; ++k) ap0[(size_t)b * ks + k] = AREA * s->dzk[k] / DT;
@@ -492,8 +537,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         S.dtime = DT;
         S.topwind = topwind;
         const bool alloc = (cfl[rx * nj2 + ry] & F_ALLOC3) != 0;
-        S.ug = alloc ? 0.5f * (UK[I3(rx, ry, NKK - 1)] + UK[I3(rx + 1, ry, NKK - 1)]) : 0.0f;
-        S.vg = alloc ? 0.5f * (VK[I3(rx, ry, NKK - 1)] + VK[I3(rx, ry + 1, NKK - 1)]) : 0.0f;
+        S.ug = alloc ? 0.5f * (rv[0] + rv[4]) : 0.0f;
+        S.vg = alloc ? 0.5f * (rv[1] + rv[5]) : 0.0f;
         S.it = 1;
         S.active = 1;
         S.it_min = q.iteration_steps_min;
@@ -773,9 +818,11 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemsetAsync(ctx->trace.p, 0, (size_t)n * tcap * sizeof(float), st));
     // host fields -> staging (one contiguous copy per field and situation)
     for (int b = 0; b < n; ++b) {
-        CK(cudaMemcpyAsync(sg.uk + ssz * b, f[b].uk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(sg.vk + ssz * b, f[b].vk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(sg.wk + ssz * b, f[b].wk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        if (!ctx->flat_met) {   // else already built on the device
+            CK(cudaMemcpyAsync(sg.uk + ssz * b, f[b].uk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(sg.vk + ssz * b, f[b].vk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(sg.wk + ssz * b, f[b].wk, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        }
         if (ctx->model != 1) {
             CK(cudaMemcpyAsync(sg.turb + ssz * b, f[b].turb, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
             CK(cudaMemcpyAsync(sg.tdiss + ssz * b, f[b].tdiss, ssz * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -1002,6 +1049,26 @@ int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const 
             stats[b].ms_iterate = ms_it;
             stats[b].ms_total = stats[b].ms_upload + ms_it + stats[b].ms_download;
         }
+    return rc;
+}
+
+int gral_prog_load_flat(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s, const gral_met *met,
+                        const gral_flat_grid *g, gral_fields *f) {
+    if (!ctx) return GRAL_EINVAL;
+    if (n < 1 || !p || !s || !met || !g || !s->cutk || !s->dzk || !s->hokart)
+        return fail(ctx, GRAL_EINVAL, "null pointer or empty batch");
+    if (g->nii != p[0].nii || g->njj != p[0].njj || g->nkk != p[0].nkk || g->vert_cells_ff != p[0].vert_cells_ff ||
+        g->dxk != p[0].dxk || g->dyk != p[0].dyk)
+        return fail(ctx, GRAL_EINVAL, "set-up grid differs from the parameters");
+    for (int b = 0; b < n; ++b) {
+        const int rc = flat_check(ctx, g, s->hokart, &met[b], s->advdom != nullptr);
+        if (rc != GRAL_OK) return rc;
+    }
+    ctx->flat_met = met;
+    ctx->flat_grid = g;
+    const int rc = gral_prog_load(ctx, n, p, s, f);
+    ctx->flat_met = nullptr;
+    ctx->flat_grid = nullptr;
     return rc;
 }
 

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "prog_ctx.cuh"
+#include "prog_prep.cuh"
 
 namespace gral {
 
@@ -229,70 +230,14 @@ int grid_warps(long long warps) { return (int)((warps + kWarps - 1) / kWarps); }
 
 }  // namespace
 
-}  // namespace gral
-
-using namespace gral;
-
-namespace {
-
-// device time between ev[0] and ev[1] of a completed set-up call
-int record_ms(gral_ctx *ctx) {
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-    ctx->prep_ms = ms;
-    return GRAL_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-int gral_prog_subdomains(gral_ctx *ctx, int32_t nii, int32_t njj, float dxk, float dyk, int32_t factor,
-                         const float *cutk, uint8_t *advdom) {
-    if (!ctx) return GRAL_EINVAL;
-    if (!cutk || !advdom) return fail(ctx, GRAL_EINVAL, "null pointer");
-    if (nii < 1 || njj < 1 || nii > ctx->cap_nii || njj > ctx->cap_njj)
-        return fail(ctx, GRAL_EINVAL, "grid outside the context's capacity");
-    if (!(dxk > 0) || !(dyk > 0) || factor < 0) return fail(ctx, GRAL_EINVAL, "bad cell size or factor");
-    const int nj2 = njj + 2;
-    const size_t ncols = (size_t)(nii + 2) * nj2;
-    // the largest reach bounds both passes' search ranges (reach grows with CUTK)
-    float cmax = 0.f;
-    for (int i = 1; i <= nii; ++i)
-        for (int j = 1; j <= njj; ++j) cmax = std::max(cmax, cutk[(size_t)i * nj2 + j]);
-    const int imax = reach_cells(factor, cmax, dxk), jmax = reach_cells(factor, cmax, dyk);
-    CK(cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
-    PrepBufs &b = ctx->prep;
-    CK(b.cutk.ensure(ncols));
-    CK(b.ints.ensure(ncols));
-    CK(b.adv.ensure(ncols));
-    CK(cudaMemcpyAsync(b.cutk.p, cutk, ncols * sizeof(float), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(b.adv.p, 0, ncols, st));
-    const dim3 grid((njj + kThreads - 1) / kThreads, nii);
-    CK(cudaEventRecord(ctx->ev[0], st));
-    k_sub_reach<<<grid, kThreads, 0, st>>>(nii, njj, dxk, dyk, factor, jmax, b.cutk.p, b.ints.p);
-    k_sub_mark<<<grid, kThreads, 0, st>>>(nii, njj, imax, b.ints.p, b.adv.p);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ctx->ev[1], st));
-    CK(cudaMemcpyAsync(advdom, b.adv.p, ncols, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return record_ms(ctx);
-}
-
-int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cutk, const float *dzk,
-                        const float *hokart, const uint8_t *advdom, const gral_met *met, int16_t *kkart,
-                        float *ahk, int32_t *kadvmax, gral_fields *f) {
-    if (!ctx) return GRAL_EINVAL;
-    if (!g || !cutk || !dzk || !hokart || !met || !kkart || !ahk || !kadvmax || !f || !f->uk || !f->vk || !f->wk)
-        return fail(ctx, GRAL_EINVAL, "null pointer");
+int flat_check(gral_ctx *ctx, const gral_flat_grid *g, const float *hokart, const gral_met *met, bool have_advdom) {
     const int NII = g->nii, NJJ = g->njj, NKK = g->nkk;
     if (NII < 1 || NJJ < 1 || NKK < 2 || NII > ctx->cap_nii || NJJ > ctx->cap_njj || NKK > ctx->cap_nkk)
         return fail(ctx, GRAL_EINVAL, "grid outside the context's capacity");
     if (g->vert_cells_ff < 0) return fail(ctx, GRAL_EINVAL, "negative vert_cells_ff");
     if ((long long)(NII + 2) * (NJJ + 2) >= (1LL << 31)) return fail(ctx, GRAL_ETOOLARGE, "more than 2^31 columns");
     if (g->near_wall < 0 || g->near_wall > 2) return fail(ctx, GRAL_EINVAL, "near_wall must be 0, 1 or 2");
-    if (g->near_wall == 1 && !advdom) return fail(ctx, GRAL_EINVAL, "near_wall 1 needs ADVDOM");
+    if (g->near_wall == 1 && !have_advdom) return fail(ctx, GRAL_EINVAL, "near_wall 1 needs ADVDOM");
     if (g->near_wall && g->igeb < 1) return fail(ctx, GRAL_EINVAL, "igeb must be at least 1");
     for (int k = 0; k < NKK + 2; ++k)
         if (!(hokart[k] >= 0)) return fail(ctx, GRAL_EINVAL, "HOKART must be non-negative");
@@ -300,6 +245,14 @@ int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cut
     const int nh = met->n_heights;
     if (nh < 1 || !met->measurement_height || !met->obs_u || !met->obs_v)
         return fail(ctx, GRAL_EINVAL, "met profile needs at least one height");
+    return GRAL_OK;
+}
+
+int flat_fill(gral_ctx *ctx, const gral_flat_grid *g, const float *d_cutk, const uint8_t *d_adv, const float *dzk,
+              const float *hokart, const gral_met *met, float *du, float *dv, float *dw, int **d_kadv_out,
+              bool timed) {
+    const int NII = g->nii, NJJ = g->njj, NKK = g->nkk;
+    const int nh = met->n_heights;
     const float *MH = met->measurement_height, *OU = met->obs_u, *OV = met->obs_v;
     const int nj2 = NJJ + 2, nk2 = NKK + 2;
     const size_t ncols = (size_t)(NII + 2) * nj2, cells = ncols * nk2;
@@ -382,17 +335,13 @@ int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cut
     }
 
     // ---- device ----
-    CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     PrepBufs &b = ctx->prep;
     const size_t ntab = (NKK + 1) + nk2 + pu.size() + pv.size() + fac.size();
-    CK(b.cutk.ensure(ncols));
     CK(b.ahk.ensure(ncols));
     CK(b.kkart.ensure(ncols));
     CK(b.tab.ensure(ntab));
     CK(b.ints.ensure(col_prof.size() + 1));
-    CK(b.fields.ensure(3 * cells));
-    if (g->near_wall == 1) CK(b.adv.ensure(ncols));
     float *d_vertk = b.tab.p, *d_hok = d_vertk + (NKK + 1), *d_pu = d_hok + nk2, *d_pv = d_pu + pu.size(),
           *d_fac = d_pv + pv.size();
     CK(cudaMemcpyAsync(d_vertk, vertk.data(), vertk.size() * 4, cudaMemcpyHostToDevice, st));
@@ -400,26 +349,103 @@ int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cut
     CK(cudaMemcpyAsync(d_pu, pu.data(), pu.size() * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d_pv, pv.data(), pv.size() * 4, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(d_fac, fac.data(), fac.size() * 4, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(b.cutk.p, cutk, ncols * 4, cudaMemcpyHostToDevice, st));
     int *d_kadv = b.ints.p + col_prof.size();
     if (!col_prof.empty())
         CK(cudaMemcpyAsync(b.ints.p, col_prof.data(), col_prof.size() * 4, cudaMemcpyHostToDevice, st));
     const int one = 1;
     CK(cudaMemcpyAsync(d_kadv, &one, 4, cudaMemcpyHostToDevice, st));
-    if (g->near_wall == 1) CK(cudaMemcpyAsync(b.adv.p, advdom, ncols, cudaMemcpyHostToDevice, st));
-    float *du = b.fields.p, *dv = du + cells, *dw = dv + cells;
-    CK(cudaMemsetAsync(du, 0, 3 * cells * sizeof(float), st));
+    CK(cudaMemsetAsync(du, 0, cells * sizeof(float), st));
+    CK(cudaMemsetAsync(dv, 0, cells * sizeof(float), st));
+    CK(cudaMemsetAsync(dw, 0, cells * sizeof(float), st));
     CK(cudaMemsetAsync(b.kkart.p, 0, ncols * sizeof(int16_t), st));
     CK(cudaMemsetAsync(b.ahk.p, 0, ncols * sizeof(float), st));
     FlatTabs t{d_vertk, d_hok, d_pu, d_pv, col_prof.empty() ? nullptr : b.ints.p};
-    CK(cudaEventRecord(ctx->ev[0], st));
-    k_flat_columns<<<dim3((NJJ + kWarps - 1) / kWarps, NII), kThreads, 0, st>>>(NII, NJJ, NKK, t, b.cutk.p, du,
-                                                                                dv, b.kkart.p, b.ahk.p, d_kadv);
+    if (timed) CK(cudaEventRecord(ctx->ev[0], st));
+    k_flat_columns<<<dim3((NJJ + kWarps - 1) / kWarps, NII), kThreads, 0, st>>>(NII, NJJ, NKK, t, d_cutk, du, dv,
+                                                                                b.kkart.p, b.ahk.p, d_kadv);
     if (g->near_wall && NII > 2 * igeb && NJJ > 2 * igeb)
         k_flat_near_wall<<<grid_warps((long long)(NII - 2 * igeb) * (NJJ - 2 * igeb)), kThreads, 0, st>>>(
-            NII, NJJ, NKK, igeb, g->near_wall, b.adv.p, b.cutk.p, b.ahk.p, b.kkart.p, d_vertk, d_fac, du, dv);
+            NII, NJJ, NKK, igeb, g->near_wall, d_adv, d_cutk, b.ahk.p, b.kkart.p, d_vertk, d_fac, du, dv);
+    CK(cudaGetLastError());
+    if (timed) CK(cudaEventRecord(ctx->ev[1], st));
+    *d_kadv_out = d_kadv;
+    return GRAL_OK;
+}
+
+}  // namespace gral
+
+using namespace gral;
+
+namespace {
+
+// device time between ev[0] and ev[1] of a completed set-up call
+int record_ms(gral_ctx *ctx) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->prep_ms = ms;
+    return GRAL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gral_prog_subdomains(gral_ctx *ctx, int32_t nii, int32_t njj, float dxk, float dyk, int32_t factor,
+                         const float *cutk, uint8_t *advdom) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!cutk || !advdom) return fail(ctx, GRAL_EINVAL, "null pointer");
+    if (nii < 1 || njj < 1 || nii > ctx->cap_nii || njj > ctx->cap_njj)
+        return fail(ctx, GRAL_EINVAL, "grid outside the context's capacity");
+    if (!(dxk > 0) || !(dyk > 0) || factor < 0) return fail(ctx, GRAL_EINVAL, "bad cell size or factor");
+    const int nj2 = njj + 2;
+    const size_t ncols = (size_t)(nii + 2) * nj2;
+    // the largest reach bounds both passes' search ranges (reach grows with CUTK)
+    float cmax = 0.f;
+    for (int i = 1; i <= nii; ++i)
+        for (int j = 1; j <= njj; ++j) cmax = std::max(cmax, cutk[(size_t)i * nj2 + j]);
+    const int imax = reach_cells(factor, cmax, dxk), jmax = reach_cells(factor, cmax, dyk);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    PrepBufs &b = ctx->prep;
+    CK(b.cutk.ensure(ncols));
+    CK(b.ints.ensure(ncols));
+    CK(b.adv.ensure(ncols));
+    CK(cudaMemcpyAsync(b.cutk.p, cutk, ncols * sizeof(float), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(b.adv.p, 0, ncols, st));
+    const dim3 grid((njj + kThreads - 1) / kThreads, nii);
+    CK(cudaEventRecord(ctx->ev[0], st));
+    k_sub_reach<<<grid, kThreads, 0, st>>>(nii, njj, dxk, dyk, factor, jmax, b.cutk.p, b.ints.p);
+    k_sub_mark<<<grid, kThreads, 0, st>>>(nii, njj, imax, b.ints.p, b.adv.p);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaMemcpyAsync(advdom, b.adv.p, ncols, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return record_ms(ctx);
+}
+
+int gral_prog_flat_init(gral_ctx *ctx, const gral_flat_grid *g, const float *cutk, const float *dzk,
+                        const float *hokart, const uint8_t *advdom, const gral_met *met, int16_t *kkart,
+                        float *ahk, int32_t *kadvmax, gral_fields *f) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!g || !cutk || !dzk || !hokart || !met || !kkart || !ahk || !kadvmax || !f || !f->uk || !f->vk || !f->wk)
+        return fail(ctx, GRAL_EINVAL, "null pointer");
+    int rc = flat_check(ctx, g, hokart, met, advdom != nullptr);
+    if (rc != GRAL_OK) return rc;
+    const int NII = g->nii, NJJ = g->njj, NKK = g->nkk;
+    const int nj2 = NJJ + 2, nk2 = NKK + 2;
+    const size_t ncols = (size_t)(NII + 2) * nj2, cells = ncols * nk2;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    PrepBufs &b = ctx->prep;
+    CK(b.cutk.ensure(ncols));
+    CK(b.fields.ensure(3 * cells));
+    if (g->near_wall == 1) CK(b.adv.ensure(ncols));
+    CK(cudaMemcpyAsync(b.cutk.p, cutk, ncols * 4, cudaMemcpyHostToDevice, st));
+    if (g->near_wall == 1) CK(cudaMemcpyAsync(b.adv.p, advdom, ncols, cudaMemcpyHostToDevice, st));
+    float *du = b.fields.p, *dv = du + cells, *dw = dv + cells;
+    int *d_kadv = nullptr;
+    rc = flat_fill(ctx, g, b.cutk.p, b.adv.p, dzk, hokart, met, du, dv, dw, &d_kadv, true);
+    if (rc != GRAL_OK) return rc;
     int kadv1 = 1;
     CK(cudaMemcpyAsync(&kadv1, d_kadv, 4, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(kkart, b.kkart.p, ncols * sizeof(int16_t), cudaMemcpyDeviceToHost, st));

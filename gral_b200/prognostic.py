@@ -26,7 +26,7 @@ EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_pro
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
            "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack",
            "gral_prog_subdomains", "gral_prog_flat_init", "gral_prog_vegetation", "gral_prog_prep_last_ms",
-           "gral_prog_wind_at", "gral_prog_solve_instances"]
+           "gral_prog_wind_at", "gral_prog_solve_instances", "gral_prog_load_flat"]
 
 # payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
 GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, GFF_TKE = 0, 1, 2, 3
@@ -110,6 +110,9 @@ def lib(build_if_stale: bool = True):
                                             C.POINTER(GralFields), C.POINTER(GralStats), C.POINTER(C.c_int32),
                                             C.c_int32, C.c_uint64]
     L.gral_prog_solve_instances.restype = C.c_int
+    L.gral_prog_load_flat.argtypes = [vp, C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralMet),
+                                      C.POINTER(GralFlatGrid), C.POINTER(GralFields)]
+    L.gral_prog_load_flat.restype = C.c_int
     _lib = L
     return L
 
@@ -179,6 +182,19 @@ class PrognosticSolver:
         fa = (GralFields * n)(*[f.to_c() for f in fields])
         self._keep = [pa, s, fa, static, fields]
         self._check(self._L.gral_prog_load(self._ctx, n, pa, C.byref(s), fa))
+
+    def load_flat(self, params: Sequence[dict], static: StaticArrays, mets: Sequence[MetProfile], grid: dict,
+                  fields: Sequence[FieldArrays]):
+        """Split-form load whose initial U, V, W are built on the device from each situation's met
+        profile (flat-terrain set-up); ``fields`` receive the results at ``store``."""
+        n = len(params)
+        pa = (GralParams * n)(*[params_to_c(p) for p in params])
+        s = static.to_c()
+        ma = (GralMet * n)(*[m.to_c() for m in mets])
+        g = GralFlatGrid(**grid)
+        fa = (GralFields * n)(*[f.to_c() for f in fields])
+        self._keep = [pa, s, ma, g, fa, static, fields, mets]
+        self._check(self._L.gral_prog_load_flat(self._ctx, n, pa, C.byref(s), ma, C.byref(g), fa))
 
     def iterate(self):
         self._check(self._L.gral_prog_iterate(self._ctx))

@@ -333,6 +333,15 @@ int gral_prog_wind_at(gral_ctx *ctx, int32_t situation, const gral_wind_grid *g,
                       const float *hokart, int32_t n, const gral_particle *particles, float *ux, float *uy,
                       float *uz, int32_t *index_k);
 
+/* gral_prog_load with the initial U, V, W of every situation built on the device from its met
+ * profile met[b] by the flat-terrain set-up of gral_prog_flat_init (grid g, the same for all
+ * situations and equal to the parameters' grid), so that a batch needs no host-built field and
+ * copies none to the device.  f[b].uk, vk, wk are not read: gral_prog_store writes the results
+ * there.  TURB/TDISS of models 0 and 2 are read from f as by gral_prog_load.  p[b].kadvmax and
+ * s->kkart must be those of the set-up (gral_prog_flat_init returns them). */
+int gral_prog_load_flat(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s, const gral_met *met,
+                        const gral_flat_grid *g, gral_fields *f);
+
 /* Instrumentation: device time in ms of the kernels of the last gral_prog_subdomains,
  * gral_prog_flat_init, gral_prog_vegetation or gral_prog_wind_at call on this context (CUDA
  * events around its launches, host copies excluded). */
