@@ -609,18 +609,20 @@ def run_ours(args, rank, world):
                    "phase_ms_per_iteration": {k: round(v / args.batched_steps, 4) for k, v in bph.items() if v > 0},
                    "clocks": bclk}
 
+    # the measurements of the rows around the solve run on single-GPU runs only
+    extras = rank == 0 and world == 1 and args.workload == "production"
     gffm = None
-    if rank == 0 and args.workload == "production" and not args.no_gff:
+    if extras and not args.no_gff:
         gffm = gff_measure(dom, sit)
     prepm = None
-    if rank == 0 and args.workload == "production" and not args.no_prep:
+    if extras and not args.no_prep:
         prepm = prep_measure(dom)
         prepm["batch_setup"] = batch_setup_measure(dom)
     windm = None
-    if rank == 0 and args.workload == "production" and not args.no_wind:
+    if extras and not args.no_wind:
         windm = wind_measure(dom, sit)
     instm = None
-    if rank == 0 and args.workload == "production" and not args.no_instances:
+    if extras and not args.no_instances:
         instm = instances_measure()
 
     cpu = None
