@@ -1305,7 +1305,7 @@ struct BVariant {
               {k_mom_b<2, COMP_U, NW, MB>, k_mom_b<2, COMP_V, NW, MB>, k_mom_b<2, COMP_W, NW, MB>}}, \
              k_tke_b<NW, MB>}
 
-const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6)};
+const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(6, 4)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 const KFn kPlainMom[3][3] = {{k_mom<0, COMP_U>, k_mom<0, COMP_V>, k_mom<0, COMP_W>},
