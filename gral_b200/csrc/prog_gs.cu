@@ -1135,15 +1135,9 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     if (act) {
         const SitCtx sc = make_sit(a, s);
-        // two levels per step: their operand loads are independent and overlap
-        int k = c.K0 + warp;
-        for (; k + NW <= c.VI; k += 2 * NW) {
-            const Coef q0 = mom_level<MODEL, COMP, true>(a, x, c, sc, k);
-            const Coef q1 = mom_level<MODEL, COMP, true>(a, x, c, sc, k + NW);
-            R.a(k) = q0.A; R.b(k) = q0.B; R.c(k) = q0.C; R.d(k) = q0.D; R.p(k) = q0.phi;
-            R.a(k + NW) = q1.A; R.b(k + NW) = q1.B; R.c(k + NW) = q1.C; R.d(k + NW) = q1.D; R.p(k + NW) = q1.phi;
-        }
-        if (k <= c.VI) {
+        // one level per step: within the register budget of four resident blocks a second level's
+        // operands did not overlap the first's (each level cost the same either way)
+        for (int k = c.K0 + warp; k <= c.VI; k += NW) {
             const Coef q = mom_level<MODEL, COMP, true>(a, x, c, sc, k);
             R.a(k) = q.A; R.b(k) = q.B; R.c(k) = q.C; R.d(k) = q.D; R.p(k) = q.phi;
         }
