@@ -222,6 +222,44 @@ __device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned
     }
 }
 
+__device__ __forceinline__ int ld_relaxed(const int *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Spin (one thread) until both predecessor flags hold at least `stamp` (a null flag has no
+// predecessor).  The two flags are polled with relaxed loads, so their round trips overlap, and
+// one fence.acquire follows: a strong read followed by an acquire fence is an acquire pattern, so
+// it synchronises with the predecessors' st.release as an acquiring load would.  Same bounds as
+// wait_stamp: gives up after limit_ns or on another warp's error and returns false then.
+__device__ inline bool wait_stamps(const int *f1, const int *f2, int stamp, int *err, unsigned long long limit_ns) {
+    int v1 = f1 ? ld_relaxed(f1) : stamp;
+    int v2 = f2 ? ld_relaxed(f2) : stamp;
+    if (v1 < stamp || v2 < stamp) {
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned ns = 16;
+        for (unsigned n = 1;; ++n) {
+            if (n > 4) {
+                __nanosleep(ns);
+                if (ns < 256) ns += ns;
+            }
+            if (v1 < stamp) v1 = ld_relaxed(f1);
+            if (v2 < stamp) v2 = ld_relaxed(f2);
+            if (v1 >= stamp && v2 >= stamp) break;
+            if ((n & 7) == 0) {
+                if (*(volatile int *)err != ERR_NONE) return false;
+                if (globaltimer_ns() - t0 > limit_ns) {
+                    atomicCAS(err, ERR_NONE, ERR_TIMEOUT);
+                    return false;
+                }
+            }
+        }
+    }
+    asm volatile("fence.acquire.gpu;" ::: "memory");
+    return true;
+}
+
 // Full-height level tables of the diagnostic pressure solve (DiagnosticFlowfield.cs:124-138):
 // APP, ATP, ABP with KKART < k-1 (abp1) and at KKART+1 (abp0), DZK; and the per-situation DTIME.
 struct DiagTabs {

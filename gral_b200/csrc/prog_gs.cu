@@ -1073,12 +1073,9 @@ __device__ __forceinline__ void gs_tasks_block(const KArgs &a, const SweepGeom &
             const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
             const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
             int *fl = a.flags + (size_t)grp * a.ncols;
-            if (threadIdx.x == 0) {
-                int ok = 1;
-                if (i1 > g.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, stamp, a.err, a.wait_limit_ns);
-                if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
-                s_ok = ok;
-            }
+            if (threadIdx.x == 0)
+                s_ok = wait_stamps((i1 > g.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
+                                   (j1 > g.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, stamp, a.err, a.wait_limit_ns);
             __syncthreads();
             auto ahead = [&]() {
                 const unsigned pt = t + gridDim.x;
