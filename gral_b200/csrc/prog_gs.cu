@@ -89,10 +89,9 @@ __device__ __forceinline__ void gs_tasks(const KArgs &a, const SweepGeom &g, Bod
             const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
             int *fl = a.flags + (size_t)u * a.ncols;
             int ok = 1;
-            if (lane == 0) {
-                if (i1 > g.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, stamp, a.err, a.wait_limit_ns);
-                if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
-            }
+            if (lane == 0)
+                ok = wait_stamps((i1 > g.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
+                                 (j1 > g.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, stamp, a.err, a.wait_limit_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             __syncwarp();
             if (ok) body(u, i, j, IS, JS, i1 == g.ia);
@@ -456,10 +455,9 @@ __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &
             int *fl = a.flags + (size_t)u * a.ncols;
             job.pre(u, i, j, IS, JS, i1 == g.ia);
             int ok = 1;
-            if (lane == 0) {
-                if (i1 > g.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, stamp, a.err, a.wait_limit_ns);
-                if (ok && j1 > g.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), stamp, a.err, a.wait_limit_ns);
-            }
+            if (lane == 0)
+                ok = wait_stamps((i1 > g.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
+                                 (j1 > g.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, stamp, a.err, a.wait_limit_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             __syncwarp();
             if (ok) job.post(u, IS, JS);
@@ -806,10 +804,12 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom
 //   U (i,j) after the averages of the 3x3 neighbourhood (which also covers the corrected U/V/W and
 //   final DPMNEW it reads) and its two U sweep predecessors.
 
-// Lanes 0..n-1 each wait on one flag; true if all flags reached their stamp.
+// Lanes 0..n-1 each wait on one flag (relaxed polls, all in flight together), then every lane
+// issues the acquire fence that completes the acquire pattern; true if all flags reached their
+// stamp.
 __device__ __forceinline__ bool wait_lanes(const KArgs &a, const int *flag, int stamp, bool mine) {
     bool ok = true;
-    if (mine) ok = wait_stamp(flag, stamp, a.err, a.wait_limit_ns);
+    if (mine) ok = wait_stamps(flag, nullptr, stamp, a.err, a.wait_limit_ns);
     return __all_sync(0xffffffffu, ok);
 }
 
@@ -864,10 +864,9 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_fused_pvau(KArgs a, FusedGeom
             stamp = sP;
             pj.pre(s, i, j, IS, JS, i1 == fg.gp.ia);
             bool ok = true;
-            if (lane == 0) {
-                if (i1 > fg.gp.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, sP, a.err, a.wait_limit_ns);
-                if (ok && j1 > fg.gp.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), sP, a.err, a.wait_limit_ns);
-            }
+            if (lane == 0)
+                ok = wait_stamps((i1 > fg.gp.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
+                                 (j1 > fg.gp.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, sP, a.err, a.wait_limit_ns);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             __syncwarp();
             if (ok) pj.post(s, IS, JS);
@@ -893,10 +892,10 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_fused_pvau(KArgs a, FusedGeom
             __syncwarp();
             if (ok) {
                 uj.pre(s, i, j, IS, JS, false);
-                if (lane == 0) {
-                    if (i1 > fg.gu.ia) ok = wait_stamp(fl + (i - IS) * a.nj2 + j, sU, a.err, a.wait_limit_ns);
-                    if (ok && j1 > fg.gu.ja) ok = wait_stamp(fl + i * a.nj2 + (j - JS), sU, a.err, a.wait_limit_ns);
-                }
+                if (lane == 0)
+                    ok = wait_stamps((i1 > fg.gu.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
+                                     (j1 > fg.gu.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, sU, a.err,
+                                     a.wait_limit_ns);
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 __syncwarp();
                 if (ok) uj.post(s, IS, JS);
