@@ -103,11 +103,11 @@ __device__ __forceinline__ void gs_tasks(const KArgs &a, const SweepGeom &g, Bod
 
 enum { COMP_U = 0, COMP_V = 1, COMP_W = 2 };
 
-template <int COMP, bool IL>
+template <int COMP, bool IL, int SW = 0>
 __device__ __forceinline__ Coef ml_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
-    if (COMP == COMP_U) return u1_level<IL>(a, x, c, sc, k);
-    if (COMP == COMP_V) return v1_level<IL>(a, x, c, sc, k);
-    return w1_level<IL>(a, x, c, sc, k);
+    if (COMP == COMP_U) return u1_level<IL, SW>(a, x, c, sc, k);
+    if (COMP == COMP_V) return v1_level<IL, SW>(a, x, c, sc, k);
+    return w1_level<IL, SW>(a, x, c, sc, k);
 }
 
 template <int COMP>
@@ -122,10 +122,11 @@ __device__ __forceinline__ float *comp_field(const KArgs &a) {
     return COMP == COMP_U ? a.uk : (COMP == COMP_V ? a.vk : a.wk);
 }
 
-// Coefficients of one level for model MODEL (0 no diffusion, 1 mixing length, 2 k-eps).
-template <int MODEL, int COMP, bool IL>
+// Coefficients of one level for model MODEL (0 no diffusion, 1 mixing length, 2 k-eps); SW as
+// for the model-1 routines.
+template <int MODEL, int COMP, bool IL, int SW = 0>
 __device__ __forceinline__ Coef mom_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
-    if (MODEL == 1) return ml_level<COMP, IL>(a, x, c, sc, k);
+    if (MODEL == 1) return ml_level<COMP, IL, SW>(a, x, c, sc, k);
     if (COMP == COMP_W) return w_scalar_level<MODEL == 2, IL>(a, x, c, sc, k);
     return uv_scalar_level<MODEL == 2, COMP, IL>(a, x, c, sc, k);
 }
@@ -1120,7 +1121,7 @@ __device__ __forceinline__ BLane blane(float *smem, int ks) {
     return R;
 }
 
-template <int MODEL, int COMP, int NW, class Ahead>
+template <int MODEL, int COMP, int NW, int SW, class Ahead>
 __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *smem, Ahead &&ahead) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int s = grp * 32 + lane;
@@ -1134,7 +1135,7 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
         // one level per step: within the register budget of four resident blocks a second level's
         // operands did not overlap the first's (each level cost the same either way)
         for (int k = c.K0 + warp; k <= c.VI; k += NW) {
-            const Coef q = mom_level<MODEL, COMP, true>(a, x, c, sc, k);
+            const Coef q = mom_level<MODEL, COMP, true, SW>(a, x, c, sc, k);
             R.a(k) = q.A; R.b(k) = q.B; R.c(k) = q.C; R.d(k) = q.D; R.p(k) = q.phi;
         }
     }
@@ -1260,13 +1261,14 @@ __global__ void __launch_bounds__(NW * 32, MINB) k_pressure_b(KArgs a, SweepGeom
     flush();
 }
 
-template <int MODEL, int COMP, int NW, int MINB>
+// SW: parity width of model 1 fixed at compile time (8 or 16; 0 for the other models).
+template <int MODEL, int COMP, int NW, int MINB, int SW>
 __global__ void __launch_bounds__(NW * 32, MINB) k_mom_b(KArgs a, SweepGeom g) {
     extern __shared__ float smem[];
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
     constexpr bool REV = (MODEL == 1 && COMP == COMP_V);
     gs_tasks_block<PH, REV>(a, g, [&](int grp, int i, int j, int, int, bool, auto &&ahead) {
-        batch_mom_column<MODEL, COMP, NW>(a, grp, i, j, smem, ahead);
+        batch_mom_column<MODEL, COMP, NW, SW>(a, grp, i, j, smem, ahead);
     });
 }
 
@@ -1284,15 +1286,17 @@ using KFn = void (*)(KArgs, SweepGeom);
 struct BVariant {
     int nw, minb;
     KFn pressure;
-    KFn mom[3][3];   // [model][comp]
+    KFn mom[3][3];   // [model][comp]; model 1 at parity width 8
+    KFn mom16[3];    // model 1 at parity width 16, [comp]
     KFn tke;
 };
 
 #define GRAL_BV(NW, MB)                                                                              \
-    BVariant{NW, MB, k_pressure_b<NW, MB>,                                                           \
-             {{k_mom_b<0, COMP_U, NW, MB>, k_mom_b<0, COMP_V, NW, MB>, k_mom_b<0, COMP_W, NW, MB>},  \
-              {k_mom_b<1, COMP_U, NW, MB>, k_mom_b<1, COMP_V, NW, MB>, k_mom_b<1, COMP_W, NW, MB>},  \
-              {k_mom_b<2, COMP_U, NW, MB>, k_mom_b<2, COMP_V, NW, MB>, k_mom_b<2, COMP_W, NW, MB>}}, \
+    BVariant{NW, MB, k_pressure_b<NW, MB>,                                                                 \
+             {{k_mom_b<0, COMP_U, NW, MB, 0>, k_mom_b<0, COMP_V, NW, MB, 0>, k_mom_b<0, COMP_W, NW, MB, 0>},  \
+              {k_mom_b<1, COMP_U, NW, MB, 8>, k_mom_b<1, COMP_V, NW, MB, 8>, k_mom_b<1, COMP_W, NW, MB, 8>},  \
+              {k_mom_b<2, COMP_U, NW, MB, 0>, k_mom_b<2, COMP_V, NW, MB, 0>, k_mom_b<2, COMP_W, NW, MB, 0>}}, \
+             {k_mom_b<1, COMP_U, NW, MB, 16>, k_mom_b<1, COMP_V, NW, MB, 16>, k_mom_b<1, COMP_W, NW, MB, 16>}, \
              k_tke_b<NW, MB>}
 
 const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(6, 4)};
@@ -1311,12 +1315,14 @@ size_t bsmem(int kind, int model, int ks) {
     return 5 * row;
 }
 
-KFn batch_kernel(const BVariant &V, int kind, int model) {
+// simd: the loaded parity width (16 selects the model-1 kernels compiled for Vector512).
+KFn batch_kernel(const BVariant &V, int kind, int model, int simd) {
+    const bool w16 = (model == 1 && simd == 16);
     switch (kind) {
         case PH_PRESSURE: return V.pressure;
-        case PH_U: return V.mom[model][0];
-        case PH_V: return V.mom[model][1];
-        case PH_W: return V.mom[model][2];
+        case PH_U: return w16 ? V.mom16[0] : V.mom[model][0];
+        case PH_V: return w16 ? V.mom16[1] : V.mom[model][1];
+        case PH_W: return w16 ? V.mom16[2] : V.mom[model][2];
         default: return V.tke;
     }
 }
@@ -1358,24 +1364,26 @@ cudaError_t gs_prepare(bool il, int ks, int model) {
     for (int v = 0; v < kNumVariants; ++v)
         for (int q = 0; q < 5; ++q) {
             const int bytes = (int)bsmem(kinds[q], model, ks);
-            cudaError_t e = cudaFuncSetAttribute(batch_kernel(kVariants[v], kinds[q], model),
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-            if (e != cudaSuccess) return e;
+            for (int simd : {8, 16}) {
+                cudaError_t e = cudaFuncSetAttribute(batch_kernel(kVariants[v], kinds[q], model, simd),
+                                                     cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+                if (e != cudaSuccess) return e;
+            }
         }
     return cudaSuccess;
 }
 
-cudaError_t gs_occupancy(bool il, int kind, int model, int ks, int variant, int *blocks_per_sm) {
+cudaError_t gs_occupancy(bool il, int kind, int model, int simd, int ks, int variant, int *blocks_per_sm) {
     const int th = gs_block_threads(il, variant);
     if (!il) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, plain_kernel(kind, model), th, 0);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, batch_kernel(kVariants[variant], kind, model),
-                                                         th, bsmem(kind, model, ks));
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        blocks_per_sm, batch_kernel(kVariants[variant], kind, model, simd), th, bsmem(kind, model, ks));
 }
 
 void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st) {
     if (a.il) {
         const BVariant &V = kVariants[a.variant];
-        KFn f = batch_kernel(V, kind, a.model);
+        KFn f = batch_kernel(V, kind, a.model, a.simd);
         const size_t sm = bsmem(kind, a.model, a.ks);
         for_group_sets(a, [&](const KArgs &b) { f<<<grid, V.nw * 32, sm, st>>>(b, g); });
     } else {

@@ -268,7 +268,7 @@ int size_grids(gral_ctx *ctx) {
     const int warps_per_block = gs_block_threads(false, 0) / 32;
     for (int q = 0; q < 5; ++q) {
         int bps = 0;
-        CK(gs_occupancy(il, kinds[q], ctx->model, ctx->ks, v, &bps));
+        CK(gs_occupancy(il, kinds[q], ctx->model, ctx->ka.simd, ctx->ks, v, &bps));
         long long blocks = (long long)std::max(1, bps) * ctx->num_sms;
         const int la = (kinds[q] == PH_PRESSURE) ? ctx->lookahead_p : ctx->lookahead;
         const long long want_blocks = (long long)std::ceil(la * diag_width / (double)warps_per_block);

@@ -25,7 +25,7 @@ struct Staging {
 int gs_num_variants();
 int gs_block_threads(bool il, int variant);
 cudaError_t gs_prepare(bool il, int ks, int model);
-cudaError_t gs_occupancy(bool il, int kind, int model, int ks, int variant, int *blocks_per_sm);
+cudaError_t gs_occupancy(bool il, int kind, int model, int simd, int ks, int variant, int *blocks_per_sm);
 // one Gauss-Seidel phase (kind = PH_PRESSURE, PH_U, PH_V, PH_W or PH_TKE) of the loaded model
 void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
 // pressure + velocity correction + averages + model-1 U in one wavefront launch (slab family)

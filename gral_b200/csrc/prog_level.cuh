@@ -107,14 +107,22 @@ __device__ __forceinline__ float pl1(bool v512, float D, float Pe, float Fs) {
     return v512 ? pl_coef512(D, Pe, Fs) : pl_coef(D, Pe, Fs);
 }
 
+// Parity width of the model-1 routines: SW = 8 or 16 fixes it when the kernel is compiled, SW = 0
+// reads the loaded width (a.simd) at run time.
+template <int SW>
+__device__ __forceinline__ bool simd16(const KArgs &a) {
+    return SW == 0 ? a.simd == 16 : SW == 16;
+}
+
 // Mixing-length eddy viscosity of level k (U-prognostic-microscale_1.cs:239-268) from the column's
 // U and V at k+1 and k-1; zero at and below KKART+1 (the reference masks those lanes).
 // The Vector512 twins take the height above KKART as HOKART[k] - fma(DZK, 0.5, HOKART[KKART])
 // (U-prognostic-microscale_1_Vec512.cs:218).
+template <int SW = 0>
 __device__ __forceinline__ float ml_vis(const KArgs &a, const ColCtx &c, int k, float dz, float ukp, float ukm,
                                         float vkp, float vkm) {
     if (k <= c.KK + 1) return 0.0f;
-    const float zs = (a.simd == 16) ? a.hokart[k] - fmaf(dz, 0.5f, c.hokK) : a.hokart[k] - c.hokK - dz * 0.5f;
+    const float zs = simd16<SW>(a) ? a.hokart[k] - fmaf(dz, 0.5f, c.hokK) : a.hokart[k] - c.hokK - dz * 0.5f;
     float mixL = vminf(0.071f * zs, 100.0f);
     if (c.cf.cov > 0) mixL *= (1.0f - 0.99f * c.cf.cov);
     float in = (ukp - ukm) / (2.0f * dz);
@@ -167,10 +175,10 @@ struct MomPre {
 // U momentum (U-prognostic-microscale_1.cs:205-470).  All operands of the level are loaded first,
 // unconditionally (every address lies inside the padded grid and levels 0..KS-1), so a level costs
 // one memory round trip; the arithmetic follows in the reference's order.
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
-    const bool v512 = (a.simd == 16);
+    const bool v512 = simd16<SW>(a);
     const float uk = __ldcg(a.uk + x.at(0, k));
     const float ukp = __ldcg(a.uk + x.at(0, k + 1)), ukm = __ldcg(a.uk + x.at(0, k - 1));
     const float vkp = a.vk[x.at(0, k + 1)], vkm = a.vk[x.at(0, k - 1)];
@@ -186,7 +194,7 @@ __device__ __forceinline__ MomPre u1_pre(const KArgs &a, const Acc<IL> &x, const
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     const float dxdz = DXK * dz, dydz = DYK * dz;
-    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
+    const float VIS = ml_vis<SW>(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -263,10 +271,10 @@ __device__ __forceinline__ float u1_post(const MomPre &p, const ColCtx &c, int k
 }
 
 // V momentum (V-prognostic-microscale_1.cs:205-488); operands first, as u1_pre.
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
-    const bool v512 = (a.simd == 16);
+    const bool v512 = simd16<SW>(a);
     const float vk = __ldcg(a.vk + x.at(0, k));
     const float ukp = a.uk[x.at(0, k + 1)], ukm = a.uk[x.at(0, k - 1)];
     const float vkp = __ldcg(a.vk + x.at(0, k + 1)), vkm = __ldcg(a.vk + x.at(0, k - 1));
@@ -282,7 +290,7 @@ __device__ __forceinline__ MomPre v1_pre(const KArgs &a, const Acc<IL> &x, const
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     const float dxdz = DXK * dz, dydz = DYK * dz;
-    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
+    const float VIS = ml_vis<SW>(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -359,10 +367,10 @@ __device__ __forceinline__ float v1_post(const MomPre &p, const ColCtx &c, int k
 
 // W momentum (W-prognostic-microscale_1.cs:205-402); its extra viscous term reads only the own
 // column, so it is complete before the wait (e0 = the whole increment).  Operands first.
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
     const long long W = -(long long)c.nj2, E = c.nj2, S = -1, N = 1;
-    const bool v512 = (a.simd == 16);
+    const bool v512 = simd16<SW>(a);
     const float uks = a.uks[x.at(0, k)], vks = a.vks[x.at(0, k)], wks = a.wks[x.at(0, k)];
     const float uksM = a.uks[x.at(0, k - 1)], vksM = a.vks[x.at(0, k - 1)];
     const float wk = __ldcg(a.wk + x.at(0, k));
@@ -381,7 +389,7 @@ __device__ __forceinline__ MomPre w1_pre(const KArgs &a, const Acc<IL> &x, const
     const float DXK = a.dxk, DYK = a.dyk, AREA = a.areaxy;
     const float dz = a.dzk[k];
     const float dxdz = DXK * dz, dydz = DYK * dz;
-    const float VIS = ml_vis(a, c, k, dz, ukp, ukm, vkp, vkm);
+    const float VIS = ml_vis<SW>(a, c, k, dz, ukp, ukm, vkp, vkm);
     const float vmx = vmaxf(VIS, a.vishmin);
     float DE = vmx * dydz / DXK;
     float DW = DE;
@@ -451,28 +459,28 @@ __device__ __forceinline__ void nbr4(const float *F, const Acc<IL> &x, const Col
     nN = __ldcg(F + x.at(1, k));
 }
 
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ Coef u1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
-    const MomPre p = u1_pre(a, x, c, sc, k);
+    const MomPre p = u1_pre<IL, SW>(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.uk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, u1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
+    return Coef{p.A, p.B, p.C, u1_post(p, c, k, nW, nS, nE, nN, simd16<SW>(a)), p.phi};
 }
 
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ Coef v1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
-    const MomPre p = v1_pre(a, x, c, sc, k);
+    const MomPre p = v1_pre<IL, SW>(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.vk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, v1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
+    return Coef{p.A, p.B, p.C, v1_post(p, c, k, nW, nS, nE, nN, simd16<SW>(a)), p.phi};
 }
 
-template <bool IL>
+template <bool IL, int SW = 0>
 __device__ __forceinline__ Coef w1_level(const KArgs &a, const Acc<IL> &x, const ColCtx &c, const SitCtx &sc, int k) {
-    const MomPre p = w1_pre(a, x, c, sc, k);
+    const MomPre p = w1_pre<IL, SW>(a, x, c, sc, k);
     float nW, nS, nE, nN;
     nbr4(a.wk, x, c, k, nW, nS, nE, nN);
-    return Coef{p.A, p.B, p.C, w1_post(p, c, k, nW, nS, nE, nN, a.simd == 16), p.phi};
+    return Coef{p.A, p.B, p.C, w1_post(p, c, k, nW, nS, nE, nN, simd16<SW>(a)), p.phi};
 }
 
 // ---------------------------------------------------------------------------------------------
