@@ -1196,15 +1196,42 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
     BLane R = blane(smem, ks);
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     const SitCtx sc = make_sit(a, act ? s : grp * 32);
+    // Row a holds DPMNEW of the level, loaded here for the update after the recurrences (only
+    // this task writes DPMNEW of its column, and no pressure task reads it).
     if (act) {
 #pragma unroll 2
-        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) R.d(k) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+        for (int k = c.KK + 1 + warp; k <= c.VI; k += NW) {
+            R.d(k) = pressure_dim<true>(a, x, c, sc, k, IS, JS);
+            R.a(k) = a.dpmnew[x.at(0, k)];
+        }
+    }
+    float P = 0.0f, Q = 0.0f;
+    if (warp == 0 && act) {      // the row carry of the predecessor (published before our wait)
+        P = __ldcg(rc + (size_t)(c.VI + 1) * 32);
+        Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
     }
     __syncthreads();
     if (threadIdx.x == 32) ahead();
     if (warp == 0 && act) {
-        float P = __ldcg(rc + (size_t)(c.VI + 1) * 32), Q = __ldcg(rc + (size_t)(ks + c.VI + 1) * 32);
-        for (int k = c.VI; k > c.KK; --k) {
+        // eight levels per step: their table and row loads are issued together, the chain is serial
+        constexpr int CH = 8;
+        int k = c.VI;
+        for (; k - (CH - 1) > c.KK; k -= CH) {
+            float ap[CH], at[CH], ab[CH], d[CH];
+#pragma unroll
+            for (int q = 0; q < CH; ++q) {
+                ap[q] = a.app[k - q]; at[q] = a.atp[k - q]; ab[q] = a.abp[k - q]; d[q] = R.d(k - q);
+            }
+#pragma unroll
+            for (int q = 0; q < CH; ++q) {
+                const float T = 1.0f / (ap[q] - at[q] * P);
+                P = ab[q] * T;
+                Q = (at[q] * Q + d[q]) * T;
+                R.b(k - q) = P;
+                R.c(k - q) = Q;
+            }
+        }
+        for (; k > c.KK; --k) {
             const float T = 1.0f / (a.app[k] - a.atp[k] * P);
             P = a.abp[k] * T;
             Q = (a.atp[k] * Q + R.d(k)) * T;
@@ -1225,7 +1252,7 @@ __device__ void batch_pressure_column(const KArgs &a, int grp, int i, int j, int
         const float temp = R.p(k);
         nmax = max(nmax, residual_key(temp, sc));
         __stcg(a.dpm + x.at(0, k), temp);
-        a.dpmnew[x.at(0, k)] += a.relaxp * temp;
+        a.dpmnew[x.at(0, k)] = R.a(k) + a.relaxp * temp;
         if (k > klo) {
             __stcg(rc + (size_t)k * 32, R.b(k));
             __stcg(rc + (size_t)(ks + k) * 32, R.c(k));
