@@ -152,7 +152,7 @@ int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const 
  * gral_prog_solve does (results are identical to n single calls): largest first, in waves of K
  * instances, whose loads run one after the other and whose iterations and stores then run side
  * by side, each in its own context, stream and host thread.  K is max_concurrent, further limited
- * to what fits in hbm_bytes of device memory (0: 90 % of the free memory at the call), judged from
+ * to what fits in hbm_bytes of device memory (0: 90 % of the free memory at the call), estimated from
  * the footprint of the largest instance, which is loaded first.  status[b] receives
  * instance b's return code (the error text of a failed instance is not kept); the call returns
  * GRAL_OK when every instance succeeded, else the code of the first failed instance in index
