@@ -199,7 +199,8 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // Spin (lane 0 only) until *flag >= stamp.  The first polls follow each other directly (the
-// predecessor is usually about to publish), later ones back off with __nanosleep up to 256 ns.
+// predecessor is usually about to publish), later ones back off with __nanosleep up to 32 ns
+// (a longer back-off delayed the wake-up on the single-situation wavefront's critical path).
 // Gives up after limit_ns, or as soon as another warp reported an error; returns false then.
 // Never waits unboundedly.
 __device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned long long limit_ns) {
@@ -209,7 +210,7 @@ __device__ inline bool wait_stamp(const int *flag, int stamp, int *err, unsigned
     for (unsigned n = 1;; ++n) {
         if (n > 4) {
             __nanosleep(ns);
-            if (ns < 256) ns += ns;
+            if (ns < 32) ns += ns;
         }
         if (ld_acquire(flag) >= stamp) return true;
         if ((n & 7) == 0) {
@@ -242,7 +243,7 @@ __device__ inline bool wait_stamps(const int *f1, const int *f2, int stamp, int 
         for (unsigned n = 1;; ++n) {
             if (n > 4) {
                 __nanosleep(ns);
-                if (ns < 256) ns += ns;
+                if (ns < 32) ns += ns;
             }
             if (v1 < stamp) v1 = ld_relaxed(f1);
             if (v2 < stamp) v2 = ld_relaxed(f2);
