@@ -93,7 +93,7 @@ struct gral_ctx {
     int grid_gs[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // indexed by PH_*
     cudaGraphExec_t graph = nullptr;
     float ms_upload = 0.f;
-    float tune_ms[16] = {0};
+    float tune_ms[64] = {0};                  // autotuner timings per launch variant x group-set mode
 
     // device buffers
     DevBuf<float> slab, stage, veg, tables, ap0, rowcarry, trace;

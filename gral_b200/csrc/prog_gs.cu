@@ -1326,7 +1326,8 @@ struct BVariant {
              {k_mom_b<1, COMP_U, NW, MB, 16>, k_mom_b<1, COMP_V, NW, MB, 16>, k_mom_b<1, COMP_W, NW, MB, 16>}, \
              k_tke_b<NW, MB>}
 
-const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(6, 4), GRAL_BV(5, 5)};
+const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_BV(6, 4),
+                              GRAL_BV(5, 5), GRAL_BV(6, 5), GRAL_BV(5, 6)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 const KFn kPlainMom[3][3] = {{k_mom<0, COMP_U>, k_mom<0, COMP_V>, k_mom<0, COMP_W>},
