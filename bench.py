@@ -213,6 +213,20 @@ def pinned_fields(f):
     return FieldArrays(pin(f.uk), pin(f.vk), pin(f.wk), pin(f.turb), pin(f.tdiss))
 
 
+def host_cpu() -> dict:
+    """The host's CPU model (first `model name` of /proc/cpuinfo) and logical CPU count."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for line in fh:
+                if line.lower().startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_threads": os.cpu_count() or 1}
+
+
 def cpu_sample(workload_name: str, iterations: int):
     """The CPU oracle on `iterations` SIMPLE iterations of the workload; returns (Mcell-it/s, s)."""
     from gral_b200 import prep
@@ -264,7 +278,8 @@ def run_reference(args, rank, world):
                                        "iterations_per_situation": iters},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{cores} independent situations x {iters} SIMPLE iterations each, "
-                                   f"one process per core (deterministic single-thread restatement)"},
+                                   f"one process per core (deterministic single-thread restatement)",
+                         **host_cpu()},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -630,7 +645,7 @@ def run_ours(args, rank, world):
         v, dt = cpu_sample("production" if args.workload == "batched" else args.workload, args.cpu_iters)
         cpu = {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
                "sample": f"{args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s), "
-                         "single-threaded deterministic restatement"}
+                         "single-threaded deterministic restatement", **host_cpu()}
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
