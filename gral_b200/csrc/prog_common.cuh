@@ -234,16 +234,18 @@ __device__ __forceinline__ int ld_relaxed(const int *p) {
 // one fence.acquire follows: a strong read followed by an acquire fence is an acquire pattern, so
 // it synchronises with the predecessors' st.release as an acquiring load would.  Same bounds as
 // wait_stamp: gives up after limit_ns or on another warp's error and returns false then.
-__device__ inline bool wait_stamps(const int *f1, const int *f2, int stamp, int *err, unsigned long long limit_ns) {
+// max_sleep_ns caps the back-off between polls (0: poll without sleeping).
+__device__ inline bool wait_stamps(const int *f1, const int *f2, int stamp, int *err, unsigned long long limit_ns,
+                                   unsigned max_sleep_ns = 32) {
     int v1 = f1 ? ld_relaxed(f1) : stamp;
     int v2 = f2 ? ld_relaxed(f2) : stamp;
     if (v1 < stamp || v2 < stamp) {
         const unsigned long long t0 = globaltimer_ns();
         unsigned ns = 16;
         for (unsigned n = 1;; ++n) {
-            if (n > 4) {
+            if (n > 4 && max_sleep_ns) {
                 __nanosleep(ns);
-                if (ns < 32) ns += ns;
+                if (ns < max_sleep_ns) ns += ns;
             }
             if (v1 < stamp) v1 = ld_relaxed(f1);
             if (v2 < stamp) v2 = ld_relaxed(f2);

@@ -456,9 +456,10 @@ __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &
             int *fl = a.flags + (size_t)u * a.ncols;
             job.pre(u, i, j, IS, JS, i1 == g.ia);
             int ok = 1;
-            if (lane == 0)
+            if (lane == 0)      // spins without sleeping: these waits sit on the sweep's critical path
                 ok = wait_stamps((i1 > g.ia) ? fl + (i - IS) * a.nj2 + j : nullptr,
-                                 (j1 > g.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, stamp, a.err, a.wait_limit_ns);
+                                 (j1 > g.ja) ? fl + i * a.nj2 + (j - JS) : nullptr, stamp, a.err, a.wait_limit_ns,
+                                 0);
             ok = __shfl_sync(0xffffffffu, ok, 0);
             __syncwarp();
             if (ok) job.post(u, IS, JS);
