@@ -12,8 +12,9 @@ model; synthetic, seeded inputs.
              set-up, 500 SIMPLE iterations, post-checks, fields back to the host), host-timed.
   roofline   dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration,
              against the measured HBM copy bandwidth.
-  cpu_baseline  the CPU oracle (a single-threaded restatement of the reference's deterministic
-             solver) on a bounded sample of the same workload.
+  cpu_baseline  the racy-order multi-threaded restatement of the reference's default parallel
+             mode on all host threads, on a bounded sample of the same workload (with the
+             single-threaded deterministic oracle beside it).
   prep       the flow-field set-up before the solve (sub-domains, flat-terrain initial field,
              vegetation) on the same grid: device kernel time (CUDA events) against HBM bandwidth,
              host-timed calls including the copies, and the oracle restatement on one core.
@@ -28,8 +29,10 @@ model; synthetic, seeded inputs.
              against HBM bandwidth, the host-timed pack into pinned memory and read back, and
              the numpy restatement of the writer timed on one core.
 
-`--impl reference` times that CPU restatement on all host cores (one independent situation per
-worker process) on the same workload and prints the same metric.
+`--impl reference` times the CPU path on this host's cores and prints the same metric: the C#
+reference cannot run here (no .NET SDK), so its racy-order restatement (the reference's default
+parallel work split over all host threads, -O3 -march=native, built on the host) solves one
+situation per step.
 Multi-GPU (torchrun): every rank solves its own replica of the workload (a single situation does
 not shard); value = all ranks' cell-iterations / max-over-ranks time.
 """
@@ -227,58 +230,57 @@ def host_cpu() -> dict:
     return {"cpu_model": model, "host_threads": os.cpu_count() or 1}
 
 
-def cpu_sample(workload_name: str, iterations: int):
-    """The CPU oracle on `iterations` SIMPLE iterations of the workload; returns (Mcell-it/s, s)."""
+def cpu_sample(workload_name: str, iterations: int, threaded: bool = True):
+    """The CPU restatement on `iterations` SIMPLE iterations of one situation of the workload;
+    returns (Mcell-it/s, seconds, threads).  threaded: the racy-order build with the sweeps over all
+    host threads (-O3 -march=native, built here), the analogue of the reference's default parallel
+    mode; otherwise the deterministic single-threaded oracle."""
     from gral_b200 import prep
     from oracle import oracle as O
     dom, sit, _, _ = workload(workload_name)
-    p = dom.params(sit, model=1, iterations=iterations)
+    p = dom.params(sit, model=1, iterations=iterations, iter_min=iterations)
     f = prep.initial_fields(dom, sit)
     t0 = time.perf_counter()
-    O.solve(p, dom.static, f)
+    O.solve(p, dom.static, f, threaded=threaded)
     dt = time.perf_counter() - t0
-    return nominal_cells(dom) * iterations / dt / 1e6, dt
+    threads = O.threads_used() if threaded else 1
+    return nominal_cells(dom) * iterations / dt / 1e6, dt, threads
 
 
-def _cpu_worker(args):
-    name, iters = args
-    return cpu_sample(name, iters)
+CPU_KIND_TEXT = ("racy-order multi-threaded C++ restatement of the reference's default parallel mode "
+                 "(i-slab / j-row work split of its Parallel.For loops, -O3 -march=native, built on this "
+                 "host); a restatement, not the reference (no .NET SDK on the host)")
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU path on this host's cores: the C# solver cannot run here (no .NET SDK),
+    so its racy-order restatement runs one situation per step with every host thread on the sweeps,
+    set-up included, for args.ref_iters SIMPLE iterations."""
     if rank != 0:
         return
-    import multiprocessing as mp
     from oracle import oracle as O
-    O.build()
-    cores = min(os.cpu_count() or 1, args.ref_procs)
+    O.build_threaded()
     iters = args.ref_iters
-    ctx = mp.get_context("spawn")
-    times = []
-    total_cells = 0
-    t_all = time.perf_counter()
-    for _ in range(args.warmup if args.ref_warmup else 0):
-        pass
-    for step in range(args.steps):
-        t0 = time.perf_counter()
-        with ctx.Pool(cores) as pool:
-            res = pool.map(_cpu_worker, [(args.workload, iters)] * cores)
-        dt = time.perf_counter() - t0
-        times.append(max(r[1] for r in res))
+    for _ in range(args.warmup):
+        cpu_sample(args.workload if args.workload != "batched" else "production", iters)
+    times, threads = [], 1
+    for _ in range(args.steps):
+        _, dt, threads = cpu_sample(args.workload if args.workload != "batched" else "production", iters)
+        times.append(dt)
     dom, _, _, desc = workload(args.workload)
     cells = nominal_cells(dom)
     per_step = statistics.median(times)
-    value = cells * iters * cores / per_step / 1e6
+    value = cells * iters / per_step / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": {"workload": args.workload, "description": desc,
-                                       "cells_per_situation": cells, "situations_per_step": cores,
+                                       "cells_per_situation": cells, "situations_per_step": 1,
                                        "iterations_per_situation": iters},
-        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{cores} independent situations x {iters} SIMPLE iterations each, "
-                                   f"one process per core (deterministic single-thread restatement)",
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"1 situation x {iters} SIMPLE iterations per step (set-up included), "
+                                   f"{threads} threads; {CPU_KIND_TEXT}",
                          **host_cpu()},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -642,10 +644,15 @@ def run_ours(args, rank, world):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, dt = cpu_sample("production" if args.workload == "batched" else args.workload, args.cpu_iters)
-        cpu = {"value": round(v, 4), "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s), "
-                         "single-threaded deterministic restatement", **host_cpu()}
+        wl = "production" if args.workload == "batched" else args.workload
+        v, dt, thr = cpu_sample(wl, args.cpu_iters)
+        v1, dt1, _ = cpu_sample(wl, 2, threaded=False)
+        cpu = {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"one situation, {args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s, "
+                         f"set-up included), {thr} threads; {CPU_KIND_TEXT}",
+               "single_thread_oracle": {"value": round(v1, 4), "unit": UNIT, "cores": 1,
+                                        "sample": f"2 iterations ({dt1:.1f} s), deterministic oracle, -O2"},
+               **host_cpu()}
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -658,9 +665,12 @@ def run_ours(args, rank, world):
                    "layout": layout, "launch_variant": st_store["launch_variant"]},
         "phase_ms_per_iteration": {k: round(v / args.steps, 4) for k, v in phases.items() if v > 0},
         "roofline": roofline(cells, args.steps, phases, layout),
-        "cpu_baseline": cpu, "e2e": e2e, "batched": batched, "gff": gffm, "prep": prepm, "wind": windm, "instances": instm,
+        "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": st_store["launches_per_iteration"] * args.steps,
         "clocks": clocks,
+        "gff": gffm, "prep": prepm, "wind": windm, "instances": instm,
+        # last on the line, so that a reader keeping only the end of the line still has it
+        "batched": batched,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -678,7 +688,7 @@ def main():
     ap.add_argument("--batch", type=int, default=144, help="situations of the batched workload")
     ap.add_argument("--grid", type=int, default=400, help="columns per side of the city grid (profiling cases)")
     ap.add_argument("--e2e-iters", type=int, default=0, help="iterations of the e2e solve (0: the workload's)")
-    ap.add_argument("--cpu-iters", type=int, default=8)
+    ap.add_argument("--cpu-iters", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-measurement")
@@ -687,9 +697,7 @@ def main():
     ap.add_argument("--no-prep", action="store_true", help="skip the set-up (sub-domains, initial field) measurement")
     ap.add_argument("--no-wind", action="store_true", help="skip the particle wind interpolation measurement")
     ap.add_argument("--no-instances", action="store_true", help="skip the uneven-domain instances measurement")
-    ap.add_argument("--ref-iters", type=int, default=4)
-    ap.add_argument("--ref-procs", type=int, default=64)
-    ap.add_argument("--ref-warmup", action="store_true")
+    ap.add_argument("--ref-iters", type=int, default=4, help="SIMPLE iterations per reference-arm step")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

@@ -92,13 +92,16 @@ __global__ void __launch_bounds__(kThreads) k_check_speeds(int nii, int njj, int
     if (threadIdx.x == 0) scratch[0] = 0u;
 }
 
-bool on_device(const void *p) {
+// True for memory the kernel on device `dev` may read: device memory of `dev` itself, or managed
+// memory.  Device memory of another GPU is refused: without peer access a kernel reading it faults.
+bool on_device(const void *p, int dev) {
     cudaPointerAttributes at{};
     if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
-        cudaGetLastError();
+        cudaGetLastError();   // clears only the error of this lookup (none was pending on entry)
         return false;
     }
-    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    if (at.type == cudaMemoryTypeManaged) return true;
+    return at.type == cudaMemoryTypeDevice && at.device == dev;
 }
 
 }  // namespace
@@ -110,18 +113,23 @@ extern "C" int gral_prog_check_speeds_noalloc(int32_t nii, int32_t njj, int32_t 
     if (!counts || nii < 1 || njj < 1 || nkk < 2 || vert_cells_ff < 0) return GRAL_EINVAL;
     if (nii > GRAL_NOALLOC_MAX_ROWS) return GRAL_ETOOLARGE;
     if (!uk || !vk || !wk || !advdom || !kkart) return GRAL_EINVAL;
+    // an error left pending by the caller's own work is reported, not cleared: the error checks
+    // below then see only what this call causes
+    if (cudaPeekAtLastError() != cudaSuccess) return GRAL_ECUDA;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         return GRAL_ENODEV;
     }
     if (dev < 0 || dev >= kMaxDevices) return GRAL_ENODEV;
-    if (!on_device(uk) || !on_device(vk) || !on_device(wk) || !on_device(advdom) || !on_device(kkart))
+    if (!on_device(uk, dev) || !on_device(vk, dev) || !on_device(wk, dev) || !on_device(advdom, dev) ||
+        !on_device(kkart, dev))
         return GRAL_EINVAL;
     unsigned int *scratch = nullptr;
     {
         // first call on this device: resolve the device address of the static scratch (the
-        // current device is the one the kernel will run on)
+        // current device is the one the kernel will run on).  The address is kept for the life of
+        // the process; cudaDeviceReset of this device would make it stale.
         std::lock_guard<std::mutex> lk(g_mutex);
         if (!g_addr[dev]) {
             void *p = nullptr;

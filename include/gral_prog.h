@@ -367,11 +367,14 @@ void gral_prog_destroy(gral_ctx *ctx);
  * legacy default stream) on the current device.  The call allocates no memory; its scratch is a
  * fixed static device array of GRAL_NOALLOC_MAX_ROWS rows (64 KiB + 256 B per device that loads
  * the library, held until the process exits), so nii above GRAL_NOALLOC_MAX_ROWS returns
- * GRAL_ETOOLARGE.  Host pointers return GRAL_EINVAL.  The first call on a device looks up that
- * array's device address (with the device current); make that first call before any stream
- * capture.  All calls on a device share the array, so calls that overlap on the GPU (two host
- * threads, or two streams) race and may return wrong counts: serialise them.  The call returns
- * after the counts are on the host. */
+ * GRAL_ETOOLARGE.  Host pointers and device memory of a GPU other than the current one return
+ * GRAL_EINVAL; an error already pending in the CUDA runtime on entry returns GRAL_ECUDA and is
+ * left pending for the caller.  The first call on a device looks up that array's device address
+ * (with the device current) and keeps it for the life of the process, so do not call it on a
+ * device after cudaDeviceReset of that device; make that first call before any stream capture.
+ * All calls on a device share the array, so calls that overlap on the GPU (two host threads, or
+ * two streams) race and may return wrong counts: serialise them.  The call synchronises `stream`
+ * and returns after the counts are on the host. */
 #define GRAL_NOALLOC_MAX_ROWS 4096
 int gral_prog_check_speeds_noalloc(int32_t nii, int32_t njj, int32_t nkk, int32_t vert_cells_ff,
                                    double geschw_max, const float *uk, const float *vk,

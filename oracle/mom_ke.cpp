@@ -38,11 +38,12 @@ static void uv_scalar(State &st, int comp, bool diffusion, int IS, int JS, float
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
     const float Cor = st.p->coriolis;
-    std::vector<float> PIM(st.nk2), QIM(st.nk2);
     const int i_lo = (comp == 0) ? 3 : 2;   /* Parallel.For(3, NII) for U, (2, NII) for V */
     const int j_lo = (comp == 0) ? 2 : 3;   /* j1 from 2 for U, from 3 for V */
+    oracle::for_slabs(i_lo, NII, [&](int i1_lo, int i1_hi) {
+    std::vector<float> PIM(st.nk2), QIM(st.nk2);
 
-    for (int i1 = i_lo; i1 < NII; i1++) {
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {
         for (int j1 = j_lo; j1 <= NJJ - 1; j1++) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
             int i = (IS == -1) ? NII - i1 + 1 : i1;
@@ -196,6 +197,7 @@ static void uv_scalar(State &st, int comp, bool diffusion, int IS, int JS, float
             }
         }
     }
+    });
 }
 
 void u_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float UG, float relax) {
@@ -218,8 +220,9 @@ void w_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAx
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
+    oracle::for_slabs(2, NII, [&](int i1_lo, int i1_hi) {
     std::vector<float> PIMW(st.nk2), QIMW(st.nk2);
-    for (int i1 = 2; i1 < NII; i1++) {
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {
         for (int j1 = 2; j1 <= NJJ - 1; j1++) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
             int i = (IS == -1) ? NII - i1 + 1 : i1;
@@ -296,6 +299,7 @@ void w_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAx
             }
         }
     }
+    });
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -305,8 +309,9 @@ void w_mom_nd(State &st, int IS, int JS, float AREAxy_L, float relax) {
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk();
+    oracle::for_slabs(2, NII, [&](int i1_lo, int i1_hi) {
     std::vector<double> PIMW(st.nk2), QIMW(st.nk2);
-    for (int i1 = 2; i1 < NII; i1++) {
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {
         for (int j1 = 2; j1 <= NJJ - 1; j1++) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
             int i = (IS == -1) ? NII - i1 + 1 : i1;
@@ -354,6 +359,7 @@ void w_mom_nd(State &st, int IS, int JS, float AREAxy_L, float relax) {
             }
         }
     }
+    });
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -368,8 +374,9 @@ void tke_ke(State &st, int IS, int JS, float Cmueh, float Ceps, float Ceps1, flo
     const float *DZK = st.dzk(), *HOKART = st.hokart();
     const float DXK_Rez = 1 / DXK, DYK_Rez = 1 / DYK;
     const float PotdTdz = st.p->potdtdz;
+    oracle::for_slabs(2, NII, [&](int i1_lo, int i1_hi) {
     std::vector<float> PIMTURB(st.nk2), QIMTURB(st.nk2), PIMTDISS(st.nk2), QIMTDISS(st.nk2);
-    for (int i1 = 2; i1 < NII; i1++) {
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {
         for (int j1 = 2; j1 <= NJJ - 1; j1++) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
             int i = (IS == -1) ? NII - i1 + 1 : i1;
@@ -535,6 +542,7 @@ void tke_ke(State &st, int IS, int JS, float Cmueh, float Ceps, float Ceps1, flo
             }
         }
     }
+    });
 }
 
 }  // namespace oracle

@@ -59,10 +59,11 @@ void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
     const float Cor = st.p->coriolis;
+    oracle::for_slabs(3, NII, [&](int i1_lo, int i1_hi) {
     std::vector<float> PIMU(st.nk2), QIMU(st.nk2);
     std::vector<float> AIM_A(SIMD), BIM_A(SIMD), CIM_A(SIMD), DIM_A(SIMD), VIS_A(SIMD), MASK(SIMD);
 
-    for (int i1 = 3; i1 < NII; i1++) {                       /* Partitioner.Create(3, NII) :61 */
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {                       /* Partitioner.Create(3, NII) :61 */
         int i = (IS == -1) ? NII - i1 + 1 : i1;
         for (int j1 = 2; j1 <= NJJ - 1; ++j1) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
@@ -268,6 +269,7 @@ void u_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
             }
         }
     }
+    });
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -280,10 +282,11 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
     const float Cor = st.p->coriolis;
+    oracle::for_slabs(2, NII, [&](int i1_lo, int i1_hi) {
     std::vector<float> PIMV(st.nk2), QIMV(st.nk2);
     std::vector<float> AIM_A(SIMD), BIM_A(SIMD), CIM_A(SIMD), DIM_A(SIMD), VIS_A(SIMD), MASK(SIMD);
 
-    for (int i1 = 2; i1 < NII; i1++) {                       /* Partitioner.Create(2, NII) :61 */
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {                       /* Partitioner.Create(2, NII) :61 */
         int i = (IS == -1) ? NII - i1 + 1 : i1;
         for (int j1 = 3; j1 <= NJJ - 1; ++j1) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
@@ -479,6 +482,7 @@ void v_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
             }
         }
     }
+    });
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -489,10 +493,11 @@ void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
     const int NII = st.nii, NJJ = st.njj;
     const float DXK = st.dxk, DYK = st.dyk;
     const float *DZK = st.dzk(), *HOKART = st.hokart();
+    oracle::for_slabs(2, NII, [&](int i1_lo, int i1_hi) {
     std::vector<float> PIMW(st.nk2), QIMW(st.nk2);
     std::vector<float> AIM_A(SIMD), BIM_A(SIMD), CIM_A(SIMD), DIM_A(SIMD), VIS_A(SIMD), MASK(SIMD);
 
-    for (int i1 = 2; i1 < NII; i1++) {
+    for (int i1 = i1_lo; i1 < i1_hi; i1++) {
         int i = (IS == -1) ? NII - i1 + 1 : i1;
         for (int j1 = 2; j1 < NJJ; ++j1) {
             int j = (JS == -1) ? NJJ - j1 + 1 : j1;
@@ -654,6 +659,7 @@ void w_mom_ml(State &st, const int SIMD, int IS, int JS, float VISHMIN, float AR
             }
         }
     }
+    });
 }
 
 }  // namespace oracle

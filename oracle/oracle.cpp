@@ -8,12 +8,31 @@
  */
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "oracle_common.h"
 
 using namespace oracle;
+
+/* Host threads of the racy-order build: ORACLE_THREADS in the environment, else every hardware
+ * thread; 1 in the deterministic build. */
+extern "C" int oracle_threads(void) { return oracle::worker_threads(); }
+
+int oracle::worker_threads() {
+#ifdef ORACLE_THREADS
+    static const int n = [] {
+        const char *e = std::getenv("ORACLE_THREADS");
+        const int v = e ? std::atoi(e) : 0;
+        return v > 0 ? v : std::max(1, (int)std::thread::hardware_concurrency());
+    }();
+    return n;
+#else
+    return 1;
+#endif
+}
 
 namespace {
 
@@ -238,6 +257,7 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
                                            pow2f(st.vk[st.i3(rx, ry, st.kadvmax)])));
     DTIME = net_min(DTIME, 5);
     float DeltaUMax = 0, DeltaFinish = 0, DeltaFirst = 0;
+    std::mutex delta_mutex;   /* row maxima of the racy-order build's pressure workers */
     const float AREAxy = DXK * DYK;
     for (int k = 1; k <= st.kadvmax; ++k) st.ap0[k] = AREAxy * DZK[k] / DTIME;
     const int MaxProgCellCount = st.vcff;
@@ -369,7 +389,8 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
         boundary_conditions(st);
 
         /* mass divergence; DPM = 0 on the prognostic levels (:723-758) */
-        for (int i = 2; i < NII; ++i) {
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
             for (int j = 2; j < NJJ; ++j) {
                 if (st.advdom(i, j) != 1) continue;
                 const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
@@ -387,6 +408,7 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
                 }
             }
         }
+        });
 
         /* sweep direction (:770-802) */
         int IS = 1, JS = 1;
@@ -396,9 +418,10 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
 
         /* pressure correction, vertical TDMA per column, rows in order (:804-901) */
         DeltaUMax = 0;
-        {
+        for_chunks(2, NJJ, 1, [&](int j1_lo, int j1_hi) {
             std::vector<float> PIMP(st.nk2), QIMP(st.nk2);
-            for (int j1 = 2; j1 < NJJ; ++j1) {
+            float DeltaUMaxRows = 0;
+            for (int j1 = j1_lo; j1 < j1_hi; ++j1) {
                 std::fill(PIMP.begin(), PIMP.end(), 0.0f);   /* new float[NKK + 2] per row */
                 std::fill(QIMP.begin(), QIMP.end(), 0.0f);
                 float DeltaUMaxIntern = 0;
@@ -430,12 +453,15 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
                         DPMNEW_L[k] += relaxp * DPM_L[k];
                     }
                 }
-                if (DeltaUMaxIntern > DeltaUMax) DeltaUMax = DeltaUMaxIntern;
+                if (DeltaUMaxIntern > DeltaUMaxRows) DeltaUMaxRows = DeltaUMaxIntern;
             }
-        }
+            std::lock_guard<std::mutex> lk(delta_mutex);
+            if (DeltaUMaxRows > DeltaUMax) DeltaUMax = DeltaUMaxRows;
+        });
 
         /* velocity correction with Frund quantisation in double (:904-949) */
-        for (int i = 2; i < NII; ++i) {
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
             for (int j = 2; j <= NJJ - 1; ++j) {
                 if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
                 const float *DPMim = st.col(st.dpm, i - 1, j), *DPMjm = st.col(st.dpm, i, j - 1);
@@ -457,9 +483,11 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
                 }
             }
         }
+        });
 
         /* staggered -> cell-centre averages and border copies (:958-1039) */
-        for (int i = 2; i < NII; ++i) {
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
             for (int j = 2; j <= NJJ - 1; ++j) {
                 if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
                 const float *UK_L = st.col(st.uk, i, j), *UKip = st.col(st.uk, i + 1, j);
@@ -486,6 +514,7 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
                 }
             }
         }
+        });
         for (int j = 2; j < NJJ; ++j) {
             if (st.advdom(1, j) == 1) {
                 float *a = st.col(st.vks, 1, j); const float *b = st.col(st.vks, 2, j);

@@ -18,32 +18,62 @@ from gral_b200.abi import (GralFields, GralParams, GralStatic, GralStats, FieldA
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
+# racy-order throughput analogue (CPU baseline only): the same sources built with the sweeps over
+# host threads, -O3 -march=native, on the machine that runs it
+_LIB_MT = os.path.join(_HERE, "liboracle_mt.so")
+_SRCS = ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "prep.cpp", "wind.cpp", "oracle_common.h", "Makefile",
+         os.path.join("..", "include", "gral_prog.h"))
 _lib = None
+_lib_mt = None
+
+
+def _make(target: str, path: str, force: bool) -> str:
+    srcs = [os.path.join(_HERE, f) for f in _SRCS]
+    if force or not os.path.exists(path) or any(os.path.getmtime(s) > os.path.getmtime(path) for s in srcs):
+        subprocess.run(["make", "-s", "-C", _HERE] + (["-B"] if force else []) + [target], check=True)
+    return path
 
 
 def build(force: bool = False) -> str:
     """Compile liboracle.so with the committed Makefile (g++, no FP contraction)."""
-    srcs = [os.path.join(_HERE, f) for f in ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "prep.cpp", "wind.cpp", "oracle_common.h",
-                                              os.path.join("..", "include", "gral_prog.h"))]
-    if force or not os.path.exists(_LIB) or any(os.path.getmtime(s) > os.path.getmtime(_LIB) for s in srcs):
-        subprocess.run(["make", "-s", "-C", _HERE, "liboracle.so"], check=True)
-    return _LIB
+    return _make("liboracle.so", _LIB, force)
+
+
+def build_threaded(force: bool = False) -> str:
+    """Compile liboracle_mt.so, the racy-order multi-threaded build (never a parity reference)."""
+    return _make("liboracle_mt.so", _LIB_MT, force)
+
+
+def _bind(path: str):
+    h = C.CDLL(path)
+    h.oracle_solve.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic),
+                               C.POINTER(GralFields), C.POINTER(GralStats)]
+    h.oracle_solve.restype = C.c_int
+    return h
 
 
 def lib():
     global _lib
     if _lib is None:
         build()
-        _lib = C.CDLL(_LIB)
-        _lib.oracle_solve.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic),
-                                      C.POINTER(GralFields), C.POINTER(GralStats)]
-        _lib.oracle_solve.restype = C.c_int
+        _lib = _bind(_LIB)
     return _lib
 
 
+def lib_threaded():
+    global _lib_mt
+    if _lib_mt is None:
+        build_threaded()
+        _lib_mt = _bind(_LIB_MT)
+    return _lib_mt
+
+
 def solve(params: dict, static: StaticArrays, fields: FieldArrays,
-          trace: Optional[np.ndarray] = None) -> dict:
-    """Run the oracle in place on ``fields``; returns the stats as a dict."""
+          trace: Optional[np.ndarray] = None, threaded: bool = False) -> dict:
+    """Run the oracle in place on ``fields``; returns the stats as a dict.  ``threaded`` runs the
+    racy-order multi-threaded build instead (thread count from ORACLE_THREADS, else all hardware
+    threads): a throughput analogue of the reference's default mode whose results depend on thread
+    timing, used only as a CPU baseline."""
     p = params_to_c(params)
     s = static.to_c()
     f = fields.to_c()
@@ -51,7 +81,14 @@ def solve(params: dict, static: StaticArrays, fields: FieldArrays,
     if trace is not None:
         st.trace_delta_umax = trace.ctypes.data_as(C.POINTER(C.c_float))
         st.trace_capacity = trace.size
-    rc = lib().oracle_solve(C.byref(p), C.byref(s), C.byref(f), C.byref(st))
+    rc = (lib_threaded() if threaded else lib()).oracle_solve(C.byref(p), C.byref(s), C.byref(f), C.byref(st))
     if rc != GRAL_OK:
         raise RuntimeError(f"oracle_solve failed: {STATUS_NAMES.get(rc, rc)}")
     return stats_to_dict(st)
+
+
+def threads_used() -> int:
+    """Host threads the racy-order build runs its sweeps on."""
+    h = lib_threaded()
+    h.oracle_threads.restype = C.c_int
+    return int(h.oracle_threads())

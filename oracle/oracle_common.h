@@ -15,15 +15,52 @@
 #ifndef GRAL_ORACLE_COMMON_H
 #define GRAL_ORACLE_COMMON_H
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
+#ifdef ORACLE_THREADS
+#include <atomic>
+#include <thread>
+#endif
 
 #include "gral_prog.h"
 
 namespace oracle {
+
+/* ---- racy-order throughput build ----
+ * Built with ORACLE_THREADS (liboracle_mt.so), the outer loops of the sweeps run over host threads
+ * the way the reference's default (non-deterministic) mode runs them: momentum and k-eps sweeps
+ * over i-slabs of min(max(4, NII/threads), 64) columns handed out dynamically (Parallel.ForEach
+ * over Partitioner.Create(3, NII, ...), U-prognostic-microscale_1.cs:59-61), the pressure sweep
+ * over rows j (Parallel.For(2, NJJ), PrognosticFlowfield.cs:812), the divergence, velocity
+ * correction and averages over i.  Neighbouring slabs then read each other's cells while they are
+ * written, so results depend on thread timing as in the reference's default mode: that build is a
+ * throughput analogue only, never a parity reference.  Without ORACLE_THREADS, for_chunks calls
+ * its body once over the whole range and every loop runs in the deterministic order. */
+int worker_threads();
+inline int slab_chunk(int n) { return std::min(std::max(4, n / worker_threads()), 64); }
+#ifdef ORACLE_THREADS
+template <class F> void for_chunks(int lo, int hi, int chunk, F &&body) {
+    std::atomic<int> next(lo);
+    auto work = [&]() {
+        for (;;) {
+            const int a = next.fetch_add(chunk);
+            if (a >= hi) break;
+            body(a, std::min(a + chunk, hi));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < worker_threads(); ++t) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+}
+#else
+template <class F> void for_chunks(int lo, int hi, int, F &&body) { body(lo, hi); }
+#endif
+template <class F> void for_slabs(int lo, int hi, F &&body) { for_chunks(lo, hi, slab_chunk(hi), body); }
 
 /* ---- .NET 8 scalar semantics (ProgramFunctions.cs:768-849 and System.Math) ---- */
 

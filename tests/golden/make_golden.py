@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py m1_small_s0
+    GRAL_REFERENCE_SRC=<GRAL checkout>/src python tests/golden/make_golden.py   # also hash the reference
 
 The oracle is the deterministic restatement of GRAL's prognostic solve under ``oracle/``; the
 C# reference cannot run in this environment, so these files pin the oracle (and through it the
@@ -26,7 +27,10 @@ sys.path.insert(0, HERE)
 import cases as G  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 
-REFERENCE_TREE = "/root/reference/src"
+# source directory of the GRAL checkout the oracle restates (its `src/` folder); taken from the
+# environment so that no machine path is built in; without it the previous manifest's reference
+# digests are kept
+REFERENCE_TREE = os.environ.get("GRAL_REFERENCE_SRC", "")
 REFERENCE_FILES = ["PrognosticFlowfield.cs", "U-prognostic-microscale_0.cs", "U-prognostic-microscale_1.cs",
                    "U-prognostic-microscale_2.cs", "V-prognostic-microscale_0.cs", "V-prognostic-microscale_1.cs",
                    "V-prognostic-microscale_2.cs", "W-prognostic-microscale_0.cs", "W-prognostic-microscale_1.cs",
@@ -74,7 +78,7 @@ def main(names):
                               for f in ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "oracle_common.h")},
            "reference": "GRAL 24.11.2 (GRAL.csproj VersionPrefix), deterministic mode",
            "generator": "tests/golden/make_golden.py"}
-    if os.path.isdir(REFERENCE_TREE):
+    if REFERENCE_TREE and os.path.isdir(REFERENCE_TREE):
         man["reference_sources"] = {f: sha_file(os.path.join(REFERENCE_TREE, f))
                                     for f in REFERENCE_FILES if os.path.exists(os.path.join(REFERENCE_TREE, f))}
     else:

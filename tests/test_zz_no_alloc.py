@@ -81,3 +81,20 @@ def test_check_speeds_noalloc_rejects(gpu_required):
                                 k.data_ptr()) == (0, 0, 0, 0)
     assert lib().gral_prog_check_speeds_noalloc(n, n, n, 4, 1.0, d.data_ptr(), d.data_ptr(), d.data_ptr(),
                                                 a.data_ptr(), k.data_ptr(), None, None) == GRAL_EINVAL
+
+
+def test_check_speeds_noalloc_rejects_other_device(gpu_required):
+    """Device memory of another GPU is refused on the host before any launch (needs two GPUs)."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs a second GPU to hold the foreign arrays")
+    n = 8
+    torch.cuda.set_device(0)
+    d0 = torch.zeros((n + 2) ** 3, dtype=torch.float32, device="cuda:0")
+    a0 = torch.zeros((n + 2) ** 2, dtype=torch.uint8, device="cuda:0")
+    k0 = torch.zeros((n + 2) ** 2, dtype=torch.int16, device="cuda:0")
+    d1 = torch.zeros((n + 2) ** 3, dtype=torch.float32, device="cuda:1")
+    with pytest.raises(GralError) as e:
+        check_speeds_noalloc(n, n, n, 4, 1.0, d1.data_ptr(), d0.data_ptr(), d0.data_ptr(), a0.data_ptr(),
+                             k0.data_ptr())
+    assert e.value.code == GRAL_EINVAL
