@@ -13,6 +13,7 @@
 #include <mutex>
 #include <vector>
 
+#include "oracle_ad.h"
 #include "oracle_common.h"
 
 using namespace oracle;
@@ -51,7 +52,8 @@ int validate(const gral_params *p, const gral_static *s, const gral_fields *f) {
 
 /* Lateral boundary conditions at the west/east and south/north borders of the prognostic
  * sub-domains (PrognosticFlowfield.cs:595-696) and at the top (:699-714). */
-void boundary_conditions(State &st) {
+template <class T>
+void boundary_conditions(StateT<T> &st) {
     const int NII = st.nii, NJJ = st.njj;
     for (int j = 2; j < NJJ + 1; ++j) {
         for (int i = 3; i < NII; ++i) {
@@ -61,7 +63,7 @@ void boundary_conditions(State &st) {
             const bool iP = (st.advdom(i + 1, j) < 1) || (i == NII - 1);
             if (iM) {
                 for (int k = 1; k <= VI; ++k) {
-                    float u = st.uk[st.i3(i - 2, j, k)];
+                    T u = st.uk[st.i3(i - 2, j, k)];
                     if (u >= 0) st.uk[st.i3(i - 1, j, k)] = u;
                     st.vk[st.i3(i - 2, j, k)] = st.vk[st.i3(i - 1, j, k)];
                     st.wk[st.i3(i - 2, j, k)] = st.wk[st.i3(i - 1, j, k)];
@@ -69,7 +71,7 @@ void boundary_conditions(State &st) {
             }
             if (iP) {
                 for (int k = 1; k <= VI; ++k) {
-                    float u = st.uk[st.i3(i + 2, j, k)];
+                    T u = st.uk[st.i3(i + 2, j, k)];
                     if (u <= 0) st.uk[st.i3(i + 1, j, k)] = u;
                     st.vk[st.i3(i + 1, j, k)] = st.vk[st.i3(i, j, k)];
                     st.wk[st.i3(i + 1, j, k)] = st.wk[st.i3(i, j, k)];
@@ -85,7 +87,7 @@ void boundary_conditions(State &st) {
             const bool jP = (st.advdom(i, j + 1) < 1) || (j == NJJ - 1);
             if (jM) {
                 for (int k = 1; k <= VI; ++k) {
-                    float v = st.vk[st.i3(i, j - 2, k)];
+                    T v = st.vk[st.i3(i, j - 2, k)];
                     if (v >= 0) st.vk[st.i3(i, j - 1, k)] = v;
                     st.uk[st.i3(i, j - 2, k)] = st.uk[st.i3(i, j - 1, k)];
                     st.wk[st.i3(i, j - 2, k)] = st.wk[st.i3(i, j - 1, k)];
@@ -93,7 +95,7 @@ void boundary_conditions(State &st) {
             }
             if (jP) {
                 for (int k = 1; k <= VI; ++k) {
-                    float v = st.vk[st.i3(i, j + 2, k)];
+                    T v = st.vk[st.i3(i, j + 2, k)];
                     if (v <= 0) st.vk[st.i3(i, j + 1, k)] = v;
                     st.uk[st.i3(i, j + 1, k)] = st.uk[st.i3(i, j, k)];
                     st.wk[st.i3(i, j + 1, k)] = st.wk[st.i3(i, j, k)];
@@ -116,6 +118,210 @@ void boundary_conditions(State &st) {
 inline double quant(double x, double Frund, bool on) {
     if (!on) return x;
     return conv_to_int(x * Frund) / Frund;
+}
+
+/* Per-solve scalars of the SIMPLE loop, fixed by the set-up (PrognosticFlowfield.cs:146-579). */
+struct LoopConsts {
+    const gral_params *p;
+    float DTIME, AREAxy, UG, VG, relax, relaxp, VISHMIN, VISVMIN, building_Z0, Ustern_factorX;
+    float Cmueh, Ceps, Ceps1, Ceps2;
+    double Frund;
+    bool quantise;
+    int model;
+};
+
+inline double val(float x) { return (double)x; }
+inline double val(double x) { return x; }
+inline double val(const AD &x) { return x.v; }
+
+/* the velocity-correction rounding of the float oracle; the FP64 twin runs without rounding */
+template <class T>
+inline T vquant(T x, double Frund, bool on) {
+    if constexpr (std::is_same<T, float>::value) return (float)quant((double)x, Frund, on);
+    else return x;
+}
+
+/* One SIMPLE iteration (PrognosticFlowfield.cs:584-1137): boundary conditions, divergence, the
+ * pressure-correction sweep, velocity correction, staggered averages and the momentum sweeps.
+ * Returns DeltaUMax of the iteration. */
+template <class T>
+float simple_iteration(StateT<T> &st, const LoopConsts &c, int IterationLoops) {
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    const float DXK = st.dxk, DYK = st.dyk;
+    const float *DZK = st.s->dzk;
+    const gral_params *p = c.p;
+    const float DTIME = c.DTIME, AREAxy = c.AREAxy, UG = c.UG, VG = c.VG, relax = c.relax, relaxp = c.relaxp;
+    const float VISHMIN = c.VISHMIN, VISVMIN = c.VISVMIN, building_Z0 = c.building_Z0;
+    const float Ustern_factorX = c.Ustern_factorX;
+    const float Cmueh = c.Cmueh, Ceps = c.Ceps, Ceps1 = c.Ceps1, Ceps2 = c.Ceps2;
+    const double Frund = c.Frund;
+    const bool quantise = c.quantise;
+    const int model = c.model;
+    (void)NKK; (void)VISVMIN; (void)building_Z0; (void)Ustern_factorX; (void)Cmueh; (void)Ceps; (void)Ceps1;
+    (void)Ceps2; (void)model;
+    float DeltaUMax = 0;
+    std::mutex delta_mutex;   /* row maxima of the racy-order build's pressure workers */
+        boundary_conditions(st);
+
+        /* mass divergence; DPM = 0 on the prognostic levels (:723-758) */
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
+            for (int j = 2; j < NJJ; ++j) {
+                if (st.advdom(i, j) != 1) continue;
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                const T *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
+                const T *UKip = st.col(st.uk, i + 1, j), *VKjp = st.col(st.vk, i, j + 1);
+                T *DIV_L = st.col(st.div, i, j), *DPM_L = st.col(st.dpm, i, j);
+                for (int k = KK + 1; k <= VI; ++k) {
+                    if (k > KK + 1)
+                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] +
+                                   (WK_L[k] - WK_L[k + 1]) * AREAxy;
+                    else
+                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] -
+                                   WK_L[k + 1] * AREAxy;
+                    DPM_L[k] = 0;
+                }
+            }
+        }
+        });
+
+        /* sweep direction (:770-802) */
+        int IS = 1, JS = 1;
+        if (IterationLoops % 4 == 0) { IS = -1; JS = 1; }
+        else if (IterationLoops % 4 == 1) { IS = -1; JS = -1; }
+        else if (IterationLoops % 4 == 2) { IS = 1; JS = -1; }
+
+        /* pressure correction, vertical TDMA per column, rows in order (:804-901) */
+        for_chunks(2, NJJ, 1, [&](int j1_lo, int j1_hi) {
+            std::vector<T> PIMP(st.nk2), QIMP(st.nk2);
+            float DeltaUMaxRows = 0;
+            for (int j1 = j1_lo; j1 < j1_hi; ++j1) {
+                std::fill(PIMP.begin(), PIMP.end(), 0.0f);   /* new float[NKK + 2] per row */
+                std::fill(QIMP.begin(), QIMP.end(), 0.0f);
+                float DeltaUMaxIntern = 0;
+                const int j = (JS == -1) ? NJJ - j1 + 1 : j1;
+                for (int i1 = 2; i1 <= NII - 1; ++i1) {
+                    const int i = (IS == -1) ? NII - i1 + 1 : i1;
+                    if (st.advdom(i, j) != 1) continue;
+                    const T *DIV_L = st.col(st.div, i, j);
+                    T *DPM_L = st.col(st.dpm, i, j);
+                    const T *DPMim = st.col(st.dpm, i - 1, j), *DPMip = st.col(st.dpm, i + 1, j);
+                    const T *DPMjm = st.col(st.dpm, i, j - 1), *DPMjp = st.col(st.dpm, i, j + 1);
+                    T *DPMNEW_L = st.col(st.dpmnew, i, j);
+                    const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                    for (int k = VI; k > KK; --k) {
+                        T DIM = DIV_L[k] / DTIME + (DPMim[k] + DPMip[k]) / DXK * DYK * DZK[k] +
+                                    (DPMjm[k] - DPMjp[k]) / DYK * DXK * DZK[k];
+                        T APP = 2.0f * (DYK * DZK[k] / DXK + DXK * DZK[k] / DYK + AREAxy / DZK[k]);
+                        T ABP = (k > 1) ? AREAxy / (0.5f * (DZK[k - 1] + DZK[k])) : AREAxy / DZK[k];
+                        T ATP = AREAxy / (0.5f * (DZK[k + 1] + DZK[k]));
+                        T TERMP = 1 / (APP - ATP * PIMP[k + 1]);
+                        PIMP[k] = ABP * TERMP;
+                        QIMP[k] = (ATP * QIMP[k + 1] + DIM) * TERMP;
+                    }
+                    for (int k = KK + 1; k <= VI; ++k) {
+                        T temp = PIMP[k] * DPM_L[k - 1] + QIMP[k];
+                        DeltaUMaxIntern = (float)net_maxd((double)DeltaUMaxIntern,
+                            std::fabs(val(DPM_L[k]) - quant(val(temp), Frund, quantise)));
+                        DPM_L[k] = temp;
+                        DPMNEW_L[k] += relaxp * DPM_L[k];
+                    }
+                }
+                if (DeltaUMaxIntern > DeltaUMaxRows) DeltaUMaxRows = DeltaUMaxIntern;
+            }
+            std::lock_guard<std::mutex> lk(delta_mutex);
+            if (DeltaUMaxRows > DeltaUMax) DeltaUMax = DeltaUMaxRows;
+        });
+
+        /* velocity correction with Frund quantisation in double (:904-949) */
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
+            for (int j = 2; j <= NJJ - 1; ++j) {
+                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
+                const T *DPMim = st.col(st.dpm, i - 1, j), *DPMjm = st.col(st.dpm, i, j - 1);
+                const T *DPM_L = st.col(st.dpm, i, j);
+                T *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                const int KKim = st.kkart(i - 1, j), KKjm = st.kkart(i, j - 1);
+                for (int k = 1; k <= VI; ++k) {
+                    const T d = DPM_L[k];
+                    if (i > 2 && KK < k && KKim < k)
+                        UK_L[k] = vquant<T>(UK_L[k] + (DPMim[k] - d) / DXK * DTIME, Frund, quantise);
+                    if (j > 2 && KK < k && KKjm < k)
+                        VK_L[k] = vquant<T>(VK_L[k] + (DPMjm[k] - d) / DYK * DTIME, Frund, quantise);
+                    if (KK + 1 < k)
+                        WK_L[k] = vquant<T>(WK_L[k] + (DPM_L[k - 1] - d) / (DZK[k] + DZK[k - 1]) * 2 * DTIME,
+                                            Frund, quantise);
+                    else
+                        WK_L[k] = 0;
+                }
+            }
+        }
+        });
+
+        /* staggered -> cell-centre averages and border copies (:958-1039) */
+        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
+        for (int i = i_lo; i < i_hi; ++i) {
+            for (int j = 2; j <= NJJ - 1; ++j) {
+                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
+                const T *UK_L = st.col(st.uk, i, j), *UKip = st.col(st.uk, i + 1, j);
+                const T *VK_L = st.col(st.vk, i, j), *VKjp = st.col(st.vk, i, j + 1);
+                const T *WK_L = st.col(st.wk, i, j);
+                T *UKS_L = st.col(st.uks, i, j), *VKS_L = st.col(st.vks, i, j), *WKS_L = st.col(st.wks, i, j);
+                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
+                int KSTART = 1;
+                if (st.cutk(i, j) == 0) KSTART = KK + 1;
+                for (int k = KSTART; k <= VI; ++k) {
+                    if (KK < k) {
+                        UKS_L[k] = 0.5f * (UK_L[k] + UKip[k]);
+                        VKS_L[k] = 0.5f * (VK_L[k] + VKjp[k]);
+                    }
+                    if (KK + 1 < k) WKS_L[k] = 0.5f * (WK_L[k] + WK_L[k + 1]);
+                }
+                if (j == 2) {
+                    T *UKS1 = st.col(st.uks, i, 1);
+                    for (int k = KSTART; k <= VI; ++k) UKS1[k] = UKS_L[k];
+                }
+                if (j == NJJ - 1 && st.advdom(i, NJJ) == 1) {
+                    T *UKSN = st.col(st.uks, i, NJJ);
+                    for (int k = KSTART; k <= VI; ++k) UKSN[k] = UKS_L[k];
+                }
+            }
+        }
+        });
+        for (int j = 2; j < NJJ; ++j) {
+            if (st.advdom(1, j) == 1) {
+                T *a = st.col(st.vks, 1, j); const T *b = st.col(st.vks, 2, j);
+                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
+            }
+            if (st.advdom(NII - 1, j) == 1) {
+                T *a = st.col(st.vks, NII, j); const T *b = st.col(st.vks, NII - 1, j);
+                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
+            }
+        }
+
+        /* momentum equations (:1049-1137), deterministic order; the FP64 twin and the tape type run
+         * model 1 only */
+        if constexpr (!std::is_same<T, float>::value) {
+            u_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, UG, relax);
+            v_mom_ml(st, p->simd_width, -IS, -JS, VISHMIN, AREAxy, VG, relax);
+            w_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, relax);
+        } else if (model == 0) {
+            u_mom_nd(st, IS, JS, AREAxy, UG, relax);
+            v_mom_nd(st, IS, JS, AREAxy, VG, relax);
+            w_mom_nd(st, IS, JS, AREAxy, relax);
+        } else if (model == 1) {
+            u_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, UG, relax);
+            v_mom_ml(st, p->simd_width, -IS, -JS, VISHMIN, AREAxy, VG, relax);
+            w_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, relax);
+        } else {
+            u_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, UG, relax);
+            v_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, VG, relax);
+            w_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, relax);
+            tke_ke(st, IS, JS, Cmueh, Ceps, Ceps1, Ceps2, VISHMIN, VISVMIN, AREAxy, building_Z0, relax,
+                   Ustern_factorX);
+        }
+    return DeltaUMax;
 }
 
 }  // namespace
@@ -209,12 +415,73 @@ static void diagnostic_post(State &st) {
         }
 }
 
-extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fields *f,
-                            gral_stats *stats) {
+/* UKS/VKS/WKS exist only where ADVDOM is set in the 3x3 neighbourhood (PrognosticFlowfield.cs:64-86). */
+template <class T>
+bool alloc3x3(const StateT<T> &st, int i, int j) {
+    const int NII = st.nii, NJJ = st.njj;
+    const int ip = std::min(i + 1, NII + 1), jp = std::min(j + 1, NJJ + 1);
+    return st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(ip, j) == 1 ||
+           st.advdom(i, j - 1) == 1 || st.advdom(i - 1, j - 1) == 1 || st.advdom(ip, j - 1) == 1 ||
+           st.advdom(i, jp) == 1 || st.advdom(i - 1, jp) == 1 || st.advdom(ip, jp) == 1;
+}
+
+/* Initial staggered-grid velocities (PrognosticFlowfield.cs:295-329); returns GESCHW_MAX. */
+template <class T>
+double initial_staggered(StateT<T> &st) {
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    double GESCHW_MAX = 0;
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            if (!alloc3x3(st, i, j)) continue;
+            for (int k = 1; k <= NKK - 1; ++k) {
+                T u = 0.5f * (st.uk[st.i3(i, j, k)] + st.uk[st.i3(i + 1, j, k)]);
+                T v = 0.5f * (st.vk[st.i3(i, j, k)] + st.vk[st.i3(i, j + 1, k)]);
+                T w = 0.5f * (st.wk[st.i3(i, j, k)] + st.wk[st.i3(i, j, k + 1)]);
+                st.uks[st.i3(i, j, k)] = u; st.vks[st.i3(i, j, k)] = v; st.wks[st.i3(i, j, k)] = w;
+                GESCHW_MAX = net_maxd(GESCHW_MAX, std::sqrt((double)(pow2f((float)val(u)) + pow2f((float)val(v)))));
+            }
+        }
+    }
+    return GESCHW_MAX;
+}
+
+/* Velocities (and TKE) inside buildings set to zero (PrognosticFlowfield.cs:518-575). */
+template <class T>
+void zero_in_buildings(StateT<T> &st, int model) {
+    const int NII = st.nii, NJJ = st.njj;
+    for (int i = 1; i < NII + 1; ++i) {
+        for (int j = 1; j <= NJJ; ++j) {
+            if (st.advdom(i, j) != 1) continue;
+            const int VI = st.vert_index[st.i2(i, j)];
+            const int KK = st.kkart(i, j);
+            for (int k = 1; k <= VI; ++k) {
+                if (KK >= k) {
+                    st.uk[st.i3(i, j, k)] = 0;
+                    if (i == NII) st.uk[st.i3(i + 1, j, k)] = 0;
+                    st.vk[st.i3(i, j, k)] = 0;
+                    if (j == NJJ) st.vk[st.i3(i, j + 1, k)] = 0;
+                    st.wk[st.i3(i, j, k)] = 0;
+                    if (k == VI) st.wk[st.i3(i, j, k + 1)] = 0;
+                    if (model != 1) { st.turb[st.i3(i, j, k)] = 0; st.tdiss[st.i3(i, j, k)] = 0; }
+                    st.uks[st.i3(i, j, k)] = 0; st.vks[st.i3(i, j, k)] = 0; st.wks[st.i3(i, j, k)] = 0;
+                }
+            }
+        }
+    }
+}
+
+struct SetupOut {
+    LoopConsts c;
+    float topwind;
+    double GESCHW_MAX;
+};
+
+/* Set-up of one solve (PrognosticFlowfield.cs:45-579) on the float state: allocations, the
+ * per-solve scalars and the initial staggered velocities; the fields are zeroed inside buildings. */
+static int setup_solve(State &st, const gral_params *p, const gral_static *s, gral_fields *f, SetupOut &o) {
     int rc = validate(p, s, f);
     if (rc != GRAL_OK) return rc;
 
-    State st;
     st.p = p; st.s = s;
     st.nii = p->nii; st.njj = p->njj; st.nkk = p->nkk;
     st.kadvmax = p->kadvmax; st.vcff = p->vert_cells_ff;
@@ -239,30 +506,19 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
     const float *DZK = s->dzk;
     const int rx = p->ref_i, ry = p->ref_j;
 
-    /* UKS/VKS/WKS/DPMNEW exist only where ADVDOM is set in the 3x3 neighbourhood (:64-86). */
-    auto alloc3x3 = [&](int i, int j) {
-        const int ip = std::min(i + 1, NII + 1), jp = std::min(j + 1, NJJ + 1);
-        return st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(ip, j) == 1 ||
-               st.advdom(i, j - 1) == 1 || st.advdom(i - 1, j - 1) == 1 || st.advdom(ip, j - 1) == 1 ||
-               st.advdom(i, jp) == 1 || st.advdom(i - 1, jp) == 1 || st.advdom(ip, jp) == 1;
-    };
 
     /* topwind, DTIME, AP0 (:146-163) */
     float topwind = (float)std::sqrt((double)(pow2f(st.uk[st.i3(rx, ry, NKK - 1)]) +
                                               pow2f(st.vk[st.i3(rx, ry, NKK - 1)])));
     topwind = net_max(topwind, 0.01f);
-    int IterationLoops = 1;
     float DTIME = 0.5f * net_min(DXK, DZK[1]) /
                   net_max(0.01f, std::sqrt(pow2f(st.uk[st.i3(rx, ry, st.kadvmax)]) +
                                            pow2f(st.vk[st.i3(rx, ry, st.kadvmax)])));
     DTIME = net_min(DTIME, 5);
-    float DeltaUMax = 0, DeltaFinish = 0, DeltaFirst = 0;
-    std::mutex delta_mutex;   /* row maxima of the racy-order build's pressure workers */
     const float AREAxy = DXK * DYK;
     for (int k = 1; k <= st.kadvmax; ++k) st.ap0[k] = AREAxy * DZK[k] / DTIME;
     const int MaxProgCellCount = st.vcff;
     const float building_Z0 = p->building_z0;
-    double DeltaMean = 0;
     const float Cmueh = 0.09f, Ceps = 1, Ceps1 = 1.44f, Ceps2 = 1.92f;
 
     /* DPM = 0 (:198-209), TURB/TDISS initial constants (:211-227) */
@@ -280,23 +536,10 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
     if (model == 2) Frund = (double)(10000 / topwind);
     const bool quantise = p->quantise != 0;
 
-    const int IterationStepsMin = p->iteration_steps_min, IterationStepsMax = p->iteration_steps_max;
     const float relax = p->relax, relaxp = p->relaxp;
 
     /* initial staggered-grid velocities and GESCHW_MAX (:295-329) */
-    double GESCHW_MAX = 0;
-    for (int i = 1; i < NII + 1; ++i) {
-        for (int j = 1; j <= NJJ; ++j) {
-            if (!alloc3x3(i, j)) continue;
-            for (int k = 1; k <= NKK - 1; ++k) {
-                float u = 0.5f * (st.uk[st.i3(i, j, k)] + st.uk[st.i3(i + 1, j, k)]);
-                float v = 0.5f * (st.vk[st.i3(i, j, k)] + st.vk[st.i3(i, j + 1, k)]);
-                float w = 0.5f * (st.wk[st.i3(i, j, k)] + st.wk[st.i3(i, j, k + 1)]);
-                st.uks[st.i3(i, j, k)] = u; st.vks[st.i3(i, j, k)] = v; st.wks[st.i3(i, j, k)] = w;
-                GESCHW_MAX = net_maxd(GESCHW_MAX, std::sqrt((double)(pow2f(u) + pow2f(v))));
-            }
-        }
-    }
+    double GESCHW_MAX = initial_staggered(st);
 
     /* VerticalIndex (:333-344) */
     for (int i = 1; i < NII + 1; ++i)
@@ -361,187 +604,39 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
     const float Ustern_factorX = (float)(0.4 / std::log((double)DXK * 0.5 / (double)building_Z0));
 
     /* velocities, TKE inside buildings set to zero (:518-575) */
-    for (int i = 1; i < NII + 1; ++i) {
-        for (int j = 1; j <= NJJ; ++j) {
-            if (st.advdom(i, j) != 1) continue;
-            const int VI = st.vert_index[st.i2(i, j)];
-            const int KK = st.kkart(i, j);
-            for (int k = 1; k <= VI; ++k) {
-                if (KK >= k) {
-                    st.uk[st.i3(i, j, k)] = 0;
-                    if (i == NII) st.uk[st.i3(i + 1, j, k)] = 0;
-                    st.vk[st.i3(i, j, k)] = 0;
-                    if (j == NJJ) st.vk[st.i3(i, j + 1, k)] = 0;
-                    st.wk[st.i3(i, j, k)] = 0;
-                    if (k == VI) st.wk[st.i3(i, j, k + 1)] = 0;
-                    if (model != 1) { st.turb[st.i3(i, j, k)] = 0; st.tdiss[st.i3(i, j, k)] = 0; }
-                    st.uks[st.i3(i, j, k)] = 0; st.vks[st.i3(i, j, k)] = 0; st.wks[st.i3(i, j, k)] = 0;
-                }
-            }
-        }
-    }
+    zero_in_buildings(st, model);
+
+    o.c = LoopConsts{p, DTIME, AREAxy, UG, VG, relax, relaxp, VISHMIN, VISVMIN, building_Z0, Ustern_factorX,
+                     Cmueh, Ceps, Ceps1, Ceps2, Frund, quantise, model};
+    o.topwind = topwind;
+    o.GESCHW_MAX = GESCHW_MAX;
+    return GRAL_OK;
+}
+
+extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fields *f,
+                            gral_stats *stats) {
+    State st;
+    SetupOut o;
+    const int rc = setup_solve(st, p, s, f, o);
+    if (rc != GRAL_OK) return rc;
+    const LoopConsts &c = o.c;
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    const float topwind = o.topwind;
+    const double GESCHW_MAX = o.GESCHW_MAX;
+    const double Frund = c.Frund;
+    const float DTIME = c.DTIME;
+    const int MaxProgCellCount = st.vcff;
+    const int IterationStepsMin = p->iteration_steps_min, IterationStepsMax = p->iteration_steps_max;
+    int IterationLoops = 1;
+    float DeltaUMax = 0, DeltaFinish = 0, DeltaFirst = 0;
+    double DeltaMean = 0;
 
     int iterations = 0;
     int n_hist = 0;
     bool converged = false;
     /* ------------------------------ SIMPLE loop (:584-1182) ------------------------------ */
     while (IterationLoops <= IterationStepsMax) {
-        boundary_conditions(st);
-
-        /* mass divergence; DPM = 0 on the prognostic levels (:723-758) */
-        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
-        for (int i = i_lo; i < i_hi; ++i) {
-            for (int j = 2; j < NJJ; ++j) {
-                if (st.advdom(i, j) != 1) continue;
-                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
-                const float *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
-                const float *UKip = st.col(st.uk, i + 1, j), *VKjp = st.col(st.vk, i, j + 1);
-                float *DIV_L = st.col(st.div, i, j), *DPM_L = st.col(st.dpm, i, j);
-                for (int k = KK + 1; k <= VI; ++k) {
-                    if (k > KK + 1)
-                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] +
-                                   (WK_L[k] - WK_L[k + 1]) * AREAxy;
-                    else
-                        DIV_L[k] = (UK_L[k] - UKip[k]) * DYK * DZK[k] + (VK_L[k] - VKjp[k]) * DXK * DZK[k] -
-                                   WK_L[k + 1] * AREAxy;
-                    DPM_L[k] = 0;
-                }
-            }
-        }
-        });
-
-        /* sweep direction (:770-802) */
-        int IS = 1, JS = 1;
-        if (IterationLoops % 4 == 0) { IS = -1; JS = 1; }
-        else if (IterationLoops % 4 == 1) { IS = -1; JS = -1; }
-        else if (IterationLoops % 4 == 2) { IS = 1; JS = -1; }
-
-        /* pressure correction, vertical TDMA per column, rows in order (:804-901) */
-        DeltaUMax = 0;
-        for_chunks(2, NJJ, 1, [&](int j1_lo, int j1_hi) {
-            std::vector<float> PIMP(st.nk2), QIMP(st.nk2);
-            float DeltaUMaxRows = 0;
-            for (int j1 = j1_lo; j1 < j1_hi; ++j1) {
-                std::fill(PIMP.begin(), PIMP.end(), 0.0f);   /* new float[NKK + 2] per row */
-                std::fill(QIMP.begin(), QIMP.end(), 0.0f);
-                float DeltaUMaxIntern = 0;
-                const int j = (JS == -1) ? NJJ - j1 + 1 : j1;
-                for (int i1 = 2; i1 <= NII - 1; ++i1) {
-                    const int i = (IS == -1) ? NII - i1 + 1 : i1;
-                    if (st.advdom(i, j) != 1) continue;
-                    const float *DIV_L = st.col(st.div, i, j);
-                    float *DPM_L = st.col(st.dpm, i, j);
-                    const float *DPMim = st.col(st.dpm, i - 1, j), *DPMip = st.col(st.dpm, i + 1, j);
-                    const float *DPMjm = st.col(st.dpm, i, j - 1), *DPMjp = st.col(st.dpm, i, j + 1);
-                    float *DPMNEW_L = st.col(st.dpmnew, i, j);
-                    const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
-                    for (int k = VI; k > KK; --k) {
-                        float DIM = DIV_L[k] / DTIME + (DPMim[k] + DPMip[k]) / DXK * DYK * DZK[k] +
-                                    (DPMjm[k] - DPMjp[k]) / DYK * DXK * DZK[k];
-                        float APP = 2.0f * (DYK * DZK[k] / DXK + DXK * DZK[k] / DYK + AREAxy / DZK[k]);
-                        float ABP = (k > 1) ? AREAxy / (0.5f * (DZK[k - 1] + DZK[k])) : AREAxy / DZK[k];
-                        float ATP = AREAxy / (0.5f * (DZK[k + 1] + DZK[k]));
-                        float TERMP = 1 / (APP - ATP * PIMP[k + 1]);
-                        PIMP[k] = ABP * TERMP;
-                        QIMP[k] = (ATP * QIMP[k + 1] + DIM) * TERMP;
-                    }
-                    for (int k = KK + 1; k <= VI; ++k) {
-                        float temp = PIMP[k] * DPM_L[k - 1] + QIMP[k];
-                        DeltaUMaxIntern = (float)net_maxd((double)DeltaUMaxIntern,
-                            std::fabs((double)DPM_L[k] - quant((double)temp, Frund, quantise)));
-                        DPM_L[k] = temp;
-                        DPMNEW_L[k] += relaxp * DPM_L[k];
-                    }
-                }
-                if (DeltaUMaxIntern > DeltaUMaxRows) DeltaUMaxRows = DeltaUMaxIntern;
-            }
-            std::lock_guard<std::mutex> lk(delta_mutex);
-            if (DeltaUMaxRows > DeltaUMax) DeltaUMax = DeltaUMaxRows;
-        });
-
-        /* velocity correction with Frund quantisation in double (:904-949) */
-        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
-        for (int i = i_lo; i < i_hi; ++i) {
-            for (int j = 2; j <= NJJ - 1; ++j) {
-                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
-                const float *DPMim = st.col(st.dpm, i - 1, j), *DPMjm = st.col(st.dpm, i, j - 1);
-                const float *DPM_L = st.col(st.dpm, i, j);
-                float *UK_L = st.col(st.uk, i, j), *VK_L = st.col(st.vk, i, j), *WK_L = st.col(st.wk, i, j);
-                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
-                const int KKim = st.kkart(i - 1, j), KKjm = st.kkart(i, j - 1);
-                for (int k = 1; k <= VI; ++k) {
-                    const float d = DPM_L[k];
-                    if (i > 2 && KK < k && KKim < k)
-                        UK_L[k] = (float)quant((double)(UK_L[k] + (DPMim[k] - d) / DXK * DTIME), Frund, quantise);
-                    if (j > 2 && KK < k && KKjm < k)
-                        VK_L[k] = (float)quant((double)(VK_L[k] + (DPMjm[k] - d) / DYK * DTIME), Frund, quantise);
-                    if (KK + 1 < k)
-                        WK_L[k] = (float)quant((double)(WK_L[k] + (DPM_L[k - 1] - d) / (DZK[k] + DZK[k - 1]) * 2 * DTIME),
-                                               Frund, quantise);
-                    else
-                        WK_L[k] = 0;
-                }
-            }
-        }
-        });
-
-        /* staggered -> cell-centre averages and border copies (:958-1039) */
-        for_chunks(2, NII, slab_chunk(NII), [&](int i_lo, int i_hi) {
-        for (int i = i_lo; i < i_hi; ++i) {
-            for (int j = 2; j <= NJJ - 1; ++j) {
-                if (!(st.advdom(i, j) == 1 || st.advdom(i - 1, j) == 1 || st.advdom(i, j - 1) == 1)) continue;
-                const float *UK_L = st.col(st.uk, i, j), *UKip = st.col(st.uk, i + 1, j);
-                const float *VK_L = st.col(st.vk, i, j), *VKjp = st.col(st.vk, i, j + 1);
-                const float *WK_L = st.col(st.wk, i, j);
-                float *UKS_L = st.col(st.uks, i, j), *VKS_L = st.col(st.vks, i, j), *WKS_L = st.col(st.wks, i, j);
-                const int KK = st.kkart(i, j), VI = st.vert_index[st.i2(i, j)];
-                int KSTART = 1;
-                if (st.cutk(i, j) == 0) KSTART = KK + 1;
-                for (int k = KSTART; k <= VI; ++k) {
-                    if (KK < k) {
-                        UKS_L[k] = 0.5f * (UK_L[k] + UKip[k]);
-                        VKS_L[k] = 0.5f * (VK_L[k] + VKjp[k]);
-                    }
-                    if (KK + 1 < k) WKS_L[k] = 0.5f * (WK_L[k] + WK_L[k + 1]);
-                }
-                if (j == 2) {
-                    float *UKS1 = st.col(st.uks, i, 1);
-                    for (int k = KSTART; k <= VI; ++k) UKS1[k] = UKS_L[k];
-                }
-                if (j == NJJ - 1 && st.advdom(i, NJJ) == 1) {
-                    float *UKSN = st.col(st.uks, i, NJJ);
-                    for (int k = KSTART; k <= VI; ++k) UKSN[k] = UKS_L[k];
-                }
-            }
-        }
-        });
-        for (int j = 2; j < NJJ; ++j) {
-            if (st.advdom(1, j) == 1) {
-                float *a = st.col(st.vks, 1, j); const float *b = st.col(st.vks, 2, j);
-                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
-            }
-            if (st.advdom(NII - 1, j) == 1) {
-                float *a = st.col(st.vks, NII, j); const float *b = st.col(st.vks, NII - 1, j);
-                for (int k = 0; k <= NKK; ++k) a[k] = b[k];
-            }
-        }
-
-        /* momentum equations (:1049-1137), deterministic order */
-        if (model == 0) {
-            u_mom_nd(st, IS, JS, AREAxy, UG, relax);
-            v_mom_nd(st, IS, JS, AREAxy, VG, relax);
-            w_mom_nd(st, IS, JS, AREAxy, relax);
-        } else if (model == 1) {
-            u_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, UG, relax);
-            v_mom_ml(st, p->simd_width, -IS, -JS, VISHMIN, AREAxy, VG, relax);
-            w_mom_ml(st, p->simd_width, IS, JS, VISHMIN, AREAxy, relax);
-        } else {
-            u_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, UG, relax);
-            v_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, VG, relax);
-            w_mom_ke(st, IS, JS, Cmueh, VISHMIN, AREAxy, relax);
-            tke_ke(st, IS, JS, Cmueh, Ceps, Ceps1, Ceps2, VISHMIN, VISVMIN, AREAxy, building_Z0, relax,
-                   Ustern_factorX);
-        }
+        DeltaUMax = simple_iteration(st, c, IterationLoops);
         iterations++;
         if (stats && stats->trace_delta_umax && iterations <= stats->trace_capacity)
             stats->trace_delta_umax[iterations - 1] = DeltaUMax;
@@ -593,5 +688,203 @@ extern "C" int oracle_solve(const gral_params *p, const gral_static *s, gral_fie
         stats->topwind = topwind; stats->dtime = DTIME; stats->frund = Frund;
         stats->last_delta_umax = DeltaUMax;
     }
+    return GRAL_OK;
+}
+
+/* ============================================================================================
+ * FP64 twin of the model-1 path and its reverse-mode differentiation (TEST INFRASTRUCTURE).
+ *
+ * The differentiated configuration of the library's adjoint: turbulence model 1, Vector<float>
+ * parity width 8, no Frund rounding (its derivative is zero almost everywhere), a fixed number of
+ * SIMPLE iterations, and the set-up's scalars (topwind, DTIME, AP0, UG, VG, help terms) held at the
+ * values the reference set-up computes from the reference initial fields `f_ref` -- constants of
+ * the differentiated map.  The twin runs the oracle's own operations (simple_iteration,
+ * initial_staggered, zero_in_buildings, the model-1 sweeps) in double, or on the tape type of
+ * oracle_ad.h for the gradient; instantiated for float it is the oracle itself.
+ * ============================================================================================ */
+
+thread_local Tape *oracle::g_tape = nullptr;
+
+namespace {
+
+constexpr int kTwinFields = 7;   /* uk, vk, wk, uks, vks, wks, dpmnew: the state between iterations */
+
+int twin_validate(const gral_params *p, int iterations) {
+    if (!p || p->turbulence_model != 1 || p->simd_width != 8 || p->quantise != 0 || iterations < 1)
+        return GRAL_EINVAL;
+    return GRAL_OK;
+}
+
+/* The float set-up on a copy of the reference fields: constants and per-column tables. */
+int twin_setup(const gral_params *p, const gral_static *s, const gral_fields *f_ref, State &st0, SetupOut &o,
+               std::vector<float> &scratch) {
+    const size_t n3 = (size_t)(p->nii + 2) * (p->njj + 2) * (p->nkk + 2);
+    scratch.assign(3 * n3, 0.f);
+    std::memcpy(scratch.data(), f_ref->uk, n3 * sizeof(float));
+    std::memcpy(scratch.data() + n3, f_ref->vk, n3 * sizeof(float));
+    std::memcpy(scratch.data() + 2 * n3, f_ref->wk, n3 * sizeof(float));
+    gral_fields g{scratch.data(), scratch.data() + n3, scratch.data() + 2 * n3, nullptr, nullptr};
+    return setup_solve(st0, p, s, &g, o);
+}
+
+/* A T state on the grid of st0 with its tables, fields from the given arrays. */
+template <class T>
+void twin_state(const State &st0, StateT<T> &st, std::vector<T> &fields, const T *veg) {
+    st.nii = st0.nii; st.njj = st0.njj; st.nkk = st0.nkk; st.kadvmax = st0.kadvmax; st.vcff = st0.vcff;
+    st.ni2 = st0.ni2; st.nj2 = st0.nj2; st.nk2 = st0.nk2; st.dxk = st0.dxk; st.dyk = st0.dyk;
+    st.p = st0.p; st.s = st0.s;
+    const size_t n3 = (size_t)st.ni2 * st.nj2 * st.nk2;
+    st.uk = fields.data(); st.vk = fields.data() + n3; st.wk = fields.data() + 2 * n3;
+    st.turb = nullptr; st.tdiss = nullptr;
+    st.uks.assign(n3, T(0.0)); st.vks.assign(n3, T(0.0)); st.wks.assign(n3, T(0.0));
+    st.dpm.assign(n3, T(0.0)); st.dpmnew.assign(n3, T(0.0)); st.div.assign(n3, T(0.0));
+    st.vert_index = st0.vert_index;
+    st.ustern_terrain = st0.ustern_terrain; st.ustern_obst = st0.ustern_obst;
+    st.ap0 = st0.ap0;
+    st.veg_t = veg;
+}
+
+template <class T>
+T *twin_field(StateT<T> &st, int q) {
+    switch (q) {
+        case 0: return st.uk;
+        case 1: return st.vk;
+        case 2: return st.wk;
+        case 3: return st.uks.data();
+        case 4: return st.vks.data();
+        case 5: return st.wks.data();
+        default: return st.dpmnew.data();
+    }
+}
+
+}  // namespace
+
+/* FP64 twin forward: `iterations` SIMPLE iterations from the initial fields uk0/vk0/wk0 (double,
+ * host layout) with vegetation density veg (double [NII+2][NJJ+2][NKK+2], or NULL for the static
+ * VEG), the set-up's scalars taken from f_ref.  Writes the final fields to uk/vk/wk. */
+extern "C" int oracle_twin_forward(const gral_params *p, const gral_static *s, const gral_fields *f_ref,
+                                   const double *uk0, const double *vk0, const double *wk0, const double *veg,
+                                   int iterations, double *uk, double *vk, double *wk) {
+    int rc = twin_validate(p, iterations);
+    if (rc != GRAL_OK) return rc;
+    State st0;
+    SetupOut o;
+    std::vector<float> scratch;
+    rc = twin_setup(p, s, f_ref, st0, o, scratch);
+    if (rc != GRAL_OK) return rc;
+    const size_t n3 = (size_t)st0.ni2 * st0.nj2 * st0.nk2;
+    std::vector<double> vegd(n3, 0.0);
+    if (veg) std::memcpy(vegd.data(), veg, n3 * sizeof(double));
+    else if (s->veg) for (size_t q = 0; q < n3; ++q) vegd[q] = s->veg[q];
+    std::vector<double> fields(3 * n3);
+    std::memcpy(fields.data(), uk0, n3 * sizeof(double));
+    std::memcpy(fields.data() + n3, vk0, n3 * sizeof(double));
+    std::memcpy(fields.data() + 2 * n3, wk0, n3 * sizeof(double));
+    StateT<double> st;
+    twin_state(st0, st, fields, vegd.data());
+    initial_staggered(st);
+    zero_in_buildings(st, 1);
+    for (int it = 1; it <= iterations; ++it) simple_iteration(st, o.c, it);
+    std::memcpy(uk, st.uk, n3 * sizeof(double));
+    std::memcpy(vk, st.vk, n3 * sizeof(double));
+    std::memcpy(wk, st.wk, n3 * sizeof(double));
+    return GRAL_OK;
+}
+
+/* FP64 reverse-mode gradient of the twin: given the cotangents g_uk/g_vk/g_wk of the final fields
+ * (dJ/dUK etc.), writes dJ/d(initial fields) to d_uk0/d_vk0/d_wk0 and dJ/dVEG to d_veg (all double,
+ * host layout).  The forward is recorded on the tape one iteration at a time from states kept by a
+ * double forward pass (one checkpoint per iteration), then differentiated backwards. */
+extern "C" int oracle_twin_vjp(const gral_params *p, const gral_static *s, const gral_fields *f_ref,
+                               const double *uk0, const double *vk0, const double *wk0, const double *veg,
+                               int iterations, const double *g_uk, const double *g_vk, const double *g_wk,
+                               double *d_uk0, double *d_vk0, double *d_wk0, double *d_veg) {
+    int rc = twin_validate(p, iterations);
+    if (rc != GRAL_OK) return rc;
+    State st0;
+    SetupOut o;
+    std::vector<float> scratch;
+    rc = twin_setup(p, s, f_ref, st0, o, scratch);
+    if (rc != GRAL_OK) return rc;
+    const size_t n3 = (size_t)st0.ni2 * st0.nj2 * st0.nk2;
+    std::vector<double> vegd(n3, 0.0);
+    if (veg) std::memcpy(vegd.data(), veg, n3 * sizeof(double));
+    else if (s->veg) for (size_t q = 0; q < n3; ++q) vegd[q] = s->veg[q];
+
+    /* double forward keeping the state at the start of every iteration */
+    std::vector<double> fields(3 * n3);
+    std::memcpy(fields.data(), uk0, n3 * sizeof(double));
+    std::memcpy(fields.data() + n3, vk0, n3 * sizeof(double));
+    std::memcpy(fields.data() + 2 * n3, wk0, n3 * sizeof(double));
+    StateT<double> st;
+    twin_state(st0, st, fields, vegd.data());
+    initial_staggered(st);
+    zero_in_buildings(st, 1);
+    std::vector<std::vector<double>> keep((size_t)iterations, std::vector<double>(kTwinFields * n3));
+    for (int it = 1; it <= iterations; ++it) {
+        for (int q = 0; q < kTwinFields; ++q)
+            std::memcpy(keep[it - 1].data() + q * n3, twin_field(st, q), n3 * sizeof(double));
+        simple_iteration(st, o.c, it);
+    }
+
+    /* cotangents of the state, seeded with those of the final fields */
+    std::vector<double> lam(kTwinFields * n3, 0.0), lveg(n3, 0.0);
+    std::memcpy(lam.data(), g_uk, n3 * sizeof(double));
+    std::memcpy(lam.data() + n3, g_vk, n3 * sizeof(double));
+    std::memcpy(lam.data() + 2 * n3, g_wk, n3 * sizeof(double));
+
+    Tape tape;
+    g_tape = &tape;
+    std::vector<AD> adf(3 * n3), adveg(n3);
+    std::vector<int32_t> leaf(kTwinFields * n3), vleaf(n3);
+    std::vector<double> adj;
+    for (int it = iterations; it >= 1; --it) {
+        tape.clear();
+        const double *kp = keep[it - 1].data();
+        for (size_t q = 0; q < 3 * n3; ++q) { adf[q] = AD::input(kp[q]); leaf[q] = adf[q].i; }
+        for (size_t q = 0; q < n3; ++q) { adveg[q] = AD::input(vegd[q]); vleaf[q] = adveg[q].i; }
+        StateT<AD> sa;
+        twin_state(st0, sa, adf, adveg.data());
+        for (int q = 3; q < kTwinFields; ++q) {
+            AD *fld = twin_field(sa, q);
+            for (size_t c = 0; c < n3; ++c) { fld[c] = AD::input(kp[q * n3 + c]); leaf[q * n3 + c] = fld[c].i; }
+        }
+        simple_iteration(sa, o.c, it);
+        adj.assign(tape.nodes.size(), 0.0);
+        for (int q = 0; q < kTwinFields; ++q) {
+            const AD *fld = twin_field(sa, q);
+            for (size_t c = 0; c < n3; ++c)
+                if (fld[c].i >= 0) adj[(size_t)fld[c].i] += lam[q * n3 + c];
+        }
+        tape.reverse(adj);
+        for (size_t q = 0; q < (size_t)kTwinFields * n3; ++q) lam[q] = adj[(size_t)leaf[q]];
+        for (size_t q = 0; q < n3; ++q) lveg[q] += adj[(size_t)vleaf[q]];
+    }
+
+    /* the set-up: initial staggered velocities and zeroing inside buildings */
+    tape.clear();
+    for (size_t q = 0; q < 3 * n3; ++q) {
+        const double v = (q < n3) ? uk0[q] : (q < 2 * n3 ? vk0[q - n3] : wk0[q - 2 * n3]);
+        adf[q] = AD::input(v);
+        leaf[q] = adf[q].i;
+    }
+    StateT<AD> sa;
+    twin_state(st0, sa, adf, adveg.data());
+    initial_staggered(sa);
+    zero_in_buildings(sa, 1);
+    adj.assign(tape.nodes.size(), 0.0);
+    for (int q = 0; q < kTwinFields; ++q) {
+        const AD *fld = twin_field(sa, q);
+        for (size_t c = 0; c < n3; ++c)
+            if (fld[c].i >= 0) adj[(size_t)fld[c].i] += lam[q * n3 + c];
+    }
+    tape.reverse(adj);
+    for (size_t c = 0; c < n3; ++c) {
+        d_uk0[c] = adj[(size_t)leaf[c]];
+        d_vk0[c] = adj[(size_t)leaf[n3 + c]];
+        d_wk0[c] = adj[(size_t)leaf[2 * n3 + c]];
+        d_veg[c] = lveg[c];
+    }
+    g_tape = nullptr;
     return GRAL_OK;
 }

@@ -92,3 +92,57 @@ def threads_used() -> int:
     h = lib_threaded()
     h.oracle_threads.restype = C.c_int
     return int(h.oracle_threads())
+
+
+def _bind_twin(h):
+    D = C.POINTER(C.c_double)
+    if getattr(h, "_twin_bound", False):
+        return h
+    h.oracle_twin_forward.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralFields),
+                                      D, D, D, D, C.c_int, D, D, D]
+    h.oracle_twin_forward.restype = C.c_int
+    h.oracle_twin_vjp.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralFields),
+                                  D, D, D, D, C.c_int, D, D, D, D, D, D, D]
+    h.oracle_twin_vjp.restype = C.c_int
+    h._twin_bound = True
+    return h
+
+
+def _dptr(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def twin_forward(params: dict, static: StaticArrays, f_ref: FieldArrays, x0, veg, iterations: int):
+    """FP64 twin of the model-1 path (no Frund rounding, parity width 8): `iterations` SIMPLE
+    iterations from the initial fields x0 = (uk0, vk0, wk0) (float64, host layout) with vegetation
+    density veg (float64, host layout, or None for the static VEG); the set-up's scalars are those
+    of the reference fields f_ref.  Returns the final (uk, vk, wk) in float64."""
+    p = params_to_c(params)
+    s = static.to_c()
+    fr = f_ref.to_c()
+    uk0, vk0, wk0 = (np.ascontiguousarray(a, np.float64) for a in x0)
+    vg = None if veg is None else np.ascontiguousarray(veg, np.float64)
+    out = [np.zeros_like(uk0) for _ in range(3)]
+    rc = _bind_twin(lib()).oracle_twin_forward(C.byref(p), C.byref(s), C.byref(fr), _dptr(uk0), _dptr(vk0),
+                                               _dptr(wk0), _dptr(vg), int(iterations), *(_dptr(o) for o in out))
+    if rc != GRAL_OK:
+        raise RuntimeError(f"oracle_twin_forward failed: {STATUS_NAMES.get(rc, rc)}")
+    return tuple(out)
+
+
+def twin_vjp(params: dict, static: StaticArrays, f_ref: FieldArrays, x0, veg, iterations: int, g):
+    """Reverse-mode gradient of the FP64 twin (tape differentiation of the oracle's operations):
+    g = (dJ/duk, dJ/dvk, dJ/dwk) of the final fields; returns (dJ/duk0, dJ/dvk0, dJ/dwk0, dJ/dveg)."""
+    p = params_to_c(params)
+    s = static.to_c()
+    fr = f_ref.to_c()
+    uk0, vk0, wk0 = (np.ascontiguousarray(a, np.float64) for a in x0)
+    vg = None if veg is None else np.ascontiguousarray(veg, np.float64)
+    gu, gv, gw = (np.ascontiguousarray(a, np.float64) for a in g)
+    out = [np.zeros_like(uk0) for _ in range(4)]
+    rc = _bind_twin(lib()).oracle_twin_vjp(C.byref(p), C.byref(s), C.byref(fr), _dptr(uk0), _dptr(vk0), _dptr(wk0),
+                                           _dptr(vg), int(iterations), _dptr(gu), _dptr(gv), _dptr(gw),
+                                           *(_dptr(o) for o in out))
+    if rc != GRAL_OK:
+        raise RuntimeError(f"oracle_twin_vjp failed: {STATUS_NAMES.get(rc, rc)}")
+    return tuple(out)

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
+#include <type_traits>
 #include <vector>
 #ifdef ORACLE_THREADS
 #include <atomic>
@@ -88,9 +89,25 @@ static inline double net_maxd(double a, double b) {
 }
 /* Program.FloatMax (ProgramFunctions.cs:768): val1 > val2 ? val1 : val2. */
 static inline float float_max(float a, float b) { return (a > b) ? a : b; }
-/* Vector.Max / Vector.Min on .NET 8 x64 (maxps / minps): left > right ? left : right. */
+/* Vector.Max / Vector.Min on .NET 8 x64 (maxps / minps): left > right ? left : right.  The double
+ * overloads serve the FP64 twin of the model-1 path (the same operations in double). */
 static inline float vmax(float a, float b) { return (a > b) ? a : b; }
 static inline float vmin(float a, float b) { return (a < b) ? a : b; }
+static inline double vmax(double a, double b) { return (a > b) ? a : b; }
+static inline double vmin(double a, double b) { return (a < b) ? a : b; }
+static inline double vmax(double a, float b) { return vmax(a, (double)b); }
+static inline double vmax(float a, double b) { return vmax((double)a, b); }
+static inline double vmin(double a, float b) { return vmin(a, (double)b); }
+static inline double vmin(float a, double b) { return vmin((double)a, b); }
+static inline float osqrt(float x) { return std::sqrt(x); }
+static inline double osqrt(double x) { return std::sqrt(x); }
+static inline float ofabs(float x) { return std::fabs(x); }
+static inline double ofabs(double x) { return std::fabs(x); }
+static inline float ofma(float a, float b, float c) { return std::fma(a, b, c); }
+template <class A, class B, class C,
+          class = typename std::enable_if<std::is_arithmetic<A>::value && std::is_arithmetic<B>::value &&
+                                          std::is_arithmetic<C>::value>::type>
+static inline double ofma(A a, B b, C c) { return std::fma((double)a, (double)b, (double)c); }
 
 /* Program.ConvToInt(double) (ProgramFunctions.cs:798): round half away from zero through a
  * truncating (int) cast.  An out-of-range or NaN operand converts to int.MinValue, as the x64
@@ -107,19 +124,25 @@ static inline float pow3f(float x) { return x * x * x; }
 static inline float pow5f(float x) { return x * x * x * x * x; }
 static inline double pow5d(double x) { return x * x * x * x * x; }
 
-/* ---- solver state: every 3-D array is [NII+2][NJJ+2][NKK+2], k fastest ---- */
-struct State {
+/* ---- solver state: every 3-D array is [NII+2][NJJ+2][NKK+2], k fastest ----
+ * T is the type of the flow fields: float for the oracle proper; double for the FP64 twin of the
+ * model-1 path and the tape type of its reverse-mode differentiation (oracle/adjoint.cpp), which
+ * run the same operations on the same grid constants (float). */
+template <class T>
+struct StateT {
     int nii, njj, nkk, kadvmax, vcff;
     int ni2, nj2, nk2;
     float dxk, dyk;
     const gral_params *p;
     const gral_static *s;
-    float *uk, *vk, *wk, *turb, *tdiss;           /* caller fields */
-    std::vector<float> uks, vks, wks, dpm, dpmnew, div;
+    T *uk, *vk, *wk;                               /* flow fields */
+    float *turb, *tdiss;                           /* k-eps fields (model 2, float only) */
+    std::vector<T> uks, vks, wks, dpm, dpmnew, div;
     std::vector<float> turb_own, tdiss_own;        /* used when model == 1 (never read) */
     std::vector<int> vert_index;                   /* Program.VerticalIndex [NII+2][NJJ+2] */
     std::vector<float> ustern_terrain, ustern_obst;/* UsternTerrain/ObstaclesHelpterm */
     std::vector<float> ap0;                        /* PrognosticFlowfield.AP0 */
+    const T *veg_t = nullptr;                      /* VEG as T (null: s->veg, float only) */
 
     size_t i3(int i, int j, int k) const { return ((size_t)i * nj2 + j) * nk2 + k; }
     size_t i2(int i, int j) const { return (size_t)i * nj2 + j; }
@@ -131,15 +154,27 @@ struct State {
     bool has_veg(int i, int j) const { return s->veg && s->veg_mask && s->veg_mask[i2(i, j)]; }
     float *col(float *a, int i, int j) const { return a + i3(i, j, 0); }
     float *col(std::vector<float> &a, int i, int j) { return a.data() + i3(i, j, 0); }
-    const float *vegcol(int i, int j) const { return s->veg + i3(i, j, 0); }
+    template <class U, class = typename std::enable_if<!std::is_same<U, float>::value>::type>
+    U *col(U *a, int i, int j) const { return a + i3(i, j, 0); }
+    template <class U, class = typename std::enable_if<!std::is_same<U, float>::value>::type>
+    U *col(std::vector<U> &a, int i, int j) { return a.data() + i3(i, j, 0); }
+    const T *vegcol(int i, int j) const {
+        if constexpr (std::is_same<T, float>::value) return veg_t ? veg_t + i3(i, j, 0) : s->veg + i3(i, j, 0);
+        else return veg_t + i3(i, j, 0);   /* the twin always supplies VEG as T */
+    }
     const float *dzk() const { return s->dzk; }
     const float *hokart() const { return s->hokart; }
 };
+using State = StateT<float>;
 
-/* Momentum routines (one translation unit each model family). */
-void u_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float UG, float relax);
-void v_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float VG, float relax);
-void w_mom_ml(State &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float relax);
+/* Momentum routines (one translation unit each model family).  The model-1 routines are
+ * instantiated for float (the oracle), double and the tape type (oracle/adjoint.cpp). */
+template <class T>
+void u_mom_ml(StateT<T> &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float UG, float relax);
+template <class T>
+void v_mom_ml(StateT<T> &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float VG, float relax);
+template <class T>
+void w_mom_ml(StateT<T> &st, int simd, int IS, int JS, float VISHMIN, float AREAxy, float relax);
 void u_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float UG, float relax);
 void v_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float VG, float relax);
 void w_mom_ke(State &st, int IS, int JS, float Cmueh, float VISHMIN, float AREAxy, float relax);
