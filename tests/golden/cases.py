@@ -3,7 +3,9 @@ Vector<float> width 8 and the Vector512 width 16).
 
 Inputs are rebuilt from ``gral_b200.prep`` with the seeds stated here, so only outputs are stored:
 ``<name>.npz`` (fields, DeltaUMax trace, statistics) for the small grids and SHA-256 digests in
-``checksums.json`` for the full-size grids (the 100x100x162 cube and the 400x400x63 city).  The
+``checksums.json`` for the full-size grids (the 100x100x162 cube and the 400x400x63 city, also at
+the benchmark lengths of 100 and 500 iterations with the reference's stop rule, and eight
+situations of the 144-situation weather set).  The
 outputs were written by ``make_golden.py`` from the CPU oracle; ``MANIFEST.json`` records the
 oracle sources' digests and the reference version the oracle restates.
 """
@@ -45,7 +47,19 @@ CASES: Dict[str, tuple] = {
     "m1_diag_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, dict(post_diagnostic=1), "sha"),
     "m1w16_cube_100": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 3, dict(simd_width=16), "sha"),
     "m1_city_400": ("city", dict(), [(225.0, 2.0, 0.5, 0.3)], 1, 2, {}, "sha"),
+    # the benchmark configurations at their own length, with the reference's stop rule (_delta <
+    # 0.012 tested every 100 iterations from IterationStepsMin = 100 on)
+    "m1_cube_full": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 100, {}, "sha"),
+    "m1_cube_conv500": ("cube", dict(), [(270.0, 3.0, 0.2, 0.3)], 1, 500, dict(iter_min=100), "sha"),
+    "m1_city_full": ("city", dict(), [(225.0, 2.0, 0.5, 0.3)], 1, 500, dict(iter_min=100), "sha"),
+    # eight situations of the 144-situation weather set on the production grid (all four speeds,
+    # directions 0..350 deg, seeded stability), each stopping at its own iteration
+    "m1_city_weather8": ("city", dict(), "weather:1,22,43,64,87,106,125,140", 1, 500, dict(iter_min=100), "sha"),
 }
+
+# cases whose oracle run takes minutes (500 iterations on the production grid): their digests are
+# written by make_golden.py and checked against the GPU only; the CPU suite re-runs the others
+LONG = {"m1_cube_conv500", "m1_city_full", "m1_city_weather8"}
 
 FIELDS = ("uk", "vk", "wk", "turb", "tdiss")
 STAT_KEYS = ("iterations", "iteration_loops", "converged", "convergence_problem", "delta_first",
@@ -64,13 +78,22 @@ def domain(name: str):
     raise KeyError(kind)
 
 
+def situations(name: str) -> List[prep.Situation]:
+    """The situations of a case: (direction, speed, z0, u*) tuples, or "weather:<indices>" naming
+    members of prep.weather_situations()."""
+    sits = CASES[name][2]
+    if isinstance(sits, str):
+        pool = prep.weather_situations()
+        return [pool[int(q)] for q in sits.split(":", 1)[1].split(",")]
+    return [prep.Situation(direction_deg=d, speed_10m=v, z0=z0, ustar=us) for d, v, z0, us in sits]
+
+
 def build(name: str):
     """(domain, [params], [initial fields]) of a case."""
     _, _, sits, model, iters, pkw, _ = CASES[name]
     dom = domain(name)
     ps, fs = [], []
-    for d, v, z0, us in sits:
-        sit = prep.Situation(direction_deg=d, speed_10m=v, z0=z0, ustar=us)
+    for sit in situations(name):
         ps.append(dom.params(sit, model=model, iterations=iters, **pkw))
         fs.append(prep.initial_fields(dom, sit, model))
     return dom, ps, fs

@@ -4,6 +4,10 @@
     python tests/golden/make_golden.py m1_small_s0
     GRAL_REFERENCE_SRC=<GRAL checkout>/src python tests/golden/make_golden.py   # also hash the reference
 
+Situations run in parallel worker processes (GOLDEN_WORKERS, default: every CPU), each one the
+oracle's serial deterministic solve; the 500-iteration production-grid cases take about 7 minutes
+of one core per situation.
+
 The oracle is the deterministic restatement of GRAL's prognostic solve under ``oracle/``; the
 C# reference cannot run in this environment, so these files pin the oracle (and through it the
 GPU path) against regressions, not against the reference itself.  The manifest records the
@@ -42,14 +46,31 @@ def sha_file(p: str) -> str:
         return hashlib.sha256(fh.read()).hexdigest()
 
 
-def run_case(name: str):
+def _solve_one(job):
+    """One situation of a case in a worker process: (fields, stats, trace)."""
+    name, b = job
     dom, ps, fs = G.build(name)
-    stats, traces = [], []
-    for p, f in zip(ps, fs):
-        tr = np.zeros(max(p["iteration_steps_max"], 1), np.float32)
-        stats.append(O.solve(p, dom.static, f, tr))
-        traces.append(tr)
-    return fs, stats, traces
+    tr = np.zeros(max(ps[b]["iteration_steps_max"], 1), np.float32)
+    st = O.solve(ps[b], dom.static, fs[b], tr)
+    return fs[b], st, tr
+
+
+def run_cases(names, workers: int):
+    """Outputs of every situation of every case; situations run in `workers` processes (spawned,
+    so nothing is inherited) and each is the oracle's serial deterministic solve."""
+    import multiprocessing as mp
+    jobs = [(n, b) for n in names for b in range(len(G.situations(n)))]
+    if workers > 1 and len(jobs) > 1:
+        with mp.get_context("spawn").Pool(min(workers, len(jobs))) as pool:
+            res = pool.map(_solve_one, jobs, chunksize=1)
+    else:
+        res = [_solve_one(j) for j in jobs]
+    out = {n: ([], [], []) for n in names}
+    for (n, _), (f, st, tr) in zip(jobs, res):
+        out[n][0].append(f)
+        out[n][1].append(st)
+        out[n][2].append(tr)
+    return out
 
 
 def main(names):
@@ -57,8 +78,9 @@ def main(names):
     path = os.path.join(HERE, "checksums.json")
     if os.path.exists(path):
         sha = G.load_sha()
+    results = run_cases(names, int(os.environ.get("GOLDEN_WORKERS", os.cpu_count() or 1)))
     for name in names:
-        fs, stats, traces = run_case(name)
+        fs, stats, traces = results[name]
         if G.storage(name) == "npz":
             arrs = {}
             for b, f in enumerate(fs):

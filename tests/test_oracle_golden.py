@@ -39,7 +39,7 @@ def test_oracle_matches_golden_arrays(name):
         assert G.stats_subset(stats[b]) == gs[b]
 
 
-@pytest.mark.parametrize("name", [n for n in G.CASES if G.storage(n) == "sha"])
+@pytest.mark.parametrize("name", [n for n in G.CASES if G.storage(n) == "sha" and n not in G.LONG])
 def test_oracle_matches_golden_digests(name):
     fs, stats, traces = run_oracle(name)
     assert G.outputs_sha(fs, stats, traces) == G.load_sha()[name]
@@ -49,6 +49,7 @@ def test_golden_covers_every_model_and_full_size_geometry():
     models = {G.CASES[n][3] for n in G.CASES}
     assert models == {0, 1, 2}
     assert {"m1_cube_100", "m1_city_400"} <= set(G.load_sha())
+    assert set(G.LONG) | {"m1_cube_full"} <= set(G.load_sha())
     for name in G.CASES:
         if G.storage(name) == "npz":
             assert os.path.exists(os.path.join(G.HERE, f"{name}.npz")), name
@@ -62,3 +63,18 @@ def test_golden_convergence_case_stops_at_cadence():
     assert st["converged"] == 1
     assert st["iterations"] % 100 == 0 and st["iterations"] < 400
     assert len(st["delta_history"]) == st["iterations"] // 100
+
+
+def test_golden_benchmark_lengths_and_stop_rule():
+    """The benchmark configurations at their own length: the 100x100 cube for 100 iterations and
+    for up to 500 with the reference's stop rule (0.012, tested every 100 iterations), the
+    production grid for 500, and eight situations of the weather set; the stop rule's decisions
+    are part of the digests (iterations, converged flag, residual history at 100, 200, ...)."""
+    sha = G.load_sha()
+    assert [x["stats"]["iterations"] for x in sha["m1_cube_full"]] == [100]
+    for name in ("m1_cube_conv500", "m1_city_full", "m1_city_weather8"):
+        for x in sha[name]:
+            st = x["stats"]
+            assert len(st["delta_history"]) == st["iterations"] // 100
+            assert st["converged"] == 1 or st["iterations"] == 500
+    assert len(sha["m1_city_weather8"]) == 8
