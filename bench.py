@@ -85,18 +85,8 @@ def workload(name: str, grid: int = 400):
 def batched_situations(n: int = 144, seed: int = 3):
     """36 directions (0-350 deg in 10-deg steps) x 4 speeds (0.5/1/2/4 m/s at 10 m), stability
     classes drawn from {stable, neutral, unstable} with a seeded generator; first n of them."""
-    import numpy as np
     from gral_b200 import prep
-    rng = np.random.default_rng(seed)
-    out = []
-    for d in range(36):
-        for sp in (0.5, 1.0, 2.0, 4.0):
-            cls = int(rng.integers(0, 3))
-            ob = {0: 50.0, 1: 1000.0, 2: -50.0}[cls]
-            pt = {0: 0.01, 1: 0.0, 2: -0.01}[cls]
-            out.append(prep.Situation(direction_deg=10.0 * d, speed_10m=sp, z0=0.5, ustar=0.1 * sp + 0.1,
-                                      obukhov=ob, potdtdz=pt))
-    return out[:n]
+    return prep.weather_situations(n, seed)
 
 
 def rank_situations(base_situation, batch: int, rank: int, world: int):

@@ -119,6 +119,13 @@ def _ptr(a: Optional[np.ndarray], ctype):
     return a.ctypes.data_as(C.POINTER(ctype))
 
 
+
+class GralVjpStats(C.Structure):
+    """gral_vjp_stats: device times of the adjoint's forward run, recomputation and reverse sweeps."""
+    _fields_ = [("iterations", C.c_int32), ("checkpoint_every", C.c_int32),
+                ("ms_forward", C.c_double), ("ms_recompute", C.c_double), ("ms_reverse", C.c_double),
+                ("ms_total", C.c_double)]
+
 @dataclass
 class StaticArrays:
     """Per-grid inputs (``gral_static``) as numpy arrays with the reference's index ranges."""

@@ -15,8 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgralprog.so")
-SOURCES = ["prog_host.cu", "prog_gs.cu", "prog_kernels.cu", "prog_gff.cu", "prog_prep.cu", "prog_wind.cu", "prog_runner.cu", "prog_noalloc.cu"]
-HEADERS = ["prog_common.cuh", "prog_ctx.cuh", "prog_kernels.cuh", "prog_level.cuh", "prog_gff.cuh", "prog_prep.cuh"]
+SOURCES = ["prog_host.cu", "prog_gs.cu", "prog_kernels.cu", "prog_gff.cu", "prog_prep.cu", "prog_wind.cu", "prog_runner.cu", "prog_noalloc.cu", "prog_adjoint.cu"]
+HEADERS = ["prog_common.cuh", "prog_ctx.cuh", "prog_kernels.cuh", "prog_level.cuh", "prog_gff.cuh", "prog_prep.cuh", "adj_level.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

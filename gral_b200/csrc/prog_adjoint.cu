@@ -1,0 +1,1244 @@
+// prog_adjoint.cu -- discrete adjoint (vector-Jacobian product) of the unrolled SIMPLE iterations
+// of one situation: gral_prog_vjp_forward and gral_prog_vjp.
+//
+// Differentiated configuration: turbulence model 1, Vector<float> parity width 8, no Frund
+// rounding (its derivative is zero almost everywhere), a fixed number of iterations.  The set-up's
+// scalars (topwind, DTIME, AP0, UG, VG, the wall-law help terms, Frund) are constants of the map.
+// Inputs of the map: the initial U, V, W fields and the vegetation density VEG; output: the final
+// U, V, W fields.
+//
+// The forward run keeps the state (UK, VK, WK, UKS, VKS, WKS, DPMNEW and the situation's loop
+// state) every `checkpoint_every` iterations.  The reverse pass walks the checkpoint segments from
+// the last: it restores the segment's checkpoint, recomputes its iterations with the solver's own
+// kernels while keeping, per iteration, the state after the staggered averages ("mid") and after
+// the W sweep ("end") and the branch taken by every lateral boundary copy, then reverses the
+// segment's iterations one by one.  Reversing one iteration (PrognosticFlowfield.cs:584-1137):
+//
+//   W, V, U momentum sweeps   reverse Gauss-Seidel wavefronts: a column waits for its two sweep
+//                             successors, reverses the relaxed back-substitution and the Thomas
+//                             recurrence (U-prognostic-microscale_1.cs:485-524) on lane 0, sends
+//                             the cotangents of its two predecessors' new values, releases its
+//                             flag, and then adds the per-level vector-Jacobian products of the
+//                             coefficient assembly (adj_level.cuh) to every other input;
+//   staggered averages        gathers (PrognosticFlowfield.cs:958-1039);
+//   velocity correction       a gather into DPM (PrognosticFlowfield.cs:904-949);
+//   pressure correction       a reverse wavefront of the transposed tridiagonal solves
+//                             (PrognosticFlowfield.cs:804-901), the row carry of Q included;
+//   divergence                a gather (PrognosticFlowfield.cs:723-758);
+//   boundary conditions       the copies reversed in reverse order (PrognosticFlowfield.cs:595-714).
+//
+// After the first iteration the set-up's staggered averages, border copies and zeroing inside
+// buildings (PrognosticFlowfield.cs:295-329, 410-432, 518-575) are reversed as well.  Cotangents
+// are accumulated with float atomics, so their summation order varies from run to run at the
+// level of float rounding.  Every wait is bounded like the forward's.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "adj_level.cuh"
+#include "prog_ctx.cuh"
+#include "prog_level.cuh"
+
+namespace gral {
+
+namespace {
+
+using namespace adj;
+
+constexpr int AW = 4;               // warps per block of the reverse sweeps
+constexpr int WL = 99;              // level marker of the wall-law inputs
+enum : int { FU = 0, FV, FW, FUS, FVS, FWS, FDP, FVEG, NLAM_IN };
+// cotangent fields: the eight input kinds above, then DPM, DIV and the pressure row-carry Q
+enum : int { L_DPM = NLAM_IN, L_DIV, L_QC, NLAM };
+constexpr int NKEEP = 10;           // per iteration: mid UK VK WK UKS VKS WKS DPMNEW, end UK VK WK
+constexpr int NCKPT = 7;            // checkpoint: UK VK WK UKS VKS WKS DPMNEW
+
+struct InDesc {
+    int8_t f, di, dj, dk;
+};
+
+// input tables of the level functions of adj_level.cuh: field, column offset (i, j), level offset
+__constant__ InDesc c_uin[U_COUNT] = {
+    {FU, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
+    {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FVS, -1, -1, 0}, {FVS, 0, -1, 0}, {FVS, -1, 1, 0}, {FVS, 0, 1, 0},
+    {FWS, -1, 0, 0}, {FWS, -1, 0, 1}, {FWS, 0, 0, 1}, {FWS, 0, 0, -1}, {FWS, -1, 0, -1},
+    {FDP, -1, 0, 0}, {FDP, 0, 0, 0},
+    {FVS, 1, 1, 0}, {FVS, 1, -1, 0}, {FW, 1, 0, 0}, {FW, 1, 0, -1},
+    {FVEG, 0, 0, -1},
+    {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
+    {FU, -1, 0, 0}, {FU, 0, -1, 0}, {FU, 1, 0, 0}, {FU, 0, 1, 0}};
+__constant__ InDesc c_vin[V_COUNT] = {
+    {FV, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
+    {FUS, 1, 0, 0}, {FUS, 0, -1, 0}, {FUS, 1, -1, 0}, {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FUS, -1, -1, 0},
+    {FVS, 0, -1, 0}, {FWS, 0, -1, 0}, {FWS, 0, 0, -1}, {FWS, 0, -1, 1}, {FWS, 0, 0, 1}, {FWS, 0, -1, -1},
+    {FDP, 0, -1, 0}, {FDP, 0, 0, 0},
+    {FUS, 1, 1, 0}, {FUS, -1, 1, 0}, {FW, 0, 1, 0}, {FW, 0, 1, -1},
+    {FVEG, 0, 0, -1},
+    {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
+    {FV, -1, 0, 0}, {FV, 0, -1, 0}, {FV, 1, 0, 0}, {FV, 0, 1, 0}};
+__constant__ InDesc c_win[W_COUNT] = {
+    {FW, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0}, {FUS, 0, 0, -1}, {FVS, 0, 0, -1},
+    {FUS, -1, 0, 0}, {FUS, -1, 0, -1}, {FVS, 0, -1, 0}, {FVS, 0, -1, -1}, {FUS, 1, 0, 0}, {FUS, 1, 0, -1},
+    {FVS, 0, 1, 0}, {FVS, 0, 1, -1},
+    {FWS, 0, 0, -1}, {FDP, 0, 0, -1}, {FDP, 0, 0, 0},
+    {FUS, 0, 0, 1}, {FUS, -1, 0, 1}, {FVS, 0, 0, 1}, {FVS, 0, -1, 1},
+    {FW, 0, 0, 1}, {FW, 0, 0, -1},
+    {FVEG, 0, 0, -1},
+    {FW, -1, 0, 0}, {FW, 0, -1, 0}, {FW, 1, 0, 0}, {FW, 0, 1, 0}};
+
+// Everything the adjoint kernels read besides the solver's KArgs (all device pointers, slab
+// layout [ncols][KS] of the one situation).
+struct AdjArgs {
+    const float *mid[7];     // UK VK WK UKS VKS WKS DPMNEW after the averages of the iteration
+    const float *end[3];     // UK VK WK after the W sweep
+    float *lam[NLAM];        // cotangents: FU..FVEG, then DPM, DIV, row-carry Q
+    const float *ptab;       // [2][2][ncols][KS]: pressure P and TERMP per i-direction (IS = +1, -1)
+    int *flags;              // reverse-sweep flags per column
+    unsigned int *ctr;       // task counter of the launch
+    int stamp;               // flag value of the launch
+    int it;                  // IterationLoops of the reversed iteration
+    const uint8_t *bits;     // boundary-copy branches of the iteration: [we events + sn events][KS]
+    int nwe;                 // W/E events (the S/N events follow)
+};
+
+__device__ __forceinline__ size_t cell(const KArgs &a, int col, int k) { return (size_t)col * a.ks + k; }
+
+__device__ __forceinline__ void sweep_dir_of(int it, int &IS, int &JS) {
+    const int m = it % 4;   // PrognosticFlowfield.cs:770-802
+    if (m == 0) { IS = -1; JS = 1; }
+    else if (m == 1) { IS = -1; JS = -1; }
+    else if (m == 2) { IS = 1; JS = -1; }
+    else { IS = 1; JS = 1; }
+}
+
+// task t -> (i1, j1): diagonal-major, then position (one situation)
+__device__ __forceinline__ void decode(unsigned t, const SweepGeom &g, int &i1, int &j1) {
+    int lo = 0, hi = g.ndiag;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if ((unsigned)g.diag_start[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int d = lo;
+    const int pos = (int)(t - (unsigned)g.diag_start[d]);
+    const int ioff = max(0, d - (g.nj - 1)) + pos;
+    i1 = g.ia + ioff;
+    j1 = g.ja + d - ioff;
+}
+
+// The reverse wavefront task loop: tasks in reverse diagonal order; a column waits for its two
+// sweep successors (i1+1, j1) and (i1, j1+1), runs job.critical, publishes its flag (after a
+// fence over the warp's writes), then runs job.after.  Successors are claimed earlier, so no task
+// waits on one that is not running or done.
+template <class Job>
+__device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, const SweepGeom &g, int IS, int JS,
+                                          Job &job) {
+    const int lane = threadIdx.x & 31;
+    const unsigned total = (unsigned)g.diag_start[g.ndiag];
+    for (;;) {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(d.ctr, 1u);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= total) break;
+        if (*(volatile int *)a.err != ERR_NONE) break;
+        int i1, j1;
+        decode(total - 1 - t, g, i1, j1);
+        const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+        const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+        job.pre(i, j, IS, JS);
+        int ok = 1;
+        if (lane == 0)
+            ok = wait_stamps((i1 < g.ia + g.ni - 1) ? d.flags + (i + IS) * a.nj2 + j : nullptr,
+                             (j1 < g.ja + g.nj - 1) ? d.flags + i * a.nj2 + (j + JS) : nullptr, d.stamp, a.err,
+                             a.wait_limit_ns);
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (ok) job.critical(IS, JS);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(d.flags + i * a.nj2 + j, d.stamp);
+        if (ok) job.after(IS, JS);
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// momentum sweeps
+// ------------------------------------------------------------------------------------------------
+template <int COMP> struct CompTraits;
+template <> struct CompTraits<0> {
+    static constexpr int N = U_COUNT;
+    static __device__ const InDesc *tab() { return c_uin; }
+    template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { u_row(c, x, o); }
+    template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
+        u_row_vjp(c, x, l, g);
+    }
+};
+template <> struct CompTraits<1> {
+    static constexpr int N = V_COUNT;
+    static __device__ const InDesc *tab() { return c_vin; }
+    template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { v_row(c, x, o); }
+    template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
+        v_row_vjp(c, x, l, g);
+    }
+};
+template <> struct CompTraits<2> {
+    static constexpr int N = W_COUNT;
+    static __device__ const InDesc *tab() { return c_win; }
+    template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { w_row(c, x, o); }
+    template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
+        w_row_vjp(c, x, l, g);
+    }
+};
+
+// shared rows per warp: A B C D (then their cotangents), the forward T P Q, the new value above
+// (`up` of the back-substitution), the cotangent of the new value, the coefficients of the two
+// predecessors in D, the cotangent of the own old value, the cotangents of P and Q
+enum : int { R_A, R_B, R_C, R_D, R_T, R_P, R_Q, R_UP, R_L0, R_C1, R_C2, R_LO, R_LP, R_LQ, NROW };
+
+template <int COMP>
+struct MomRev {
+    const KArgs &a;
+    const AdjArgs &d;
+    float (*S)[KMAX_LEVELS];
+    ColCtx c;
+    bool act;
+    int kkm, kwl;
+    float top_carry;
+
+    __device__ LevelConst level_const(int k) const {
+        LevelConst L;
+        const float dz = a.dzk[k];
+        L.dz = dz; L.dxdz = a.dxk * dz; L.dydz = a.dyk * dz;
+        L.dxk = a.dxk; L.dyk = a.dyk; L.area = a.areaxy;
+        L.ap0 = a.ap0[k]; L.vishmin = a.vishmin; L.cor = a.coriolis;
+        L.geo = (COMP == 0) ? a.sit[0].ug : a.sit[0].vg;
+        L.hok = a.hokart[k]; L.hokK = c.hokK; L.cov = c.cf.cov;
+        L.help_t = c.cf.help_t; L.help_o = c.cf.help_o;
+        L.k = k; L.KK = c.KK; L.kad = c.kad; L.wlo = c.wlo; L.whi = c.whi;
+        L.fl = c.fl;
+        return L;
+    }
+
+    // the state a level input is read from: the swept field's predecessors hold their new values
+    __device__ const float *src(int f, int di, int dj, int IS, int JS) const {
+        if (f == FVEG) return a.veg;
+        if (f >= FUS) return d.mid[f];
+        if (f == COMP) {
+            const bool pred = (di == -IS && dj == 0) || (di == 0 && dj == -JS);
+            return pred ? d.end[f] : d.mid[f];
+        }
+        // other components: U is final in the V and W sweeps, V in the W sweep
+        return (f < COMP) ? d.end[f] : d.mid[f];
+    }
+
+    __device__ void load(int k, int IS, int JS, float *x) const {
+        const InDesc *t = CompTraits<COMP>::tab();
+#pragma unroll
+        for (int q = 0; q < CompTraits<COMP>::N; ++q) {
+            const InDesc e = t[q];
+            const int kk = (e.dk == WL) ? kwl : k + e.dk;
+            const float *p = src(e.f, e.di, e.dj, IS, JS);
+            if (!p) { x[q] = 0.0f; continue; }
+            x[q] = __ldcg(p + cell(a, c.col + e.di * a.nj2 + e.dj, kk));
+        }
+    }
+
+    // before the wait: the forward rows of the column from the kept states and its Thomas
+    // recurrence (U-prognostic-microscale_1.cs:485-504)
+    __device__ void pre(int i, int j, int IS, int JS) {
+        const int lane = threadIdx.x & 31;
+        c = make_col(a, i, j);
+        act = (c.fl & F_ADV) != 0;
+        kkm = (COMP == 0) ? c.kkm_u : (COMP == 1 ? c.kkm_v : -32768);
+        kwl = ((c.fl & F_CUTKLT1) && (c.fl & F_Z0GE)) ? c.KK + 2 : c.KK + 1;
+        top_carry = 0.0f;
+        if (!act) return;
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            float x[CompTraits<COMP>::N];
+            load(k, IS, JS, x);
+            const LevelConst LC = level_const(k);
+            float o[8];
+            CompTraits<COMP>::row(LC, x, o);
+            S[R_A][k] = o[0]; S[R_B][k] = o[1]; S[R_C][k] = o[2]; S[R_D][k] = o[3];
+            // predecessor 1 is (i - IS, j): W (o[4]) or E (o[6]); predecessor 2 is (i, j - JS): S or N
+            S[R_C1][k] = (IS == 1) ? o[4] : o[6];
+            S[R_C2][k] = (JS == 1) ? o[5] : o[7];
+            S[R_UP][k] = __ldcg(d.end[COMP] + cell(a, c.col, k + 1));
+        }
+        __syncwarp();
+        if (lane == 0) {
+            float P = 0.0f, Q = 0.0f;
+            for (int k = c.K0; k <= c.VI; ++k) {
+                const float A = S[R_A][k], B = S[R_B][k], C = S[R_C][k], D = S[R_D][k];
+                const bool ch = k > c.KK + 1;
+                const float T = ch ? 1.0f / (A - C * P) : 1.0f / A;
+                Q = ch ? (D + C * Q) * T : D * T;
+                P = B * T;
+                S[R_T][k] = T; S[R_P][k] = P; S[R_Q][k] = Q;
+            }
+        }
+        __syncwarp();
+    }
+
+    // after the wait: the cotangents of the column's new values are complete (later phases and
+    // both successors have added theirs); reverse the back-substitution and the recurrence and
+    // send the predecessors their cotangents
+    __device__ void critical(int IS, int JS) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        float *L = d.lam[COMP];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            // an updated level's cotangent is handed over from its new to its old value
+            S[R_L0][k] = (kkm < k) ? atomicExch(L + cell(a, c.col, k), 0.0f) : 0.0f;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int K0 = c.K0, KK = c.KK, VI = c.VI;
+            const float relax = a.relax;
+            // relaxed back-substitution (:513-524) reversed, bottom up: phi'_k = phi_k +
+            // relax*(P_k*up + Q_k - phi_k) with up = phi'_{k+1}
+            float carry = 0.0f;
+            for (int k = K0; k <= VI; ++k) {
+                if (kkm < k) {
+                    const float mu = S[R_L0][k] + carry;
+                    S[R_LO][k] = (1.0f - relax) * mu;
+                    S[R_LP][k] = relax * S[R_UP][k] * mu;
+                    S[R_LQ][k] = relax * mu;
+                    carry = relax * S[R_P][k] * mu;
+                } else {
+                    S[R_LO][k] = carry;
+                    S[R_LP][k] = 0.0f;
+                    S[R_LQ][k] = 0.0f;
+                    carry = 0.0f;
+                }
+            }
+            top_carry = carry;
+            // Thomas recurrence reversed, top down
+            float lPn = 0.0f, lQn = 0.0f;
+            for (int k = VI; k >= K0; --k) {
+                const float B = S[R_B][k], C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
+                const bool ch = k > KK + 1;
+                const float lP = S[R_LP][k] + lPn, lQ = S[R_LQ][k] + lQn;
+                const float Pp = ch ? S[R_P][k - 1] : 0.0f, Qp = ch ? S[R_Q][k - 1] : 0.0f;
+                const float lT = lQ * (ch ? (D + C * Qp) : D) + lP * B;
+                const float lden = -lT * T * T;
+                S[R_A][k] = lden;
+                S[R_B][k] = lP * T;
+                S[R_C][k] = ch ? (lQ * Qp * T - lden * Pp) : 0.0f;
+                S[R_D][k] = lQ * T;
+                lQn = ch ? lQ * C * T : 0.0f;
+                lPn = ch ? -lden * C : 0.0f;
+            }
+        }
+        __syncwarp();
+        // cotangents of the predecessors' new values (they run after this column)
+        const long long dP1 = -(long long)IS * a.nj2, dP2 = -(long long)JS;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            const float lD = S[R_D][k];
+            if (lD == 0.0f) continue;
+            const float g1 = lD * S[R_C1][k], g2 = lD * S[R_C2][k];
+            if (g1 != 0.0f) atomicAdd(L + cell(a, (int)(c.col + dP1), k), g1);
+            if (g2 != 0.0f) atomicAdd(L + cell(a, (int)(c.col + dP2), k), g2);
+        }
+    }
+
+    __device__ void after(int IS, int JS) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        const InDesc *t = CompTraits<COMP>::tab();
+        constexpr int N = CompTraits<COMP>::N;
+        if (lane == 0 && top_carry != 0.0f) atomicAdd(d.lam[COMP] + cell(a, c.col, c.VI + 1), top_carry);
+#pragma unroll 1
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k < c.K0 || k > c.VI) continue;
+            float x[N], g[N];
+            load(k, IS, JS, x);
+#pragma unroll
+            for (int q = 0; q < N; ++q) g[q] = 0.0f;
+            const float l4[4] = {S[R_A][k], S[R_B][k], S[R_C][k], S[R_D][k]};
+            const LevelConst LC = level_const(k);
+            CompTraits<COMP>::vjp(LC, x, l4, g);
+            g[0] += S[R_LO][k];
+#pragma unroll
+            for (int q = 0; q < N; ++q) {
+                const InDesc e = t[q];
+                // the predecessors' cotangents were sent before the flag
+                if (e.f == COMP && ((e.di == -IS && e.dj == 0) || (e.di == 0 && e.dj == -JS))) continue;
+                const float v = g[q];
+                if (v == 0.0f) continue;
+                if (e.f == FVEG && !a.veg) continue;
+                const int kk = (e.dk == WL) ? kwl : k + e.dk;
+                atomicAdd(d.lam[e.f] + cell(a, c.col + e.di * a.nj2 + e.dj, kk), v);
+            }
+        }
+    }
+};
+
+template <int COMP>
+__global__ void __launch_bounds__(AW * 32) k_adj_mom(KArgs a, AdjArgs d, SweepGeom g) {
+    __shared__ float sm[AW][NROW][KMAX_LEVELS];
+    MomRev<COMP> job{a, d, sm[threadIdx.x >> 5]};
+    int IS, JS;
+    sweep_dir_of(d.it, IS, JS);
+    if (COMP == 1) { IS = -IS; JS = -JS; }   // model-1 V sweeps with (-IS, -JS)
+    rev_tasks(a, d, g, IS, JS, job);
+}
+
+// ------------------------------------------------------------------------------------------------
+// pressure correction (PrognosticFlowfield.cs:804-901): per column, for k = VI..KK+1
+//   DIM_k = DIV_k/DTIME + (DPM_im + DPM_ip)/DXK*DYK*DZK + (DPM_jm - DPM_jp)/DYK*DXK*DZK
+//   Q_k = (ATP_k*Q_{k+1} + DIM_k)*TERMP_k   (Q_{VI+1} from the row carry)
+// then DPM_k = P_k*DPM_{k-1} + Q_k and DPMNEW_k += relaxp*DPM_k for k = KK+1..VI.  The neighbours
+// not yet swept hold 0 (DPM is zeroed before the sweep), so only the two predecessors carry
+// cotangents; P and TERMP do not depend on the state.
+// ------------------------------------------------------------------------------------------------
+struct PresRev {
+    const KArgs &a;
+    const AdjArgs &d;
+    float (*S)[KMAX_LEVELS];     // rows: 0 cotangent of DPM (mu), 1 cotangent of DIM, 2 P, 3 TERMP
+    ColCtx c;
+    bool act;
+    int dirx;                    // 0: IS = +1, 1: IS = -1
+
+    __device__ void pre(int i, int j, int IS, int) {
+        const int lane = threadIdx.x & 31;
+        c = make_col(a, i, j);
+        act = (c.fl & F_ADV) != 0;
+        dirx = (IS == 1) ? 0 : 1;
+        if (!act) return;
+        const size_t fsz = (size_t)a.ncols * a.ks;
+        const float *P = d.ptab + (size_t)(2 * dirx) * fsz, *TM = d.ptab + (size_t)(2 * dirx + 1) * fsz;
+        for (int k = lane; k <= c.VI + 1 && k < KMAX_LEVELS; k += 32) {
+            S[2][k] = P[cell(a, c.col, k)];
+            S[3][k] = TM[cell(a, c.col, k)];
+        }
+        __syncwarp();
+    }
+
+    __device__ void critical(int IS, int JS) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        float *LD = d.lam[L_DPM], *LN = d.lam[FDP], *LQ = d.lam[L_QC];
+        for (int k = lane; k < KMAX_LEVELS; k += 32) {
+            if (k <= c.KK || k > c.VI) continue;
+            const size_t e = cell(a, c.col, k);
+            S[0][k] = __ldcg(LD + e) + a.relaxp * __ldcg(LN + e);
+            S[1][k] = __ldcg(LQ + e);   // carry cotangents left by readers later in the row
+            LQ[e] = 0.0f;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int KK = c.KK, VI = c.VI;
+            // back-substitution reversed, top down: cotangent of Q_k
+            float next = 0.0f;
+            for (int k = VI; k > KK; --k) {
+                const float mu = S[0][k] + next;
+                S[0][k] = mu;
+                next = S[2][k] * mu;
+            }
+            // elimination reversed, bottom up: cotangent of DIM_k
+            float prev = 0.0f;
+            for (int k = KK + 1; k <= VI; ++k) {
+                const float lam = S[0][k] + S[1][k] + prev;
+                const float tm = S[3][k];
+                S[1][k] = lam * tm;
+                prev = a.atp[k] * tm * lam;
+            }
+            // the top level read Q_{VI+1} of the row carry: its writer runs after this column
+            const short2 w = a.rcw[c.col];
+            const int wi = dirx == 0 ? w.x : w.y;
+            if (wi >= 0 && prev != 0.0f) atomicAdd(LQ + cell(a, wi * a.nj2 + c.j, VI + 1), prev);
+        }
+        __syncwarp();
+        const long long d1 = -(long long)IS * a.nj2, d2 = -(long long)JS;
+        for (int k = lane; k < KMAX_LEVELS; k += 32) {
+            if (k <= c.KK || k > c.VI) continue;
+            const float lD = S[1][k];
+            if (lD == 0.0f) continue;
+            const float dz = a.dzk[k];
+            atomicAdd(LD + cell(a, (int)(c.col + d1), k), lD * (a.dyk * dz / a.dxk));
+            // DPM_jm enters with +, DPM_jp with - (the reference's sign, :853-854)
+            atomicAdd(LD + cell(a, (int)(c.col + d2), k), (JS == 1 ? 1.0f : -1.0f) * lD * (a.dxk * dz / a.dyk));
+        }
+    }
+
+    __device__ void after(int, int) {
+        if (!act) return;
+        const int lane = threadIdx.x & 31;
+        const float dt = a.sit[0].dtime;
+        for (int k = lane; k < KMAX_LEVELS; k += 32) {
+            if (k <= c.KK || k > c.VI) continue;
+            d.lam[L_DIV][cell(a, c.col, k)] = S[1][k] / dt;
+        }
+    }
+};
+
+__global__ void __launch_bounds__(AW * 32) k_adj_pressure(KArgs a, AdjArgs d, SweepGeom g) {
+    __shared__ float sm[AW][4][KMAX_LEVELS];
+    PresRev job{a, d, sm[threadIdx.x >> 5]};
+    int IS, JS;
+    sweep_dir_of(d.it, IS, JS);
+    rev_tasks(a, d, g, IS, JS, job);
+}
+
+// ------------------------------------------------------------------------------------------------
+// pointwise phases: one warp per column, lanes over levels
+// ------------------------------------------------------------------------------------------------
+__device__ __forceinline__ bool warp_col(const KArgs &a, int &col, int &i, int &j) {
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (gw >= a.ncols) return false;
+    col = (int)gw;
+    i = col / a.nj2;
+    j = col - i * a.nj2;
+    return true;
+}
+
+// velocity correction (:904-949) reversed: cotangent of DPM gathered from the corrected U, V, W
+// (DPM is only read), and the cotangent of a W the correction sets to 0 cleared
+__device__ __forceinline__ bool vc_u(const KArgs &a, int i, int j, int k) {
+    if (i < 3 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return false;   // du: i > 2
+    const int col = i * a.nj2 + j;
+    if (!(a.cflags[col] & F_VC)) return false;
+    const ColMeta m = a.meta[col];
+    return k >= 1 && k <= m.vi && m.kkm_u < k;
+}
+__device__ __forceinline__ bool vc_v(const KArgs &a, int i, int j, int k) {
+    if (i < 2 || i > a.nii - 1 || j < 3 || j > a.njj - 1) return false;   // dv: j > 2
+    const int col = i * a.nj2 + j;
+    if (!(a.cflags[col] & F_VC)) return false;
+    const ColMeta m = a.meta[col];
+    return k >= 1 && k <= m.vi && m.kkm_v < k;
+}
+// 1: W corrected, 0: W set to 0, -1: not touched
+__device__ __forceinline__ int vc_w(const KArgs &a, int i, int j, int k) {
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return -1;
+    const int col = i * a.nj2 + j;
+    if (!(a.cflags[col] & F_VC)) return -1;
+    const ColMeta m = a.meta[col];
+    if (k < 1 || k > m.vi) return -1;
+    return (m.kkart + 1 < k) ? 1 : 0;
+}
+
+__global__ void k_adj_velcorr(KArgs a, AdjArgs d) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const float DT = a.sit[0].dtime;
+    const float *LU = d.lam[FU], *LV = d.lam[FV];
+    float *LW = d.lam[FW];
+    const int nj2 = a.nj2;
+    for (int k = lane; k < a.ks; k += 32) {
+        float g = 0.0f;
+        if (k >= 1) {
+            if (vc_u(a, i, j, k)) g -= LU[cell(a, col, k)] / a.dxk * DT;
+            if (vc_u(a, i + 1, j, k)) g += LU[cell(a, col + nj2, k)] / a.dxk * DT;
+            if (vc_v(a, i, j, k)) g -= LV[cell(a, col, k)] / a.dyk * DT;
+            if (vc_v(a, i, j + 1, k)) g += LV[cell(a, col + 1, k)] / a.dyk * DT;
+            if (vc_w(a, i, j, k) == 1) g -= LW[cell(a, col, k)] / (a.dzk[k] + a.dzk[k - 1]) * 2.0f * DT;
+            if (k + 1 < a.ks && vc_w(a, i, j, k + 1) == 1)
+                g += LW[cell(a, col, k + 1)] / (a.dzk[k + 1] + a.dzk[k]) * 2.0f * DT;
+        }
+        d.lam[L_DPM][cell(a, col, k)] = g;
+    }
+    __syncwarp();
+    for (int k = lane; k < a.ks; k += 32)
+        if (vc_w(a, i, j, k) == 0) LW[cell(a, col, k)] = 0.0f;
+}
+
+// staggered averages (:958-1039) reversed in three passes: the border copies, the gathers into
+// U, V, W, the clearing of the overwritten averages' cotangents
+__device__ __forceinline__ bool av_col(const KArgs &a, int i, int j) {
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return false;
+    return (a.cflags[i * a.nj2 + j] & F_VC) != 0;
+}
+
+__global__ void k_adj_avg_copies(KArgs a, AdjArgs d) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    if (!av_col(a, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nj2 = a.nj2;
+    float *LUS = d.lam[FUS], *LVS = d.lam[FVS];
+    // VKS[1][j] = VKS[2][j], VKS[NII][j] = VKS[NII-1][j] on every level (after the level loop)
+    const bool west = (i == 2) && (a.cflags[1 * nj2 + j] & F_ADV);
+    const bool east = (i == a.nii - 1) && (a.cflags[col] & F_ADV);
+    if (west || east) {
+        const long long dd = west ? -(long long)nj2 : nj2;
+        for (int k = lane; k < a.ks; k += 32) {
+            const size_t e = cell(a, (int)(col + dd), k);
+            LVS[cell(a, col, k)] += LVS[e];
+            LVS[e] = 0.0f;
+        }
+    }
+    // UKS[i][1] = UKS[i][2] and UKS[i][NJJ] = UKS[i][NJJ-1] on KSTART..VI
+    const ColMeta m = a.meta[col];
+    const bool cpS = (j == 2);
+    const bool cpN = (j == a.njj - 1) && (a.cflags[i * nj2 + a.njj] & F_ADV);
+    if (cpS || cpN) {
+        for (int k = lane; k < a.ks; k += 32) {
+            if (k < m.kstart || k > m.vi) continue;
+            float add = 0.0f;
+            if (cpS) { const size_t e = cell(a, col - 1, k); add += LUS[e]; LUS[e] = 0.0f; }
+            if (cpN) { const size_t e = cell(a, col + 1, k); add += LUS[e]; LUS[e] = 0.0f; }
+            LUS[cell(a, col, k)] += add;
+        }
+    }
+}
+
+// level k of column (i, j) gets a new UKS/VKS (kind 0) or WKS (kind 1) from the averages
+__device__ __forceinline__ bool av_new(const KArgs &a, int i, int j, int k, int kind) {
+    if (!av_col(a, i, j)) return false;
+    const ColMeta m = a.meta[i * a.nj2 + j];
+    if (k < m.kstart || k > m.vi) return false;
+    return kind == 0 ? (m.kkart < k) : (m.kkart + 1 < k);
+}
+
+__global__ void k_adj_avg_gather(KArgs a, AdjArgs d) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nj2 = a.nj2;
+    const float *LUS = d.lam[FUS], *LVS = d.lam[FVS], *LWS = d.lam[FWS];
+    for (int k = lane; k < a.ks; k += 32) {
+        float gu = 0.0f, gv = 0.0f, gw = 0.0f;
+        if (av_new(a, i, j, k, 0)) { gu += 0.5f * LUS[cell(a, col, k)]; gv += 0.5f * LVS[cell(a, col, k)]; }
+        if (av_new(a, i - 1, j, k, 0)) gu += 0.5f * LUS[cell(a, col - nj2, k)];
+        if (av_new(a, i, j - 1, k, 0)) gv += 0.5f * LVS[cell(a, col - 1, k)];
+        if (av_new(a, i, j, k, 1)) gw += 0.5f * LWS[cell(a, col, k)];
+        if (k >= 1 && av_new(a, i, j, k - 1, 1)) gw += 0.5f * LWS[cell(a, col, k - 1)];
+        if (gu != 0.0f) d.lam[FU][cell(a, col, k)] += gu;
+        if (gv != 0.0f) d.lam[FV][cell(a, col, k)] += gv;
+        if (gw != 0.0f) d.lam[FW][cell(a, col, k)] += gw;
+    }
+}
+
+__global__ void k_adj_avg_clear(KArgs a, AdjArgs d) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    for (int k = lane; k < a.ks; k += 32) {
+        if (av_new(a, i, j, k, 0)) { d.lam[FUS][cell(a, col, k)] = 0.0f; d.lam[FVS][cell(a, col, k)] = 0.0f; }
+        if (av_new(a, i, j, k, 1)) d.lam[FWS][cell(a, col, k)] = 0.0f;
+    }
+}
+
+// divergence (:723-758) reversed: a gather of the cotangent of DIV into U, V, W
+__device__ __forceinline__ bool div_at(const KArgs &a, int i, int j, int k) {
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return false;
+    const int col = i * a.nj2 + j;
+    if (!(a.cflags[col] & F_ADV)) return false;
+    const ColMeta m = a.meta[col];
+    return k > m.kkart && k <= m.vi;
+}
+
+__global__ void k_adj_div(KArgs a, AdjArgs d) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nj2 = a.nj2;
+    const float *LDV = d.lam[L_DIV];
+    const float AREA = a.areaxy;
+    for (int k = lane; k < a.ks; k += 32) {
+        if (k < 1) continue;
+        const float dz = a.dzk[k];
+        float gu = 0.0f, gv = 0.0f, gw = 0.0f;
+        if (div_at(a, i, j, k)) {
+            const float l = LDV[cell(a, col, k)];
+            gu += l * a.dyk * dz;
+            gv += l * a.dxk * dz;
+            if (k > a.meta[col].kkart + 1) gw += l * AREA;
+        }
+        if (div_at(a, i - 1, j, k)) gu -= LDV[cell(a, col - nj2, k)] * a.dyk * dz;
+        if (div_at(a, i, j - 1, k)) gv -= LDV[cell(a, col - 1, k)] * a.dxk * dz;
+        if (div_at(a, i, j, k - 1)) gw -= LDV[cell(a, col, k - 1)] * AREA;
+        if (gu != 0.0f) d.lam[FU][cell(a, col, k)] += gu;
+        if (gv != 0.0f) d.lam[FV][cell(a, col, k)] += gv;
+        if (gw != 0.0f) d.lam[FW][cell(a, col, k)] += gw;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// lateral and top boundary conditions (:595-714).  The recompute runs the forward copies itself
+// (the same operations as the solver's boundary kernels) and keeps the branch of every
+// sign-conditioned copy; the reverse undoes the copies in reverse order.
+// ------------------------------------------------------------------------------------------------
+__global__ void k_adj_bc_we_fwd(KArgs a, BcLists bc, uint8_t *bits) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 2 + (int)(t / a.ks);
+    const int k = (int)(t % a.ks);
+    if (j > a.njj || k < 1) return;
+    const int nj2 = a.nj2;
+    for (int e = bc.we_ptr[j]; e < bc.we_ptr[j + 1]; ++e) {
+        const int ev = bc.we_ev[e];
+        const int i = ev & 0xffff;
+        const int c = i * nj2 + j;
+        if (k > a.meta[c].vi) continue;
+        uint8_t b = 0;
+        if (ev & (1 << 16)) {
+            const float u = a.uk[cell(a, c - 2 * nj2, k)];
+            if (u >= 0) { a.uk[cell(a, c - nj2, k)] = u; b |= 1; }
+            a.vk[cell(a, c - 2 * nj2, k)] = a.vk[cell(a, c - nj2, k)];
+            a.wk[cell(a, c - 2 * nj2, k)] = a.wk[cell(a, c - nj2, k)];
+        }
+        if (ev & (1 << 17)) {
+            const float u = a.uk[cell(a, c + 2 * nj2, k)];
+            if (u <= 0) { a.uk[cell(a, c + nj2, k)] = u; b |= 2; }
+            a.vk[cell(a, c + nj2, k)] = a.vk[cell(a, c, k)];
+            a.wk[cell(a, c + nj2, k)] = a.wk[cell(a, c, k)];
+        }
+        bits[(size_t)e * a.ks + k] = b;
+    }
+}
+
+__global__ void k_adj_bc_sn_fwd(KArgs a, BcLists bc, uint8_t *bits, int nwe) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = 2 + (int)(t / a.ks);
+    const int k = (int)(t % a.ks);
+    if (i > a.nii || k < 1) return;
+    const int nj2 = a.nj2;
+    for (int e = bc.sn_ptr[i]; e < bc.sn_ptr[i + 1]; ++e) {
+        const int ev = bc.sn_ev[e];
+        const int j = ev & 0xffff;
+        const int c = i * nj2 + j;
+        if (k > a.meta[c].vi) continue;
+        uint8_t b = 0;
+        if (ev & (1 << 16)) {
+            const float v = a.vk[cell(a, c - 2, k)];
+            if (v >= 0) { a.vk[cell(a, c - 1, k)] = v; b |= 1; }
+            a.uk[cell(a, c - 2, k)] = a.uk[cell(a, c - 1, k)];
+            a.wk[cell(a, c - 2, k)] = a.wk[cell(a, c - 1, k)];
+        }
+        if (ev & (1 << 17)) {
+            const float v = a.vk[cell(a, c + 2, k)];
+            if (v <= 0) { a.vk[cell(a, c + 1, k)] = v; b |= 2; }
+            a.uk[cell(a, c + 1, k)] = a.uk[cell(a, c, k)];
+            a.wk[cell(a, c + 1, k)] = a.wk[cell(a, c, k)];
+        }
+        bits[(size_t)(nwe + e) * a.ks + k] = b;
+    }
+}
+
+__global__ void k_adj_bc_top_fwd(KArgs a) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ncols) return;
+    const int col = (int)t, i = col / a.nj2, j = col - i * a.nj2;
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+    if (!(a.cflags[col] & F_ADV)) return;
+    const int k = a.meta[col].vi;
+    a.wk[cell(a, col, k + 1)] = a.wk[cell(a, col, k)];
+    a.uk[cell(a, col, k + 1)] = a.uk[cell(a, col, k)];
+    a.vk[cell(a, col, k + 1)] = a.vk[cell(a, col, k)];
+}
+
+// a = b reversed: the cotangent of a moves to b
+__device__ __forceinline__ void rev_copy(float *L, size_t dst, size_t src) {
+    L[src] += L[dst];
+    L[dst] = 0.0f;
+}
+
+__global__ void k_adj_bc_top_rev(KArgs a, AdjArgs d) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.ncols) return;
+    const int col = (int)t, i = col / a.nj2, j = col - i * a.nj2;
+    if (i < 2 || i > a.nii - 1 || j < 2 || j > a.njj - 1) return;
+    if (!(a.cflags[col] & F_ADV)) return;
+    const int k = a.meta[col].vi;
+    rev_copy(d.lam[FV], cell(a, col, k + 1), cell(a, col, k));
+    rev_copy(d.lam[FU], cell(a, col, k + 1), cell(a, col, k));
+    rev_copy(d.lam[FW], cell(a, col, k + 1), cell(a, col, k));
+}
+
+__global__ void k_adj_bc_sn_rev(KArgs a, BcLists bc, AdjArgs d) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = 2 + (int)(t / a.ks);
+    const int k = (int)(t % a.ks);
+    if (i > a.nii || k < 1) return;
+    float *LU = d.lam[FU], *LV = d.lam[FV], *LW = d.lam[FW];
+    for (int e = bc.sn_ptr[i + 1] - 1; e >= bc.sn_ptr[i]; --e) {
+        const int ev = bc.sn_ev[e];
+        const int j = ev & 0xffff;
+        const int c = i * a.nj2 + j;
+        if (k > a.meta[c].vi) continue;
+        const uint8_t b = d.bits[(size_t)(d.nwe + e) * a.ks + k];
+        if (ev & (1 << 17)) {
+            rev_copy(LW, cell(a, c + 1, k), cell(a, c, k));
+            rev_copy(LU, cell(a, c + 1, k), cell(a, c, k));
+            if (b & 2) rev_copy(LV, cell(a, c + 1, k), cell(a, c + 2, k));
+        }
+        if (ev & (1 << 16)) {
+            rev_copy(LW, cell(a, c - 2, k), cell(a, c - 1, k));
+            rev_copy(LU, cell(a, c - 2, k), cell(a, c - 1, k));
+            if (b & 1) rev_copy(LV, cell(a, c - 1, k), cell(a, c - 2, k));
+        }
+    }
+}
+
+__global__ void k_adj_bc_we_rev(KArgs a, BcLists bc, AdjArgs d) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 2 + (int)(t / a.ks);
+    const int k = (int)(t % a.ks);
+    if (j > a.njj || k < 1) return;
+    const int nj2 = a.nj2;
+    float *LU = d.lam[FU], *LV = d.lam[FV], *LW = d.lam[FW];
+    for (int e = bc.we_ptr[j + 1] - 1; e >= bc.we_ptr[j]; --e) {
+        const int ev = bc.we_ev[e];
+        const int i = ev & 0xffff;
+        const int c = i * nj2 + j;
+        if (k > a.meta[c].vi) continue;
+        const uint8_t b = d.bits[(size_t)e * a.ks + k];
+        if (ev & (1 << 17)) {
+            rev_copy(LW, cell(a, c + nj2, k), cell(a, c, k));
+            rev_copy(LV, cell(a, c + nj2, k), cell(a, c, k));
+            if (b & 2) rev_copy(LU, cell(a, c + nj2, k), cell(a, c + 2 * nj2, k));
+        }
+        if (ev & (1 << 16)) {
+            rev_copy(LW, cell(a, c - 2 * nj2, k), cell(a, c - nj2, k));
+            rev_copy(LV, cell(a, c - 2 * nj2, k), cell(a, c - nj2, k));
+            if (b & 1) rev_copy(LU, cell(a, c - nj2, k), cell(a, c - 2 * nj2, k));
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// set-up (:295-329, 410-432, 518-575) reversed, on the full-height staging layout of the initial
+// fields: gather of the device layout, zeroing inside buildings, border copies, staggered averages
+// ------------------------------------------------------------------------------------------------
+struct StageLam {
+    float *u, *v, *w;   // [NII+2][NJJ+2][NKK+2]
+};
+
+__device__ __forceinline__ size_t sx(const KArgs &a, int i, int j, int k) {
+    return ((size_t)i * a.nj2 + j) * (a.nkk + 2) + k;
+}
+
+// levels below KS come from the device-layout cotangents (the levels above pass through)
+__global__ void k_adj_setup_scatter(KArgs a, AdjArgs d, StageLam L) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nk2 = a.nkk + 2;
+    for (int k = lane; k < a.ks && k < nk2; k += 32) {
+        const size_t s = (size_t)col * nk2 + k;
+        L.u[s] = d.lam[FU][cell(a, col, k)];
+        L.v[s] = d.lam[FV][cell(a, col, k)];
+        L.w[s] = d.lam[FW][cell(a, col, k)];
+    }
+}
+
+__global__ void k_adj_setup_zero(KArgs a, AdjArgs d, StageLam L) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    if (i < 1 || i > a.nii || j < 1 || j > a.njj) return;
+    if (!(a.cflags[col] & F_ADV)) return;
+    const int lane = threadIdx.x & 31;
+    const ColMeta m = a.meta[col];
+    for (int k = 1 + lane; k <= m.vi; k += 32) {
+        if (m.kkart < k) continue;
+        L.u[sx(a, i, j, k)] = 0.0f;
+        if (i == a.nii) L.u[sx(a, i + 1, j, k)] = 0.0f;
+        L.v[sx(a, i, j, k)] = 0.0f;
+        if (j == a.njj) L.v[sx(a, i, j + 1, k)] = 0.0f;
+        L.w[sx(a, i, j, k)] = 0.0f;
+        if (k == m.vi) L.w[sx(a, i, j, k + 1)] = 0.0f;
+        d.lam[FUS][cell(a, col, k)] = 0.0f;
+        d.lam[FVS][cell(a, col, k)] = 0.0f;
+        d.lam[FWS][cell(a, col, k)] = 0.0f;
+    }
+}
+
+// UK[NII+1] = UK[NII], VK[.][NJJ+1] = VK[.][NJJ] on levels 1..NKK-1, reversed
+__global__ void k_adj_setup_border(KArgs a, StageLam L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nk = a.nkk - 1;
+    const long long per = (long long)(a.njj + a.nii) * nk;
+    if (t >= per) return;
+    const int k = 1 + (int)(t % nk);
+    const int q = (int)(t / nk);
+    if (q < a.njj) {
+        const int j = 1 + q;
+        L.u[sx(a, a.nii, j, k)] += L.u[sx(a, a.nii + 1, j, k)];
+        L.u[sx(a, a.nii + 1, j, k)] = 0.0f;
+    } else {
+        const int i = 1 + (q - a.njj);
+        L.v[sx(a, i, a.njj, k)] += L.v[sx(a, i, a.njj + 1, k)];
+        L.v[sx(a, i, a.njj + 1, k)] = 0.0f;
+    }
+}
+
+// initial staggered averages UKS = (UK_i + UK_i+1)/2 etc. on the columns with ADVDOM in their 3x3
+// neighbourhood, levels 1..NKK-1 (those below KS are kept), reversed as a gather
+__device__ __forceinline__ bool uks0(const KArgs &a, int i, int j, int k) {
+    if (i < 1 || i > a.nii || j < 1 || j > a.njj) return false;
+    if (!(a.cflags[i * a.nj2 + j] & F_ALLOC3)) return false;
+    return k >= 1 && k <= a.nkk - 1 && k < a.ks;
+}
+
+__global__ void k_adj_setup_avg(KArgs a, AdjArgs d, StageLam L) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nj2 = a.nj2;
+    for (int k = lane; k < a.ks && k <= a.nkk; k += 32) {
+        float gu = 0.0f, gv = 0.0f, gw = 0.0f;
+        if (uks0(a, i, j, k)) {
+            gu += 0.5f * d.lam[FUS][cell(a, col, k)];
+            gv += 0.5f * d.lam[FVS][cell(a, col, k)];
+            gw += 0.5f * d.lam[FWS][cell(a, col, k)];
+        }
+        if (uks0(a, i - 1, j, k)) gu += 0.5f * d.lam[FUS][cell(a, col - nj2, k)];
+        if (uks0(a, i, j - 1, k)) gv += 0.5f * d.lam[FVS][cell(a, col - 1, k)];
+        if (k >= 1 && uks0(a, i, j, k - 1)) gw += 0.5f * d.lam[FWS][cell(a, col, k - 1)];
+        const size_t s = (size_t)col * (a.nkk + 2) + k;
+        L.u[s] += gu;
+        L.v[s] += gv;
+        L.w[s] += gw;
+    }
+}
+
+// VEG cotangent in the host layout [NII+2][NJJ+2][NKK+2] (device layout index k-1 -> level k-1)
+__global__ void k_adj_veg_out(KArgs a, AdjArgs d, float *out) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nk2 = a.nkk + 2;
+    for (int k = lane; k < nk2; k += 32)
+        out[(size_t)col * nk2 + k] = (k < a.ks) ? d.lam[FVEG][cell(a, col, k)] : 0.0f;
+}
+
+// host-layout cotangents of the final fields -> device layout (levels below KS)
+__global__ void k_adj_gather_in(KArgs a, AdjArgs d, StageLam L) {
+    int col, i, j;
+    if (!warp_col(a, col, i, j)) return;
+    const int lane = threadIdx.x & 31;
+    const int nk2 = a.nkk + 2;
+    for (int k = lane; k < a.ks; k += 32) {
+        const bool in = k < nk2;
+        const size_t s = (size_t)col * nk2 + k;
+        d.lam[FU][cell(a, col, k)] = in ? L.u[s] : 0.0f;
+        d.lam[FV][cell(a, col, k)] = in ? L.v[s] : 0.0f;
+        d.lam[FW][cell(a, col, k)] = in ? L.w[s] : 0.0f;
+    }
+}
+
+}  // namespace
+
+// ================================================================================================
+// host side
+// ================================================================================================
+
+namespace {
+
+int col_blocks(const KArgs &a) { return (a.ncols * 32 + 255) / 256; }
+
+// one forward SIMPLE iteration with separate phase launches; when `keep` is given, the mid and
+// end states go there and the boundary copies' branches to `bits`
+int forward_iteration(gral_ctx *ctx, float *keep, uint8_t *bits) {
+    const KArgs &a = ctx->ka;
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st));
+    if (bits) {
+        const long long nw = (long long)(a.njj - 1) * a.ks, ns = (long long)(a.nii - 1) * a.ks;
+        k_adj_bc_we_fwd<<<(int)((nw + 127) / 128), 128, 0, st>>>(a, ctx->bc, bits);
+        k_adj_bc_sn_fwd<<<(int)((ns + 127) / 128), 128, 0, st>>>(a, ctx->bc, bits, ctx->adj_nwe);
+        k_adj_bc_top_fwd<<<(a.ncols + 127) / 128, 128, 0, st>>>(a);
+    } else {
+        launch_bc(a, ctx->bc, st);
+    }
+    launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
+    launch_velcorr(a, st);
+    launch_average(a, st);
+    const size_t fsz = (size_t)a.ncols * a.ks;
+    if (keep) {
+        const float *src[7] = {a.uk, a.vk, a.wk, a.uks, a.vks, a.wks, a.dpmnew};
+        for (int q = 0; q < 7; ++q)
+            CK(cudaMemcpyAsync(keep + q * fsz, src[q], fsz * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
+    launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
+    launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
+    launch_bookkeeping(a, st);
+    if (keep) {
+        const float *src[3] = {a.uk, a.vk, a.wk};
+        for (int q = 0; q < 3; ++q)
+            CK(cudaMemcpyAsync(keep + (7 + q) * fsz, src[q], fsz * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    }
+    return GRAL_OK;
+}
+
+// the state of a checkpoint: fields, loop state, IterationLoops; wavefront flags cleared
+int save_checkpoint(gral_ctx *ctx, int q) {
+    const KArgs &a = ctx->ka;
+    cudaStream_t st = ctx->stream;
+    const size_t fsz = (size_t)a.ncols * a.ks;
+    const float *src[NCKPT] = {a.uk, a.vk, a.wk, a.uks, a.vks, a.wks, a.dpmnew};
+    float *dst = ctx->adj_ckpt.p + (size_t)q * NCKPT * fsz;
+    for (int f = 0; f < NCKPT; ++f)
+        CK(cudaMemcpyAsync(dst + f * fsz, src[f], fsz * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(ctx->adj_cksit.p + q, a.sit, sizeof(SitDev), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(ctx->adj_ckit.p + q, a.it_global, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    return GRAL_OK;
+}
+
+int restore_checkpoint(gral_ctx *ctx, int q) {
+    const KArgs &a = ctx->ka;
+    cudaStream_t st = ctx->stream;
+    const size_t fsz = (size_t)a.ncols * a.ks;
+    float *dst[NCKPT] = {a.uk, a.vk, a.wk, a.uks, a.vks, a.wks, a.dpmnew};
+    const float *src = ctx->adj_ckpt.p + (size_t)q * NCKPT * fsz;
+    for (int f = 0; f < NCKPT; ++f)
+        CK(cudaMemcpyAsync(dst[f], src + f * fsz, fsz * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(a.sit, ctx->adj_cksit.p + q, sizeof(SitDev), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(a.it_global, ctx->adj_ckit.p + q, sizeof(int), cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemsetAsync(a.flags, 0, (size_t)a.ncols * sizeof(int), st));
+    return GRAL_OK;
+}
+
+// P and TERMP of the pressure elimination per column, level and i-direction (they depend on the
+// grid and on the row carry of P, not on the state): the forward's row loop replayed on the host
+int pressure_tables(gral_ctx *ctx) {
+    const KArgs &a = ctx->ka;
+    const int ks = a.ks, nj2 = a.nj2, NII = a.nii, NJJ = a.njj;
+    std::vector<ColMeta> meta(a.ncols);
+    std::vector<uint32_t> fl(a.ncols);
+    std::vector<float> tab(5 * (size_t)ks);
+    CK(cudaMemcpy(meta.data(), a.meta, meta.size() * sizeof(ColMeta), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(fl.data(), a.cflags, fl.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(tab.data(), ctx->tables.p, tab.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    const float *APP = tab.data() + 2 * ks, *ABP = tab.data() + 3 * ks, *ATP = tab.data() + 4 * ks;
+    const size_t fsz = (size_t)a.ncols * ks;
+    std::vector<float> pt(4 * fsz, 0.0f);
+    std::vector<float> PIMP(ks + 1);
+    for (int dir = 0; dir < 2; ++dir) {
+        float *P = pt.data() + (size_t)(2 * dir) * fsz, *TM = pt.data() + (size_t)(2 * dir + 1) * fsz;
+        for (int j = 2; j <= NJJ - 1; ++j) {
+            std::fill(PIMP.begin(), PIMP.end(), 0.0f);
+            for (int q = 2; q <= NII - 1; ++q) {
+                const int i = (dir == 0) ? q : NII + 1 - q;
+                const int c = i * nj2 + j;
+                if (!(fl[c] & F_ADV)) continue;
+                for (int k = meta[c].vi; k > meta[c].kkart; --k) {
+                    const float termp = 1 / (APP[k] - ATP[k] * PIMP[k + 1]);
+                    PIMP[k] = ABP[k] * termp;
+                    P[(size_t)c * ks + k] = PIMP[k];
+                    TM[(size_t)c * ks + k] = termp;
+                }
+            }
+        }
+    }
+    CK(ctx->adj_ptab.ensure(pt.size()));
+    CK(cudaMemcpy(ctx->adj_ptab.p, pt.data(), pt.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return GRAL_OK;
+}
+
+int rev_grid(gral_ctx *ctx, const SweepGeom &g) {
+    const double width = (double)g.ni * g.nj / std::max(1, g.ni + g.nj - 1);
+    const long long want = (long long)std::ceil(6.0 * width / AW);
+    return (int)std::max<long long>(ctx->num_sms, std::min<long long>(4LL * ctx->num_sms, want));
+}
+
+}  // namespace
+
+}  // namespace gral
+
+using namespace gral;
+
+extern "C" {
+
+int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static *s, gral_fields *f,
+                          int32_t iterations, int32_t checkpoint_every) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!p || !s || !f) return fail(ctx, GRAL_EINVAL, "null argument");
+    if (p->turbulence_model != 1 || p->simd_width != 8 || p->quantise != 0)
+        return fail(ctx, GRAL_EINVAL, "the adjoint differentiates turbulence model 1, parity width 8, quantise 0");
+    if (iterations < 1 || checkpoint_every < 1) return fail(ctx, GRAL_EINVAL, "iterations and checkpoint_every must be >= 1");
+    ctx->adj_ready = false;
+    gral_params q = *p;
+    q.iteration_steps_min = iterations;
+    q.iteration_steps_max = iterations;
+    q.post_diagnostic = 0;
+    CK(cudaSetDevice(ctx->device));
+    CK_RC(gral_prog_load(ctx, 1, &q, s, f));
+    if (ctx->il) return fail(ctx, GRAL_EINVAL, "the adjoint runs the slab layout (unset GRAL_PROG_LAYOUT)");
+    ctx->fused = false;
+    const KArgs &a = ctx->ka;
+    const size_t fsz = (size_t)a.ncols * a.ks;
+    const int nck = (iterations + checkpoint_every - 1) / checkpoint_every;
+    CK(ctx->adj_ckpt.ensure((size_t)nck * NCKPT * fsz));
+    CK(ctx->adj_cksit.ensure(nck));
+    CK(ctx->adj_ckit.ensure(nck));
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    for (int it = 0; it < iterations; ++it) {
+        if (it % checkpoint_every == 0) CK_RC(save_checkpoint(ctx, it / checkpoint_every));
+        CK_RC(forward_iteration(ctx, nullptr, nullptr));
+    }
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+    ctx->adj_ms_forward = ms;
+    int herr = 0;
+    CK(cudaMemcpy(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "a wavefront wait exceeded its time limit");
+    ctx->it_host = iterations + 1;
+    CK_RC(gral_prog_store(ctx, f, nullptr));
+    int nev[2] = {0, 0};
+    CK(cudaMemcpy(&nev[0], ctx->bc.we_ptr + a.nj2, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&nev[1], ctx->bc.sn_ptr + a.nii + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    ctx->adj_nwe = nev[0];
+    ctx->adj_nsn = nev[1];
+    CK_RC(pressure_tables(ctx));
+    ctx->adj_iters = iterations;
+    ctx->adj_every = checkpoint_every;
+    ctx->adj_ready = true;
+    return GRAL_OK;
+}
+
+int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const float *dj_dwk, float *dj_dveg,
+                  float *dj_duk0, float *dj_dvk0, float *dj_dwk0, gral_vjp_stats *stats) {
+    if (!ctx) return GRAL_EINVAL;
+    if (!ctx->adj_ready) return fail(ctx, GRAL_ESTATE, "gral_prog_vjp before gral_prog_vjp_forward");
+    CK(cudaSetDevice(ctx->device));
+    KArgs &a = ctx->ka;
+    cudaStream_t st = ctx->stream;
+    const int K = ctx->adj_every, N = ctx->adj_iters;
+    const size_t fsz = (size_t)a.ncols * a.ks, ssz = (size_t)a.ncols * (a.nkk + 2);
+    const int nev = ctx->adj_nwe + ctx->adj_nsn;
+    CK(ctx->adj_keep.ensure((size_t)K * NKEEP * fsz));
+    CK(ctx->adj_lam.ensure((size_t)NLAM * fsz));
+    CK(ctx->adj_stg.ensure(3 * ssz));
+    CK(ctx->adj_flags.ensure(a.ncols));
+    CK(ctx->adj_ctr.ensure(4));
+    CK(ctx->adj_bits.ensure((size_t)K * std::max(nev, 1) * a.ks));
+    CK(cudaMemsetAsync(ctx->adj_lam.p, 0, (size_t)NLAM * fsz * sizeof(float), st));
+    CK(cudaMemsetAsync(ctx->adj_flags.p, 0, a.ncols * sizeof(int), st));
+    CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)K * std::max(nev, 1) * a.ks, st));
+    StageLam L{ctx->adj_stg.p, ctx->adj_stg.p + ssz, ctx->adj_stg.p + 2 * ssz};
+    const float *gin[3] = {dj_duk, dj_dvk, dj_dwk};
+    float *stg[3] = {L.u, L.v, L.w};
+    for (int q = 0; q < 3; ++q) {
+        if (gin[q]) CK(cudaMemcpyAsync(stg[q], gin[q], ssz * sizeof(float), cudaMemcpyHostToDevice, st));
+        else CK(cudaMemsetAsync(stg[q], 0, ssz * sizeof(float), st));
+    }
+    AdjArgs d{};
+    for (int q = 0; q < NLAM; ++q) d.lam[q] = ctx->adj_lam.p + (size_t)q * fsz;
+    d.ptab = ctx->adj_ptab.p;
+    d.flags = ctx->adj_flags.p;
+    d.ctr = ctx->adj_ctr.p;
+    d.nwe = ctx->adj_nwe;
+    const int cb = col_blocks(a);
+    k_adj_gather_in<<<cb, 256, 0, st>>>(a, d, L);
+    CK(cudaEventRecord(ctx->ev[0], st));
+    const int g_p = rev_grid(ctx, ctx->geo_p.g), g_u = rev_grid(ctx, ctx->geo_u.g), g_v = rev_grid(ctx, ctx->geo_v.g);
+    int stamp = 0;
+    float ms_re = 0.f, ms_rev = 0.f;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    const int nseg = (N + K - 1) / K;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int it0 = sg * K, n = std::min(K, N - it0);   // iterations it0+1 .. it0+n
+        CK(cudaEventRecord(e0, st));
+        CK_RC(restore_checkpoint(ctx, sg));
+        for (int q = 0; q < n; ++q)
+            CK_RC(forward_iteration(ctx, ctx->adj_keep.p + (size_t)q * NKEEP * fsz,
+                                    ctx->adj_bits.p + (size_t)q * std::max(nev, 1) * a.ks));
+        CK(cudaEventRecord(e1, st));
+        for (int q = n - 1; q >= 0; --q) {
+            const float *kp = ctx->adj_keep.p + (size_t)q * NKEEP * fsz;
+            for (int f = 0; f < 7; ++f) d.mid[f] = kp + f * fsz;
+            for (int f = 0; f < 3; ++f) d.end[f] = kp + (7 + f) * fsz;
+            d.bits = ctx->adj_bits.p + (size_t)q * std::max(nev, 1) * a.ks;
+            d.it = it0 + q + 1;
+            CK(cudaMemsetAsync(d.ctr, 0, 4 * sizeof(unsigned int), st));
+            d.stamp = ++stamp;
+            k_adj_mom<2><<<g_p, AW * 32, 0, st>>>(a, d, ctx->geo_p.g);
+            d.ctr = ctx->adj_ctr.p + 1;
+            d.stamp = ++stamp;
+            k_adj_mom<1><<<g_v, AW * 32, 0, st>>>(a, d, ctx->geo_v.g);
+            d.ctr = ctx->adj_ctr.p + 2;
+            d.stamp = ++stamp;
+            k_adj_mom<0><<<g_u, AW * 32, 0, st>>>(a, d, ctx->geo_u.g);
+            k_adj_avg_copies<<<cb, 256, 0, st>>>(a, d);
+            k_adj_avg_gather<<<cb, 256, 0, st>>>(a, d);
+            k_adj_avg_clear<<<cb, 256, 0, st>>>(a, d);
+            k_adj_velcorr<<<cb, 256, 0, st>>>(a, d);
+            d.ctr = ctx->adj_ctr.p + 3;
+            d.stamp = ++stamp;
+            k_adj_pressure<<<g_p, AW * 32, 0, st>>>(a, d, ctx->geo_p.g);
+            d.ctr = ctx->adj_ctr.p;
+            k_adj_div<<<cb, 256, 0, st>>>(a, d);
+            k_adj_bc_top_rev<<<(a.ncols + 127) / 128, 128, 0, st>>>(a, d);
+            const long long ns = (long long)(a.nii - 1) * a.ks, nw = (long long)(a.njj - 1) * a.ks;
+            k_adj_bc_sn_rev<<<(int)((ns + 127) / 128), 128, 0, st>>>(a, ctx->bc, d);
+            k_adj_bc_we_rev<<<(int)((nw + 127) / 128), 128, 0, st>>>(a, ctx->bc, d);
+        }
+        CK(cudaEventRecord(e2, st));
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        float m1 = 0.f, m2 = 0.f;
+        CK(cudaEventElapsedTime(&m1, e0, e1));
+        CK(cudaEventElapsedTime(&m2, e1, e2));
+        ms_re += m1;
+        ms_rev += m2;
+        int herr = 0;
+        CK(cudaMemcpy(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (herr == ERR_TIMEOUT) {
+            cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+            ctx->adj_ready = false;
+            return fail(ctx, GRAL_ETIMEDOUT, "an adjoint wavefront wait exceeded its time limit");
+        }
+    }
+    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+    // the set-up, reversed
+    k_adj_setup_scatter<<<cb, 256, 0, st>>>(a, d, L);
+    k_adj_setup_zero<<<cb, 256, 0, st>>>(a, d, L);
+    const long long nbd = (long long)(a.njj + a.nii) * (a.nkk - 1);
+    k_adj_setup_border<<<(int)((nbd + 255) / 256), 256, 0, st>>>(a, L);
+    k_adj_setup_avg<<<cb, 256, 0, st>>>(a, d, L);
+    CK(cudaGetLastError());
+    float *out[3] = {dj_duk0, dj_dvk0, dj_dwk0};
+    for (int q = 0; q < 3; ++q)
+        if (out[q]) CK(cudaMemcpyAsync(out[q], stg[q], ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+    if (dj_dveg) {
+        // reuse the first staging block for the VEG cotangent
+        k_adj_veg_out<<<cb, 256, 0, st>>>(a, d, L.u);
+        CK(cudaMemcpyAsync(dj_dveg, L.u, ssz * sizeof(float), cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaEventRecord(ctx->ev[1], st));
+    CK(cudaStreamSynchronize(st));
+    float ms_all = 0.f;
+    CK(cudaEventElapsedTime(&ms_all, ctx->ev[0], ctx->ev[1]));
+    int herr = 0;
+    CK(cudaMemcpy(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "an adjoint wavefront wait exceeded its time limit");
+    if (stats) {
+        stats->iterations = N;
+        stats->checkpoint_every = K;
+        stats->ms_forward = ctx->adj_ms_forward;
+        stats->ms_recompute = ms_re;
+        stats->ms_reverse = ms_rev;
+        stats->ms_total = ms_all;
+    }
+    return GRAL_OK;
+}
+
+}  // extern "C"

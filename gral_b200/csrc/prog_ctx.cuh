@@ -127,6 +127,16 @@ struct gral_ctx {
     DevBuf<unsigned int> counters;
     std::vector<SitDev> h_sit;
     std::vector<int> h_act;
+    // discrete adjoint (gral_prog_vjp_forward / gral_prog_vjp): checkpoints of the forward state,
+    // the states kept for one checkpoint segment, cotangent fields, reverse-sweep flags
+    bool adj_ready = false;
+    int adj_iters = 0, adj_every = 0, adj_nwe = 0, adj_nsn = 0;
+    double adj_ms_forward = 0.0;
+    DevBuf<float> adj_ckpt, adj_keep, adj_lam, adj_ptab, adj_stg;
+    DevBuf<SitDev> adj_cksit;
+    DevBuf<int> adj_ckit, adj_flags;
+    DevBuf<unsigned int> adj_ctr;
+    DevBuf<uint8_t> adj_bits;
 
     ~gral_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -139,6 +149,8 @@ struct gral_ctx {
         prep.release();
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
+        adj_ckpt.release(); adj_keep.release(); adj_lam.release(); adj_ptab.release(); adj_stg.release();
+        adj_cksit.release(); adj_ckit.release(); adj_flags.release(); adj_ctr.release(); adj_bits.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
     }

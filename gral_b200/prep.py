@@ -66,6 +66,23 @@ class Situation:
     potdtdz: float = 0.0
 
 
+def weather_situations(n: int = 144, seed: int = 3) -> List[Situation]:
+    """The batched weather-situation set on a production grid: 36 directions (0-350 deg in 10-deg
+    steps) x 4 speeds (0.5/1/2/4 m/s at 10 m), direction outer, z0 0.5 m, u* = 0.1*speed + 0.1,
+    stability class drawn per situation from {stable, neutral, unstable} with a seeded generator
+    (Obukhov length 50 / 1000 / -50 m, potential temperature gradient 0.01 / 0 / -0.01 K/m); the
+    first n of them."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for d in range(36):
+        for sp in (0.5, 1.0, 2.0, 4.0):
+            cls = int(rng.integers(0, 3))
+            out.append(Situation(direction_deg=10.0 * d, speed_10m=sp, z0=0.5, ustar=0.1 * sp + 0.1,
+                                 obukhov={0: 50.0, 1: 1000.0, 2: -50.0}[cls],
+                                 potdtdz={0: 0.01, 1: 0.0, 2: -0.01}[cls]))
+    return out[:n]
+
+
 @dataclass
 class Domain:
     """Everything a solve needs except the per-situation fields."""
@@ -200,29 +217,23 @@ def log_profile(z: np.ndarray, speed_10m: float, z0: float) -> np.ndarray:
     return speed_10m * np.maximum(np.log(np.maximum(z, 1e-6) / z0), 0.0) / math.log(10.0 / z0)
 
 
-def initial_fields(dom: Domain, sit: Situation, model: int = 1) -> FieldArrays:
-    """Initial UK/VK/WK (and TURB/TDISS buffers) with the obstacle rules of MicroscaleFlat.cs."""
+def _masked_fields(dom: Domain, u: np.ndarray, v: np.ndarray, dtype):
+    """UK, VK of the domain from per-level profiles u, v (index = level), with the obstacle rules
+    of MicroscaleFlat.cs: zero inside obstacles and on faces shared with an obstacle cell, the
+    east/north edge copies, zero at level 0."""
     nii, njj, nkk = dom.nii, dom.njj, dom.nkk
     st = dom.static
     shape = (nii + 2, njj + 2, nkk + 2)
-    uk = np.zeros(shape, F32)
-    vk = np.zeros(shape, F32)
-    wk = np.zeros(shape, F32)
+    uk = np.zeros(shape, dtype)
+    vk = np.zeros(shape, dtype)
     vertk = np.zeros(nkk + 2, F32)
     vertk[1:nkk + 1] = st.hokart[0:nkk] + st.dzk[1:nkk + 1] * F32(0.5)
-    sp = log_profile(vertk.astype(np.float64), sit.speed_10m, sit.z0)
-    th = math.radians(sit.direction_deg)
-    u = (-sp * math.sin(th)).astype(F32)
-    v = (-sp * math.cos(th)).astype(F32)
-    u[0] = v[0] = 0
-    u[nkk + 1] = v[nkk + 1] = 0
     cut = st.cutk
     inside = vertk[None, None, :] <= cut[:, :, None]             # cell (i,j,k) inside an obstacle
     inside[..., 0] = False
     inside[..., nkk + 1] = False
     uk[1:nii + 1, 1:njj + 1, :] = u
     vk[1:nii + 1, 1:njj + 1, :] = v
-    # zero inside obstacles and on faces shared with an obstacle cell
     uk[inside] = 0
     vk[inside] = 0
     uk[2:nii + 1][inside[1:nii]] = 0                              # west neighbour is an obstacle
@@ -231,11 +242,68 @@ def initial_fields(dom: Domain, sit: Situation, model: int = 1) -> FieldArrays:
     vk[1:nii + 1, njj + 1, :] = vk[1:nii + 1, njj, :]
     uk[..., 0] = 0
     vk[..., 0] = 0
+    return uk, vk
+
+
+def _cell_heights(dom: Domain) -> np.ndarray:
+    nkk = dom.nkk
+    vertk = np.zeros(nkk + 2, F32)
+    vertk[1:nkk + 1] = dom.static.hokart[0:nkk] + dom.static.dzk[1:nkk + 1] * F32(0.5)
+    return vertk
+
+
+def initial_fields(dom: Domain, sit: Situation, model: int = 1) -> FieldArrays:
+    """Initial UK/VK/WK (and TURB/TDISS buffers) with the obstacle rules of MicroscaleFlat.cs."""
+    nii, njj, nkk = dom.nii, dom.njj, dom.nkk
+    shape = (nii + 2, njj + 2, nkk + 2)
+    vertk = _cell_heights(dom)
+    sp = log_profile(vertk.astype(np.float64), sit.speed_10m, sit.z0)
+    th = math.radians(sit.direction_deg)
+    u = (-sp * math.sin(th)).astype(F32)
+    v = (-sp * math.cos(th)).astype(F32)
+    u[0] = v[0] = 0
+    u[nkk + 1] = v[nkk + 1] = 0
+    uk, vk = _masked_fields(dom, u, v, F32)
+    wk = np.zeros(shape, F32)
     turb = tdiss = None
     if model != 1:
         turb = np.zeros(shape, F32)
         tdiss = np.zeros(shape, F32)
     return FieldArrays(uk, vk, wk, turb, tdiss)
+
+
+KARMAN = 0.4
+
+
+def inflow_tangents(dom: Domain, sit: Situation) -> dict:
+    """Derivatives of the initial UK, VK of ``initial_fields`` with respect to the inflow
+    parameters of the neutral log-law profile u(z) = (u*/0.4) ln(z/z0) along the direction
+    (u* = 0.4 * speed_10m / ln(10/z0)): name -> (dUK, dVK) in float64 for "ustar" (z0 and the
+    direction fixed), "z0" (u* and the direction fixed) and "direction_deg" (per degree)."""
+    nkk = dom.nkk
+    z = _cell_heights(dom).astype(np.float64)
+    ustar = KARMAN * sit.speed_10m / math.log(10.0 / sit.z0)
+    lnz = np.log(np.maximum(z, 1e-6) / sit.z0)
+    pos = lnz > 0
+    sp = np.where(pos, ustar / KARMAN * lnz, 0.0)
+    th = math.radians(sit.direction_deg)
+    dsp = {"ustar": np.where(pos, lnz / KARMAN, 0.0), "z0": np.where(pos, -ustar / (KARMAN * sit.z0), 0.0)}
+    out = {}
+    for name, d in dsp.items():
+        du, dv = -d * math.sin(th), -d * math.cos(th)
+        du[0] = dv[0] = du[nkk + 1] = dv[nkk + 1] = 0.0
+        out[name] = _masked_fields(dom, du, dv, np.float64)
+    du, dv = -sp * math.cos(th) * math.pi / 180.0, sp * math.sin(th) * math.pi / 180.0
+    du[0] = dv[0] = du[nkk + 1] = dv[nkk + 1] = 0.0
+    out["direction_deg"] = _masked_fields(dom, du, dv, np.float64)
+    return out
+
+
+def inflow_gradient(dom: Domain, sit: Situation, dj_duk0: np.ndarray, dj_dvk0: np.ndarray) -> dict:
+    """dJ/d(u*, z0, direction) from the cotangents of the initial UK, VK (chain rule through
+    ``inflow_tangents``)."""
+    return {name: float((du * dj_duk0).sum() + (dv * dj_dvk0).sum())
+            for name, (du, dv) in inflow_tangents(dom, sit).items()}
 
 
 # --------------------------------------------------------------------------------------------
@@ -283,6 +351,73 @@ def city_domain(n: int = 400, dx: float = 2.0, dz1: float = 2.0, stretch: float 
     """Production-size grid: 400x400 cells at 2 m, 64 seeded buildings, 10-30 m tall."""
     bl = random_buildings(n, n, dx, n_buildings, seed)
     return make_domain(n, n, dx, dz1, stretch, vert_cells_ff, bl, **kw)
+
+
+def adjoint_domain(n: int = 200, dx: float = 2.0, dz1: float = 2.0, stretch: float = 1.05, vert_cells_ff: int = 25,
+                   n_buildings: int = 30, veg_fraction: float = 0.2, veg_max: float = 0.5, seed: int = 5) -> Domain:
+    """The differentiation workload: an n x n grid at 2 m (first layer 2 m, stretching 1.05),
+    seeded buildings, and a vegetation drag density over `veg_fraction` of the columns: a smooth
+    random field in [0, veg_max] m^-1 (sums of Gaussian bumps, thresholded to the wanted cover) on
+    the levels of a 2-15 m canopy, with cover 0.5 where it is set."""
+    rng = np.random.default_rng(7000 + seed)
+    fmax = min(40.0, (n - 2 * 6 - 2) * dx / 2)        # footprints 10-40 m, narrowed on small grids
+    bl = random_buildings(n, n, dx, n_buildings, seed, foot_m=(min(10.0, fmax), fmax),
+                          height_m=(10.0, 30.0) if n >= 100 else (4.0, 14.0))
+    nkk, dzk, hok = vertical_grid_flat(dz1, stretch)
+    xs = np.arange(n + 2, dtype=np.float64)
+    field2 = np.zeros((n + 2, n + 2))
+    for _ in range(max(4, n // 8)):
+        cx, cy, sg = rng.uniform(0, n), rng.uniform(0, n), rng.uniform(2.0, max(3.0, n / 10))
+        field2 += rng.uniform(0.3, 1.0) * np.exp(-((xs[:, None] - cx) ** 2 + (xs[None, :] - cy) ** 2) / (2 * sg * sg))
+    field2[0, :] = field2[:, 0] = field2[n + 1, :] = field2[:, n + 1] = 0
+    inner = field2[1:n + 1, 1:n + 1]
+    thr = np.quantile(inner, 1.0 - veg_fraction)
+    dens = np.where(field2 > thr, (field2 - thr) / max(float(inner.max() - thr), 1e-12), 0.0) * veg_max
+    veg = np.zeros((n + 2, n + 2, nkk + 2), F32)
+    zc = hok[0:nkk + 1] + 0.5 * dzk[1:nkk + 2]
+    canopy = (zc >= 0.0) & (zc <= 15.0)
+    for k in range(1, nkk + 1):
+        if canopy[k - 1]:
+            veg[:, :, k - 1] = dens.astype(F32)
+    cov = np.where(dens > 0, F32(0.5), F32(0)).astype(F32)
+    return make_domain(n, n, dx, dz1, stretch, vert_cells_ff, bl, veg=veg, cov=cov)
+
+
+def probe_misfit(dom: Domain, fields, n_probes: int = 1000, seed: int = 11, noise: float = 0.1):
+    """Seeded probe cells (i, j, k) inside the prognostic sub-domains, above the surface and within
+    the prognostic levels, and targets u_target = the given fields there plus seeded noise, for the
+    misfit J = sum over probes of |(U, V, W) - target|^2.  Returns (flat indices, targets [n, 3])."""
+    rng = np.random.default_rng(seed)
+    st = dom.static
+    cand = []
+    for i in range(3, dom.nii - 1):
+        for j in range(3, dom.njj - 1):
+            if st.advdom[i, j] == 1:
+                cand.append((i, j))
+    idx = []
+    nk2 = dom.nkk + 2
+    for q in rng.integers(0, len(cand), n_probes):
+        i, j = cand[int(q)]
+        kk = int(st.kkart[i, j])
+        k = int(rng.integers(kk + 2, kk + dom.vert_cells_ff))
+        idx.append((i * (dom.njj + 2) + j) * nk2 + k)
+    idx = np.array(idx, np.int64)
+    tgt = np.stack([a.reshape(-1)[idx] for a in (fields.uk, fields.vk, fields.wk)], axis=1).astype(np.float64)
+    tgt = tgt + rng.normal(0.0, noise, tgt.shape)
+    return idx, tgt
+
+
+def misfit_and_cotangent(idx: np.ndarray, tgt: np.ndarray, uk, vk, wk, dtype=np.float64):
+    """J = sum |(U, V, W)(probe) - target|^2 and its cotangents dJ/dUK, dJ/dVK, dJ/dWK."""
+    J = 0.0
+    gs = []
+    for q, a in enumerate((uk, vk, wk)):
+        r = a.reshape(-1)[idx].astype(np.float64) - tgt[:, q]
+        J += float((r * r).sum())
+        g = np.zeros(a.size, np.float64)
+        np.add.at(g, idx, 2.0 * r)
+        gs.append(g.reshape(a.shape).astype(dtype))
+    return J, gs
 
 
 def hilly_domain(nii: int, njj: int, dx: float, vert_cells_ff: int, seed: int, n_hills: Optional[int] = None,

@@ -16,8 +16,8 @@ import numpy as np
 
 from . import build as _build
 from .abi import (GRAL_OK, PARTICLE_DTYPE, STATUS_NAMES, FieldArrays, GralFields, GralFlatGrid, GralMet,
-                  GralParams, GralStatic, GralStats, GralVegPoint, GralWindGrid, MetProfile, StaticArrays,
-                  params_to_c, stats_to_dict, veg_points_to_c)
+                  GralParams, GralStatic, GralStats, GralVegPoint, GralVjpStats, GralWindGrid, MetProfile,
+                  StaticArrays, params_to_c, stats_to_dict, veg_points_to_c)
 
 _lib = None
 
@@ -26,7 +26,8 @@ EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_pro
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
            "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack",
            "gral_prog_subdomains", "gral_prog_flat_init", "gral_prog_vegetation", "gral_prog_prep_last_ms",
-           "gral_prog_wind_at", "gral_prog_solve_instances", "gral_prog_load_flat"]
+           "gral_prog_wind_at", "gral_prog_solve_instances", "gral_prog_load_flat", "gral_prog_vjp_forward",
+           "gral_prog_vjp"]
 
 # payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
 GFF_COLUMNS, GFF_LEVELS, GFF_TERRAIN, GFF_TKE = 0, 1, 2, 3
@@ -113,6 +114,11 @@ def lib(build_if_stale: bool = True):
     L.gral_prog_load_flat.argtypes = [vp, C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralMet),
                                       C.POINTER(GralFlatGrid), C.POINTER(GralFields)]
     L.gral_prog_load_flat.restype = C.c_int
+    L.gral_prog_vjp_forward.argtypes = [vp, C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralFields),
+                                        C.c_int32, C.c_int32]
+    L.gral_prog_vjp_forward.restype = C.c_int
+    L.gral_prog_vjp.argtypes = [vp] + [vp] * 7 + [C.POINTER(GralVjpStats)]
+    L.gral_prog_vjp.restype = C.c_int
     _lib = L
     return L
 
@@ -212,6 +218,32 @@ class PrognosticSolver:
         st = self._stats_array(n, traces)
         self._check(self._L.gral_prog_store(self._ctx, fa, st))
         return [stats_to_dict(st[b]) for b in range(n)]
+
+    # discrete adjoint of the unrolled SIMPLE iterations (model 1, parity width 8, no rounding)
+    def vjp_forward(self, params: dict, static: StaticArrays, fields: FieldArrays, iterations: int,
+                    checkpoint_every: int = 20):
+        """Forward run of the differentiated map: `iterations` SIMPLE iterations of one situation,
+        in place on ``fields``, with checkpoints kept on the device for ``vjp``."""
+        p = params_to_c(params)
+        s = static.to_c()
+        f = fields.to_c()
+        self._keep = [p, s, f, static, fields]
+        self._check(self._L.gral_prog_vjp_forward(self._ctx, C.byref(p), C.byref(s), C.byref(f), iterations,
+                                                  checkpoint_every))
+
+    def vjp(self, dj_duk: Optional[np.ndarray], dj_dvk: Optional[np.ndarray] = None,
+            dj_dwk: Optional[np.ndarray] = None):
+        """Vector-Jacobian product of the last ``vjp_forward``: cotangents of its final UK, VK, WK
+        (float32 host layout, None = zero) -> (dJ/dVEG, dJ/dUK0, dJ/dVK0, dJ/dWK0, stats dict)."""
+        ref = next(a for a in (dj_duk, dj_dvk, dj_dwk) if a is not None)
+        shape = ref.shape
+        ins = [None if a is None else np.ascontiguousarray(a, np.float32) for a in (dj_duk, dj_dvk, dj_dwk)]
+        outs = [np.zeros(shape, np.float32) for _ in range(4)]
+        st = GralVjpStats()
+        ptr = [None if a is None else a.ctypes.data for a in ins]
+        self._check(self._L.gral_prog_vjp(self._ctx, *ptr, *(o.ctypes.data for o in outs), C.byref(st)))
+        stats = {name: getattr(st, name) for name, _ in GralVjpStats._fields_}
+        return outs[0], outs[1], outs[2], outs[3], stats
 
     # flow-field cache payloads (GFFWrite.cs / GFFRead.cs); the zip container stays with the caller
     def gff_size(self, mode: int) -> int:

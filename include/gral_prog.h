@@ -347,6 +347,40 @@ int gral_prog_load_flat(gral_ctx *ctx, int32_t n, const gral_params *p, const gr
  * events around its launches, host copies excluded). */
 int gral_prog_prep_last_ms(gral_ctx *ctx, double *kernel_ms);
 
+/* ---- Discrete adjoint of the unrolled SIMPLE iterations (vector-Jacobian product) ----
+ *
+ * Differentiates the map that PrognosticFlowfield.Calculate (PrognosticFlowfield.cs:584-1137)
+ * applies to one situation's initial U, V, W and its vegetation density VEG over a fixed number
+ * of iterations, in the configuration turbulence_model = 1, simd_width = 8, quantise = 0 (the Frund
+ * rounding has derivative zero almost everywhere).  The set-up's scalars (topwind, DTIME, AP0,
+ * UG, VG, the wall-law help terms) are constants of the map; kinks of max/min/abs follow the
+ * branch the forward takes.  Every wait of the reverse sweeps is bounded (GRAL_ETIMEDOUT). */
+
+/* Runs `iterations` SIMPLE iterations of one situation (p, s, f as for gral_prog_solve; p's
+ * iteration limits are replaced by `iterations`, post_diagnostic is ignored), keeping the state
+ * every `checkpoint_every` iterations on the device, and writes the final fields to f.  The
+ * checkpoints stay for gral_prog_vjp until the next load of the context.  GRAL_EINVAL for another
+ * model, parity width or rounding, or a batched layout. */
+int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static *s, gral_fields *f,
+                          int32_t iterations, int32_t checkpoint_every);
+
+typedef struct gral_vjp_stats {
+    int32_t iterations, checkpoint_every;
+    double ms_forward;     /* device time of the forward run in gral_prog_vjp_forward */
+    double ms_recompute;   /* device time of the segment recomputations inside gral_prog_vjp */
+    double ms_reverse;     /* device time of the reverse sweeps */
+    double ms_total;       /* device time of gral_prog_vjp */
+} gral_vjp_stats;
+
+/* The vector-Jacobian product of the last gral_prog_vjp_forward: given the cotangents dJ/dUK,
+ * dJ/dVK, dJ/dWK of its final fields ([NII+2][NJJ+2][NKK+2] host arrays, NULL = zero), writes
+ * dJ/dVEG (same layout; zero where VEG[i][j] is null) and dJ/d(initial UK, VK, WK) (same layout).
+ * Any output may be NULL.  The checkpoint segments are recomputed from the kept states (each
+ * segment once), so the fields resident on the device afterwards are those of an intermediate
+ * iteration.  stats may be NULL. */
+int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const float *dj_dwk, float *dj_dveg,
+                  float *dj_duk0, float *dj_dvk0, float *dj_dwk0, gral_vjp_stats *stats);
+
 /* Text of the last error on this context (never NULL). */
 const char *gral_prog_last_error(gral_ctx *ctx);
 

@@ -679,6 +679,9 @@ template void u_mom_ml<double>(StateT<double> &, int, int, int, float, float, fl
 template void v_mom_ml<double>(StateT<double> &, int, int, int, float, float, float, float);
 template void w_mom_ml<double>(StateT<double> &, int, int, int, float, float, float);
 template void u_mom_ml<AD>(StateT<AD> &, int, int, int, float, float, float, float);
+template void u_mom_ml<Dual>(StateT<Dual> &, int, int, int, float, float, float, float);
+template void v_mom_ml<Dual>(StateT<Dual> &, int, int, int, float, float, float, float);
+template void w_mom_ml<Dual>(StateT<Dual> &, int, int, int, float, float, float);
 template void v_mom_ml<AD>(StateT<AD> &, int, int, int, float, float, float, float);
 template void w_mom_ml<AD>(StateT<AD> &, int, int, int, float, float, float);
 

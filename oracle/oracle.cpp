@@ -133,6 +133,7 @@ struct LoopConsts {
 inline double val(float x) { return (double)x; }
 inline double val(double x) { return x; }
 inline double val(const AD &x) { return x.v; }
+inline double val(const Dual &x) { return x.v; }
 
 /* the velocity-correction rounding of the float oracle; the FP64 twin runs without rounding */
 template <class T>
@@ -443,6 +444,17 @@ double initial_staggered(StateT<T> &st) {
         }
     }
     return GESCHW_MAX;
+}
+
+/* Border copies UK[NII+1] = UK[NII], VK[.][NJJ+1] = VK[.][NJJ] on levels 1..NKK-1 of the set-up
+ * (PrognosticFlowfield.cs:410-432); setup_solve makes them in its TURB loop. */
+template <class T>
+void border_copies(StateT<T> &st) {
+    const int NII = st.nii, NJJ = st.njj, NKK = st.nkk;
+    for (int j = 1; j <= NJJ; ++j)
+        for (int k = 1; k <= NKK - 1; ++k) st.uk[st.i3(NII + 1, j, k)] = st.uk[st.i3(NII, j, k)];
+    for (int i = 1; i < NII + 1; ++i)
+        for (int k = 1; k <= NKK - 1; ++k) st.vk[st.i3(i, NJJ + 1, k)] = st.vk[st.i3(i, NJJ, k)];
 }
 
 /* Velocities (and TKE) inside buildings set to zero (PrognosticFlowfield.cs:518-575). */
@@ -783,6 +795,7 @@ extern "C" int oracle_twin_forward(const gral_params *p, const gral_static *s, c
     StateT<double> st;
     twin_state(st0, st, fields, vegd.data());
     initial_staggered(st);
+    border_copies(st);
     zero_in_buildings(st, 1);
     for (int it = 1; it <= iterations; ++it) simple_iteration(st, o.c, it);
     std::memcpy(uk, st.uk, n3 * sizeof(double));
@@ -819,6 +832,7 @@ extern "C" int oracle_twin_vjp(const gral_params *p, const gral_static *s, const
     StateT<double> st;
     twin_state(st0, st, fields, vegd.data());
     initial_staggered(st);
+    border_copies(st);
     zero_in_buildings(st, 1);
     std::vector<std::vector<double>> keep((size_t)iterations, std::vector<double>(kTwinFields * n3));
     for (int it = 1; it <= iterations; ++it) {
@@ -871,6 +885,7 @@ extern "C" int oracle_twin_vjp(const gral_params *p, const gral_static *s, const
     StateT<AD> sa;
     twin_state(st0, sa, adf, adveg.data());
     initial_staggered(sa);
+    border_copies(sa);
     zero_in_buildings(sa, 1);
     adj.assign(tape.nodes.size(), 0.0);
     for (int q = 0; q < kTwinFields; ++q) {
@@ -886,5 +901,36 @@ extern "C" int oracle_twin_vjp(const gral_params *p, const gral_static *s, const
         d_veg[c] = lveg[c];
     }
     g_tape = nullptr;
+    return GRAL_OK;
+}
+
+/* Forward-mode tangent of the twin: d(final UK, VK, WK) along the direction (duk0, dvk0, dwk0, dveg)
+ * of (initial fields, VEG), all double host layout (dveg may be NULL). */
+extern "C" int oracle_twin_jvp(const gral_params *p, const gral_static *s, const gral_fields *f_ref,
+                               const double *uk0, const double *vk0, const double *wk0, const double *veg,
+                               const double *duk0, const double *dvk0, const double *dwk0, const double *dveg,
+                               int iterations, double *duk, double *dvk, double *dwk) {
+    int rc = twin_validate(p, iterations);
+    if (rc != GRAL_OK) return rc;
+    State st0;
+    SetupOut o;
+    std::vector<float> scratch;
+    rc = twin_setup(p, s, f_ref, st0, o, scratch);
+    if (rc != GRAL_OK) return rc;
+    const size_t n3 = (size_t)st0.ni2 * st0.nj2 * st0.nk2;
+    std::vector<Dual> vegd(n3), fields(3 * n3);
+    for (size_t q = 0; q < n3; ++q) {
+        vegd[q] = Dual(veg ? veg[q] : (s->veg ? (double)s->veg[q] : 0.0), dveg ? dveg[q] : 0.0);
+        fields[q] = Dual(uk0[q], duk0[q]);
+        fields[n3 + q] = Dual(vk0[q], dvk0[q]);
+        fields[2 * n3 + q] = Dual(wk0[q], dwk0[q]);
+    }
+    StateT<Dual> st;
+    twin_state(st0, st, fields, vegd.data());
+    initial_staggered(st);
+    border_copies(st);
+    zero_in_buildings(st, 1);
+    for (int it = 1; it <= iterations; ++it) simple_iteration(st, o.c, it);
+    for (size_t q = 0; q < n3; ++q) { duk[q] = st.uk[q].d; dvk[q] = st.vk[q].d; dwk[q] = st.wk[q].d; }
     return GRAL_OK;
 }

@@ -21,7 +21,7 @@ _LIB = os.path.join(_HERE, "liboracle.so")
 # racy-order throughput analogue (CPU baseline only): the same sources built with the sweeps over
 # host threads, -O3 -march=native, on the machine that runs it
 _LIB_MT = os.path.join(_HERE, "liboracle_mt.so")
-_SRCS = ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "prep.cpp", "wind.cpp", "oracle_common.h", "Makefile",
+_SRCS = ("oracle.cpp", "mom_ml.cpp", "mom_ke.cpp", "prep.cpp", "wind.cpp", "oracle_common.h", "oracle_ad.h", "Makefile",
          os.path.join("..", "include", "gral_prog.h"))
 _lib = None
 _lib_mt = None
@@ -104,6 +104,9 @@ def _bind_twin(h):
     h.oracle_twin_vjp.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralFields),
                                   D, D, D, D, C.c_int, D, D, D, D, D, D, D]
     h.oracle_twin_vjp.restype = C.c_int
+    h.oracle_twin_jvp.argtypes = [C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralFields),
+                                  D, D, D, D, D, D, D, D, C.c_int, D, D, D]
+    h.oracle_twin_jvp.restype = C.c_int
     h._twin_bound = True
     return h
 
@@ -145,4 +148,23 @@ def twin_vjp(params: dict, static: StaticArrays, f_ref: FieldArrays, x0, veg, it
                                            *(_dptr(o) for o in out))
     if rc != GRAL_OK:
         raise RuntimeError(f"oracle_twin_vjp failed: {STATUS_NAMES.get(rc, rc)}")
+    return tuple(out)
+
+
+def twin_jvp(params: dict, static: StaticArrays, f_ref: FieldArrays, x0, veg, iterations: int, dx0, dveg=None):
+    """Forward-mode tangent of the FP64 twin along (dx0 = (duk0, dvk0, dwk0), dveg): returns the
+    derivative of the final (uk, vk, wk)."""
+    p = params_to_c(params)
+    s = static.to_c()
+    fr = f_ref.to_c()
+    a = [np.ascontiguousarray(q, np.float64) for q in x0]
+    da = [np.ascontiguousarray(q, np.float64) for q in dx0]
+    vg = None if veg is None else np.ascontiguousarray(veg, np.float64)
+    dv = None if dveg is None else np.ascontiguousarray(dveg, np.float64)
+    out = [np.zeros_like(a[0]) for _ in range(3)]
+    rc = _bind_twin(lib()).oracle_twin_jvp(C.byref(p), C.byref(s), C.byref(fr), *(_dptr(q) for q in a), _dptr(vg),
+                                           *(_dptr(q) for q in da), _dptr(dv), int(iterations),
+                                           *(_dptr(q) for q in out))
+    if rc != GRAL_OK:
+        raise RuntimeError(f"oracle_twin_jvp failed: {STATUS_NAMES.get(rc, rc)}")
     return tuple(out)

@@ -5,8 +5,9 @@
  * prognostic path (oracle/adjoint.cpp).  Every arithmetic operation on tape values appends one
  * node holding the indices of its (at most two) operands and the local partial derivatives; the
  * reverse sweep walks the tape backwards.  Values that depend on no input (grid constants) carry
- * index -1 and record nothing.  Comparisons act on values, so max/min/abs and the branches of the
- * solver differentiate along the branch taken (the subgradient of the kink).
+ * index -1 and record nothing.  Comparisons act on values, so the branches of the solver differentiate
+ * along the branch taken; max/min at a tie and |x| at zero take the mean of the one-sided
+ * derivatives.
  *
  * This is an independent derivation of the gradient: it differentiates the oracle's own
  * operations, not the library's hand-written adjoint.
@@ -89,14 +90,67 @@ inline bool operator>=(const AD &x, const AD &y) { return x.v >= y.v; }
 inline bool operator==(const AD &x, const AD &y) { return x.v == y.v; }
 inline bool operator!=(const AD &x, const AD &y) { return x.v != y.v; }
 
-inline AD vmax(const AD &a, const AD &b) { return (a > b) ? a : b; }
-inline AD vmin(const AD &a, const AD &b) { return (a < b) ? a : b; }
+/* At a tie of max/min and at the kink of |x| the derivative is the mean of the two one-sided
+ * ones, which is what a central difference across the kink measures (and the true derivative
+ * where two kinks cancel, as |F| and max(F, 0) do in the power law at F = 0). */
+inline AD vmax(const AD &a, const AD &b) {
+    if (a.v == b.v) return AD::make(a.v, a.i, 0.5, b.i, 0.5);
+    return (a > b) ? a : b;
+}
+inline AD vmin(const AD &a, const AD &b) {
+    if (a.v == b.v) return AD::make(a.v, a.i, 0.5, b.i, 0.5);
+    return (a < b) ? a : b;
+}
 inline AD osqrt(const AD &x) {
     const double r = std::sqrt(x.v);
     return AD::make(r, x.i, r > 0.0 ? 0.5 / r : 0.0, -1, 0.0);   /* subgradient 0 at the root */
 }
-inline AD ofabs(const AD &x) { return AD::make(std::fabs(x.v), x.i, x.v < 0.0 ? -1.0 : 1.0, -1, 0.0); }
+inline AD ofabs(const AD &x) {
+    return AD::make(std::fabs(x.v), x.i, x.v < 0.0 ? -1.0 : (x.v > 0.0 ? 1.0 : 0.0), -1, 0.0);
+}
 inline AD ofma(const AD &a, const AD &b, const AD &c) { return a * b + c; }
+
+/* Forward-mode dual number (value, derivative along one direction): the tangent of the same
+ * operations, an independent check of the tape's reverse sweep. */
+struct Dual {
+    double v = 0.0, d = 0.0;
+    Dual() = default;
+    Dual(double x) : v(x), d(0.0) {}
+    Dual(float x) : v((double)x), d(0.0) {}
+    Dual(int x) : v((double)x), d(0.0) {}
+    Dual(double x, double dx) : v(x), d(dx) {}
+};
+inline Dual operator+(const Dual &x, const Dual &y) { return Dual(x.v + y.v, x.d + y.d); }
+inline Dual operator-(const Dual &x, const Dual &y) { return Dual(x.v - y.v, x.d - y.d); }
+inline Dual operator*(const Dual &x, const Dual &y) { return Dual(x.v * y.v, x.d * y.v + x.v * y.d); }
+inline Dual operator/(const Dual &x, const Dual &y) {
+    const double q = x.v / y.v;
+    return Dual(q, (x.d - q * y.d) / y.v);
+}
+inline Dual operator-(const Dual &x) { return Dual(-x.v, -x.d); }
+inline Dual &operator+=(Dual &x, const Dual &y) { return x = x + y; }
+inline Dual &operator-=(Dual &x, const Dual &y) { return x = x - y; }
+inline Dual &operator*=(Dual &x, const Dual &y) { return x = x * y; }
+inline bool operator<(const Dual &x, const Dual &y) { return x.v < y.v; }
+inline bool operator>(const Dual &x, const Dual &y) { return x.v > y.v; }
+inline bool operator<=(const Dual &x, const Dual &y) { return x.v <= y.v; }
+inline bool operator>=(const Dual &x, const Dual &y) { return x.v >= y.v; }
+inline bool operator==(const Dual &x, const Dual &y) { return x.v == y.v; }
+inline bool operator!=(const Dual &x, const Dual &y) { return x.v != y.v; }
+inline Dual vmax(const Dual &a, const Dual &b) {
+    if (a.v == b.v) return Dual(a.v, 0.5 * (a.d + b.d));
+    return (a > b) ? a : b;
+}
+inline Dual vmin(const Dual &a, const Dual &b) {
+    if (a.v == b.v) return Dual(a.v, 0.5 * (a.d + b.d));
+    return (a < b) ? a : b;
+}
+inline Dual osqrt(const Dual &x) {
+    const double r = std::sqrt(x.v);
+    return Dual(r, r > 0.0 ? 0.5 * x.d / r : 0.0);
+}
+inline Dual ofabs(const Dual &x) { return Dual(std::fabs(x.v), x.v < 0.0 ? -x.d : (x.v > 0.0 ? x.d : 0.0)); }
+inline Dual ofma(const Dual &a, const Dual &b, const Dual &c) { return a * b + c; }
 
 }  // namespace oracle
 
