@@ -12,6 +12,11 @@ model; synthetic, seeded inputs.
              set-up, 500 SIMPLE iterations, post-checks, fields back to the host), host-timed.
   roofline   dominant kernel's algorithmic bytes per launch / its mean CUDA-event duration,
              against the measured HBM copy bandwidth.
+  batched    the batched form on the same grid: the 144-situation weather set (36 directions x 4
+             speeds, seeded stability) as one batch, 10 device-timed iterations (throughput, phase
+             split, roofline), and `to_stop`: the whole set solved to its stop rule (_delta < 1e-3
+             tested every 100 iterations, or 800 iterations) in one batched call against plain
+             single-situation calls, both host-timed end to end, in situations/hour.
   cpu_baseline  the racy-order multi-threaded restatement of the reference's default parallel
              mode on all host threads, on a bounded sample of the same workload (with the
              single-threaded deterministic oracle beside it).
@@ -24,6 +29,9 @@ model; synthetic, seeded inputs.
   instances  independent situations on grids of different sizes (the uneven-domain batch: grids
              log-uniform 128x128x20 .. 512x512x40 at 2-4 m, hills and buildings, random inflow),
              solved one at a time and side by side (gral_prog_solve_instances), host-timed.
+  adjoint    the discrete adjoint (gral_prog_vjp) of 200 unrolled iterations on a 200x200x25 grid
+             with vegetation drag over 20 % of the columns and a 1000-probe misfit: device times of
+             the forward with checkpoints and of the vector-Jacobian product, and their ratio.
   gff        the flow-field cache writer/reader (GFFWrite.cs / GFFRead.cs formats) on the same
              grid: device pack kernel per format (CUDA events, L2 flushed before each launch)
              against HBM bandwidth, the host-timed pack into pinned memory and read back, and
@@ -555,6 +563,85 @@ def instances_measure(n: int = 16, iterations: int = 100, concurrent: int = 16, 
     return out
 
 
+def to_stop_measure(dom, batch: int = 144, max_iters: int = 800, threshold: float = 1e-3, plain_n: int = 1):
+    """The weather-situation set solved to its stop rule (rank 0 only): each situation stops at
+    _delta < threshold at a test every 100 iterations (from iteration 100) or at max_iters, as one
+    batched solve through gral_prog_solve_batch, against plain single-situation solves of the first
+    plain_n situations of the set (one call each); both host-timed end to end (fields in, set-up,
+    iterations, post-checks, fields out), situations/hour measured, not extrapolated."""
+    from gral_b200 import prep
+    from gral_b200.prognostic import PrognosticSolver
+    sits = batched_situations(batch)
+    ps = [dom.params(x, model=1, iterations=max_iters, iter_min=100, conv_threshold=threshold) for x in sits]
+    fs = [prep.initial_fields(dom, x) for x in sits]
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax, max_batch=batch) as s:
+        t0 = time.perf_counter()
+        sts = s.calculate_batch(ps, dom.static, fs)
+        bt = time.perf_counter() - t0
+    its = [x["iterations"] for x in sts]
+    plain_s = []
+    plain_its = []
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
+        for q in range(plain_n):
+            f = prep.initial_fields(dom, sits[q])
+            t0 = time.perf_counter()
+            st = s.calculate(ps[q], dom.static, f)
+            plain_s.append(time.perf_counter() - t0)
+            plain_its.append(st["iterations"])
+    per_plain = statistics.mean(plain_s)
+    return {"workload": f"{batch} situations of the weather set on the {dom.nii}x{dom.njj}x{dom.vert_cells_ff} grid, "
+                        f"stop at _delta < {threshold} (tested every 100 iterations) or {max_iters} iterations",
+            "batched": {"seconds": round(bt, 3), "situations_per_hour": round(3600.0 * batch / bt, 1),
+                        "iterations_min": min(its), "iterations_max": max(its),
+                        "iterations_mean": round(statistics.mean(its), 1),
+                        "converged": int(sum(x["converged"] for x in sts))},
+            "plain": {"situations_timed": plain_n, "seconds_per_situation": round(per_plain, 3),
+                      "iterations": plain_its, "situations_per_hour": round(3600.0 / per_plain, 1)},
+            "batched_over_plain": round((3600.0 * batch / bt) / (3600.0 / per_plain), 3),
+            "note": "one GPU; the plain form's situations/hour assumes the timed situations are representative "
+                    "(same stop rule; every situation of the set ran to the same limit when none converged)"}
+
+
+def adjoint_measure(iterations: int = 200, every: int = 20, n: int = 200):
+    """The discrete adjoint on the differentiation workload (rank 0 only): a 200x200 grid at 2 m
+    with 25 prognostic levels, 30 buildings, vegetation drag over 20 % of the columns, J = sum over
+    1000 seeded probe cells of |(U, V, W) - target|^2 after 200 iterations, checkpoints every 20."""
+    import numpy as np
+    from gral_b200 import prep
+    from gral_b200.prognostic import PrognosticSolver
+
+    dom = prep.adjoint_domain(n)
+    sit = prep.Situation(direction_deg=250.0, speed_10m=2.0, z0=0.3)
+    f0 = prep.initial_fields(dom, sit)
+    p = dom.params(sit, model=1, iterations=iterations, quantise=0)
+    with PrognosticSolver(dom.nii, dom.njj, dom.nkk, dom.kadvmax) as s:
+        fr = f0.copy()
+        s.load([p], dom.static, [fr])               # the plain solve of the same map: fused launches
+        s.iterate_timed(3)
+        plain_ms, _ = s.iterate_timed(iterations - 3)
+        plain_ms *= iterations / (iterations - 3)
+        f = f0.copy()
+        s.vjp_forward(p, dom.static, f, iterations, every)
+        idx, tgt = prep.probe_misfit(dom, f, n_probes=1000, seed=11)
+        J, g = prep.misfit_and_cotangent(idx, tgt, f.uk, f.vk, f.wk, np.float32)
+        d_veg, d_uk0, d_vk0, d_wk0, st = s.vjp(*g)
+        d_veg, d_uk0, d_vk0, d_wk0, st = s.vjp(*g)   # second call timed (first one pays the allocations)
+    inflow = prep.inflow_gradient(dom, sit, d_uk0.astype(np.float64), d_vk0.astype(np.float64))
+    fwd = st["ms_forward"]
+    return {"workload": f"{n}x{n}x{dom.vert_cells_ff} at 2 m, {len(dom.buildings)} buildings, VEG over "
+                        f"{float(dom.static.veg_mask[1:n + 1, 1:n + 1].mean()):.2f} of the columns, 1000 probes, "
+                        f"{iterations} iterations, checkpoints every {every}",
+            "J": J, "iterations": iterations, "checkpoint_every": every,
+            "forward_ms": round(fwd, 2), "plain_solve_ms": round(plain_ms, 2),
+            "vjp_ms": round(st["ms_total"], 2), "recompute_ms": round(st["ms_recompute"], 2),
+            "reverse_ms": round(st["ms_reverse"], 2),
+            "cost_multiple_of_forward": round((fwd + st["ms_total"]) / fwd, 3),
+            "cost_multiple_of_plain_solve": round((fwd + st["ms_total"]) / plain_ms, 3),
+            "grad_norm_veg": float(np.linalg.norm(d_veg)), "dJ_dinflow": inflow,
+            "checks": "GPU gradients against FP64 central differences (20 directions, 32x32, 20 iterations) and "
+                      "the FP64 tape gradient in tests/test_adjoint_gpu.py"}
+
+
 def run_ours(args, rank, world):
     import torch
     from gral_b200 import prep
@@ -616,6 +703,13 @@ def run_ours(args, rank, world):
                    "phase_ms_per_iteration": {k: round(v / args.batched_steps, 4) for k, v in bph.items() if v > 0},
                    "clocks": bclk}
 
+    # the weather set solved to its stop rule, batched against plain (single GPU)
+    tostop = None
+    if args.workload == "production" and rank == 0 and world == 1 and not args.no_batched and not args.no_to_stop:
+        tostop = to_stop_measure(dom, args.batch)
+        if batched is not None:
+            batched["to_stop"] = tostop
+
     # the measurements of the rows around the solve run on single-GPU runs only
     extras = rank == 0 and world == 1 and args.workload == "production"
     gffm = None
@@ -631,6 +725,9 @@ def run_ours(args, rank, world):
     instm = None
     if extras and not args.no_instances:
         instm = instances_measure()
+    adjm = None
+    if extras and not args.no_adjoint:
+        adjm = adjoint_measure()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -658,7 +755,7 @@ def run_ours(args, rank, world):
         "cpu_baseline": cpu, "e2e": e2e,
         "gpu_launches": st_store["launches_per_iteration"] * args.steps,
         "clocks": clocks,
-        "gff": gffm, "prep": prepm, "wind": windm, "instances": instm,
+        "gff": gffm, "prep": prepm, "wind": windm, "instances": instm, "adjoint": adjm,
         # last on the line, so that a reader keeping only the end of the line still has it
         "batched": batched,
     }
@@ -687,6 +784,8 @@ def main():
     ap.add_argument("--no-prep", action="store_true", help="skip the set-up (sub-domains, initial field) measurement")
     ap.add_argument("--no-wind", action="store_true", help="skip the particle wind interpolation measurement")
     ap.add_argument("--no-instances", action="store_true", help="skip the uneven-domain instances measurement")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint measurement")
+    ap.add_argument("--no-to-stop", action="store_true", help="skip the weather set solved to its stop rule")
     ap.add_argument("--ref-iters", type=int, default=4, help="SIMPLE iterations per reference-arm step")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
