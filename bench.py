@@ -17,9 +17,9 @@ model; synthetic, seeded inputs.
              split, roofline), and `to_stop`: the whole set solved to its stop rule (_delta < 1e-3
              tested every 100 iterations, or 800 iterations) in one batched call against plain
              single-situation calls, both host-timed end to end, in situations/hour.
-  cpu_baseline  the racy-order multi-threaded restatement of the reference's default parallel
-             mode on all host threads, on a bounded sample of the same workload (with the
-             single-threaded deterministic oracle beside it).
+  cpu_baseline  the C++ restatement on all host cores, in the faster of its two host forms (one
+             situation over all threads in the reference's racy work split, or one single-threaded
+             situation per core), on a bounded sample of the same workload.
   prep       the flow-field set-up before the solve (sub-domains, flat-terrain initial field,
              vegetation) on the same grid: device kernel time (CUDA events) against HBM bandwidth,
              host-timed calls including the copies, and the oracle restatement on one core.
@@ -38,9 +38,10 @@ model; synthetic, seeded inputs.
              the numpy restatement of the writer timed on one core.
 
 `--impl reference` times the CPU path on this host's cores and prints the same metric: the C#
-reference cannot run here (no .NET SDK), so its racy-order restatement (the reference's default
-parallel work split over all host threads, -O3 -march=native, built on the host) solves one
-situation per step.
+reference cannot run here (no .NET SDK), so its C++ restatement (-O3 -march=native, built on the
+host) runs each step both as one situation with its sweeps over all host threads in the
+reference's default (racy) work split and as one single-threaded situation per core in separate
+processes; the faster form is the value.
 Multi-GPU (torchrun): every rank solves its own replica of the workload (a single situation does
 not shard); value = all ranks' cell-iterations / max-over-ranks time.
 """
@@ -245,42 +246,86 @@ def cpu_sample(workload_name: str, iterations: int, threaded: bool = True):
     return nominal_cells(dom) * iterations / dt / 1e6, dt, threads
 
 
-CPU_KIND_TEXT = ("racy-order multi-threaded C++ restatement of the reference's default parallel mode "
-                 "(i-slab / j-row work split of its Parallel.For loops, -O3 -march=native, built on this "
-                 "host); a restatement, not the reference (no .NET SDK on the host)")
+CPU_KIND_TEXT = ("C++ restatement of the reference's solver, -O3 -march=native, built on this host; a "
+                 "restatement, not the reference (no .NET SDK on the host)")
+
+
+def _one_thread_env():
+    os.environ["ORACLE_THREADS"] = "1"
+
+
+def _cpu_worker(job):
+    name, iters = job
+    return cpu_sample(name, iters)
+
+
+class CpuBaseline:
+    """The CPU path on every host core in the two ways a host runs it: one situation with the sweeps
+    split over all threads in the reference's default (racy) work split -- what one GRAL process
+    does -- and one single-threaded situation per core in independent processes -- what several
+    GRAL processes on one host do.  The faster of the two is the baseline."""
+
+    def __init__(self, workload_name: str, iters: int):
+        import multiprocessing as mp
+        from oracle import oracle as O
+        O.build_threaded()
+        self.name = workload_name if workload_name != "batched" else "production"
+        self.iters = iters
+        self.cores = os.cpu_count() or 1
+        self.pool = mp.get_context("spawn").Pool(self.cores, initializer=_one_thread_env)
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+    def step(self):
+        """One sample of each form: (threaded Mcell-it/s, threads, seconds; processes Mcell-it/s, seconds)."""
+        v_t, dt_t, thr = cpu_sample(self.name, self.iters)
+        t0 = time.perf_counter()
+        res = self.pool.map(_cpu_worker, [(self.name, self.iters)] * self.cores, chunksize=1)
+        dt_p = time.perf_counter() - t0
+        dom, _, _, _ = workload(self.name)
+        v_p = nominal_cells(dom) * self.iters * self.cores / dt_p / 1e6
+        return v_t, thr, dt_t, v_p, dt_p
+
+    def describe(self, v_t, thr, dt_t, v_p, dt_p):
+        best = "threaded" if v_t >= v_p else "processes"
+        return {"value": round(max(v_t, v_p), 4), "unit": UNIT, "cores": self.cores, "kind": "port",
+                "form": best,
+                "sample": (f"{self.iters} SIMPLE iterations (set-up included) of one situation with its sweeps over "
+                           f"{thr} threads in the reference's default work split: {v_t:.3f} Mcell-it/s ({dt_t:.1f} s); "
+                           f"{self.cores} situations in {self.cores} single-threaded processes: {v_p:.3f} Mcell-it/s "
+                           f"({dt_p:.1f} s); the faster is the baseline; {CPU_KIND_TEXT}"),
+                "threaded": round(v_t, 4), "processes": round(v_p, 4), **host_cpu()}
 
 
 def run_reference(args, rank, world):
     """The reference's CPU path on this host's cores: the C# solver cannot run here (no .NET SDK),
-    so its racy-order restatement runs one situation per step with every host thread on the sweeps,
-    set-up included, for args.ref_iters SIMPLE iterations."""
+    so its restatement runs each step in both host forms (CpuBaseline), set-up included, for
+    args.ref_iters SIMPLE iterations per situation."""
     if rank != 0:
         return
-    from oracle import oracle as O
-    O.build_threaded()
-    iters = args.ref_iters
-    for _ in range(args.warmup):
-        cpu_sample(args.workload if args.workload != "batched" else "production", iters)
-    times, threads = [], 1
-    for _ in range(args.steps):
-        _, dt, threads = cpu_sample(args.workload if args.workload != "batched" else "production", iters)
-        times.append(dt)
-    dom, _, _, desc = workload(args.workload)
+    cb = CpuBaseline(args.workload, args.ref_iters)
+    try:
+        for _ in range(args.warmup):
+            cb.step()
+        samples = [cb.step() for _ in range(args.steps)]
+    finally:
+        cb.close()
+    med = [statistics.median(x[q] for x in samples) for q in range(5)]
+    desc = cb.describe(med[0], samples[0][1], med[2], med[3], med[4])
+    value = desc["value"]
+    dom, _, _, wdesc = workload(args.workload)
     cells = nominal_cells(dom)
-    per_step = statistics.median(times)
-    value = cells * iters / per_step / 1e6
+    per_step = cells * args.ref_iters / (value * 1e6)
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(per_step * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic", "config": {"workload": args.workload, "description": desc,
-                                       "cells_per_situation": cells, "situations_per_step": 1,
-                                       "iterations_per_situation": iters},
-        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"1 situation x {iters} SIMPLE iterations per step (set-up included), "
-                                   f"{threads} threads; {CPU_KIND_TEXT}",
-                         **host_cpu()},
-        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "data": "synthetic", "config": {"workload": args.workload, "description": wdesc,
+                                       "cells_per_situation": cells, "iterations_per_situation": args.ref_iters},
+        "cpu_baseline": desc,
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
@@ -731,15 +776,11 @@ def run_ours(args, rank, world):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        wl = "production" if args.workload == "batched" else args.workload
-        v, dt, thr = cpu_sample(wl, args.cpu_iters)
-        v1, dt1, _ = cpu_sample(wl, 2, threaded=False)
-        cpu = {"value": round(v, 4), "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"one situation, {args.cpu_iters} SIMPLE iterations of the same workload ({dt:.1f} s, "
-                         f"set-up included), {thr} threads; {CPU_KIND_TEXT}",
-               "single_thread_oracle": {"value": round(v1, 4), "unit": UNIT, "cores": 1,
-                                        "sample": f"2 iterations ({dt1:.1f} s), deterministic oracle, -O2"},
-               **host_cpu()}
+        cb = CpuBaseline(args.workload, args.cpu_iters)
+        try:
+            cpu = cb.describe(*cb.step())
+        finally:
+            cb.close()
 
     line = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -775,7 +816,7 @@ def main():
     ap.add_argument("--batch", type=int, default=144, help="situations of the batched workload")
     ap.add_argument("--grid", type=int, default=400, help="columns per side of the city grid (profiling cases)")
     ap.add_argument("--e2e-iters", type=int, default=0, help="iterations of the e2e solve (0: the workload's)")
-    ap.add_argument("--cpu-iters", type=int, default=10)
+    ap.add_argument("--cpu-iters", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched sub-measurement")
