@@ -71,6 +71,12 @@ struct gral_ctx {
     int lookahead = 8;         // GRAL_PROG_LOOKAHEAD: plain-family warps per average diagonal width
     int lookahead_p = 3;       // GRAL_PROG_LOOKAHEAD_P: the same for the pressure sweep
     int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
+    // slab family, model 1: 0 = the diagonal-claim wavefront (fused pressure..U, then V, W);
+    // 1+v = strip variant v for pressure, U, V, W (-1: not tuned yet)
+    int pmode = -1;
+    int forced_pmode = -1;     // GRAL_PROG_PLAIN_MODE
+    int strip_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // indexed by PH_*
+    float ptune_ms[16] = {0};  // autotuner timings per plain mode
     std::string err = "no error";
 
     // current load

@@ -792,6 +792,121 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom
     gs_tasks_split<PH_PRESSURE, false>(a, g, job);
 }
 
+// ---------------------------- strip schedule, slab family -------------------------------------
+// The same split tasks, scheduled by strips of sweep rows.  A block claims a strip (one situation,
+// SR consecutive rows i1) from an atomic counter, in order, and runs it column by column: warp
+// (r, m) takes row r's columns j1 = ja+m, ja+m+SMW, ...  A task's row predecessor (i1, j1-1) is
+// then another warp of the block, and so is its column predecessor (i1-1, j1) unless r = 0.  Those
+// hand-offs go through per-row progress counters in shared memory (CTA-scope release/acquire)
+// instead of a global flag's round trips through L2; only a strip's first row waits on a global
+// flag, published by the previous strip's last row.  Every task still publishes its global flag,
+// after the shared counter, for the waits of other tasks on it (the pressure row carry's writer).
+// Strips are claimed in order and a strip only waits on earlier ones, so no co-residency is
+// assumed.  While one warp of a row waits and solves, the row's other warps evaluate the pre-wait
+// parts of its next columns.
+
+__device__ __forceinline__ int ld_acquire_cta(const int *p) {
+    int v;
+    asm volatile("ld.acquire.cta.shared::cta.s32 %0, [%1];"
+                 : "=r"(v)
+                 : "r"((unsigned)__cvta_generic_to_shared(p))
+                 : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_cta(int *p, int v) {
+    asm volatile("st.release.cta.shared::cta.s32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)), "r"(v)
+                 : "memory");
+}
+
+// Spin (one thread) until the shared progress counter *cnt reaches `need`.  Bounded like
+// wait_stamps: gives up after limit_ns or on another warp's error and returns false then.
+__device__ inline bool wait_count(const int *cnt, int need, int *err, unsigned long long limit_ns) {
+    if (ld_acquire_cta(cnt) >= need) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    for (unsigned n = 1;; ++n) {
+        if (ld_acquire_cta(cnt) >= need) return true;
+        if ((n & 15) == 0) {
+            if (*(volatile int *)err != ERR_NONE) return false;
+            if (globaltimer_ns() - t0 > limit_ns) {
+                atomicCAS(err, ERR_NONE, ERR_TIMEOUT);
+                return false;
+            }
+        }
+    }
+}
+
+template <int PHASE, bool REVERSE, int SR, int SMW, class Job>
+__device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &g, Job &job, int *s_done,
+                                               unsigned *s_claim) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int r = warp / SMW, m = warp % SMW;
+    const unsigned units = (unsigned)*a.nact;
+    const unsigned total = (unsigned)((g.ni + SR - 1) / SR) * units;
+    unsigned int *ctr = a.counters + PHASE;
+    const int it = *a.it_global;
+    int IS, JS;
+    sweep_dir(it, IS, JS);
+    if (REVERSE) { IS = -IS; JS = -JS; }
+    const int stamp = it * 8 + PHASE;
+    job.stamp = stamp;
+    for (;;) {
+        if (threadIdx.x == 0) *s_claim = (*(volatile int *)a.err != ERR_NONE) ? 0xffffffffu : atomicAdd(ctr, 1u);
+        if (threadIdx.x < SR) s_done[threadIdx.x] = 0;
+        __syncthreads();
+        const unsigned t = *s_claim;
+        if (t >= total) break;
+        const int u = a.act[t % units];
+        const int i1 = g.ia + (int)(t / units) * SR + r;
+        if (i1 < g.ia + g.ni) {
+            const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+            int *fl = a.flags + (size_t)u * a.ncols;
+            for (int c = m; c < g.nj; c += SMW) {
+                const int j1 = g.ja + c;
+                const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                job.pre(u, i, j, IS, JS, i1 == g.ia);
+                int ok = 1;
+                if (lane == 0) {
+                    ok = wait_count(s_done + r, c, a.err, a.wait_limit_ns);
+                    if (ok && r > 0) ok = wait_count(s_done + r - 1, c + 1, a.err, a.wait_limit_ns);
+                    else if (ok && i1 > g.ia)
+                        ok = wait_stamps(fl + (i - IS) * a.nj2 + j, nullptr, stamp, a.err, a.wait_limit_ns, 0);
+                }
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                __syncwarp();
+                if (ok) job.post(u, IS, JS);
+                __syncwarp();
+                if (lane == 0) {
+                    st_release_cta(s_done + r, c + 1);
+                    st_release(fl + i * a.nj2 + j, stamp);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    job.finish();
+}
+
+template <int SR, int SMW>
+__global__ void __launch_bounds__(SR * SMW * 32, 1) k_pressure_strip(KArgs a, SweepGeom g) {
+    __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ int s_done[SR];
+    __shared__ unsigned s_claim;
+    PressJob job{a, sm[threadIdx.x >> 5], 0};
+    job.run_max = 0;
+    job.run_s = -1;
+    gs_tasks_strip<PH_PRESSURE, false, SR, SMW>(a, g, job, s_done, &s_claim);
+}
+
+template <int COMP, int SR, int SMW>
+__global__ void __launch_bounds__(SR * SMW * 32, 1) k_mom1_strip(KArgs a, SweepGeom g) {
+    __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ int s_done[SR];
+    __shared__ unsigned s_claim;
+    Mom1Job<COMP> job{a, sm[threadIdx.x >> 5], 0};
+    constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
+    gs_tasks_strip<PH, COMP == COMP_V, SR, SMW>(a, g, job, s_done, &s_claim);   // model-1 V sweeps with (-IS,-JS)
+}
+
 // ---------------------------- fused wavefront, slab family --------------------------------
 // Pressure, velocity correction, averages and the model-1 U sweep of one iteration in one launch.
 // U sweeps in the pressure's direction and reads only the averages of its 3x3 neighbourhood, so
@@ -1331,6 +1446,30 @@ const BVariant kVariants[] = {GRAL_BV(8, 2), GRAL_BV(4, 4), GRAL_BV(4, 6), GRAL_
                               GRAL_BV(5, 5), GRAL_BV(6, 5), GRAL_BV(5, 6)};
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
+// Strip variants of the slab family's model-1 sweeps: (rows per strip, warps per row).
+struct SVariant {
+    int sr, smw;
+    KFn pressure;
+    KFn mom[3];   // [comp]
+};
+
+#define GRAL_SV(SR, SMW)                                                                           \
+    SVariant{SR, SMW, k_pressure_strip<SR, SMW>,                                                   \
+             {k_mom1_strip<COMP_U, SR, SMW>, k_mom1_strip<COMP_V, SR, SMW>, k_mom1_strip<COMP_W, SR, SMW>}}
+
+const SVariant kStrips[] = {GRAL_SV(4, 4), GRAL_SV(2, 8), GRAL_SV(3, 5), GRAL_SV(2, 6)};
+constexpr int kNumStrips = sizeof(kStrips) / sizeof(kStrips[0]);
+
+KFn strip_kernel(int v, int kind) {
+    const SVariant &S = kStrips[v];
+    switch (kind) {
+        case PH_PRESSURE: return S.pressure;
+        case PH_U: return S.mom[0];
+        case PH_V: return S.mom[1];
+        default: return S.mom[2];
+    }
+}
+
 const KFn kPlainMom[3][3] = {{k_mom<0, COMP_U>, k_mom<0, COMP_V>, k_mom<0, COMP_W>},
                              {k_mom1s<COMP_U>, k_mom1s<COMP_V>, k_mom1s<COMP_W>},
                              {k_mom<2, COMP_U>, k_mom<2, COMP_V>, k_mom<2, COMP_W>}};
@@ -1418,6 +1557,21 @@ void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStrea
     } else {
         plain_kernel(kind, a.model)<<<grid, GS_WARPS * 32, 0, st>>>(a, g);
     }
+}
+
+int strip_num_variants() { return kNumStrips; }
+
+int strip_rows(int variant) { return kStrips[variant].sr; }
+
+int strip_block_threads(int variant) { return kStrips[variant].sr * kStrips[variant].smw * 32; }
+
+cudaError_t strip_occupancy(int kind, int variant, int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, strip_kernel(variant, kind),
+                                                         strip_block_threads(variant), 0);
+}
+
+void launch_strip(int kind, const KArgs &a, const SweepGeom &g, int variant, int grid, cudaStream_t st) {
+    strip_kernel(variant, kind)<<<grid, strip_block_threads(variant), 0, st>>>(a, g);
 }
 
 size_t diag_smem(int ks) { return (size_t)GS_WARPS * 6 * ks * sizeof(float); }

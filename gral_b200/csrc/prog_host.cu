@@ -216,11 +216,26 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
     return GRAL_OK;
 }
 
+// The slab family's model-1 sweeps run on the strip schedule (pmode 1+v) rather than the
+// diagonal-claim wavefront (pmode 0).
+bool use_strips(const gral_ctx *ctx) { return !ctx->il && ctx->model == 1 && ctx->pmode > 0; }
+
 // One SIMPLE iteration (PrognosticFlowfield.cs:584-1182), enqueued on st.
 void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
     cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
+    if (use_strips(ctx)) {
+        const int v = ctx->pmode - 1;
+        launch_strip(PH_PRESSURE, a, ctx->geo_p.g, v, ctx->strip_grid[PH_PRESSURE], st);
+        launch_velcorr(a, st);
+        launch_average(a, st);
+        launch_strip(PH_U, a, ctx->geo_u.g, v, ctx->strip_grid[PH_U], st);
+        launch_strip(PH_V, a, ctx->geo_v.g, v, ctx->strip_grid[PH_V], st);
+        launch_strip(PH_W, a, ctx->geo_p.g, v, ctx->strip_grid[PH_W], st);
+        launch_bookkeeping(a, st);
+        return;
+    }
     if (ctx->fused) {
         launch_fused_pvau(a, ctx->fgeo, ctx->fused_grid, st);
     } else {
@@ -242,6 +257,7 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
 int launches_per_iteration(const gral_ctx *ctx) {
     const int gs = ctx->ka.group_set <= 0 ? ctx->ngroups : ctx->ka.group_set;
     const int sets = ctx->il ? (ctx->ngroups + gs - 1) / gs : 1;
+    if (use_strips(ctx)) return 3 + 4 + 3;
     if (ctx->fused) return 3 + 1 + 2 + 1;
     const int phases = (ctx->model == 2) ? 5 : 4;
     return 3 + phases * sets + 3;
@@ -275,6 +291,19 @@ int size_grids(gral_ctx *ctx) {
         if (!il && la > 0) blocks = std::max<long long>(ctx->num_sms, std::min(blocks, want_blocks));
         ctx->grid_gs[kinds[q]] = (int)blocks;
     }
+    if (use_strips(ctx)) {
+        // one block per strip at most: the strip kernels are persistent and claim strips in order
+        const int sv = ctx->pmode - 1;
+        const Geom *gk[4] = {&ctx->geo_p, &ctx->geo_u, &ctx->geo_v, &ctx->geo_p};
+        for (int q = 0; q < 4; ++q) {
+            int bps = 0;
+            CK(strip_occupancy(kinds[q], sv, &bps));
+            const int sr = strip_rows(sv);
+            const long long strips = (long long)((gk[q]->g.ni + sr - 1) / sr) * ctx->nb;
+            ctx->strip_grid[kinds[q]] =
+                (int)std::max<long long>(1, std::min<long long>((long long)std::max(1, bps) * ctx->num_sms, strips));
+        }
+    }
     const int warps = ctx->grid_gs[PH_PRESSURE] * gs_block_threads(il, v) / 32;
     const long long per_diag = (long long)(il ? ctx->ngroups : ctx->nb) * std::min(ctx->nii, ctx->njj);
     ctx->ka.chunk = il ? 1 : (int)std::max(1LL, std::min(16LL, per_diag / (2LL * warps)));
@@ -300,8 +329,11 @@ int build_graph(gral_ctx *ctx) {
 // iterations of the solve each run one variant, timed with CUDA events, and the fastest is kept
 // and captured into the iteration graph.  Runs only when enough iterations remain before the
 // first convergence test; otherwise variant 0 is used.
+int tune_plain(gral_ctx *ctx);
+
 int tune_variants(gral_ctx *ctx) {
-    if (!ctx->il || ctx->variant >= 0) return GRAL_OK;
+    if (!ctx->il) return tune_plain(ctx);
+    if (ctx->variant >= 0) return GRAL_OK;
     const int nv = gs_num_variants() * (ctx->ngroups > 2 ? 3 : (ctx->ngroups > 1 ? 2 : 1));
     const int first_stop = std::min(((ctx->it_host + ctx->cadence - 1) / ctx->cadence) * ctx->cadence, ctx->it_max);
     if (ctx->forced_variant >= 0 && ctx->forced_variant < nv) {
@@ -327,6 +359,50 @@ int tune_variants(gral_ctx *ctx) {
         ctx->variant = best_v;
     } else {
         ctx->variant = 0;
+    }
+    int rc = size_grids(ctx);
+    if (rc != GRAL_OK) return rc;
+    return build_graph(ctx);
+}
+
+// Autotuner of the slab family (model 1): the diagonal-claim wavefront and every strip variant
+// give bit-identical results, so before the first convergence test each mode runs two live
+// iterations (the first warms the kernels up), the second timed with CUDA events, and the fastest
+// mode is kept and captured into the iteration graph.  Without room for the trials the default
+// mode is kept.
+constexpr int kDefaultPlainMode = 1;   // strips of 4 rows, 4 warps per row (fastest on the 400x400 grid)
+
+int tune_plain(gral_ctx *ctx) {
+    if (ctx->pmode >= 0) return GRAL_OK;
+    const int nv = 1 + strip_num_variants();
+    const int first_stop = std::min(((ctx->it_host + ctx->cadence - 1) / ctx->cadence) * ctx->cadence, ctx->it_max);
+    if (ctx->model != 1) {
+        ctx->pmode = 0;
+    } else if (ctx->forced_pmode >= 0 && ctx->forced_pmode < nv) {
+        ctx->pmode = ctx->forced_pmode;
+    } else if (first_stop - ctx->it_host + 1 > 2 * nv) {
+        cudaStream_t st = ctx->stream;
+        float best = 1e30f;
+        int best_v = 0;
+        for (int v = 0; v < nv; ++v) {
+            ctx->pmode = v;
+            int rc = size_grids(ctx);
+            if (rc != GRAL_OK) return rc;
+            launch_iteration(ctx, st);
+            ctx->it_host++;
+            CK(cudaEventRecord(ctx->ev[2], st));
+            launch_iteration(ctx, st);
+            CK(cudaEventRecord(ctx->ev[3], st));
+            CK(cudaEventSynchronize(ctx->ev[3]));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+            if (v < 16) ctx->ptune_ms[v] = ms;
+            if (ms < best) { best = ms; best_v = v; }
+            ctx->it_host++;
+        }
+        ctx->pmode = best_v;
+    } else {
+        ctx->pmode = kDefaultPlainMode;
     }
     int rc = size_grids(ctx);
     if (rc != GRAL_OK) return rc;
@@ -383,6 +459,7 @@ int gral_prog_create(int32_t nii, int32_t njj, int32_t nkk, int32_t kadvmax, int
         else if (std::strcmp(lay, "slab") == 0) ctx->il_min_batch = 1 << 30;
     }
     if (const char *v = std::getenv("GRAL_PROG_BATCH_VARIANT")) ctx->forced_variant = std::atoi(v);
+    if (const char *v = std::getenv("GRAL_PROG_PLAIN_MODE")) ctx->forced_pmode = std::atoi(v);
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD")) ctx->lookahead = std::max(0, std::atoi(v));
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD_P")) ctx->lookahead_p = std::max(0, std::atoi(v));
     if (const char *v = std::getenv("GRAL_PROG_LOOKAHEAD_F")) ctx->lookahead_f = std::max(0, std::atoi(v));
@@ -836,12 +913,9 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(gs_prepare(il, ks, ctx->model));
     ctx->it_host = 1;
     ctx->variant = -1;
+    ctx->pmode = -1;
     int brc = size_grids(ctx);
     if (brc != GRAL_OK) return brc;
-    if (!il) {
-        brc = build_graph(ctx);
-        if (brc != GRAL_OK) return brc;
-    }
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(cudaStreamSynchronize(st));
     CK(cudaEventElapsedTime(&ctx->ms_upload, ctx->ev[0], ctx->ev[1]));
@@ -900,7 +974,15 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
         cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
         launch_bc(a, ctx->bc, st);
     }});
-    if (ctx->fused) {
+    const int sv = ctx->pmode - 1;
+    if (use_strips(ctx)) {
+        seq.push_back({GRAL_PHASE_PRESSURE, [&] { launch_strip(PH_PRESSURE, a, ctx->geo_p.g, sv, ctx->strip_grid[PH_PRESSURE], st); }});
+        seq.push_back({GRAL_PHASE_VELCORR, [&] { launch_velcorr(a, st); }});
+        seq.push_back({GRAL_PHASE_AVERAGE, [&] { launch_average(a, st); }});
+        seq.push_back({GRAL_PHASE_U, [&] { launch_strip(PH_U, a, ctx->geo_u.g, sv, ctx->strip_grid[PH_U], st); }});
+        seq.push_back({GRAL_PHASE_V, [&] { launch_strip(PH_V, a, ctx->geo_v.g, sv, ctx->strip_grid[PH_V], st); }});
+        seq.push_back({GRAL_PHASE_W, [&] { launch_strip(PH_W, a, ctx->geo_p.g, sv, ctx->strip_grid[PH_W], st); }});
+    } else if (ctx->fused) {
         seq.push_back({GRAL_PHASE_FUSED, [&] { launch_fused_pvau(a, ctx->fgeo, ctx->fused_grid, st); }});
     } else {
         seq.push_back({GRAL_PHASE_PRESSURE, [&] { launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st); }});
@@ -908,8 +990,10 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
         seq.push_back({GRAL_PHASE_AVERAGE, [&] { launch_average(a, st); }});
         seq.push_back({GRAL_PHASE_U, [&] { launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st); }});
     }
-    seq.push_back({GRAL_PHASE_V, [&] { launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st); }});
-    seq.push_back({GRAL_PHASE_W, [&] { launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st); }});
+    if (!use_strips(ctx)) {
+        seq.push_back({GRAL_PHASE_V, [&] { launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st); }});
+        seq.push_back({GRAL_PHASE_W, [&] { launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st); }});
+    }
     if (ctx->model == 2)
         seq.push_back({GRAL_PHASE_TKE, [&] { launch_gs(PH_TKE, a, ctx->geo_p.g, ctx->grid_gs[PH_TKE], st); }});
     seq.push_back({GRAL_PHASE_BOOKKEEPING, [&] { launch_bookkeeping(a, st); }});
@@ -1024,7 +1108,7 @@ int gral_prog_store(gral_ctx *ctx, gral_fields *f, gral_stats *stats) {
         o.ms_upload = ctx->ms_upload;
         o.ms_download = ms_down;
         o.layout = ctx->il ? 1 : 0;
-        o.launch_variant = ctx->il ? ctx->variant : -1;
+        o.launch_variant = ctx->il ? ctx->variant : ctx->pmode;
         o.launches_per_iteration = launches_per_iteration(ctx);
     }
     if (rc != GRAL_OK) fail(ctx, rc, "non-finite values in the solved fields");

@@ -28,6 +28,13 @@ cudaError_t gs_prepare(bool il, int ks, int model);
 cudaError_t gs_occupancy(bool il, int kind, int model, int simd, int ks, int variant, int *blocks_per_sm);
 // one Gauss-Seidel phase (kind = PH_PRESSURE, PH_U, PH_V, PH_W or PH_TKE) of the loaded model
 void launch_gs(int kind, const KArgs &a, const SweepGeom &g, int grid, cudaStream_t st);
+// strip schedule of the slab family's model-1 sweeps (kind = PH_PRESSURE, PH_U, PH_V, PH_W): a
+// block per strip of strip_rows(variant) sweep rows, hand-offs inside a strip in shared memory
+int strip_num_variants();
+int strip_rows(int variant);
+int strip_block_threads(int variant);
+cudaError_t strip_occupancy(int kind, int variant, int *blocks_per_sm);
+void launch_strip(int kind, const KArgs &a, const SweepGeom &g, int variant, int grid, cudaStream_t st);
 // pressure + velocity correction + averages + model-1 U in one wavefront launch (slab family)
 cudaError_t fused_occupancy(int *blocks_per_sm);
 void launch_fused_pvau(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st);

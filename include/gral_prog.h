@@ -121,7 +121,10 @@ typedef struct gral_stats {
     double ms_total, ms_upload, ms_iterate, ms_download;
     int32_t layout;              /* device layout used: 0 slab (one warp per column), 1 interleaved
                                     (32 situations per group, one block per group-column) */
-    int32_t launch_variant;      /* launch variant the autotuner kept (interleaved layout) */
+    int32_t launch_variant;      /* launch variant the autotuner kept: interleaved layout, the batched
+                                    kernels' variant; slab layout, the schedule of the model-1 sweeps
+                                    (0 diagonal-claim wavefront, 1+v strip variant v; GRAL_PROG_PLAIN_MODE
+                                    forces one) */
     int32_t launches_per_iteration; /* kernel launches of one SIMPLE iteration in the kept configuration */
 } gral_stats;
 
