@@ -504,47 +504,49 @@ __device__ __forceinline__ void ml_forward(float (*S)[KMAX_LEVELS], int K0, int 
 
 __device__ __forceinline__ void ml_backward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI, int kkm, float relax,
                                             float top) {
-    float Q = 0.0f;
-    int k = K0;
+    // Q_k = D_k*T_k up to KKART+1 (K0 <= KKART+1 always), then Q_k = (D_k + C_k*Q_{k-1})*T_k;
+    // the level ranges are split instead of selecting per level, which keeps the chain short
+    const int kq = min(KK + 1, VI);
+    for (int k = K0; k <= kq; ++k) S[3][k] = S[3][k] * S[0][k];
+    float Q = S[3][kq];
+    int k = kq + 1;
     for (; k + TCH - 1 <= VI; k += TCH) {
         float T[TCH], D[TCH], C[TCH];
 #pragma unroll
         for (int q = 0; q < TCH; ++q) { T[q] = S[0][k + q]; D[q] = S[3][k + q]; C[q] = S[2][k + q]; }
 #pragma unroll
         for (int q = 0; q < TCH; ++q) {
-            Q = (k + q > KK + 1) ? (D[q] + C[q] * Q) * T[q] : D[q] * T[q];
+            Q = (D[q] + C[q] * Q) * T[q];
             D[q] = Q;
         }
 #pragma unroll
         for (int q = 0; q < TCH; ++q) S[3][k + q] = D[q];
     }
     for (; k <= VI; ++k) {
-        const float T = S[0][k], D = S[3][k];
-        Q = (k > KK + 1) ? (D + S[2][k] * Q) * T : D * T;
+        Q = (S[3][k] + S[2][k] * Q) * S[0][k];
         S[3][k] = Q;
     }
+    // relaxed back-substitution downwards over the levels above kkm (the others keep their value
+    // and lie below every updated level)
+    const int kb = max(K0, kkm + 1);
     float up = top;
     k = VI;
-    for (; k - (TCH - 1) >= K0; k -= TCH) {
+    for (; k - (TCH - 1) >= kb; k -= TCH) {
         float P[TCH], Qv[TCH], U[TCH];
 #pragma unroll
         for (int q = 0; q < TCH; ++q) { P[q] = S[1][k - q]; Qv[q] = S[3][k - q]; U[q] = S[4][k - q]; }
 #pragma unroll
         for (int q = 0; q < TCH; ++q) {
-            float u = U[q];
-            if (kkm < k - q) u += relax * (P[q] * up + Qv[q] - u);
+            const float u = U[q] + relax * (P[q] * up + Qv[q] - U[q]);
             U[q] = u;
             up = u;
         }
 #pragma unroll
         for (int q = 0; q < TCH; ++q) S[4][k - q] = U[q];
     }
-    for (; k >= K0; --k) {
-        float u = S[4][k];
-        if (kkm < k) {
-            u += relax * (S[1][k] * up + S[3][k] - u);
-            S[4][k] = u;
-        }
+    for (; k >= kb; --k) {
+        const float u = S[4][k] + relax * (S[1][k] * up + S[3][k] - S[4][k]);
+        S[4][k] = u;
         up = u;
     }
 }
@@ -559,6 +561,9 @@ struct Mom1Job {
     bool act;
     float top;          // the column's value at VerticalIndex+1 (not swept)
     MomPre p[2];
+    float own[2];       // strip schedule: the swept field's column at levels lane, lane+32 (final after post)
+    float suc[2][2];    // strip schedule: the sweep successors (i+IS, j), (i, j+JS) at the task's levels
+    static constexpr bool kAllFlags = false;   // no task of another column waits on this phase's flags
 
     __device__ void pre(int s, int i, int j, int, int, bool) {
         const int lane = threadIdx.x & 31;
@@ -583,7 +588,28 @@ struct Mom1Job {
         }
     }
 
-    __device__ void post(int, int, int) {
+    // Strip schedule: besides pre(), the column's values at every level (for the shared-memory copy
+    // the next tasks of the strip read) and the successors' old values, so that after the wait only
+    // the predecessors' values are read.  Neither changes before this task finishes.
+    __device__ void pre_strip(int s, int i, int j, int IS, int JS, bool first) {
+        pre(s, i, j, IS, JS, first);
+        const int lane = threadIdx.x & 31;
+        const float *F = comp_field<COMP>(a);
+        const size_t base = ((size_t)s * a.ncols + (size_t)(i * a.nj2 + j)) * a.ks;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            own[r] = (k < a.ks) ? __ldcg(F + base + k) : 0.0f;
+            if (act && k >= c.K0 && k <= c.VI) {
+                suc[r][0] = __ldcg(F + x.at((long long)IS * c.nj2, k));
+                suc[r][1] = __ldcg(F + x.at((long long)JS, k));
+            }
+        }
+    }
+
+    // pI, pJ (strip schedule): this sweep's values of the predecessors (i-IS, j), (i, j-JS) in
+    // shared memory, or null to read them from the field.
+    __device__ void post(int, int IS, int JS, bool strip = false, const float *pI = nullptr, const float *pJ = nullptr) {
         if (!act) return;
         const int lane = threadIdx.x & 31;
         float *F = comp_field<COMP>(a);
@@ -592,7 +618,16 @@ struct Mom1Job {
             const int k = lane + 32 * r;
             if (k < c.K0 || k > c.VI) continue;
             float nW, nS, nE, nN;
-            nbr4(F, x, c, k, nW, nS, nE, nN);
+            if (strip) {
+                const float vI = pI ? pI[k] : __ldcg(F + x.at(-(long long)IS * c.nj2, k));
+                const float vJ = pJ ? pJ[k] : __ldcg(F + x.at(-(long long)JS, k));
+                nW = (IS == 1) ? vI : suc[r][0];
+                nE = (IS == 1) ? suc[r][0] : vI;
+                nS = (JS == 1) ? vJ : suc[r][1];
+                nN = (JS == 1) ? suc[r][1] : vJ;
+            } else {
+                nbr4(F, x, c, k, nW, nS, nE, nN);
+            }
             if (COMP == COMP_U) S[3][k] = u1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
             else if (COMP == COMP_V) S[3][k] = v1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
             else S[3][k] = w1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
@@ -604,7 +639,10 @@ struct Mom1Job {
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int k = lane + 32 * r;
-            if (k >= c.K0 && k <= c.VI && kkm < k) __stcg(F + x.at(0, k), S[4][k]);
+            if (k < c.K0 || k > c.VI) continue;
+            const float v = S[4][k];
+            own[r] = v;
+            if (kkm < k) __stcg(F + x.at(0, k), v);
         }
     }
 
@@ -642,6 +680,8 @@ struct PressJob {
     float dn[2];        // DPMNEW of the column (only this task updates it)
     unsigned run_max;   // residual key maximum of this warp's tasks of situation run_s so far
     int run_s;
+    float own[2];       // strip schedule: the column's DPM at levels lane, lane+32 (final after post)
+    static constexpr bool kAllFlags = true;    // the row carry's readers wait on its writer's flag
 
     // The residual maximum is only read after the phase (k_bookkeeping), so each warp keeps a
     // running maximum and publishes it once per situation instead of once per column.
@@ -709,7 +749,22 @@ struct PressJob {
         }
     }
 
-    __device__ void post(int s, int IS, int JS) {
+    // Strip schedule: besides pre(), the column's DPM at every level for the shared-memory copy
+    // the next tasks of the strip read (unchanged before this task finishes).
+    __device__ void pre_strip(int s, int i, int j, int IS, int JS, bool first) {
+        pre(s, i, j, IS, JS, first);
+        const int lane = threadIdx.x & 31;
+        const size_t base = ((size_t)s * a.ncols + (size_t)(i * a.nj2 + j)) * a.ks;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            own[r] = (k < a.ks) ? __ldcg(a.dpm + base + k) : 0.0f;
+        }
+    }
+
+    // pI, pJ (strip schedule): this sweep's DPM of the predecessors (i-IS, j), (i, j-JS) in shared
+    // memory, or null to read them from the field.
+    __device__ void post(int s, int IS, int JS, bool strip = false, const float *pI = nullptr, const float *pJ = nullptr) {
         if (!act) return;
         const int lane = threadIdx.x & 31;
         const int ks = a.ks;
@@ -719,7 +774,9 @@ struct PressJob {
         for (int r = 0; r < 2; ++r) {
             const int k = lane + 32 * r;
             if (k <= c.KK || k > c.VI) continue;
-            S[3][k] = pressure_post<false>(a, x, c, t0[r], k, IS, JS);
+            const float vI = (strip && pI) ? pI[k] : __ldcg(a.dpm + x.at(-(long long)IS * c.nj2, k));
+            const float vJ = (strip && pJ) ? pJ[k] : __ldcg(a.dpm + x.at(-(long long)JS, k));
+            S[3][k] = pressure_post_v(a, t0[r], k, IS, JS, vI, vJ);
         }
         __syncwarp();
         if (lane == 0) {
@@ -767,6 +824,7 @@ struct PressJob {
             const int k = lane + 32 * r;
             if (k <= c.KK || k > c.VI) continue;
             const float temp = S[4][k];
+            own[r] = temp;
             dmax = max(dmax, residual_key(temp, sc));
             __stcg(a.dpm + x.at(0, k), temp);
             a.dpmnew[x.at(0, k)] = dn[r] + a.relaxp * temp;
@@ -835,9 +893,15 @@ __device__ inline bool wait_count(const int *cnt, int need, int *err, unsigned l
     }
 }
 
+// Shared-memory copies of finished columns: a ring of SDEPTH slots per row of the strip, slot
+// c % SDEPTH holding the swept field of the row's column c at every level.  A task reads its row
+// predecessor's slot and, for r > 0, its column predecessor's slot of the row above; before it
+// overwrites a slot, the row below must have finished the column that slot held.
+constexpr int SDEPTH = 4;
+
 template <int PHASE, bool REVERSE, int SR, int SMW, class Job>
 __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &g, Job &job, int *s_done,
-                                               unsigned *s_claim) {
+                                               unsigned *s_claim, float (*s_col)[KMAX_LEVELS]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int r = warp / SMW, m = warp % SMW;
     const unsigned units = (unsigned)*a.nact;
@@ -860,10 +924,11 @@ __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &
         if (i1 < g.ia + g.ni) {
             const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
             int *fl = a.flags + (size_t)u * a.ncols;
+            const bool below = r + 1 < SR && i1 + 1 < g.ia + g.ni;   // the row below runs in this block
             for (int c = m; c < g.nj; c += SMW) {
                 const int j1 = g.ja + c;
                 const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
-                job.pre(u, i, j, IS, JS, i1 == g.ia);
+                job.pre_strip(u, i, j, IS, JS, i1 == g.ia);
                 int ok = 1;
                 if (lane == 0) {
                     ok = wait_count(s_done + r, c, a.err, a.wait_limit_ns);
@@ -873,11 +938,18 @@ __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &
                 }
                 ok = __shfl_sync(0xffffffffu, ok, 0);
                 __syncwarp();
-                if (ok) job.post(u, IS, JS);
+                if (ok)
+                    job.post(u, IS, JS, true, (r > 0) ? s_col[(r - 1) * SDEPTH + c % SDEPTH] : nullptr,
+                             (c > 0) ? s_col[r * SDEPTH + (c - 1) % SDEPTH] : nullptr);
+                if (lane == 0 && below && c >= SDEPTH) wait_count(s_done + r + 1, c - SDEPTH + 1, a.err, a.wait_limit_ns);
+                __syncwarp();
+                float *slot = s_col[r * SDEPTH + c % SDEPTH];
+                slot[lane] = job.own[0];
+                if (lane + 32 < KMAX_LEVELS) slot[lane + 32] = job.own[1];
                 __syncwarp();
                 if (lane == 0) {
                     st_release_cta(s_done + r, c + 1);
-                    st_release(fl + i * a.nj2 + j, stamp);
+                    if (Job::kAllFlags || r == SR - 1 || i1 + 1 == g.ia + g.ni) st_release(fl + i * a.nj2 + j, stamp);
                 }
             }
         }
@@ -889,22 +961,24 @@ __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &
 template <int SR, int SMW>
 __global__ void __launch_bounds__(SR * SMW * 32, 1) k_pressure_strip(KArgs a, SweepGeom g) {
     __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ float s_col[SR * SDEPTH][KMAX_LEVELS];
     __shared__ int s_done[SR];
     __shared__ unsigned s_claim;
     PressJob job{a, sm[threadIdx.x >> 5], 0};
     job.run_max = 0;
     job.run_s = -1;
-    gs_tasks_strip<PH_PRESSURE, false, SR, SMW>(a, g, job, s_done, &s_claim);
+    gs_tasks_strip<PH_PRESSURE, false, SR, SMW>(a, g, job, s_done, &s_claim, s_col);
 }
 
 template <int COMP, int SR, int SMW>
 __global__ void __launch_bounds__(SR * SMW * 32, 1) k_mom1_strip(KArgs a, SweepGeom g) {
     __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ float s_col[SR * SDEPTH][KMAX_LEVELS];
     __shared__ int s_done[SR];
     __shared__ unsigned s_claim;
     Mom1Job<COMP> job{a, sm[threadIdx.x >> 5], 0};
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
-    gs_tasks_strip<PH, COMP == COMP_V, SR, SMW>(a, g, job, s_done, &s_claim);   // model-1 V sweeps with (-IS,-JS)
+    gs_tasks_strip<PH, COMP == COMP_V, SR, SMW>(a, g, job, s_done, &s_claim, s_col);   // model-1 V sweeps with (-IS,-JS)
 }
 
 // ---------------------------- fused wavefront, slab family --------------------------------

@@ -505,16 +505,21 @@ __device__ __forceinline__ float pressure_pre(const KArgs &a, const Acc<IL> &x, 
     return DIV / sc.dtime;
 }
 
-template <bool IL>
-__device__ __forceinline__ float pressure_post(const KArgs &a, const Acc<IL> &x, const ColCtx &c, float t0, int k,
-                                               int IS, int JS) {
+// pi, pj: this sweep's DPM of the predecessors (i-IS, j) and (i, j-JS) at level k
+__device__ __forceinline__ float pressure_post_v(const KArgs &a, float t0, int k, int IS, int JS, float pi, float pj) {
     const float DXK = a.dxk, DYK = a.dyk;
     const float dz = a.dzk[k];
-    const float pi = __ldcg(a.dpm + x.at(-(long long)IS * c.nj2, k));
-    const float pj = __ldcg(a.dpm + x.at(-(long long)JS, k));
     const float si = (IS == 1) ? (pi + 0.0f) : (0.0f + pi);    // DPMim + DPMip
     const float sj = (JS == 1) ? (pj - 0.0f) : (0.0f - pj);    // DPMjm - DPMjp
     return t0 + si / DXK * DYK * dz + sj / DYK * DXK * dz;
+}
+
+template <bool IL>
+__device__ __forceinline__ float pressure_post(const KArgs &a, const Acc<IL> &x, const ColCtx &c, float t0, int k,
+                                               int IS, int JS) {
+    const float pi = __ldcg(a.dpm + x.at(-(long long)IS * c.nj2, k));
+    const float pj = __ldcg(a.dpm + x.at(-(long long)JS, k));
+    return pressure_post_v(a, t0, k, IS, JS, pi, pj);
 }
 
 template <bool IL>
