@@ -57,6 +57,7 @@ struct ColKE {            // 16 bytes
 // Per-situation scalars and convergence state (PrognosticFlowfield.cs:146-163, 231-240, 1144-1170).
 struct SitDev {
     double frund;
+    double rfrund;           // 1/Frund correctly rounded (host), for rcp_ok
     double delta_mean;
     double conv_threshold;
     double hist[MAX_HIST];
@@ -74,7 +75,7 @@ struct SitDev {
     int32_t n_hist;
     int32_t it_min, it_max, cadence;
     int32_t quantise;
-    int32_t pad_;
+    int32_t rcp_ok;          // ConvToInt(x*Frund)/Frund by the reciprocal (verified at the load)
 };
 
 // Everything a kernel needs, passed by value (all pointers are device pointers).
@@ -181,6 +182,20 @@ __device__ __forceinline__ int conv_to_int(double v) {
 }
 __device__ __forceinline__ double quantd(double x, double frund, int on) {
     return on ? (double)conv_to_int(x * frund) / frund : x;
+}
+// The same with the division n/Frund (n = ConvToInt(x*Frund), an integer) done as Markstein's
+// correction step on the precomputed y = RN(1/Frund): q0 = RN(n*y), r = n - q0*Frund (exact by
+// FMA), q = RN(q0 + r*y).  rok says that the load-time check (k_rcp_check) found q equal to the
+// IEEE quotient n/Frund for every integer n of magnitude up to 2^31 with this Frund; without it
+// the IEEE division is used.
+__device__ __forceinline__ double quantd_r(double x, double frund, double rfrund, bool rok, int on) {
+    if (!on) return x;
+    const double n = (double)conv_to_int(x * frund);
+    if (rok) {
+        const double q0 = n * rfrund;
+        return fma(fma(-q0, frund, n), rfrund, q0);
+    }
+    return n / frund;
 }
 
 // ---- inter-warp ordering of the Gauss-Seidel wavefront ----

@@ -1302,29 +1302,50 @@ struct BLane {
     __device__ __forceinline__ float &e1(int k) { return row(8, k); }
 };
 
-__device__ __forceinline__ BLane blane(float *smem, int ks) {
+__device__ __forceinline__ BLane blane(float *smem, int ks, int slot = -1) {
     BLane R;
     R.base = smem;
     R.dbase = reinterpret_cast<double *>(smem + (size_t)9 * ks * 32);
     R.ks = ks;
-    R.lane = threadIdx.x & 31;
+    R.lane = slot >= 0 ? slot : (threadIdx.x & 31);
     return R;
+}
+
+// Lanes of a batched task in its level loops.  A group that holds at most 16 situations (the
+// last group of a batch such as 144 = 4 x 32 + 16) runs them two levels per warp instruction:
+// lanes 16-31 take the odd levels of the situations of lanes 0-15.  slot = the situation's lane
+// in the group, k = k0 + ofs, k0 + ofs + step, ...  The serial recurrences keep lane = slot.
+struct BLoop {
+    int slot, ofs, step;
+    bool half;
+};
+
+template <int NW>
+__device__ __forceinline__ BLoop bloop(const KArgs &a, int grp) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    BLoop L;
+    L.half = a.nb - grp * 32 <= 16;
+    L.slot = L.half ? (lane & 15) : lane;
+    L.ofs = L.half ? 2 * warp + (lane >> 4) : warp;
+    L.step = L.half ? 2 * NW : NW;
+    return L;
 }
 
 template <int MODEL, int COMP, int NW, int SW, class Ahead>
 __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *smem, Ahead &&ahead) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int s = grp * 32 + lane;
     const ColCtx c = make_col(a, i, j);
     if (!(c.fl & F_ADV)) return;
+    const BLoop L = bloop<NW>(a, grp);
+    const int s = grp * 32 + L.slot;
     const bool act = (s < a.nb) && a.sit[s].active;
-    BLane R = blane(smem, a.ks);
+    BLane R = blane(smem, a.ks, L.slot);
     const Acc<true> x = make_acc<true>(a, act ? s : grp * 32, c.col);
     if (act) {
         const SitCtx sc = make_sit(a, s);
         // one level per step: within the register budget of four resident blocks a second level's
         // operands did not overlap the first's (each level cost the same either way)
-        for (int k = c.K0 + warp; k <= c.VI; k += NW) {
+        for (int k = c.K0 + L.ofs; k <= c.VI; k += L.step) {
             const Coef q = mom_level<MODEL, COMP, true, SW>(a, x, c, sc, k);
             R.a(k) = q.A; R.b(k) = q.B; R.c(k) = q.C; R.d(k) = q.D; R.p(k) = q.phi;
         }
@@ -1333,10 +1354,17 @@ __device__ void batch_mom_column(const KArgs &a, int grp, int i, int j, float *s
     if (threadIdx.x == 32) ahead();
     float *F = comp_field<COMP>(a);
     const int kkm = back_limit<COMP>(c);
-    if (warp == 0 && act) mom_sweep<MODEL, COMP>(R, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x.at(0, c.VI + 1)));
+    if (warp == 0) {     // the recurrences: lane = situation slot
+        const int s0 = grp * 32 + lane;
+        if (!L.half ? act : (s0 < a.nb && a.sit[s0].active)) {
+            BLane R0 = blane(smem, a.ks);
+            const Acc<true> x0 = L.half ? make_acc<true>(a, s0, c.col) : x;
+            mom_sweep<MODEL, COMP>(R0, c.K0, c.KK, c.VI, kkm, a.relax, __ldcg(F + x0.at(0, c.VI + 1)));
+        }
+    }
     __syncthreads();
     if (!act) return;
-    for (int k = max(c.K0, kkm + 1) + warp; k <= c.VI; k += NW) __stcg(F + x.at(0, k), R.p(k));
+    for (int k = max(c.K0, kkm + 1) + L.ofs; k <= c.VI; k += L.step) __stcg(F + x.at(0, k), R.p(k));
 }
 
 template <int NW, class Ahead>

@@ -610,6 +610,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
         for (int k = 1; k <= q.kadvmax; ++k) ap0[(size_t)b * ks + k] = AREA * s->dzk[k] / DT;
         SitDev &S = ctx->h_sit[b];
         S.frund = (double)((q.turbulence_model == 2 ? 10000 : 8000) / topwind);
+        S.rfrund = 1.0 / S.frund;
+        S.rcp_ok = 0;                 // set on the device by the check after the upload
         S.conv_threshold = q.conv_threshold;
         S.dtime = DT;
         S.topwind = topwind;
@@ -876,6 +878,12 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     CK(cudaMemcpyAsync(ctx->tables.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->ap0.p, ap0.data(), ap0.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->sit.p, ctx->h_sit.data(), n * sizeof(SitDev), cudaMemcpyHostToDevice, st));
+    bool any_quant = false;
+    for (int b = 0; b < n; ++b) any_quant |= ctx->h_sit[b].quantise != 0;
+    if (any_quant) {
+        CK(cudaMemsetAsync(ctx->counts.p, 0, n * sizeof(int), st));
+        launch_rcp_check(ctx->ka, ctx->counts.p, st);
+    }
     ctx->h_act.resize(3 + n);
     ctx->h_act[0] = 0;
     ctx->h_act[1] = n;

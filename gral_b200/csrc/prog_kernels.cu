@@ -32,10 +32,15 @@ template <bool IL, bool WIDE = false, class Body>
 __device__ __forceinline__ void col_loop(const KArgs &a, bool need_active, Body &&body) {
     const int lane = threadIdx.x & 31;
     int s, col, kbeg, kstep;
+    // A group holding at most 16 situations runs two levels per warp instruction: lanes 16-31
+    // take the odd levels of the situations of lanes 0-15 (the body is expanded for both forms,
+    // so each keeps a compile-time level step).
+    bool half = false;
     if (IL && WIDE) {
         const int unit = blockIdx.x / a.ncols;
         col = blockIdx.x - unit * a.ncols;
-        s = unit * 32 + lane;
+        half = a.nb - unit * 32 <= 16;
+        s = unit * 32 + (half ? (lane & 15) : lane);
         if (unit >= a.ngroups || s >= a.nb) return;
         kbeg = threadIdx.x >> 5;
         kstep = COL_WARPS;
@@ -44,7 +49,8 @@ __device__ __forceinline__ void col_loop(const KArgs &a, bool need_active, Body 
         const long long unit = gw / a.ncols;
         col = (int)(gw - unit * a.ncols);
         if (IL) {
-            s = (int)unit * 32 + lane;
+            half = a.nb - (int)unit * 32 <= 16;
+            s = (int)unit * 32 + (half ? (lane & 15) : lane);
             if (unit >= a.ngroups || s >= a.nb) return;
             kbeg = 0;
             kstep = 1;
@@ -58,7 +64,12 @@ __device__ __forceinline__ void col_loop(const KArgs &a, bool need_active, Body 
     if (need_active && !a.sit[s].active) return;
     const int i = col / a.nj2, j = col - (col / a.nj2) * a.nj2;
     const Acc<IL> x = make_acc<IL>(a, s, col);
-    body(s, col, i, j, x, kbeg, kstep);
+    if (IL && half) {
+        if (WIDE) body(s, col, i, j, x, 2 * kbeg + (lane >> 4), 2 * COL_WARPS);
+        else body(s, col, i, j, x, lane >> 4, 2);
+    } else {
+        body(s, col, i, j, x, kbeg, kstep);
+    }
 }
 
 // ---- boundary conditions (PrognosticFlowfield.cs:595-714) ----
@@ -328,6 +339,32 @@ __global__ void k_gather(KArgs a, Staging sg, int model, int to_dev) {
     });
 }
 
+// Admission of the reciprocal form of ConvToInt(x*Frund)/Frund (quantd_r): for each situation,
+// Markstein's quotient is compared with the IEEE quotient for every integer n in [2^30, 2^31),
+// i.e. every 31-bit significand.  Every other dividend of that step is such an integer scaled by a
+// power of two (ConvToInt gives magnitudes up to 2^31; 0 and the signs are exact), and scaling by
+// a power of two changes no rounding of the three operations while no value leaves the normal
+// range, so the comparison covers them all.
+__global__ void k_rcp_check(KArgs a, int *bad) {
+    const int s = blockIdx.y;
+    if (s >= a.nb || !a.sit[s].quantise) return;
+    const double b = a.sit[s].frund, y = a.sit[s].rfrund;
+    const unsigned long long n0 = 1ull << 30;
+    bool fail = false;
+    for (unsigned long long t = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; t < n0;
+         t += (unsigned long long)gridDim.x * blockDim.x) {
+        const double n = (double)(n0 + t);
+        const double q0 = n * y;
+        fail |= (fma(fma(-q0, b, n), y, q0) != n / b);
+    }
+    if (__any_sync(0xffffffffu, fail) && (threadIdx.x & 31) == 0) atomicOr(bad + s, 1);
+}
+
+__global__ void k_rcp_set(KArgs a, const int *bad) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < a.nb) a.sit[s].rcp_ok = (a.sit[s].quantise && bad[s] == 0) ? 1 : 0;
+}
+
 // unrealistic-speed counts and non-finite values (:1193-1243)
 template <bool IL>
 __global__ void k_postcheck(KArgs a, int *counts) {
@@ -472,6 +509,11 @@ void launch_diag_velcorr(const KArgs &a, const DiagTabs &t, cudaStream_t st) {
 void launch_diag_wfinal(const KArgs &a, const DiagTabs &t, cudaStream_t st) {
     const long long n = (long long)a.nb * a.ncols;
     k_diag_wfinal<<<(int)((n + 255) / 256), 256, 0, st>>>(a, t);
+}
+
+void launch_rcp_check(const KArgs &a, int *bad, cudaStream_t st) {
+    k_rcp_check<<<dim3(512, a.nb), 256, 0, st>>>(a, bad);
+    k_rcp_set<<<(a.nb + 127) / 128, 128, 0, st>>>(a, bad);
 }
 
 void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st) {

@@ -50,6 +50,9 @@ void launch_setup(const KArgs &a, const Staging &sg, int model, const float *var
                   cudaStream_t st);
 void launch_gather(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
 void launch_scatter(const KArgs &a, const Staging &sg, int model, cudaStream_t st);
+// for every situation with quantisation: whether ConvToInt(x*Frund)/Frund may use the reciprocal
+// (SitDev::rcp_ok); bad = n ints of zeroed scratch
+void launch_rcp_check(const KArgs &a, int *bad, cudaStream_t st);
 // post-checks (PrognosticFlowfield.cs:1193-1243); counts[s*4 + 0..3] = UK, VK, WK, non-finite
 void launch_postcheck(const KArgs &a, int *counts, cudaStream_t st);
 

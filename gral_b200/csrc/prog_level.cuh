@@ -864,7 +864,8 @@ __device__ __forceinline__ void velcorr_col(const KArgs &a, int s, int col, int 
     const ColMeta m = a.meta[col];
     const SitDev &sd = a.sit[s];
     const float DT = sd.dtime, DXK = a.dxk, DYK = a.dyk;
-    const double fr = sd.frund;
+    const double fr = sd.frund, rfr = sd.rfrund;
+    const bool rok = sd.rcp_ok != 0;
     const int qz = sd.quantise;
     const long long dW = -(long long)a.nj2;
     const bool du = i > 2, dv = j > 2;
@@ -888,11 +889,11 @@ __device__ __forceinline__ void velcorr_col(const KArgs &a, int s, int col, int 
         for (int q = 0; q < CH; ++q) {
             const int k = kb + q * kstep;
             if (k < 1 || k > m.vi) continue;
-            if (du && m.kkm_u < k) a.uk[x.at(0, k)] = (float)quantd((double)(u[q] + (dw[q] - d[q]) / DXK * DT), fr, qz);
-            if (dv && m.kkm_v < k) a.vk[x.at(0, k)] = (float)quantd((double)(v[q] + (ds[q] - d[q]) / DYK * DT), fr, qz);
+            if (du && m.kkm_u < k) a.uk[x.at(0, k)] = (float)quantd_r((double)(u[q] + (dw[q] - d[q]) / DXK * DT), fr, rfr, rok, qz);
+            if (dv && m.kkm_v < k) a.vk[x.at(0, k)] = (float)quantd_r((double)(v[q] + (ds[q] - d[q]) / DYK * DT), fr, rfr, rok, qz);
             if (m.kkart + 1 < k)
                 a.wk[x.at(0, k)] =
-                    (float)quantd((double)(w[q] + (dk[q] - d[q]) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, qz);
+                    (float)quantd_r((double)(w[q] + (dk[q] - d[q]) / (a.dzk[k] + a.dzk[k - 1]) * 2 * DT), fr, rfr, rok, qz);
             else
                 a.wk[x.at(0, k)] = 0;
         }
