@@ -132,9 +132,9 @@ __device__ __forceinline__ void decode(unsigned t, const SweepGeom &g, int &i1, 
 }
 
 // The reverse wavefront task loop: tasks in reverse diagonal order; a column waits for its two
-// sweep successors (i1+1, j1) and (i1, j1+1), runs job.critical, publishes its flag (after a
-// fence over the warp's writes), then runs job.after.  Successors are claimed earlier, so no task
-// waits on one that is not running or done.
+// sweep successors (i1+1, j1) and (i1, j1+1), runs job.critical, publishes its flag (a warp
+// barrier, then a gpu-scope release by lane 0), then runs job.after.  Successors are claimed
+// earlier, so no task waits on one that is not running or done.
 template <class Job>
 __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, const SweepGeom &g, int IS, int JS,
                                           Job &job) {
@@ -159,8 +159,7 @@ __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, cons
         ok = __shfl_sync(0xffffffffu, ok, 0);
         __syncwarp();
         if (ok) job.critical(IS, JS);
-        __threadfence();
-        __syncwarp();
+        __syncwarp();     // orders every lane's writes and atomics before lane 0's release
         if (lane == 0) st_release(d.flags + i * a.nj2 + j, d.stamp);
         if (ok) job.after(IS, JS);
         __syncwarp();
@@ -946,11 +945,16 @@ namespace {
 
 int col_blocks(const KArgs &a) { return (a.ncols * 32 + 255) / 256; }
 
-// one forward SIMPLE iteration with separate phase launches; when `keep` is given, the mid and
-// end states go there and the boundary copies' branches to `bits`
-int forward_iteration(gral_ctx *ctx, float *keep, uint8_t *bits) {
+// one Gauss-Seidel phase of the forward on the loaded schedule (strips or diagonal claims)
+void forward_phase(gral_ctx *ctx, int kind, const SweepGeom &g, cudaStream_t st) {
+    if (ctx->pmode > 0) launch_strip(kind, ctx->ka, g, ctx->pmode - 1, ctx->strip_grid[kind], st);
+    else launch_gs(kind, ctx->ka, g, ctx->grid_gs[kind], st);
+}
+
+// one forward SIMPLE iteration with separate phase launches on stream st; when `keep` is given,
+// the mid and end states go there and the boundary copies' branches to `bits`
+int forward_iteration(gral_ctx *ctx, float *keep, uint8_t *bits, cudaStream_t st) {
     const KArgs &a = ctx->ka;
-    cudaStream_t st = ctx->stream;
     CK(cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st));
     if (bits) {
         const long long nw = (long long)(a.njj - 1) * a.ks, ns = (long long)(a.nii - 1) * a.ks;
@@ -960,7 +964,7 @@ int forward_iteration(gral_ctx *ctx, float *keep, uint8_t *bits) {
     } else {
         launch_bc(a, ctx->bc, st);
     }
-    launch_gs(PH_PRESSURE, a, ctx->geo_p.g, ctx->grid_gs[PH_PRESSURE], st);
+    forward_phase(ctx, PH_PRESSURE, ctx->geo_p.g, st);
     launch_velcorr(a, st);
     launch_average(a, st);
     const size_t fsz = (size_t)a.ncols * a.ks;
@@ -969,9 +973,9 @@ int forward_iteration(gral_ctx *ctx, float *keep, uint8_t *bits) {
         for (int q = 0; q < 7; ++q)
             CK(cudaMemcpyAsync(keep + q * fsz, src[q], fsz * sizeof(float), cudaMemcpyDeviceToDevice, st));
     }
-    launch_gs(PH_U, a, ctx->geo_u.g, ctx->grid_gs[PH_U], st);
-    launch_gs(PH_V, a, ctx->geo_v.g, ctx->grid_gs[PH_V], st);
-    launch_gs(PH_W, a, ctx->geo_p.g, ctx->grid_gs[PH_W], st);
+    forward_phase(ctx, PH_U, ctx->geo_u.g, st);
+    forward_phase(ctx, PH_V, ctx->geo_v.g, st);
+    forward_phase(ctx, PH_W, ctx->geo_p.g, st);
     launch_bookkeeping(a, st);
     if (keep) {
         const float *src[3] = {a.uk, a.vk, a.wk};
@@ -995,9 +999,8 @@ int save_checkpoint(gral_ctx *ctx, int q) {
     return GRAL_OK;
 }
 
-int restore_checkpoint(gral_ctx *ctx, int q) {
+int restore_checkpoint(gral_ctx *ctx, int q, cudaStream_t st) {
     const KArgs &a = ctx->ka;
-    cudaStream_t st = ctx->stream;
     const size_t fsz = (size_t)a.ncols * a.ks;
     float *dst[NCKPT] = {a.uk, a.vk, a.wk, a.uks, a.vks, a.wks, a.dpmnew};
     const float *src = ctx->adj_ckpt.p + (size_t)q * NCKPT * fsz;
@@ -1076,6 +1079,7 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
     CK_RC(gral_prog_load(ctx, 1, &q, s, f));
     if (ctx->il) return fail(ctx, GRAL_EINVAL, "the adjoint runs the slab layout (unset GRAL_PROG_LAYOUT)");
     ctx->fused = false;
+    CK_RC(plain_schedule_default(ctx));
     const KArgs &a = ctx->ka;
     const size_t fsz = (size_t)a.ncols * a.ks;
     const int nck = (iterations + checkpoint_every - 1) / checkpoint_every;
@@ -1086,7 +1090,7 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
     CK(cudaEventRecord(ctx->ev[0], st));
     for (int it = 0; it < iterations; ++it) {
         if (it % checkpoint_every == 0) CK_RC(save_checkpoint(ctx, it / checkpoint_every));
-        CK_RC(forward_iteration(ctx, nullptr, nullptr));
+        CK_RC(forward_iteration(ctx, nullptr, nullptr, st));
     }
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(cudaGetLastError());
@@ -1121,15 +1125,20 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     const int K = ctx->adj_every, N = ctx->adj_iters;
     const size_t fsz = (size_t)a.ncols * a.ks, ssz = (size_t)a.ncols * (a.nkk + 2);
     const int nev = ctx->adj_nwe + ctx->adj_nsn;
-    CK(ctx->adj_keep.ensure((size_t)K * NKEEP * fsz));
+    const int nseg = (N + K - 1) / K;
+    const int nbuf = nseg > 1 ? 2 : 1;     // the next segment is recomputed while this one is reversed
+    const size_t nevk = (size_t)std::max(nev, 1) * a.ks;
+    CK(ctx->adj_keep.ensure((size_t)nbuf * K * NKEEP * fsz));
     CK(ctx->adj_lam.ensure((size_t)NLAM * fsz));
     CK(ctx->adj_stg.ensure(3 * ssz));
     CK(ctx->adj_flags.ensure(a.ncols));
     CK(ctx->adj_ctr.ensure(4));
-    CK(ctx->adj_bits.ensure((size_t)K * std::max(nev, 1) * a.ks));
+    CK(ctx->adj_bits.ensure((size_t)nbuf * K * nevk));
     CK(cudaMemsetAsync(ctx->adj_lam.p, 0, (size_t)NLAM * fsz * sizeof(float), st));
     CK(cudaMemsetAsync(ctx->adj_flags.p, 0, a.ncols * sizeof(int), st));
-    CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)K * std::max(nev, 1) * a.ks, st));
+    CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)nbuf * K * nevk, st));
+    if (!ctx->adj_stream) CK(cudaStreamCreateWithFlags(&ctx->adj_stream, cudaStreamNonBlocking));
+    cudaStream_t st2 = ctx->adj_stream;
     StageLam L{ctx->adj_stg.p, ctx->adj_stg.p + ssz, ctx->adj_stg.p + 2 * ssz};
     const float *gin[3] = {dj_duk, dj_dvk, dj_dwk};
     float *stg[3] = {L.u, L.v, L.w};
@@ -1148,25 +1157,38 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     CK(cudaEventRecord(ctx->ev[0], st));
     const int g_p = rev_grid(ctx, ctx->geo_p.g), g_u = rev_grid(ctx, ctx->geo_u.g), g_v = rev_grid(ctx, ctx->geo_v.g);
     int stamp = 0;
-    float ms_re = 0.f, ms_rev = 0.f;
-    cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventCreate(&e2));
-    const int nseg = (N + K - 1) / K;
+    // Segments are reversed from the last one down.  The recomputation of segment sg-1 (restore its
+    // checkpoint, run its iterations keeping the states) runs on a second stream into the other
+    // keep buffer while segment sg is reversed: the reverse sweeps read only the kept states, the
+    // cotangents and the static tables, never the solver's fields, so the two only share the GPU.
+    // Events order a buffer's recomputation after the reverse that last read it.
+    std::vector<cudaEvent_t> ev(4 * (size_t)nseg, nullptr);   // per segment: recompute start/end, reverse start/end
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    auto E = [&](int sg, int q) { return ev[4 * (size_t)sg + q]; };
+    auto keep_of = [&](int sg, int q) { return ctx->adj_keep.p + ((size_t)(sg % nbuf) * K + q) * NKEEP * fsz; };
+    auto bits_of = [&](int sg, int q) { return ctx->adj_bits.p + ((size_t)(sg % nbuf) * K + q) * nevk; };
+    auto recompute = [&](int sg) -> int {
+        if (sg + nbuf < nseg) CK(cudaStreamWaitEvent(st2, E(sg + nbuf, 3), 0));   // that buffer's last reader
+        CK(cudaEventRecord(E(sg, 0), st2));
+        CK_RC(restore_checkpoint(ctx, sg, st2));
+        const int n = std::min(K, N - sg * K);
+        for (int q = 0; q < n; ++q) CK_RC(forward_iteration(ctx, keep_of(sg, q), bits_of(sg, q), st2));
+        CK(cudaEventRecord(E(sg, 1), st2));
+        return GRAL_OK;
+    };
+    CK(cudaEventRecord(ctx->ev[2], st));
+    CK(cudaStreamWaitEvent(st2, ctx->ev[2], 0));
+    CK_RC(recompute(nseg - 1));
     for (int sg = nseg - 1; sg >= 0; --sg) {
+        if (sg > 0) CK_RC(recompute(sg - 1));
         const int it0 = sg * K, n = std::min(K, N - it0);   // iterations it0+1 .. it0+n
-        CK(cudaEventRecord(e0, st));
-        CK_RC(restore_checkpoint(ctx, sg));
-        for (int q = 0; q < n; ++q)
-            CK_RC(forward_iteration(ctx, ctx->adj_keep.p + (size_t)q * NKEEP * fsz,
-                                    ctx->adj_bits.p + (size_t)q * std::max(nev, 1) * a.ks));
-        CK(cudaEventRecord(e1, st));
+        CK(cudaStreamWaitEvent(st, E(sg, 1), 0));
+        CK(cudaEventRecord(E(sg, 2), st));
         for (int q = n - 1; q >= 0; --q) {
-            const float *kp = ctx->adj_keep.p + (size_t)q * NKEEP * fsz;
+            const float *kp = keep_of(sg, q);
             for (int f = 0; f < 7; ++f) d.mid[f] = kp + f * fsz;
             for (int f = 0; f < 3; ++f) d.end[f] = kp + (7 + f) * fsz;
-            d.bits = ctx->adj_bits.p + (size_t)q * std::max(nev, 1) * a.ks;
+            d.bits = bits_of(sg, q);
             d.it = it0 + q + 1;
             CK(cudaMemsetAsync(d.ctr, 0, 4 * sizeof(unsigned int), st));
             d.stamp = ++stamp;
@@ -1191,23 +1213,28 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
             k_adj_bc_sn_rev<<<(int)((ns + 127) / 128), 128, 0, st>>>(a, ctx->bc, d);
             k_adj_bc_we_rev<<<(int)((nw + 127) / 128), 128, 0, st>>>(a, ctx->bc, d);
         }
-        CK(cudaEventRecord(e2, st));
+        CK(cudaEventRecord(E(sg, 3), st));
         CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(st));
+    }
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(st2));
+    float ms_re = 0.f, ms_rev = 0.f;
+    for (int sg = 0; sg < nseg; ++sg) {
         float m1 = 0.f, m2 = 0.f;
-        CK(cudaEventElapsedTime(&m1, e0, e1));
-        CK(cudaEventElapsedTime(&m2, e1, e2));
+        CK(cudaEventElapsedTime(&m1, E(sg, 0), E(sg, 1)));
+        CK(cudaEventElapsedTime(&m2, E(sg, 2), E(sg, 3)));
         ms_re += m1;
         ms_rev += m2;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    {
         int herr = 0;
         CK(cudaMemcpy(&herr, ctx->misc.p, sizeof(int), cudaMemcpyDeviceToHost));
         if (herr == ERR_TIMEOUT) {
-            cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
             ctx->adj_ready = false;
             return fail(ctx, GRAL_ETIMEDOUT, "an adjoint wavefront wait exceeded its time limit");
         }
     }
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
     // the set-up, reversed
     k_adj_setup_scatter<<<cb, 256, 0, st>>>(a, d, L);
     k_adj_setup_zero<<<cb, 256, 0, st>>>(a, d, L);

@@ -143,6 +143,7 @@ struct gral_ctx {
     DevBuf<int> adj_ckit, adj_flags;
     DevBuf<unsigned int> adj_ctr;
     DevBuf<uint8_t> adj_bits;
+    cudaStream_t adj_stream = nullptr;   // recomputation of the next segment beside the reverse sweeps
 
     ~gral_ctx() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -158,11 +159,16 @@ struct gral_ctx {
         adj_ckpt.release(); adj_keep.release(); adj_lam.release(); adj_ptab.release(); adj_stg.release();
         adj_cksit.release(); adj_ckit.release(); adj_flags.release(); adj_ctr.release(); adj_bits.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
+        if (adj_stream) cudaStreamDestroy(adj_stream);
         if (stream) cudaStreamDestroy(stream);
     }
 };
 
 namespace gral {
+
+// Slab family, model 1: keep the default schedule of the sweeps (or GRAL_PROG_PLAIN_MODE) without
+// trial iterations, and size its grids (prog_host.cu).
+int plain_schedule_default(gral_ctx *ctx);
 
 inline int fail(gral_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;

@@ -372,6 +372,16 @@ int tune_variants(gral_ctx *ctx) {
 // mode is kept.
 constexpr int kDefaultPlainMode = 1;   // strips of 4 rows, 4 warps per row (fastest on the 400x400 grid)
 
+}  // namespace
+
+int gral::plain_schedule_default(gral_ctx *ctx) {
+    const int nv = 1 + strip_num_variants();
+    ctx->pmode = (ctx->model != 1) ? 0 : ((ctx->forced_pmode >= 0 && ctx->forced_pmode < nv) ? ctx->forced_pmode : kDefaultPlainMode);
+    return size_grids(ctx);
+}
+
+namespace {
+
 int tune_plain(gral_ctx *ctx) {
     if (ctx->pmode >= 0) return GRAL_OK;
     const int nv = 1 + strip_num_variants();
