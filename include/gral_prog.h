@@ -370,17 +370,19 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
 typedef struct gral_vjp_stats {
     int32_t iterations, checkpoint_every;
     double ms_forward;     /* device time of the forward run in gral_prog_vjp_forward */
-    double ms_recompute;   /* device time of the segment recomputations inside gral_prog_vjp */
+    double ms_recompute;   /* device time of the segment recomputations inside gral_prog_vjp (each but
+                              the last segment's runs beside the reverse sweeps of the segment after it) */
     double ms_reverse;     /* device time of the reverse sweeps */
-    double ms_total;       /* device time of gral_prog_vjp */
+    double ms_total;       /* device time of gral_prog_vjp (less than recompute + reverse: they overlap) */
 } gral_vjp_stats;
 
 /* The vector-Jacobian product of the last gral_prog_vjp_forward: given the cotangents dJ/dUK,
  * dJ/dVK, dJ/dWK of its final fields ([NII+2][NJJ+2][NKK+2] host arrays, NULL = zero), writes
  * dJ/dVEG (same layout; zero where VEG[i][j] is null) and dJ/d(initial UK, VK, WK) (same layout).
  * Any output may be NULL.  The checkpoint segments are recomputed from the kept states (each
- * segment once), so the fields resident on the device afterwards are those of an intermediate
- * iteration.  stats may be NULL. */
+ * segment once, the next one on a second stream of the context while the current one is reversed,
+ * so two segments' states are held), and the fields resident on the device afterwards are those of
+ * an intermediate iteration.  stats may be NULL. */
 int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const float *dj_dwk, float *dj_dveg,
                   float *dj_duk0, float *dj_dvk0, float *dj_dwk0, gral_vjp_stats *stats);
 
