@@ -574,28 +574,33 @@ def wind_measure(dom, sit, n: int = 1 << 20, repeats: int = 5):
             "cpu_oracle_particles_per_s": round(n / cpu_s, 0), "cpu_kind": "oracle restatement, 1 core"}
 
 
-def instances_measure(n: int = 16, iterations: int = 100, concurrent: int = 16, seed: int = 0):
-    """Uneven-domain instances, sequential against side by side (rank 0 only)."""
+def instances_measure(n: int = 16, iterations: int = 100, concurrent: int = 16, seed: int = 0, distinct: int = 32):
+    """Uneven-domain instances, sequential against side by side (rank 0 only).  Up to `distinct`
+    grids are drawn (log-uniform 128..512 columns a side at 2-4 m, hills and buildings); instance q
+    solves grid q % distinct with its own random inflow."""
     import numpy as np
     from gral_b200 import prep
     from gral_b200.prognostic import solve_instances
 
     rng = np.random.default_rng(seed)
-    doms, ps, fs = [], [], []
-    for q in range(n):
+    grids = []
+    for q in range(min(n, distinct)):
         side = int(round(math.exp(rng.uniform(math.log(128), math.log(512)))))
         nj = int(round(side * rng.uniform(0.8, 1.0)))
         vc = int(round(20 + (side - 128) / (512 - 128) * 20))
         dx = float(rng.choice([2.0, 3.0, 4.0]))
-        d = prep.hilly_domain(side, nj, dx, vc, seed=100 + q)
+        grids.append(prep.hilly_domain(side, nj, dx, vc, seed=100 + q))
+    doms, ps, fs = [], [], []
+    for q in range(n):
+        d = grids[q % len(grids)]
         sit = prep.random_situation(100 + q)
         doms.append(d)
         ps.append(d.params(sit, model=1, iterations=iterations))
         fs.append(prep.initial_fields(d, sit))
     statics = [d.static for d in doms]
     cells = sum(int((d.static.advdom[1:d.nii + 1, 1:d.njj + 1] == 1).sum()) * d.vert_cells_ff for d in doms)
-    out = {"workload": f"{n} instances, grids {min(d.nii for d in doms)}..{max(d.nii for d in doms)} columns a side, "
-                       f"{iterations} iterations each, model 1", "cells": cells}
+    out = {"workload": f"{n} instances on {len(grids)} grids of {min(d.nii for d in doms)}..{max(d.nii for d in doms)} "
+                       f"columns a side, {iterations} iterations each, model 1", "cells": cells}
     for name, k in (("sequential", 1), ("side_by_side", concurrent)):
         f2 = [f.copy() for f in fs]
         t0 = time.perf_counter()
@@ -769,7 +774,7 @@ def run_ours(args, rank, world):
         windm = wind_measure(dom, sit)
     instm = None
     if extras and not args.no_instances:
-        instm = instances_measure()
+        instm = instances_measure(args.instances, args.instances_iters, args.instances_concurrent)
     adjm = None
     if extras and not args.no_adjoint:
         adjm = adjoint_measure()
@@ -825,6 +830,9 @@ def main():
     ap.add_argument("--no-prep", action="store_true", help="skip the set-up (sub-domains, initial field) measurement")
     ap.add_argument("--no-wind", action="store_true", help="skip the particle wind interpolation measurement")
     ap.add_argument("--no-instances", action="store_true", help="skip the uneven-domain instances measurement")
+    ap.add_argument("--instances", type=int, default=16, help="instances of the uneven-domain measurement")
+    ap.add_argument("--instances-iters", type=int, default=100, help="SIMPLE iterations per uneven-domain instance")
+    ap.add_argument("--instances-concurrent", type=int, default=16, help="slots of the packed uneven-domain run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint measurement")
     ap.add_argument("--no-to-stop", action="store_true", help="skip the weather set solved to its stop rule")
     ap.add_argument("--ref-iters", type=int, default=4, help="SIMPLE iterations per reference-arm step")

@@ -7,13 +7,16 @@
 // wavefront kernels claim their tasks in dependency order from an atomic counter, so they need no
 // co-residency and make progress next to each other's launches.
 //
-// The instances go in waves of K (largest first, so a wave holds instances of similar size): the
-// calling thread loads the wave's instances one after the other while nothing else runs on the
-// device, then K threads iterate and store them at the same time.  Loading in between running
-// solves would not overlap with them: a device allocation (DevBuf growth at load) and the memsets
-// of the set-up wait for all work already in flight on the device.  Loads of later waves mostly
-// reuse the buffers of the first, larger ones.
+// Admission and packing: the instances are ordered by their device footprint, largest first.
+// The largest is loaded and its footprint measured; the others' are scaled from it by their field
+// sizes, and K slots are opened for the largest K instances whose footprints fit the HBM budget
+// together.  Those K loads run one after the other before any solve starts, so every device
+// allocation happens while nothing else runs (an allocation can wait for work in flight on the
+// device).  Then each slot's thread solves its instance and takes the next largest one left from a
+// shared queue as soon as it is done, loading it into the buffers of its first (larger) instance:
+// no slot waits for another, and the memory in use never exceeds what was admitted.
 #include <algorithm>
+#include <atomic>
 #include <numeric>
 #include <thread>
 #include <vector>
@@ -48,13 +51,22 @@ void drop_if_failed(gral_ctx *&ctx, int rc) {
     ctx = nullptr;
 }
 
+// Device bytes of one instance's load, up to a common factor: the solver fields and row carry
+// ([col][KS] floats, ten fields), the staging copies ([col][NKK+2], three fields) and the
+// per-column tables.
+double footprint_units(const gral_params &q) {
+    const double ncols = (double)(q.nii + 2) * (q.njj + 2);
+    const double ks = (double)(((q.kadvmax + 2) + 7) / 8 * 8);
+    return ncols * (10.0 * ks + 3.0 * (q.nkk + 2) + 16.0);
+}
+
 }  // namespace
 
 extern "C" int gral_prog_solve_instances(int32_t n, const gral_params *p, const gral_static *s, gral_fields *f,
                                          gral_stats *stats, int32_t *status, int32_t max_concurrent,
                                          uint64_t hbm_bytes) {
     if (n < 1 || !p || !s || !f || !status || max_concurrent < 1) return GRAL_EINVAL;
-    int dims[4] = {4, 4, 3, 2};   // capacity of every context: the largest of each dimension
+    int dims[4] = {4, 4, 3, 2};   // capacity bounds of every context: the largest of each dimension
     for (int b = 0; b < n; ++b) {
         dims[0] = std::max(dims[0], p[b].nii);
         dims[1] = std::max(dims[1], p[b].njj);
@@ -64,8 +76,8 @@ extern "C" int gral_prog_solve_instances(int32_t n, const gral_params *p, const 
     }
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
-    auto cells = [&](int b) { return (long long)(p[b].nii + 2) * (p[b].njj + 2) * (p[b].nkk + 2); };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells(a) > cells(b); });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return footprint_units(p[a]) > footprint_units(p[b]); });
 
     size_t free0 = 0, total = 0, free1 = 0;
     if (cudaMemGetInfo(&free0, &total) != cudaSuccess) {
@@ -77,46 +89,54 @@ extern "C" int gral_prog_solve_instances(int32_t n, const gral_params *p, const 
     std::vector<gral_ctx *> slot(1, nullptr);
     int rc = gral_prog_create(dims[0], dims[1], dims[2], dims[3], 1, &slot[0]);
     if (rc != GRAL_OK) return rc;
-    // the largest instance is loaded first: its footprint decides the wave size K
-    int first_rc = gral_prog_load(slot[0], 1, p + order[0], s + order[0], f + order[0]);
+    // the largest instance is loaded first; its measured footprint scales the others'
+    const int first_rc = gral_prog_load(slot[0], 1, p + order[0], s + order[0], f + order[0]);
     cudaMemGetInfo(&free1, &total);
-    const size_t footprint = std::max<size_t>(free0 > free1 ? free0 - free1 : 0, 64u << 20) * 11 / 10;
-    const uint64_t budget = hbm_bytes ? hbm_bytes : (uint64_t)(0.9 * (double)free0);
-    int K = (int)std::min<uint64_t>((uint64_t)max_concurrent, std::max<uint64_t>(1, budget / footprint));
-    K = std::min(K, n);
+    const double bytes0 = (double)std::max<size_t>(free0 > free1 ? free0 - free1 : 0, 64u << 20) * 1.1;
+    const double per_unit = bytes0 / footprint_units(p[order[0]]);
+    const double budget = hbm_bytes ? (double)hbm_bytes : 0.9 * (double)free0;
+    int K = 1;
+    double used = bytes0;
+    while (K < std::min(n, max_concurrent)) {
+        const double next = per_unit * footprint_units(p[order[K]]);
+        if (used + next > budget) break;
+        used += next;
+        ++K;
+    }
     slot.resize(K, nullptr);
 
-    std::vector<int> rcs(K);
-    for (int w0 = 0; w0 < n; w0 += K) {
-        const int m = std::min(K, n - w0);
-        // loads of the wave, nothing else on the device
-        for (int t = 0; t < m; ++t) {
-            const int b = order[w0 + t];
-            if (w0 == 0 && t == 0) {
-                rcs[t] = first_rc;
-                continue;
-            }
-            rcs[t] = GRAL_OK;
-            if (!slot[t]) rcs[t] = gral_prog_create(dims[0], dims[1], dims[2], dims[3], 1, &slot[t]);
-            if (rcs[t] == GRAL_OK) rcs[t] = gral_prog_load(slot[t], 1, p + b, s + b, f + b);
-        }
-        // iterations and stores of the wave, side by side
-        std::vector<std::thread> pool;
-        pool.reserve(m);
-        for (int t = 0; t < m; ++t) {
-            if (rcs[t] != GRAL_OK) continue;
-            const int b = order[w0 + t];
-            pool.emplace_back([&, t, b]() {
-                cudaSetDevice(dev);
-                rcs[t] = finish_one(slot[t], f + b, stats ? stats + b : nullptr);
-            });
-        }
-        for (auto &th : pool) th.join();
-        for (int t = 0; t < m; ++t) {
-            status[order[w0 + t]] = rcs[t];
-            drop_if_failed(slot[t], rcs[t]);
-        }
+    // the first K loads, one after the other, before any solve
+    std::vector<int> rcs(K, GRAL_OK);
+    rcs[0] = first_rc;
+    for (int t = 1; t < K; ++t) {
+        const int b = order[t];
+        rcs[t] = gral_prog_create(dims[0], dims[1], dims[2], dims[3], 1, &slot[t]);
+        if (rcs[t] == GRAL_OK) rcs[t] = gral_prog_load(slot[t], 1, p + b, s + b, f + b);
     }
+    // each slot solves its instance, then takes the next largest one left
+    std::atomic<int> next{K};
+    std::vector<std::thread> pool;
+    pool.reserve(K);
+    for (int t = 0; t < K; ++t) {
+        pool.emplace_back([&, t]() {
+            cudaSetDevice(dev);
+            int q = t;
+            int lrc = rcs[t];
+            for (;;) {
+                const int b = order[q];
+                if (lrc == GRAL_OK) lrc = finish_one(slot[t], f + b, stats ? stats + b : nullptr);
+                status[b] = lrc;
+                drop_if_failed(slot[t], lrc);
+                q = next.fetch_add(1);
+                if (q >= n) break;
+                const int nb = order[q];
+                lrc = GRAL_OK;
+                if (!slot[t]) lrc = gral_prog_create(dims[0], dims[1], dims[2], dims[3], 1, &slot[t]);
+                if (lrc == GRAL_OK) lrc = gral_prog_load(slot[t], 1, p + nb, s + nb, f + nb);
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
     for (auto *c : slot)
         if (c) gral_prog_destroy(c);
     for (int b = 0; b < n; ++b)

@@ -152,11 +152,13 @@ int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const 
 
 /* Independent situations whose grids differ (one gral_params, gral_static and gral_fields per
  * instance; GRAL solves such sets one after the other), several at once, each exactly as
- * gral_prog_solve does (results are identical to n single calls): largest first, in waves of K
- * instances, whose loads run one after the other and whose iterations and stores then run side
- * by side, each in its own context, stream and host thread.  K is max_concurrent, further limited
- * to what fits in hbm_bytes of device memory (0: 90 % of the free memory at the call), estimated from
- * the footprint of the largest instance, which is loaded first.  status[b] receives
+ * gral_prog_solve does (results are identical to n single calls).  The instances are ordered by
+ * device footprint, largest first; K slots (each a context, stream and host thread) take the K
+ * largest, whose loads run one after the other, then every slot solves its instance and takes the
+ * next largest one left as soon as it is done, reusing its buffers.  K is max_concurrent, further
+ * limited to the largest instances whose footprints fit in hbm_bytes of device memory together
+ * (0: 90 % of the free memory at the call; the largest instance is loaded first and its measured
+ * footprint scales the others' by their field sizes).  status[b] receives
  * instance b's return code (the error text of a failed instance is not kept); the call returns
  * GRAL_OK when every instance succeeded, else the code of the first failed instance in index
  * order.  stats may be NULL. */

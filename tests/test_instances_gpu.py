@@ -72,3 +72,24 @@ def test_instance_failure_is_its_own(gpu_required):
     stats, status, rc = solve_instances(ps, [x.static for x in doms], fs, max_concurrent=2)
     assert status[bad] == abi.GRAL_ENONFINITE and rc == abi.GRAL_ENONFINITE
     assert [s for b, s in enumerate(status) if b != bad] == [abi.GRAL_OK] * 3
+
+
+def test_instances_queue_and_memory_budget(gpu_required):
+    """More instances than slots: each slot takes the next largest instance left when its own is
+    done, in buffers sized by its first (larger) one.  An HBM budget of about twice the largest
+    instance's footprint admits fewer slots than max_concurrent; results stay bit-identical."""
+    sizes = SIZES + [(28, 24, 2.0, 9), (44, 40, 3.0, 12), (22, 30, 2.5, 8), (34, 26, 4.0, 10)]
+    doms, ps, fs = instances(sizes, 8, seed0=60)
+    want = []
+    for b, d in enumerate(doms):
+        w = fs[b].copy()
+        O.solve(ps[b], d.static, w)
+        want.append(w)
+    for k, budget in ((4, 0), (8, 48 << 20)):
+        got = [f.copy() for f in fs]
+        stats, status, rc = solve_instances(ps, [d.static for d in doms], got, max_concurrent=k, hbm_bytes=budget)
+        assert rc == abi.GRAL_OK and status == [abi.GRAL_OK] * len(sizes), status
+        for b in range(len(sizes)):
+            assert_same(got[b], want[b])
+            assert stats[b]["iterations"] == 8
+
