@@ -947,7 +947,7 @@ int col_blocks(const KArgs &a) { return (a.ncols * 32 + 255) / 256; }
 
 // one Gauss-Seidel phase of the forward on the loaded schedule (strips or diagonal claims)
 void forward_phase(gral_ctx *ctx, int kind, const SweepGeom &g, cudaStream_t st) {
-    if (ctx->pmode > 0) launch_strip(kind, ctx->ka, g, ctx->pmode - 1, ctx->strip_grid[kind], st);
+    if (ctx->pmode > 0) launch_strip(kind, ctx->ka, g, strip_variant_of(ctx), ctx->strip_grid[kind], st);
     else launch_gs(kind, ctx->ka, g, ctx->grid_gs[kind], st);
 }
 

@@ -72,8 +72,10 @@ struct gral_ctx {
     int lookahead_p = 3;       // GRAL_PROG_LOOKAHEAD_P: the same for the pressure sweep
     int variant = -1;          // chosen launch variant of the batched family (-1: not tuned yet)
     // slab family, model 1: 0 = the diagonal-claim wavefront (fused pressure..U, then V, W);
-    // 1+v = strip variant v for pressure, U, V, W (-1: not tuned yet)
+    // 1+v = strip variant v for pressure, U, V, W; 1+strip_num_variants() = pressure..U fused on
+    // strips, then V, W on strip variant 0 (-1: not tuned yet)
     int pmode = -1;
+    int fstrip_grid = 0;       // grid of the fused strip launch
     int forced_pmode = -1;     // GRAL_PROG_PLAIN_MODE
     int strip_grid[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // indexed by PH_*
     float ptune_ms[16] = {0};  // autotuner timings per plain mode
@@ -169,6 +171,10 @@ namespace gral {
 // Slab family, model 1: keep the default schedule of the sweeps (or GRAL_PROG_PLAIN_MODE) without
 // trial iterations, and size its grids (prog_host.cu).
 int plain_schedule_default(gral_ctx *ctx);
+// the strip variant of the separate phase launches of the loaded plain mode (pmode > 0)
+int strip_variant_of(const gral_ctx *ctx);
+// the loaded plain mode runs pressure..U as one fused strip launch
+bool fused_strips(const gral_ctx *ctx);
 
 inline int fail(gral_ctx *c, int code, const std::string &msg) {
     if (c) c->err = msg;

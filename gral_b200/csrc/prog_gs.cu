@@ -899,11 +899,71 @@ __device__ inline bool wait_count(const int *cnt, int need, int *err, unsigned l
 // overwrites a slot, the row below must have finished the column that slot held.
 constexpr int SDEPTH = 4;
 
+// Lanes 0..n-1 each wait on one flag (relaxed polls, all in flight together), then every lane
+// issues the acquire fence that completes the acquire pattern; true if all flags reached their
+// stamp.
+__device__ __forceinline__ bool wait_lanes(const KArgs &a, const int *flag, int stamp, bool mine) {
+    bool ok = true;
+    if (mine) ok = wait_stamps(flag, nullptr, stamp, a.err, a.wait_limit_ns);
+    return __all_sync(0xffffffffu, ok);
+}
+
+// The sweep rows i1_first + r (r = 0..SR-1; rows outside the geometry are skipped) of one strip,
+// run by warps w = r*SMW + m of a group of SR*SMW warps.  With AVW, a column first waits until the
+// averages of its 3x3 neighbourhood are done (the U part of the fused strip kernel).
+template <int SR, int SMW, bool AVW, class Job>
+__device__ __forceinline__ void strip_run(const KArgs &a, const SweepGeom &g, Job &job, int w, int u, int i1_first,
+                                          int IS, int JS, int stamp, int *s_done, float (*s_col)[KMAX_LEVELS]) {
+    const int lane = threadIdx.x & 31;
+    const int r = w / SMW, m = w % SMW;
+    const int i1 = i1_first + r;
+    if (i1 < g.ia || i1 >= g.ia + g.ni) return;
+    const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+    int *fl = a.flags + (size_t)u * a.ncols;
+    const bool above = i1 > g.ia;                            // a predecessor row exists
+    const bool above_here = above && r > 0;                  // ... and runs in this block
+    const bool below = r + 1 < SR && i1 + 1 < g.ia + g.ni;   // the row below runs in this block
+    const bool last = r == SR - 1 || i1 + 1 == g.ia + g.ni;  // the next strip's first row reads this one
+    const int sAV = stamp - PH_U + PH_AV;
+    for (int c = m; c < g.nj; c += SMW) {
+        const int j1 = g.ja + c;
+        const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
+        bool okav = true;
+        if (AVW) {
+            const int wi = i + (lane % 3) - 1, wj = j + (lane / 3) - 1;
+            const bool mine = lane < 9 && wi >= 2 && wi <= a.nii - 1 && wj >= 2 && wj <= a.njj - 1;
+            okav = wait_lanes(a, fl + wi * a.nj2 + wj, sAV, mine);
+            __syncwarp();
+        }
+        job.pre_strip(u, i, j, IS, JS, i1 == g.ia);
+        int ok = okav;
+        if (lane == 0 && ok) {
+            ok = wait_count(s_done + r, c, a.err, a.wait_limit_ns);
+            if (ok && above_here) ok = wait_count(s_done + r - 1, c + 1, a.err, a.wait_limit_ns);
+            else if (ok && above)
+                ok = wait_stamps(fl + (i - IS) * a.nj2 + j, nullptr, stamp, a.err, a.wait_limit_ns, 0);
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        __syncwarp();
+        if (ok)
+            job.post(u, IS, JS, true, above_here ? s_col[(r - 1) * SDEPTH + c % SDEPTH] : nullptr,
+                     (c > 0) ? s_col[r * SDEPTH + (c - 1) % SDEPTH] : nullptr);
+        if (lane == 0 && below && c >= SDEPTH) wait_count(s_done + r + 1, c - SDEPTH + 1, a.err, a.wait_limit_ns);
+        __syncwarp();
+        float *slot = s_col[r * SDEPTH + c % SDEPTH];
+        slot[lane] = job.own[0];
+        if (lane + 32 < KMAX_LEVELS) slot[lane + 32] = job.own[1];
+        __syncwarp();
+        if (lane == 0) {
+            st_release_cta(s_done + r, c + 1);
+            if (Job::kAllFlags || last) st_release(fl + i * a.nj2 + j, stamp);
+        }
+    }
+}
+
 template <int PHASE, bool REVERSE, int SR, int SMW, class Job>
 __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &g, Job &job, int *s_done,
                                                unsigned *s_claim, float (*s_col)[KMAX_LEVELS]) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int r = warp / SMW, m = warp % SMW;
     const unsigned units = (unsigned)*a.nact;
     const unsigned total = (unsigned)((g.ni + SR - 1) / SR) * units;
     unsigned int *ctr = a.counters + PHASE;
@@ -919,43 +979,127 @@ __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &
         __syncthreads();
         const unsigned t = *s_claim;
         if (t >= total) break;
-        const int u = a.act[t % units];
-        const int i1 = g.ia + (int)(t / units) * SR + r;
-        if (i1 < g.ia + g.ni) {
-            const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
+        strip_run<SR, SMW, false>(a, g, job, threadIdx.x >> 5, a.act[t % units], g.ia + (int)(t / units) * SR, IS, JS,
+                                  stamp, s_done, s_col);
+        __syncthreads();
+    }
+    job.finish();
+}
+
+// ------------------------ fused strips: pressure -> velocity correction -> averages -> U --------
+// One launch claims, in order, pressure strip 0, U strip 0, pressure strip 1, U strip 1, ...,
+// and a last U strip.  Pressure strip s (16 warps) runs sweep rows ia + 4s .. ia + 4s + 3 as
+// k_pressure_strip.  U strip s runs the velocity corrections of the rows one behind (ia + 4s - 1
+// ...), the averages of the rows two behind and the U sweep of the rows three behind: warps 0-3
+// take one velocity-correction row and one averages row each, in column order (the averages two
+// columns behind), and warps 4-15 the U rows on the strip schedule (3 warps per row), each U column
+// first waiting until the averages of its 3x3 neighbourhood are done.  The dependencies across
+// cells are those of k_fused_pvau and go through the global flags (stamps it*8 + kind): velocity
+// correction (i,j) after pressure at (i,j), (i-1,j), (i,j-1); averages (i,j) after the velocity
+// corrections at (i,j), (i+1,j), (i,j+1); U (i,j) after the averages of its 3x3 neighbourhood.  With
+// those row offsets every wait is on a strip claimed earlier: a velocity correction reads the
+// pressure of at most the next row, an average the velocity correction of at most the next row,
+// and U the averages of at most the next row.
+constexpr int FSR = 4;     // rows per strip
+
+__global__ void __launch_bounds__(16 * 32, 1) k_fused_strip(KArgs a, FusedGeom fg) {
+    __shared__ float sm[16][SM_ROWS][KMAX_LEVELS];
+    __shared__ float s_col[FSR * SDEPTH][KMAX_LEVELS];
+    __shared__ int s_done[FSR];
+    __shared__ unsigned s_claim;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const SweepGeom &gp = fg.gp, &gu = fg.gu;
+    const int it = *a.it_global;
+    int IS, JS;
+    sweep_dir(it, IS, JS);
+    const int sP = it * 8 + PH_PRESSURE, sVC = it * 8 + PH_VC, sAV = it * 8 + PH_AV, sU = it * 8 + PH_U;
+    PressJob pj{a, sm[warp], sP};
+    pj.run_max = 0;
+    pj.run_s = -1;
+    Mom1Job<COMP_U> uj{a, sm[warp], sU};
+    const unsigned units = (unsigned)*a.nact;
+    const int np = (gp.ni + FSR - 1) / FSR;
+    const unsigned total = (unsigned)(2 * np + 1) * units;
+    unsigned int *ctr = a.counters + PH_PRESSURE;
+    const int ilo = 2, ihi = a.nii - 1, jlo = 2, jhi = a.njj - 1;   // velocity correction / averages range
+    for (;;) {
+        if (threadIdx.x == 0) s_claim = (*(volatile int *)a.err != ERR_NONE) ? 0xffffffffu : atomicAdd(ctr, 1u);
+        if (threadIdx.x < FSR) s_done[threadIdx.x] = 0;
+        __syncthreads();
+        const unsigned t = s_claim;
+        if (t >= total) break;
+        const int item = (int)(t / units), u = a.act[t % units];
+        const bool pstrip = item < 2 * np && (item & 1) == 0;
+        const int s = pstrip ? item / 2 : (item < 2 * np ? item / 2 : np);
+        const int base = gp.ia + s * FSR;
+        if (pstrip) {
+            strip_run<FSR, 4, false>(a, gp, pj, warp, u, base, IS, JS, sP, s_done, s_col);
+        } else if (warp >= 4) {
+            strip_run<FSR, 3, true>(a, gu, uj, warp - 4, u, base - 3, IS, JS, sU, s_done, s_col);
+        } else {
             int *fl = a.flags + (size_t)u * a.ncols;
-            const bool below = r + 1 < SR && i1 + 1 < g.ia + g.ni;   // the row below runs in this block
-            for (int c = m; c < g.nj; c += SMW) {
-                const int j1 = g.ja + c;
-                const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
-                job.pre_strip(u, i, j, IS, JS, i1 == g.ia);
-                int ok = 1;
-                if (lane == 0) {
-                    ok = wait_count(s_done + r, c, a.err, a.wait_limit_ns);
-                    if (ok && r > 0) ok = wait_count(s_done + r - 1, c + 1, a.err, a.wait_limit_ns);
-                    else if (ok && i1 > g.ia)
-                        ok = wait_stamps(fl + (i - IS) * a.nj2 + j, nullptr, stamp, a.err, a.wait_limit_ns, 0);
+            const bool act = a.sit[u].active != 0;
+            const int iv1 = base - 1 + warp, ia1 = base - 2 + warp;   // sweep rows of this warp
+            const bool vrow = iv1 >= gp.ia && iv1 < gp.ia + gp.ni, arow = ia1 >= gp.ia && ia1 < gp.ia + gp.ni;
+            const int iv = (IS == 1) ? iv1 : a.nii - iv1 + 1, ia = (IS == 1) ? ia1 : a.nii - ia1 + 1;
+            // columns in chunks of VCH: the chunk's three dependency flags per column are polled by
+            // lanes 3q..3q+2 together, the columns run one after the other, and lanes q publish
+            // their column's flag; the averages trail the velocity corrections by one chunk
+            constexpr int VCH = 4;
+            const int q = lane / 3, k3 = lane % 3;
+            for (int c0 = 0; c0 < gp.nj + VCH; c0 += VCH) {
+                if (vrow && c0 < gp.nj) {
+                    const int nc = min(VCH, gp.nj - c0);
+                    bool mine = false;
+                    const int *fp = fl;
+                    if (q < nc) {
+                        const int j1 = gp.ja + c0 + q, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        const int wi = (k3 == 1) ? iv - 1 : iv, wj = (k3 == 2) ? j - 1 : j;
+                        mine = wi >= ilo && wj >= jlo;
+                        fp = fl + wi * a.nj2 + wj;
+                    }
+                    const bool ok = wait_lanes(a, fp, sP, mine);
+                    __syncwarp();
+                    for (int qq = 0; qq < nc; ++qq) {
+                        const int j1 = gp.ja + c0 + qq, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        const int col = iv * a.nj2 + j;
+                        if (ok && act) velcorr_col<false>(a, u, col, iv, j, make_acc<false>(a, u, col), lane, 32);
+                    }
+                    __syncwarp();
+                    if (lane < nc) {
+                        const int j1 = gp.ja + c0 + lane, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        st_release(fl + iv * a.nj2 + j, sVC);
+                    }
                 }
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                __syncwarp();
-                if (ok)
-                    job.post(u, IS, JS, true, (r > 0) ? s_col[(r - 1) * SDEPTH + c % SDEPTH] : nullptr,
-                             (c > 0) ? s_col[r * SDEPTH + (c - 1) % SDEPTH] : nullptr);
-                if (lane == 0 && below && c >= SDEPTH) wait_count(s_done + r + 1, c - SDEPTH + 1, a.err, a.wait_limit_ns);
-                __syncwarp();
-                float *slot = s_col[r * SDEPTH + c % SDEPTH];
-                slot[lane] = job.own[0];
-                if (lane + 32 < KMAX_LEVELS) slot[lane + 32] = job.own[1];
-                __syncwarp();
-                if (lane == 0) {
-                    st_release_cta(s_done + r, c + 1);
-                    if (Job::kAllFlags || r == SR - 1 || i1 + 1 == g.ia + g.ni) st_release(fl + i * a.nj2 + j, stamp);
+                const int ca = c0 - VCH;
+                if (arow && ca >= 0 && ca < gp.nj) {
+                    const int nc = min(VCH, gp.nj - ca);
+                    bool mine = false;
+                    const int *fp = fl;
+                    if (q < nc) {
+                        const int j1 = gp.ja + ca + q, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        const int wi = (k3 == 1) ? ia + 1 : ia, wj = (k3 == 2) ? j + 1 : j;
+                        mine = wi <= ihi && wj <= jhi;
+                        fp = fl + wi * a.nj2 + wj;
+                    }
+                    const bool ok = wait_lanes(a, fp, sVC, mine);
+                    __syncwarp();
+                    for (int qq = 0; qq < nc; ++qq) {
+                        const int j1 = gp.ja + ca + qq, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        const int col = ia * a.nj2 + j;
+                        if (ok && act) average_col<false>(a, col, ia, j, make_acc<false>(a, u, col), lane, 32);
+                    }
+                    __syncwarp();
+                    if (lane < nc) {
+                        const int j1 = gp.ja + ca + lane, j = (JS == 1) ? j1 : a.njj - j1 + 1;
+                        st_release(fl + ia * a.nj2 + j, sAV);
+                    }
                 }
             }
         }
         __syncthreads();
     }
-    job.finish();
+    pj.finish();
 }
 
 template <int SR, int SMW>
@@ -994,15 +1138,6 @@ __global__ void __launch_bounds__(SR * SMW * 32, 1) k_mom1_strip(KArgs a, SweepG
 //   averages (i,j) after the velocity corrections at (i,j), (i+1,j), (i,j+1);
 //   U (i,j) after the averages of the 3x3 neighbourhood (which also covers the corrected U/V/W and
 //   final DPMNEW it reads) and its two U sweep predecessors.
-
-// Lanes 0..n-1 each wait on one flag (relaxed polls, all in flight together), then every lane
-// issues the acquire fence that completes the acquire pattern; true if all flags reached their
-// stamp.
-__device__ __forceinline__ bool wait_lanes(const KArgs &a, const int *flag, int stamp, bool mine) {
-    bool ok = true;
-    if (mine) ok = wait_stamps(flag, nullptr, stamp, a.err, a.wait_limit_ns);
-    return __all_sync(0xffffffffu, ok);
-}
 
 __global__ void __launch_bounds__(GS_WARPS * 32) k_fused_pvau(KArgs a, FusedGeom fg) {
     __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
@@ -1674,6 +1809,16 @@ cudaError_t strip_occupancy(int kind, int variant, int *blocks_per_sm) {
 
 void launch_strip(int kind, const KArgs &a, const SweepGeom &g, int variant, int grid, cudaStream_t st) {
     strip_kernel(variant, kind)<<<grid, strip_block_threads(variant), 0, st>>>(a, g);
+}
+
+cudaError_t fused_strip_occupancy(int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k_fused_strip, 16 * 32, 0);
+}
+
+int fused_strip_claims(const SweepGeom &gp) { return 2 * ((gp.ni + FSR - 1) / FSR) + 1; }
+
+void launch_fused_strip(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st) {
+    k_fused_strip<<<grid, 16 * 32, 0, st>>>(a, fg);
 }
 
 size_t diag_smem(int ks) { return (size_t)GS_WARPS * 6 * ks * sizeof(float); }

@@ -220,17 +220,33 @@ int validate(gral_ctx *ctx, int n, const gral_params *p, const gral_static *s, c
 // diagonal-claim wavefront (pmode 0).
 bool use_strips(const gral_ctx *ctx) { return !ctx->il && ctx->model == 1 && ctx->pmode > 0; }
 
+}  // namespace
+
+int gral::strip_variant_of(const gral_ctx *ctx) {
+    return (ctx->pmode - 1 < strip_num_variants()) ? ctx->pmode - 1 : 0;
+}
+
+bool gral::fused_strips(const gral_ctx *ctx) {
+    return use_strips(ctx) && ctx->pmode == 1 + strip_num_variants();
+}
+
+namespace {
+
 // One SIMPLE iteration (PrognosticFlowfield.cs:584-1182), enqueued on st.
 void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
     const KArgs &a = ctx->ka;
     cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
     launch_bc(a, ctx->bc, st);
     if (use_strips(ctx)) {
-        const int v = ctx->pmode - 1;
-        launch_strip(PH_PRESSURE, a, ctx->geo_p.g, v, ctx->strip_grid[PH_PRESSURE], st);
-        launch_velcorr(a, st);
-        launch_average(a, st);
-        launch_strip(PH_U, a, ctx->geo_u.g, v, ctx->strip_grid[PH_U], st);
+        const int v = strip_variant_of(ctx);
+        if (fused_strips(ctx)) {
+            launch_fused_strip(a, ctx->fgeo, ctx->fstrip_grid, st);
+        } else {
+            launch_strip(PH_PRESSURE, a, ctx->geo_p.g, v, ctx->strip_grid[PH_PRESSURE], st);
+            launch_velcorr(a, st);
+            launch_average(a, st);
+            launch_strip(PH_U, a, ctx->geo_u.g, v, ctx->strip_grid[PH_U], st);
+        }
         launch_strip(PH_V, a, ctx->geo_v.g, v, ctx->strip_grid[PH_V], st);
         launch_strip(PH_W, a, ctx->geo_p.g, v, ctx->strip_grid[PH_W], st);
         launch_bookkeeping(a, st);
@@ -257,6 +273,7 @@ void launch_iteration(gral_ctx *ctx, cudaStream_t st) {
 int launches_per_iteration(const gral_ctx *ctx) {
     const int gs = ctx->ka.group_set <= 0 ? ctx->ngroups : ctx->ka.group_set;
     const int sets = ctx->il ? (ctx->ngroups + gs - 1) / gs : 1;
+    if (fused_strips(ctx)) return 3 + 3 + 1;
     if (use_strips(ctx)) return 3 + 4 + 3;
     if (ctx->fused) return 3 + 1 + 2 + 1;
     const int phases = (ctx->model == 2) ? 5 : 4;
@@ -293,7 +310,7 @@ int size_grids(gral_ctx *ctx) {
     }
     if (use_strips(ctx)) {
         // one block per strip at most: the strip kernels are persistent and claim strips in order
-        const int sv = ctx->pmode - 1;
+        const int sv = strip_variant_of(ctx);
         const Geom *gk[4] = {&ctx->geo_p, &ctx->geo_u, &ctx->geo_v, &ctx->geo_p};
         for (int q = 0; q < 4; ++q) {
             int bps = 0;
@@ -302,6 +319,12 @@ int size_grids(gral_ctx *ctx) {
             const long long strips = (long long)((gk[q]->g.ni + sr - 1) / sr) * ctx->nb;
             ctx->strip_grid[kinds[q]] =
                 (int)std::max<long long>(1, std::min<long long>((long long)std::max(1, bps) * ctx->num_sms, strips));
+        }
+        if (fused_strips(ctx)) {
+            int bps = 0;
+            CK(fused_strip_occupancy(&bps));
+            const long long claims = (long long)fused_strip_claims(ctx->geo_p.g) * ctx->nb;
+            ctx->fstrip_grid = (int)std::max<long long>(1, std::min<long long>((long long)std::max(1, bps) * ctx->num_sms, claims));
         }
     }
     const int warps = ctx->grid_gs[PH_PRESSURE] * gs_block_threads(il, v) / 32;
@@ -375,7 +398,7 @@ constexpr int kDefaultPlainMode = 1;   // strips of 4 rows, 4 warps per row (fas
 }  // namespace
 
 int gral::plain_schedule_default(gral_ctx *ctx) {
-    const int nv = 1 + strip_num_variants();
+    const int nv = 2 + strip_num_variants();
     ctx->pmode = (ctx->model != 1) ? 0 : ((ctx->forced_pmode >= 0 && ctx->forced_pmode < nv) ? ctx->forced_pmode : kDefaultPlainMode);
     return size_grids(ctx);
 }
@@ -384,7 +407,7 @@ namespace {
 
 int tune_plain(gral_ctx *ctx) {
     if (ctx->pmode >= 0) return GRAL_OK;
-    const int nv = 1 + strip_num_variants();
+    const int nv = 2 + strip_num_variants();
     const int first_stop = std::min(((ctx->it_host + ctx->cadence - 1) / ctx->cadence) * ctx->cadence, ctx->it_max);
     if (ctx->model != 1) {
         ctx->pmode = 0;
@@ -796,6 +819,8 @@ int gral_prog_load(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_st
     put_geom(ctx->geo_u);
     put_geom(ctx->geo_v);
 
+    ctx->fgeo.gp = ctx->geo_p.g;     // also read by the fused strip launch
+    ctx->fgeo.gu = ctx->geo_u.g;
     // task list of the fused pressure/velcorr/average/U wavefront: step s holds pressure diagonal
     // s, velocity-correction diagonal s-1, averages s-2 and U-diagonal s-5 (P-diagonal s-4)
     {
@@ -992,12 +1017,16 @@ int gral_prog_iterate_timed(gral_ctx *ctx, int32_t iterations, double *phase_ms,
         cudaMemsetAsync(ctx->counters.p, 0, 8 * kCounterSlots * sizeof(unsigned int), st);
         launch_bc(a, ctx->bc, st);
     }});
-    const int sv = ctx->pmode - 1;
+    const int sv = strip_variant_of(ctx);
     if (use_strips(ctx)) {
-        seq.push_back({GRAL_PHASE_PRESSURE, [&] { launch_strip(PH_PRESSURE, a, ctx->geo_p.g, sv, ctx->strip_grid[PH_PRESSURE], st); }});
-        seq.push_back({GRAL_PHASE_VELCORR, [&] { launch_velcorr(a, st); }});
-        seq.push_back({GRAL_PHASE_AVERAGE, [&] { launch_average(a, st); }});
-        seq.push_back({GRAL_PHASE_U, [&] { launch_strip(PH_U, a, ctx->geo_u.g, sv, ctx->strip_grid[PH_U], st); }});
+        if (fused_strips(ctx)) {
+            seq.push_back({GRAL_PHASE_FUSED, [&] { launch_fused_strip(a, ctx->fgeo, ctx->fstrip_grid, st); }});
+        } else {
+            seq.push_back({GRAL_PHASE_PRESSURE, [&] { launch_strip(PH_PRESSURE, a, ctx->geo_p.g, sv, ctx->strip_grid[PH_PRESSURE], st); }});
+            seq.push_back({GRAL_PHASE_VELCORR, [&] { launch_velcorr(a, st); }});
+            seq.push_back({GRAL_PHASE_AVERAGE, [&] { launch_average(a, st); }});
+            seq.push_back({GRAL_PHASE_U, [&] { launch_strip(PH_U, a, ctx->geo_u.g, sv, ctx->strip_grid[PH_U], st); }});
+        }
         seq.push_back({GRAL_PHASE_V, [&] { launch_strip(PH_V, a, ctx->geo_v.g, sv, ctx->strip_grid[PH_V], st); }});
         seq.push_back({GRAL_PHASE_W, [&] { launch_strip(PH_W, a, ctx->geo_p.g, sv, ctx->strip_grid[PH_W], st); }});
     } else if (ctx->fused) {

@@ -35,6 +35,11 @@ int strip_rows(int variant);
 int strip_block_threads(int variant);
 cudaError_t strip_occupancy(int kind, int variant, int *blocks_per_sm);
 void launch_strip(int kind, const KArgs &a, const SweepGeom &g, int variant, int grid, cudaStream_t st);
+// pressure, velocity correction, averages and model-1 U in one launch on the strip schedule:
+// claims (per situation) alternate pressure strips and U strips, 2*strips+1 of them
+cudaError_t fused_strip_occupancy(int *blocks_per_sm);
+int fused_strip_claims(const SweepGeom &gp);
+void launch_fused_strip(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st);
 // pressure + velocity correction + averages + model-1 U in one wavefront launch (slab family)
 cudaError_t fused_occupancy(int *blocks_per_sm);
 void launch_fused_pvau(const KArgs &a, const FusedGeom &fg, int grid, cudaStream_t st);

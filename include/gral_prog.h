@@ -123,7 +123,7 @@ typedef struct gral_stats {
                                     (32 situations per group, one block per group-column) */
     int32_t launch_variant;      /* launch variant the autotuner kept: interleaved layout, the batched
                                     kernels' variant; slab layout, the schedule of the model-1 sweeps
-                                    (0 diagonal-claim wavefront, 1+v strip variant v; GRAL_PROG_PLAIN_MODE
+                                    (0 diagonal-claim wavefront, 1+v strip variant v, 5 fused strips; GRAL_PROG_PLAIN_MODE
                                     forces one) */
     int32_t launches_per_iteration; /* kernel launches of one SIMPLE iteration in the kept configuration */
 } gral_stats;

@@ -3,7 +3,8 @@
 The slab family (one or a few situations) runs the pressure and the U, V, W sweeps either on the
 diagonal-claim wavefront (mode 0: one warp per column task, every hand-off through a global flag)
 or on a strip schedule (mode 1+v: a block per strip of sweep rows, hand-offs inside the strip
-through shared-memory progress counters).  The autotuner may keep any of them, so each is forced
+through shared-memory progress counters; the last mode runs pressure, velocity correction,
+averages and U as one launch whose claims alternate pressure strips and U strips).  The autotuner may keep any of them, so each is forced
 in turn (GRAL_PROG_PLAIN_MODE) over six iterations, which cover all four sweep directions, on a
 grid whose row count is not a multiple of any strip height, with buildings and vegetation, for
 one situation and for three (strips of different situations claimed from one counter), at both
@@ -50,5 +51,5 @@ def test_every_plain_mode_matches_oracle(gpu_required, monkeypatch, n_sit, simd)
             for name in ("uk", "vk", "wk"):
                 assert np.array_equal(getattr(fg[b], name), getattr(want[b], name)), (mode, b, name)
             assert np.array_equal(tg[b], want_tr[b]), (mode, b, "DeltaUMax trace")
-    # the diagonal-claim wavefront and at least four strip variants
-    assert len(seen) >= 5, seen
+    # the diagonal-claim wavefront, four strip variants and the fused strips
+    assert len(seen) >= 6, seen
