@@ -143,3 +143,36 @@ extern "C" int gral_prog_solve_instances(int32_t n, const gral_params *p, const 
         if (status[b] != GRAL_OK) return status[b];
     return GRAL_OK;
 }
+
+extern "C" int gral_prog_solve_batch_devices(int32_t ndev, const int32_t *devices, int32_t n, const gral_params *p,
+                                             const gral_static *s, gral_fields *f, gral_stats *stats) {
+    if (ndev < 1 || !devices || n < ndev || !p || !s || !f) return GRAL_EINVAL;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+        cudaGetLastError();
+        return GRAL_ENODEV;
+    }
+    for (int d = 0; d < ndev; ++d)
+        if (devices[d] < 0 || devices[d] >= count) return GRAL_EINVAL;
+    std::vector<int> rcs(ndev, GRAL_OK);
+    std::vector<std::thread> pool;
+    pool.reserve(ndev);
+    for (int d = 0; d < ndev; ++d) {
+        pool.emplace_back([&, d]() {
+            const int b0 = (int)((long long)d * n / ndev), b1 = (int)((long long)(d + 1) * n / ndev);
+            if (cudaSetDevice(devices[d]) != cudaSuccess) {
+                rcs[d] = GRAL_ENODEV;
+                return;
+            }
+            gral_ctx *ctx = nullptr;
+            int rc = gral_prog_create(p[b0].nii, p[b0].njj, p[b0].nkk, p[b0].kadvmax, b1 - b0, &ctx);
+            if (rc == GRAL_OK) rc = gral_prog_solve_batch(ctx, b1 - b0, p + b0, s, f + b0, stats ? stats + b0 : nullptr);
+            if (ctx) gral_prog_destroy(ctx);
+            rcs[d] = rc;
+        });
+    }
+    for (auto &th : pool) th.join();
+    for (int d = 0; d < ndev; ++d)
+        if (rcs[d] != GRAL_OK) return rcs[d];
+    return GRAL_OK;
+}

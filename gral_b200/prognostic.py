@@ -26,7 +26,7 @@ EXPORTS = ["gral_prog_version", "gral_prog_create", "gral_prog_solve", "gral_pro
            "gral_prog_last_error", "gral_prog_destroy", "gral_prog_check_speeds_noalloc",
            "gral_prog_gff_size", "gral_prog_gff_pack", "gral_prog_gff_pack_timed", "gral_prog_gff_unpack",
            "gral_prog_subdomains", "gral_prog_flat_init", "gral_prog_vegetation", "gral_prog_prep_last_ms",
-           "gral_prog_wind_at", "gral_prog_solve_instances", "gral_prog_load_flat", "gral_prog_vjp_forward",
+           "gral_prog_wind_at", "gral_prog_solve_instances", "gral_prog_solve_batch_devices", "gral_prog_load_flat", "gral_prog_vjp_forward",
            "gral_prog_vjp"]
 
 # payload modes of gral_prog_gff_pack (GFFWrite.cs writingMode 0, 1, 2 and the model-2 .tke file)
@@ -111,6 +111,9 @@ def lib(build_if_stale: bool = True):
                                             C.POINTER(GralFields), C.POINTER(GralStats), C.POINTER(C.c_int32),
                                             C.c_int32, C.c_uint64]
     L.gral_prog_solve_instances.restype = C.c_int
+    L.gral_prog_solve_batch_devices.argtypes = [C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(GralParams),
+                                                C.POINTER(GralStatic), C.POINTER(GralFields), C.POINTER(GralStats)]
+    L.gral_prog_solve_batch_devices.restype = C.c_int
     L.gral_prog_load_flat.argtypes = [vp, C.c_int32, C.POINTER(GralParams), C.POINTER(GralStatic), C.POINTER(GralMet),
                                       C.POINTER(GralFlatGrid), C.POINTER(GralFields)]
     L.gral_prog_load_flat.restype = C.c_int
@@ -396,4 +399,20 @@ def solve_instances(params: Sequence[dict], statics: Sequence[StaticArrays], fie
     rc = L.gral_prog_solve_instances(n, pa, sa, fa, st, status, max_concurrent, hbm_bytes)
     stats = [stats_to_dict(st[b]) for b in range(n)]
     return stats, [int(x) for x in status], rc
+
+
+def solve_batch_devices(devices: Sequence[int], params: Sequence[dict], static: StaticArrays,
+                        fields: Sequence[FieldArrays]):
+    """A batch of situations on one grid spread over several GPUs of the node
+    (``gral_prog_solve_batch_devices``): devices[d] takes the d-th contiguous shard; fields are
+    updated in place.  Returns (stats, rc)."""
+    L = lib()
+    n, nd = len(params), len(devices)
+    dv = (C.c_int32 * max(nd, 1))(*devices)
+    pa = (GralParams * n)(*[params_to_c(p) for p in params])
+    sa = static.to_c()
+    fa = (GralFields * n)(*[f.to_c() for f in fields])
+    st = (GralStats * n)()
+    rc = L.gral_prog_solve_batch_devices(nd, dv, n, pa, C.byref(sa), fa, st)
+    return [stats_to_dict(st[b]) for b in range(n)], rc
 

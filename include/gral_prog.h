@@ -150,6 +150,16 @@ int gral_prog_solve(gral_ctx *ctx, const gral_params *p, const gral_static *s,
 int gral_prog_solve_batch(gral_ctx *ctx, int32_t n, const gral_params *p, const gral_static *s,
                           gral_fields *f, gral_stats *stats);
 
+/* A batch of n situations on one grid (as gral_prog_solve_batch) spread over ndev devices of this
+ * node: devices[d] (a CUDA device ordinal; one may repeat) takes the contiguous shard of situations
+ * [d*n/ndev, (d+1)*n/ndev) in a context of its own, created and released inside the call, each
+ * shard solved by its own host thread with no exchange between devices (weather situations are
+ * independent, Program.cs:403-742).  Results are those of n single solves.  Returns GRAL_OK, or
+ * the code of the first shard in device order that failed; GRAL_EINVAL for ndev < 1, n < ndev or an
+ * ordinal outside 0..cudaGetDeviceCount()-1.  stats may be NULL. */
+int gral_prog_solve_batch_devices(int32_t ndev, const int32_t *devices, int32_t n, const gral_params *p,
+                                  const gral_static *s, gral_fields *f, gral_stats *stats);
+
 /* Independent situations whose grids differ (one gral_params, gral_static and gral_fields per
  * instance; GRAL solves such sets one after the other), several at once, each exactly as
  * gral_prog_solve does (results are identical to n single calls).  The instances are ordered by

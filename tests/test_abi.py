@@ -105,3 +105,17 @@ def test_phase_names_match_header():
     assert len(PHASES) == n
     ids = {int(v): k for k, v in re.findall(r"#define GRAL_PHASE_(\w+) (\d+)", text)}
     assert sorted(ids) == list(range(n))
+
+
+def test_batch_devices_argument_checks_need_no_gpu():
+    """gral_prog_solve_batch_devices rejects an empty device list and fewer situations than
+    devices before touching a device."""
+    L = lib()
+    dv = (C.c_int32 * 2)(0, 0)
+    p = (abi.GralParams * 1)()
+    s = abi.GralStatic()
+    f = (abi.GralFields * 1)()
+    assert L.gral_prog_solve_batch_devices(0, dv, 1, p, C.byref(s), f, None) == abi.GRAL_EINVAL
+    assert L.gral_prog_solve_batch_devices(2, dv, 1, p, C.byref(s), f, None) == abi.GRAL_EINVAL
+    assert L.gral_prog_solve_batch_devices(1, None, 1, p, C.byref(s), f, None) == abi.GRAL_EINVAL
+
