@@ -198,7 +198,10 @@ template <> struct CompTraits<2> {
 // shared rows per warp: A B C D (then their cotangents), the forward T P Q, the new value above
 // (`up` of the back-substitution), the cotangent of the new value, the coefficients of the two
 // predecessors in D, the cotangent of the own old value, the cotangents of P and Q
-enum : int { R_A, R_B, R_C, R_D, R_T, R_P, R_Q, R_UP, R_L0, R_C1, R_C2, R_LO, R_LP, R_LQ, NROW };
+enum : int { R_A, R_B, R_C, R_D, R_T, R_P, R_Q, R_UP, R_L0, R_C1, R_C2, R_LO, R_LP, R_LQ,
+              // per-level products of the reversed recurrence (zero where the level has no
+              // predecessor in the recurrence): D + C*Q_{k-1}, C*T, T*T*C, -T*T, relax*P, Q_{k-1}*T, P_{k-1}
+              R_E, R_CT, R_TTC, R_NT2, R_RP, R_QPT, R_PP, NROW };
 
 template <int COMP>
 struct MomRev {
@@ -286,6 +289,20 @@ struct MomRev {
             }
         }
         __syncwarp();
+        // the products the reversed recurrence needs, off its critical path
+        for (int k = c.K0 + lane; k <= c.VI; k += 32) {
+            const bool ch = k > c.KK + 1;
+            const float C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
+            const float Qp = ch ? S[R_Q][k - 1] : 0.0f;
+            S[R_E][k] = ch ? D + C * Qp : D;
+            S[R_CT][k] = ch ? C * T : 0.0f;
+            S[R_TTC][k] = ch ? T * T * C : 0.0f;
+            S[R_NT2][k] = -(T * T);
+            S[R_RP][k] = a.relax * S[R_P][k];
+            S[R_QPT][k] = Qp * T;
+            S[R_PP][k] = ch ? S[R_P][k - 1] : 0.0f;
+        }
+        __syncwarp();
     }
 
     // after the wait: the cotangents of the column's new values are complete (later phases and
@@ -304,41 +321,36 @@ struct MomRev {
         }
         __syncwarp();
         if (lane == 0) {
-            const int K0 = c.K0, KK = c.KK, VI = c.VI;
-            const float relax = a.relax;
+            const int K0 = c.K0, VI = c.VI;
+            const float relax = a.relax, r1 = 1.0f - relax;
             // relaxed back-substitution (:513-524) reversed, bottom up: phi'_k = phi_k +
-            // relax*(P_k*up + Q_k - phi_k) with up = phi'_{k+1}
+            // relax*(P_k*up + Q_k - phi_k) with up = phi'_{k+1}; the levels up to kkm are not
+            // updated and carry nothing, the chain per level is one add and one multiply
+            const int kb = max(K0, kkm + 1);
+            for (int k = K0; k < kb && k <= VI; ++k) { S[R_LO][k] = 0.0f; S[R_LP][k] = 0.0f; S[R_LQ][k] = 0.0f; }
             float carry = 0.0f;
-            for (int k = K0; k <= VI; ++k) {
-                if (kkm < k) {
-                    const float mu = S[R_L0][k] + carry;
-                    S[R_LO][k] = (1.0f - relax) * mu;
-                    S[R_LP][k] = relax * S[R_UP][k] * mu;
-                    S[R_LQ][k] = relax * mu;
-                    carry = relax * S[R_P][k] * mu;
-                } else {
-                    S[R_LO][k] = carry;
-                    S[R_LP][k] = 0.0f;
-                    S[R_LQ][k] = 0.0f;
-                    carry = 0.0f;
-                }
+            for (int k = kb; k <= VI; ++k) {
+                const float mu = S[R_L0][k] + carry;
+                S[R_LO][k] = r1 * mu;
+                S[R_LP][k] = relax * S[R_UP][k] * mu;
+                S[R_LQ][k] = relax * mu;
+                carry = S[R_RP][k] * mu;
             }
             top_carry = carry;
-            // Thomas recurrence reversed, top down
+            // Thomas recurrence reversed, top down, on the products made before the wait (zero
+            // at the levels without predecessor, which ends the carried cotangents there)
             float lPn = 0.0f, lQn = 0.0f;
             for (int k = VI; k >= K0; --k) {
-                const float B = S[R_B][k], C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
-                const bool ch = k > KK + 1;
                 const float lP = S[R_LP][k] + lPn, lQ = S[R_LQ][k] + lQn;
-                const float Pp = ch ? S[R_P][k - 1] : 0.0f, Qp = ch ? S[R_Q][k - 1] : 0.0f;
-                const float lT = lQ * (ch ? (D + C * Qp) : D) + lP * B;
-                const float lden = -lT * T * T;
+                const float lT = fmaf(lP, S[R_B][k], lQ * S[R_E][k]);
+                const float lden = lT * S[R_NT2][k];
+                const float T = S[R_T][k];
+                lQn = lQ * S[R_CT][k];
+                lPn = lT * S[R_TTC][k];
                 S[R_A][k] = lden;
                 S[R_B][k] = lP * T;
-                S[R_C][k] = ch ? (lQ * Qp * T - lden * Pp) : 0.0f;
+                S[R_C][k] = lQ * S[R_QPT][k] - lden * S[R_PP][k];
                 S[R_D][k] = lQ * T;
-                lQn = ch ? lQ * C * T : 0.0f;
-                lPn = ch ? -lden * C : 0.0f;
             }
         }
         __syncwarp();
