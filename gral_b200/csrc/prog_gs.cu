@@ -664,9 +664,9 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_mom1s(KArgs a, SweepGeom g) {
 // Split at the wait.  Before it: the divergence terms and the downward Thomas elimination, which
 // starts from the carry's P at VerticalIndex+1: zero when no earlier column of the row writes that
 // level (a host-built table names the last writer), else read after waiting for that writer --
-// an ancestor of this column in the wavefront, usually finished long before.  After the wait: the
-// swept neighbours' DPM, Q (started from the carry's Q, which the predecessor may have written),
-// the back-substitution, the residual and the stores.
+// an ancestor of this column in the wavefront, usually finished long before; the carry's Q at that
+// level comes from the same writer and is read there too.  After the wait: the swept neighbours'
+// DPM, Q from that start, the back-substitution, the residual and the stores.
 struct PressJob {
     const KArgs &a;
     float (*S)[KMAX_LEVELS];
@@ -681,6 +681,7 @@ struct PressJob {
     unsigned run_max;   // residual key maximum of this warp's tasks of situation run_s so far
     int run_s;
     float own[2];       // strip schedule: the column's DPM at levels lane, lane+32 (final after post)
+    float q0;           // lane 0: the row carry's Q at VerticalIndex+1
     static constexpr bool kAllFlags = true;    // the row carry's readers wait on its writer's flag
 
     // The residual maximum is only read after the phase (k_bookkeeping), so each warp keeps a
@@ -740,10 +741,16 @@ struct PressJob {
         if (lane == 0) {
             const short2 w = a.rcw[c.col];
             const int wi = (IS == 1) ? w.x : w.y;
+            // the carry's P and Q at VerticalIndex+1 are final once their writer, the last column
+            // before this one in its row that writes that level, has finished (zero without one)
             float P0 = 0.0f;
+            q0 = 0.0f;
             if (wi >= 0) {
                 const int *fl = a.flags + (size_t)s * a.ncols;
-                if (wait_stamp(fl + wi * a.nj2 + j, stamp, a.err, a.wait_limit_ns)) P0 = __ldcg(rc + c.VI + 1);
+                if (wait_stamp(fl + wi * a.nj2 + j, stamp, a.err, a.wait_limit_ns)) {
+                    P0 = __ldcg(rc + c.VI + 1);
+                    q0 = __ldcg(rc + a.ks + c.VI + 1);
+                }
             }
             forward(P0);
         }
@@ -769,7 +776,7 @@ struct PressJob {
         const int lane = threadIdx.x & 31;
         const int ks = a.ks;
         float Q = 0.0f;
-        if (lane == 0) Q = __ldcg(rc + ks + c.VI + 1);
+        if (lane == 0) Q = q0;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int k = lane + 32 * r;
