@@ -30,7 +30,7 @@ namespace gral {
 namespace {
 
 constexpr int GS_WARPS = 4;      // warps per block, plain family
-constexpr int SM_ROWS = 5;       // shared rows per warp of the plain family: A, B, C, D, phi
+constexpr int SM_ROWS = 5;       // shared rows per warp of the plain family: A, B, C, D, phi (model 1: rows 0-3 hold 16-byte level records)
 
 __device__ __forceinline__ void sweep_dir(int it, int &IS, int &JS) {
     // PrognosticFlowfield.cs:770-802
@@ -391,7 +391,7 @@ __device__ void plain_tke_column(const KArgs &a, int s, int i, int j, float (*S)
 
 template <int MODEL, int COMP>
 __global__ void __launch_bounds__(GS_WARPS * 32) k_mom(KArgs a, SweepGeom g) {
-    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
     __shared__ double smd[(MODEL == 0 && COMP == COMP_W) ? GS_WARPS : 1][2][KMAX_LEVELS];
     const int w = threadIdx.x >> 5;
     float (*S)[KMAX_LEVELS] = sm[w];
@@ -470,61 +470,64 @@ __device__ __forceinline__ void gs_tasks_split(const KArgs &a, const SweepGeom &
     job.finish();
 }
 
-// Model-1 Thomas recurrence split at the wait (U-prognostic-microscale_1.cs:485-524): before it,
-// rows A, B become T = 1/(A - C*P) and P; after it, D becomes Q and the relaxed back-substitution
-// updates phi.  Lane 0 runs the recurrences eight levels at a time: the eight levels' operands are
-// loaded from shared memory together, so only the arithmetic chain is serial.
+// Model-1 Thomas recurrence split at the wait (U-prognostic-microscale_1.cs:485-524).  Each level's
+// operands are one 16-byte record L[k] = {A -> T, C, D -> Q, B -> P} in shared memory (the level's
+// old value phi in a row of its own), so lane 0 reads a level with one load.  Before the wait, A, B
+// become T = 1/(A - C*P) and P; after it, D becomes Q and the relaxed back-substitution updates
+// phi.  Lane 0 runs the recurrences eight levels at a time: the eight levels' records are loaded
+// together, so only the arithmetic chain is serial.
 constexpr int TCH = 8;
 
-__device__ __forceinline__ void ml_forward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI) {
+__device__ __forceinline__ void ml_forward(float4 *L, int K0, int KK, int VI) {
     float P = 0.0f;
     int k = K0;
     for (; k + TCH - 1 <= VI; k += TCH) {
-        float A[TCH], B[TCH], C[TCH];
+        float4 r[TCH];
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) { A[q] = S[0][k + q]; B[q] = S[1][k + q]; C[q] = S[2][k + q]; }
+        for (int q = 0; q < TCH; ++q) r[q] = L[k + q];
 #pragma unroll
         for (int q = 0; q < TCH; ++q) {
-            const float T = (k + q > KK + 1) ? 1.0f / (A[q] - C[q] * P) : 1.0f / A[q];
-            P = B[q] * T;
-            A[q] = T;
-            B[q] = P;
+            const float T = (k + q > KK + 1) ? 1.0f / (r[q].x - r[q].y * P) : 1.0f / r[q].x;
+            P = r[q].w * T;
+            r[q].x = T;
+            r[q].w = P;
         }
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) { S[0][k + q] = A[q]; S[1][k + q] = B[q]; }
+        for (int q = 0; q < TCH; ++q) L[k + q] = r[q];
     }
     for (; k <= VI; ++k) {
-        const float A = S[0][k], B = S[1][k], C = S[2][k];
-        const float T = (k > KK + 1) ? 1.0f / (A - C * P) : 1.0f / A;
-        P = B * T;
-        S[0][k] = T;
-        S[1][k] = P;
+        float4 r = L[k];
+        const float T = (k > KK + 1) ? 1.0f / (r.x - r.y * P) : 1.0f / r.x;
+        P = r.w * T;
+        r.x = T;
+        r.w = P;
+        L[k] = r;
     }
 }
 
-__device__ __forceinline__ void ml_backward(float (*S)[KMAX_LEVELS], int K0, int KK, int VI, int kkm, float relax,
+__device__ __forceinline__ void ml_backward(float4 *L, float *U0, int K0, int KK, int VI, int kkm, float relax,
                                             float top) {
     // Q_k = D_k*T_k up to KKART+1 (K0 <= KKART+1 always), then Q_k = (D_k + C_k*Q_{k-1})*T_k;
     // the level ranges are split instead of selecting per level, which keeps the chain short
     const int kq = min(KK + 1, VI);
-    for (int k = K0; k <= kq; ++k) S[3][k] = S[3][k] * S[0][k];
-    float Q = S[3][kq];
+    for (int k = K0; k <= kq; ++k) L[k].z = L[k].z * L[k].x;
+    float Q = L[kq].z;
     int k = kq + 1;
     for (; k + TCH - 1 <= VI; k += TCH) {
-        float T[TCH], D[TCH], C[TCH];
+        float4 r[TCH];
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) { T[q] = S[0][k + q]; D[q] = S[3][k + q]; C[q] = S[2][k + q]; }
+        for (int q = 0; q < TCH; ++q) r[q] = L[k + q];
 #pragma unroll
         for (int q = 0; q < TCH; ++q) {
-            Q = (D[q] + C[q] * Q) * T[q];
-            D[q] = Q;
+            Q = (r[q].z + r[q].y * Q) * r[q].x;
+            r[q].z = Q;
         }
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) S[3][k + q] = D[q];
+        for (int q = 0; q < TCH; ++q) L[k + q].z = r[q].z;
     }
     for (; k <= VI; ++k) {
-        Q = (S[3][k] + S[2][k] * Q) * S[0][k];
-        S[3][k] = Q;
+        Q = (L[k].z + L[k].y * Q) * L[k].x;
+        L[k].z = Q;
     }
     // relaxed back-substitution downwards over the levels above kkm (the others keep their value
     // and lie below every updated level)
@@ -532,21 +535,22 @@ __device__ __forceinline__ void ml_backward(float (*S)[KMAX_LEVELS], int K0, int
     float up = top;
     k = VI;
     for (; k - (TCH - 1) >= kb; k -= TCH) {
-        float P[TCH], Qv[TCH], U[TCH];
+        float4 r[TCH];
+        float U[TCH];
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) { P[q] = S[1][k - q]; Qv[q] = S[3][k - q]; U[q] = S[4][k - q]; }
+        for (int q = 0; q < TCH; ++q) { r[q] = L[k - q]; U[q] = U0[k - q]; }
 #pragma unroll
         for (int q = 0; q < TCH; ++q) {
-            const float u = U[q] + relax * (P[q] * up + Qv[q] - U[q]);
+            const float u = U[q] + relax * (r[q].w * up + r[q].z - U[q]);
             U[q] = u;
             up = u;
         }
 #pragma unroll
-        for (int q = 0; q < TCH; ++q) S[4][k - q] = U[q];
+        for (int q = 0; q < TCH; ++q) U0[k - q] = U[q];
     }
     for (; k >= kb; --k) {
-        const float u = S[4][k] + relax * (S[1][k] * up + S[3][k] - S[4][k]);
-        S[4][k] = u;
+        const float u = U0[k] + relax * (L[k].w * up + L[k].z - U0[k]);
+        U0[k] = u;
         up = u;
     }
 }
@@ -565,6 +569,9 @@ struct Mom1Job {
     float suc[2][2];    // strip schedule: the sweep successors (i+IS, j), (i, j+JS) at the task's levels
     static constexpr bool kAllFlags = false;   // no task of another column waits on this phase's flags
 
+    // the level records of the recurrences: rows 0-3 of the warp's shared memory, 16-byte aligned
+    __device__ __forceinline__ float4 *lev() const { return reinterpret_cast<float4 *>(S[0]); }
+
     __device__ void pre(int s, int i, int j, int, int, bool) {
         const int lane = threadIdx.x & 31;
         c = make_col(a, i, j);
@@ -579,12 +586,13 @@ struct Mom1Job {
             if (COMP == COMP_U) p[r] = u1_pre<false>(a, x, c, sc, k);
             else if (COMP == COMP_V) p[r] = v1_pre<false>(a, x, c, sc, k);
             else p[r] = w1_pre<false>(a, x, c, sc, k);
-            S[0][k] = p[r].A; S[1][k] = p[r].B; S[2][k] = p[r].C; S[4][k] = p[r].phi;
+            lev()[k] = make_float4(p[r].A, p[r].C, 0.0f, p[r].B);
+            S[4][k] = p[r].phi;
         }
         __syncwarp();
         if (lane == 0) {
             top = __ldcg(comp_field<COMP>(a) + x.at(0, c.VI + 1));
-            ml_forward(S, c.K0, c.KK, c.VI);
+            ml_forward(lev(), c.K0, c.KK, c.VI);
         }
     }
 
@@ -628,13 +636,13 @@ struct Mom1Job {
             } else {
                 nbr4(F, x, c, k, nW, nS, nE, nN);
             }
-            if (COMP == COMP_U) S[3][k] = u1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
-            else if (COMP == COMP_V) S[3][k] = v1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
-            else S[3][k] = w1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
+            if (COMP == COMP_U) lev()[k].z = u1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
+            else if (COMP == COMP_V) lev()[k].z = v1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
+            else lev()[k].z = w1_post(p[r], c, k, nW, nS, nE, nN, a.simd == 16);
         }
         __syncwarp();
         const int kkm = back_limit<COMP>(c);
-        if (lane == 0) ml_backward(S, c.K0, c.KK, c.VI, kkm, a.relax, top);
+        if (lane == 0) ml_backward(lev(), S[4], c.K0, c.KK, c.VI, kkm, a.relax, top);
         __syncwarp();
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -651,7 +659,7 @@ struct Mom1Job {
 
 template <int COMP>
 __global__ void __launch_bounds__(GS_WARPS * 32) k_mom1s(KArgs a, SweepGeom g) {
-    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
     Mom1Job<COMP> job{a, sm[threadIdx.x >> 5], 0};
     constexpr int PH = COMP == COMP_U ? PH_U : (COMP == COMP_V ? PH_V : PH_W);
     gs_tasks_split<PH, COMP == COMP_V>(a, g, job);     // model-1 V sweeps with (-IS,-JS)
@@ -850,7 +858,7 @@ struct PressJob {
 };
 
 __global__ void __launch_bounds__(GS_WARPS * 32) k_pressure_s(KArgs a, SweepGeom g) {
-    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
     PressJob job{a, sm[threadIdx.x >> 5], 0};
     job.run_max = 0;
     job.run_s = -1;
@@ -1010,7 +1018,7 @@ __device__ __forceinline__ void gs_tasks_strip(const KArgs &a, const SweepGeom &
 constexpr int FSR = 4;     // rows per strip
 
 __global__ void __launch_bounds__(16 * 32, 1) k_fused_strip(KArgs a, FusedGeom fg) {
-    __shared__ float sm[16][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[16][SM_ROWS][KMAX_LEVELS];
     __shared__ float s_col[FSR * SDEPTH][KMAX_LEVELS];
     __shared__ int s_done[FSR];
     __shared__ unsigned s_claim;
@@ -1111,7 +1119,7 @@ __global__ void __launch_bounds__(16 * 32, 1) k_fused_strip(KArgs a, FusedGeom f
 
 template <int SR, int SMW>
 __global__ void __launch_bounds__(SR * SMW * 32, 1) k_pressure_strip(KArgs a, SweepGeom g) {
-    __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
     __shared__ float s_col[SR * SDEPTH][KMAX_LEVELS];
     __shared__ int s_done[SR];
     __shared__ unsigned s_claim;
@@ -1123,7 +1131,7 @@ __global__ void __launch_bounds__(SR * SMW * 32, 1) k_pressure_strip(KArgs a, Sw
 
 template <int COMP, int SR, int SMW>
 __global__ void __launch_bounds__(SR * SMW * 32, 1) k_mom1_strip(KArgs a, SweepGeom g) {
-    __shared__ float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[SR * SMW][SM_ROWS][KMAX_LEVELS];
     __shared__ float s_col[SR * SDEPTH][KMAX_LEVELS];
     __shared__ int s_done[SR];
     __shared__ unsigned s_claim;
@@ -1147,7 +1155,7 @@ __global__ void __launch_bounds__(SR * SMW * 32, 1) k_mom1_strip(KArgs a, SweepG
 //   final DPMNEW it reads) and its two U sweep predecessors.
 
 __global__ void __launch_bounds__(GS_WARPS * 32) k_fused_pvau(KArgs a, FusedGeom fg) {
-    __shared__ float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
+    __shared__ __align__(16) float sm[GS_WARPS][SM_ROWS][KMAX_LEVELS];
     float (*S)[KMAX_LEVELS] = sm[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int it = *a.it_global;
