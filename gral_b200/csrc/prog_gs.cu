@@ -700,8 +700,13 @@ struct PressJob {
     }
     __device__ void finish() { flush(); }
 
+    // the level records of the recurrences, 16 bytes each in rows 0-3 of the warp's shared memory:
+    // {T, P, DIM -> Q, ATP}; row 4 holds the new DPM
+    __device__ __forceinline__ float4 *lev() const { return reinterpret_cast<float4 *>(S[0]); }
+
     // T = 1/(APP - ATP*P), P = ABP*T from level VI down to KKART+1, eight levels per step.
     __device__ void forward(float P) {
+        float4 *L = lev();
         int k = c.VI;
         for (; k - (TCH - 1) > c.KK; k -= TCH) {
             float ap[TCH], at[TCH], ab[TCH];
@@ -715,13 +720,12 @@ struct PressJob {
                 ab[q] = P;
             }
 #pragma unroll
-            for (int q = 0; q < TCH; ++q) { S[0][k - q] = ap[q]; S[1][k - q] = ab[q]; }
+            for (int q = 0; q < TCH; ++q) L[k - q] = make_float4(ap[q], ab[q], 0.0f, at[q]);
         }
         for (; k > c.KK; --k) {
             const float T = 1.0f / (a.app[k] - a.atp[k] * P);
             P = a.abp[k] * T;
-            S[0][k] = T;
-            S[1][k] = P;
+            L[k] = make_float4(T, P, 0.0f, a.atp[k]);
         }
     }
 
@@ -791,43 +795,45 @@ struct PressJob {
             if (k <= c.KK || k > c.VI) continue;
             const float vI = (strip && pI) ? pI[k] : __ldcg(a.dpm + x.at(-(long long)IS * c.nj2, k));
             const float vJ = (strip && pJ) ? pJ[k] : __ldcg(a.dpm + x.at(-(long long)JS, k));
-            S[3][k] = pressure_post_v(a, t0[r], k, IS, JS, vI, vJ);
+            lev()[k].z = pressure_post_v(a, t0[r], k, IS, JS, vI, vJ);
         }
         __syncwarp();
         if (lane == 0) {
+            float4 *L = lev();
             int k = c.VI;
             for (; k - (TCH - 1) > c.KK; k -= TCH) {
-                float at[TCH], d[TCH], t[TCH];
+                float4 r[TCH];
 #pragma unroll
-                for (int q = 0; q < TCH; ++q) { at[q] = a.atp[k - q]; d[q] = S[3][k - q]; t[q] = S[0][k - q]; }
+                for (int q = 0; q < TCH; ++q) r[q] = L[k - q];
 #pragma unroll
                 for (int q = 0; q < TCH; ++q) {
-                    Q = (at[q] * Q + d[q]) * t[q];
-                    d[q] = Q;
+                    Q = (r[q].w * Q + r[q].z) * r[q].x;
+                    r[q].z = Q;
                 }
 #pragma unroll
-                for (int q = 0; q < TCH; ++q) S[2][k - q] = d[q];
+                for (int q = 0; q < TCH; ++q) L[k - q].z = r[q].z;
             }
             for (; k > c.KK; --k) {
-                Q = (a.atp[k] * Q + S[3][k]) * S[0][k];
-                S[2][k] = Q;
+                Q = (L[k].w * Q + L[k].z) * L[k].x;
+                L[k].z = Q;
             }
             float prev = 0.0f;                                     // DPM[KKART] is always 0
             k = c.KK + 1;
             for (; k + TCH - 1 <= c.VI; k += TCH) {
-                float pp[TCH], qq[TCH];
+                float4 r[TCH];
+                float qq[TCH];
 #pragma unroll
-                for (int q = 0; q < TCH; ++q) { pp[q] = S[1][k + q]; qq[q] = S[2][k + q]; }
+                for (int q = 0; q < TCH; ++q) r[q] = L[k + q];
 #pragma unroll
                 for (int q = 0; q < TCH; ++q) {
-                    prev = pp[q] * prev + qq[q];
+                    prev = r[q].y * prev + r[q].z;
                     qq[q] = prev;
                 }
 #pragma unroll
                 for (int q = 0; q < TCH; ++q) S[4][k + q] = qq[q];
             }
             for (; k <= c.VI; ++k) {
-                prev = S[1][k] * prev + S[2][k];
+                prev = L[k].y * prev + L[k].z;
                 S[4][k] = prev;
             }
         }
@@ -844,8 +850,9 @@ struct PressJob {
             __stcg(a.dpm + x.at(0, k), temp);
             a.dpmnew[x.at(0, k)] = dn[r] + a.relaxp * temp;
             if (k > klo) {
-                __stcg(rc + k, S[1][k]);
-                __stcg(rc + ks + k, S[2][k]);
+                const float4 r = lev()[k];
+                __stcg(rc + k, r.y);
+                __stcg(rc + ks + k, r.z);
             }
         }
         for (int d = 16; d > 0; d >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, d));
