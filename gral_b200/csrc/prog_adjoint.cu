@@ -38,6 +38,8 @@
 #include <string>
 #include <vector>
 
+#include <cstdlib>
+
 #include "adj_level.cuh"
 #include "prog_ctx.cuh"
 #include "prog_level.cuh"
@@ -1063,7 +1065,9 @@ int pressure_tables(gral_ctx *ctx) {
 
 int rev_grid(gral_ctx *ctx, const SweepGeom &g) {
     const double width = (double)g.ni * g.nj / std::max(1, g.ni + g.nj - 1);
-    const long long want = (long long)std::ceil(6.0 * width / AW);
+    double la = 12.0;   // diagonals of wavefront width the reverse sweeps keep warps for (6: 12 % slower)
+    if (const char *v = std::getenv("GRAL_PROG_ADJ_LOOKAHEAD")) la = std::max(1.0, std::atof(v));
+    const long long want = (long long)std::ceil(la * width / AW);
     return (int)std::max<long long>(ctx->num_sms, std::min<long long>(4LL * ctx->num_sms, want));
 }
 
