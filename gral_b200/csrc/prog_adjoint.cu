@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cstdlib>
@@ -62,37 +63,68 @@ struct InDesc {
     int8_t f, di, dj, dk;
 };
 
-// input tables of the level functions of adj_level.cuh: field, column offset (i, j), level offset
-__constant__ InDesc c_uin[U_COUNT] = {
-    {FU, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
-    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
-    {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FVS, -1, -1, 0}, {FVS, 0, -1, 0}, {FVS, -1, 1, 0}, {FVS, 0, 1, 0},
-    {FWS, -1, 0, 0}, {FWS, -1, 0, 1}, {FWS, 0, 0, 1}, {FWS, 0, 0, -1}, {FWS, -1, 0, -1},
-    {FDP, -1, 0, 0}, {FDP, 0, 0, 0},
-    {FVS, 1, 1, 0}, {FVS, 1, -1, 0}, {FW, 1, 0, 0}, {FW, 1, 0, -1},
-    {FVEG, 0, 0, -1},
-    {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
-    {FU, -1, 0, 0}, {FU, 0, -1, 0}, {FU, 1, 0, 0}, {FU, 0, 1, 0}};
-__constant__ InDesc c_vin[V_COUNT] = {
-    {FV, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
-    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
-    {FUS, 1, 0, 0}, {FUS, 0, -1, 0}, {FUS, 1, -1, 0}, {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FUS, -1, -1, 0},
-    {FVS, 0, -1, 0}, {FWS, 0, -1, 0}, {FWS, 0, 0, -1}, {FWS, 0, -1, 1}, {FWS, 0, 0, 1}, {FWS, 0, -1, -1},
-    {FDP, 0, -1, 0}, {FDP, 0, 0, 0},
-    {FUS, 1, 1, 0}, {FUS, -1, 1, 0}, {FW, 0, 1, 0}, {FW, 0, 1, -1},
-    {FVEG, 0, 0, -1},
-    {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
-    {FV, -1, 0, 0}, {FV, 0, -1, 0}, {FV, 1, 0, 0}, {FV, 0, 1, 0}};
-__constant__ InDesc c_win[W_COUNT] = {
-    {FW, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
-    {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0}, {FUS, 0, 0, -1}, {FVS, 0, 0, -1},
-    {FUS, -1, 0, 0}, {FUS, -1, 0, -1}, {FVS, 0, -1, 0}, {FVS, 0, -1, -1}, {FUS, 1, 0, 0}, {FUS, 1, 0, -1},
-    {FVS, 0, 1, 0}, {FVS, 0, 1, -1},
-    {FWS, 0, 0, -1}, {FDP, 0, 0, -1}, {FDP, 0, 0, 0},
-    {FUS, 0, 0, 1}, {FUS, -1, 0, 1}, {FVS, 0, 0, 1}, {FVS, 0, -1, 1},
-    {FW, 0, 0, 1}, {FW, 0, 0, -1},
-    {FVEG, 0, 0, -1},
-    {FW, -1, 0, 0}, {FW, 0, -1, 0}, {FW, 1, 0, 0}, {FW, 0, 1, 0}};
+// Input tables of the level functions of adj_level.cuh: field, column offset (i, j), level offset.
+// They are constexpr and read with compile-time indices (InTab<COMP>::at inside for_inputs), so the
+// choice of field, the cell offset and the wall-law level of every input fold into the code.
+template <int COMP> struct InTab;
+template <> struct InTab<0> {
+    static constexpr int N = U_COUNT;
+    static constexpr __host__ __device__ InDesc at(int q) {
+        constexpr InDesc t[U_COUNT] = {
+            {FU, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+            {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
+            {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FVS, -1, -1, 0}, {FVS, 0, -1, 0}, {FVS, -1, 1, 0}, {FVS, 0, 1, 0},
+            {FWS, -1, 0, 0}, {FWS, -1, 0, 1}, {FWS, 0, 0, 1}, {FWS, 0, 0, -1}, {FWS, -1, 0, -1},
+            {FDP, -1, 0, 0}, {FDP, 0, 0, 0},
+            {FVS, 1, 1, 0}, {FVS, 1, -1, 0}, {FW, 1, 0, 0}, {FW, 1, 0, -1},
+            {FVEG, 0, 0, -1},
+            {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
+            {FU, -1, 0, 0}, {FU, 0, -1, 0}, {FU, 1, 0, 0}, {FU, 0, 1, 0}};
+        return t[q];
+    }
+};
+template <> struct InTab<1> {
+    static constexpr int N = V_COUNT;
+    static constexpr __host__ __device__ InDesc at(int q) {
+        constexpr InDesc t[V_COUNT] = {
+            {FV, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+            {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0},
+            {FUS, 1, 0, 0}, {FUS, 0, -1, 0}, {FUS, 1, -1, 0}, {FUS, -1, 0, 0}, {FVS, -1, 0, 0}, {FUS, -1, -1, 0},
+            {FVS, 0, -1, 0}, {FWS, 0, -1, 0}, {FWS, 0, 0, -1}, {FWS, 0, -1, 1}, {FWS, 0, 0, 1}, {FWS, 0, -1, -1},
+            {FDP, 0, -1, 0}, {FDP, 0, 0, 0},
+            {FUS, 1, 1, 0}, {FUS, -1, 1, 0}, {FW, 0, 1, 0}, {FW, 0, 1, -1},
+            {FVEG, 0, 0, -1},
+            {FUS, -1, 0, WL}, {FUS, 0, 0, WL}, {FVS, -1, 0, WL}, {FVS, 0, 0, WL},
+            {FV, -1, 0, 0}, {FV, 0, -1, 0}, {FV, 1, 0, 0}, {FV, 0, 1, 0}};
+        return t[q];
+    }
+};
+template <> struct InTab<2> {
+    static constexpr int N = W_COUNT;
+    static constexpr __host__ __device__ InDesc at(int q) {
+        constexpr InDesc t[W_COUNT] = {
+            {FW, 0, 0, 0}, {FU, 0, 0, 1}, {FU, 0, 0, -1}, {FV, 0, 0, 1}, {FV, 0, 0, -1},
+            {FUS, 0, 0, 0}, {FVS, 0, 0, 0}, {FWS, 0, 0, 0}, {FUS, 0, 0, -1}, {FVS, 0, 0, -1},
+            {FUS, -1, 0, 0}, {FUS, -1, 0, -1}, {FVS, 0, -1, 0}, {FVS, 0, -1, -1}, {FUS, 1, 0, 0}, {FUS, 1, 0, -1},
+            {FVS, 0, 1, 0}, {FVS, 0, 1, -1},
+            {FWS, 0, 0, -1}, {FDP, 0, 0, -1}, {FDP, 0, 0, 0},
+            {FUS, 0, 0, 1}, {FUS, -1, 0, 1}, {FVS, 0, 0, 1}, {FVS, 0, -1, 1},
+            {FW, 0, 0, 1}, {FW, 0, 0, -1},
+            {FVEG, 0, 0, -1},
+            {FW, -1, 0, 0}, {FW, 0, -1, 0}, {FW, 1, 0, 0}, {FW, 0, 1, 0}};
+        return t[q];
+    }
+};
+
+// f(std::integral_constant<int, q>) for q = 0 .. N-1, unrolled at compile time
+template <class F, int... Q>
+__device__ __forceinline__ void for_inputs_(F &&f, std::integer_sequence<int, Q...>) {
+    (f(std::integral_constant<int, Q>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void for_inputs(F &&f) {
+    for_inputs_(f, std::make_integer_sequence<int, N>{});
+}
 
 // Everything the adjoint kernels read besides the solver's KArgs (all device pointers, slab
 // layout [ncols][KS] of the one situation).
@@ -174,7 +206,6 @@ __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, cons
 template <int COMP> struct CompTraits;
 template <> struct CompTraits<0> {
     static constexpr int N = U_COUNT;
-    static __device__ const InDesc *tab() { return c_uin; }
     template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { u_row(c, x, o); }
     template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
         u_row_vjp(c, x, l, g);
@@ -182,7 +213,6 @@ template <> struct CompTraits<0> {
 };
 template <> struct CompTraits<1> {
     static constexpr int N = V_COUNT;
-    static __device__ const InDesc *tab() { return c_vin; }
     template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { v_row(c, x, o); }
     template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
         v_row_vjp(c, x, l, g);
@@ -190,7 +220,6 @@ template <> struct CompTraits<1> {
 };
 template <> struct CompTraits<2> {
     static constexpr int N = W_COUNT;
-    static __device__ const InDesc *tab() { return c_win; }
     template <class T> static __device__ void row(const LevelConst &c, const T *x, T *o) { w_row(c, x, o); }
     template <class T> static __device__ void vjp(const LevelConst &c, const T *x, const T *l, T *g) {
         w_row_vjp(c, x, l, g);
@@ -229,28 +258,26 @@ struct MomRev {
         return L;
     }
 
-    // the state a level input is read from: the swept field's predecessors hold their new values
-    __device__ const float *src(int f, int di, int dj, int IS, int JS) const {
-        if (f == FVEG) return a.veg;
-        if (f >= FUS) return d.mid[f];
-        if (f == COMP) {
-            const bool pred = (di == -IS && dj == 0) || (di == 0 && dj == -JS);
-            return pred ? d.end[f] : d.mid[f];
+    // input q of the level at k: the swept field's predecessors hold their new values, U is final
+    // in the V and W sweeps and V in the W sweep; every other input is the state after the averages
+    template <int Q> __device__ __forceinline__ float input(int k, int IS, int JS) const {
+        constexpr InDesc e = InTab<COMP>::at(Q);
+        const int kk = (e.dk == WL) ? kwl : k + e.dk;
+        const size_t at = (size_t)(c.col + e.di * a.nj2 + e.dj) * a.ks + kk;
+        if constexpr (e.f == FVEG) {
+            return a.veg ? __ldcg(a.veg + at) : 0.0f;
+        } else if constexpr (e.f >= FUS) {
+            return __ldcg(d.mid[e.f] + at);
+        } else if constexpr (e.f == COMP) {
+            const bool pred = (e.di != 0 && e.dj == 0 && e.di == -IS) || (e.di == 0 && e.dj != 0 && e.dj == -JS);
+            return __ldcg((pred ? d.end[e.f] : d.mid[e.f]) + at);
+        } else {
+            return __ldcg((e.f < COMP ? d.end[e.f] : d.mid[e.f]) + at);
         }
-        // other components: U is final in the V and W sweeps, V in the W sweep
-        return (f < COMP) ? d.end[f] : d.mid[f];
     }
 
-    __device__ void load(int k, int IS, int JS, float *x) const {
-        const InDesc *t = CompTraits<COMP>::tab();
-#pragma unroll
-        for (int q = 0; q < CompTraits<COMP>::N; ++q) {
-            const InDesc e = t[q];
-            const int kk = (e.dk == WL) ? kwl : k + e.dk;
-            const float *p = src(e.f, e.di, e.dj, IS, JS);
-            if (!p) { x[q] = 0.0f; continue; }
-            x[q] = __ldcg(p + cell(a, c.col + e.di * a.nj2 + e.dj, kk));
-        }
+    __device__ __forceinline__ void load(int k, int IS, int JS, float *x) const {
+        for_inputs<InTab<COMP>::N>([&](auto q) { x[q.value] = input<q.value>(k, IS, JS); });
     }
 
     // before the wait: the forward rows of the column from the kept states and its Thomas
@@ -373,7 +400,6 @@ struct MomRev {
     __device__ void after(int IS, int JS) {
         if (!act) return;
         const int lane = threadIdx.x & 31;
-        const InDesc *t = CompTraits<COMP>::tab();
         constexpr int N = CompTraits<COMP>::N;
         if (lane == 0 && top_carry != 0.0f) atomicAdd(d.lam[COMP] + cell(a, c.col, c.VI + 1), top_carry);
 #pragma unroll 1
@@ -388,17 +414,20 @@ struct MomRev {
             const LevelConst LC = level_const(k);
             CompTraits<COMP>::vjp(LC, x, l4, g);
             g[0] += S[R_LO][k];
-#pragma unroll
-            for (int q = 0; q < N; ++q) {
-                const InDesc e = t[q];
-                // the predecessors' cotangents were sent before the flag
-                if (e.f == COMP && ((e.di == -IS && e.dj == 0) || (e.di == 0 && e.dj == -JS))) continue;
-                const float v = g[q];
-                if (v == 0.0f) continue;
-                if (e.f == FVEG && !a.veg) continue;
+            for_inputs<N>([&](auto q) {
+                constexpr InDesc e = InTab<COMP>::at(q.value);
+                const float v = g[q.value];
+                if constexpr (e.f == COMP) {
+                    // the predecessors' cotangents were sent before the flag
+                    if ((e.di != 0 && e.dj == 0 && e.di == -IS) || (e.di == 0 && e.dj != 0 && e.dj == -JS)) return;
+                }
+                if constexpr (e.f == FVEG) {
+                    if (!a.veg) return;
+                }
+                if (v == 0.0f) return;
                 const int kk = (e.dk == WL) ? kwl : k + e.dk;
-                atomicAdd(d.lam[e.f] + cell(a, c.col + e.di * a.nj2 + e.dj, kk), v);
-            }
+                atomicAdd(d.lam[e.f] + (size_t)(c.col + e.di * a.nj2 + e.dj) * a.ks + kk, v);
+            });
         }
     }
 };
