@@ -227,17 +227,27 @@ template <> struct CompTraits<2> {
 };
 
 // shared rows per warp: A B C D (then their cotangents), the forward T P Q, the new value above
-// (`up` of the back-substitution), the cotangent of the new value, the coefficients of the two
-// predecessors in D, the cotangent of the own old value, the cotangents of P and Q
-enum : int { R_A, R_B, R_C, R_D, R_T, R_P, R_Q, R_UP, R_L0, R_C1, R_C2, R_LO, R_LP, R_LQ,
-              // per-level products of the reversed recurrence (zero where the level has no
-              // predecessor in the recurrence): D + C*Q_{k-1}, C*T, T*T*C, -T*T, relax*P, Q_{k-1}*T, P_{k-1}
-              R_E, R_CT, R_TTC, R_NT2, R_RP, R_QPT, R_PP, NROW };
+// (`up` of the back-substitution), the coefficients of the two predecessors in D, the cotangent
+// of the new value (then of the old value, LO), and per-level products of the reversed
+// recurrence: -T*T, Q_{k-1}*T, P_{k-1} (zero where the level has no predecessor in the recurrence)
+enum : int { R_A, R_B, R_C, R_D, R_T, R_P, R_Q, R_UP, R_C1, R_C2, R_LO, R_NT2, R_QPT, R_PP, NROW };
+
+// The two reversed recurrences run on lane 0 over level records packed so that one shared-memory
+// load brings a level's coefficients, prefetched four levels ahead; the records are offset by RPAD
+// levels so that the prefetch past either end of the column stays inside the arrays.
+constexpr int RPAD = 8;
+struct __align__(16) MomShared {
+    float4 bect[KMAX_LEVELS + 2 * RPAD];   // B, D + C*Q_{k-1}, C*T, T*T*C (the last two zero without predecessor)
+    float2 lrp[KMAX_LEVELS + 2 * RPAD];    // cotangent L0 of the new value, relax*P
+    float2 lpq[KMAX_LEVELS + 2 * RPAD];    // relax*UP*mu, relax*mu; then the cotangents of P and Q
+    float rows[NROW][KMAX_LEVELS];
+};
 
 template <int COMP>
 struct MomRev {
     const KArgs &a;
     const AdjArgs &d;
+    MomShared &M;
     float (*S)[KMAX_LEVELS];
     ColCtx c;
     bool act;
@@ -321,13 +331,11 @@ struct MomRev {
         // the products the reversed recurrence needs, off its critical path
         for (int k = c.K0 + lane; k <= c.VI; k += 32) {
             const bool ch = k > c.KK + 1;
-            const float C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
+            const float B = S[R_B][k], C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
             const float Qp = ch ? S[R_Q][k - 1] : 0.0f;
-            S[R_E][k] = ch ? D + C * Qp : D;
-            S[R_CT][k] = ch ? C * T : 0.0f;
-            S[R_TTC][k] = ch ? T * T * C : 0.0f;
+            M.bect[RPAD + k] = make_float4(B, ch ? D + C * Qp : D, ch ? C * T : 0.0f, ch ? T * T * C : 0.0f);
+            M.lrp[RPAD + k].y = a.relax * S[R_P][k];
             S[R_NT2][k] = -(T * T);
-            S[R_RP][k] = a.relax * S[R_P][k];
             S[R_QPT][k] = Qp * T;
             S[R_PP][k] = ch ? S[R_P][k - 1] : 0.0f;
         }
@@ -341,55 +349,104 @@ struct MomRev {
         if (!act) return;
         const int lane = threadIdx.x & 31;
         float *L = d.lam[COMP];
+        float2 *lrp = M.lrp + RPAD, *lpq = M.lpq + RPAD;
+        const float4 *bect = M.bect + RPAD;
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
             const int k = lane + 32 * r;
             if (k < c.K0 || k > c.VI) continue;
             // an updated level's cotangent is handed over from its new to its old value
-            S[R_L0][k] = (kkm < k) ? atomicExch(L + cell(a, c.col, k), 0.0f) : 0.0f;
+            lrp[k].x = (kkm < k) ? atomicExch(L + cell(a, c.col, k), 0.0f) : 0.0f;
         }
         __syncwarp();
+        const int K0 = c.K0, VI = c.VI;
+        const float relax = a.relax, r1 = 1.0f - relax;
+        // relaxed back-substitution (:513-524) reversed, bottom up: phi'_k = phi_k +
+        // relax*(P_k*up + Q_k - phi_k) with up = phi'_{k+1}, so the cotangent of the new value at k
+        // is mu_k = L0_k + carry with carry = relax*P_{k-1}*mu_{k-1}; the levels up to kkm are not
+        // updated, have L0 = 0 and carry nothing.  Lane 0 runs only the chain (one add, one multiply
+        // per level) and keeps mu in the LO row.
         if (lane == 0) {
-            const int K0 = c.K0, VI = c.VI;
-            const float relax = a.relax, r1 = 1.0f - relax;
-            // relaxed back-substitution (:513-524) reversed, bottom up: phi'_k = phi_k +
-            // relax*(P_k*up + Q_k - phi_k) with up = phi'_{k+1}; the levels up to kkm are not
-            // updated and carry nothing, the chain per level is one add and one multiply
-            const int kb = max(K0, kkm + 1);
-            for (int k = K0; k < kb && k <= VI; ++k) { S[R_LO][k] = 0.0f; S[R_LP][k] = 0.0f; S[R_LQ][k] = 0.0f; }
-            float carry = 0.0f;
-            for (int k = kb; k <= VI; ++k) {
-                const float mu = S[R_L0][k] + carry;
-                S[R_LO][k] = r1 * mu;
-                S[R_LP][k] = relax * S[R_UP][k] * mu;
-                S[R_LQ][k] = relax * mu;
-                carry = S[R_RP][k] * mu;
+            float carry = 0.0f, topc = 0.0f;
+            float2 x0 = lrp[K0], x1 = lrp[K0 + 1], x2 = lrp[K0 + 2], x3 = lrp[K0 + 3];
+            for (int k = K0; k <= VI; k += 4) {
+                const float2 y0 = lrp[k + 4], y1 = lrp[k + 5], y2 = lrp[k + 6], y3 = lrp[k + 7];
+                float mu = x0.x + carry;
+                carry = x0.y * mu;
+                S[R_LO][k] = mu;
+                if (k == VI) topc = carry;
+                mu = x1.x + carry;
+                carry = x1.y * mu;
+                if (k + 1 <= VI) S[R_LO][k + 1] = mu;
+                if (k + 1 == VI) topc = carry;
+                mu = x2.x + carry;
+                carry = x2.y * mu;
+                if (k + 2 <= VI) S[R_LO][k + 2] = mu;
+                if (k + 2 == VI) topc = carry;
+                mu = x3.x + carry;
+                carry = x3.y * mu;
+                if (k + 3 <= VI) S[R_LO][k + 3] = mu;
+                if (k + 3 == VI) topc = carry;
+                x0 = y0; x1 = y1; x2 = y2; x3 = y3;
             }
-            top_carry = carry;
-            // Thomas recurrence reversed, top down, on the products made before the wait (zero
-            // at the levels without predecessor, which ends the carried cotangents there)
+            top_carry = topc;
+        }
+        __syncwarp();
+        for (int k = K0 + lane; k <= VI; k += 32) {
+            const float mu = S[R_LO][k];
+            S[R_LO][k] = r1 * mu;
+            lpq[k] = make_float2(relax * S[R_UP][k] * mu, relax * mu);
+        }
+        __syncwarp();
+        // Thomas recurrence reversed, top down, on the products made before the wait (zero at
+        // the levels without predecessor, which ends the carried cotangents there):
+        //   lP_k = LP_k + TTC_{k+1}*lT_{k+1},  lQ_k = LQ_k + CT_{k+1}*lQ_{k+1},  lT_k = lP_k*B_k + lQ_k*E_k
+        if (lane == 0) {
             float lPn = 0.0f, lQn = 0.0f;
-            for (int k = VI; k >= K0; --k) {
-                const float lP = S[R_LP][k] + lPn, lQ = S[R_LQ][k] + lQn;
-                const float lT = fmaf(lP, S[R_B][k], lQ * S[R_E][k]);
-                const float lden = lT * S[R_NT2][k];
-                const float T = S[R_T][k];
-                lQn = lQ * S[R_CT][k];
-                lPn = lT * S[R_TTC][k];
-                S[R_A][k] = lden;
-                S[R_B][k] = lP * T;
-                S[R_C][k] = lQ * S[R_QPT][k] - lden * S[R_PP][k];
-                S[R_D][k] = lQ * T;
+            float2 q0 = lpq[VI], q1 = lpq[VI - 1], q2 = lpq[VI - 2], q3 = lpq[VI - 3];
+            float4 e0 = bect[VI], e1 = bect[VI - 1], e2 = bect[VI - 2], e3 = bect[VI - 3];
+            for (int k = VI; k >= K0; k -= 4) {
+                const float2 p0 = lpq[k - 4], p1 = lpq[k - 5], p2 = lpq[k - 6], p3 = lpq[k - 7];
+                const float4 f0 = bect[k - 4], f1 = bect[k - 5], f2 = bect[k - 6], f3 = bect[k - 7];
+                float lP = q0.x + lPn, lQ = q0.y + lQn;
+                float lT = fmaf(lP, e0.x, lQ * e0.y);
+                lQn = lQ * e0.z;
+                lPn = lT * e0.w;
+                lpq[k] = make_float2(lP, lQ);
+                lP = q1.x + lPn; lQ = q1.y + lQn;
+                lT = fmaf(lP, e1.x, lQ * e1.y);
+                lQn = lQ * e1.z;
+                lPn = lT * e1.w;
+                if (k - 1 >= K0) lpq[k - 1] = make_float2(lP, lQ);
+                lP = q2.x + lPn; lQ = q2.y + lQn;
+                lT = fmaf(lP, e2.x, lQ * e2.y);
+                lQn = lQ * e2.z;
+                lPn = lT * e2.w;
+                if (k - 2 >= K0) lpq[k - 2] = make_float2(lP, lQ);
+                lP = q3.x + lPn; lQ = q3.y + lQn;
+                lT = fmaf(lP, e3.x, lQ * e3.y);
+                lQn = lQ * e3.z;
+                lPn = lT * e3.w;
+                if (k - 3 >= K0) lpq[k - 3] = make_float2(lP, lQ);
+                q0 = p0; q1 = p1; q2 = p2; q3 = p3;
+                e0 = f0; e1 = f1; e2 = f2; e3 = f3;
             }
         }
         __syncwarp();
-        // cotangents of the predecessors' new values (they run after this column)
+        // the cotangents of the row (A, B, C, D) on all lanes, and those of the predecessors' new
+        // values (they run after this column)
         const long long dP1 = -(long long)IS * a.nj2, dP2 = -(long long)JS;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int k = lane + 32 * r;
-            if (k < c.K0 || k > c.VI) continue;
-            const float lD = S[R_D][k];
+        for (int k = K0 + lane; k <= VI; k += 32) {
+            const float2 pq = lpq[k];
+            const float4 e = bect[k];
+            const float lP = pq.x, lQ = pq.y, T = S[R_T][k];
+            const float lT = fmaf(lP, e.x, lQ * e.y);
+            const float lden = lT * S[R_NT2][k];
+            const float lD = lQ * T;
+            S[R_A][k] = lden;
+            S[R_B][k] = lP * T;
+            S[R_C][k] = lQ * S[R_QPT][k] - lden * S[R_PP][k];
+            S[R_D][k] = lD;
             if (lD == 0.0f) continue;
             const float g1 = lD * S[R_C1][k], g2 = lD * S[R_C2][k];
             if (g1 != 0.0f) atomicAdd(L + cell(a, (int)(c.col + dP1), k), g1);
@@ -434,8 +491,9 @@ struct MomRev {
 
 template <int COMP>
 __global__ void __launch_bounds__(AW * 32) k_adj_mom(KArgs a, AdjArgs d, SweepGeom g) {
-    __shared__ float sm[AW][NROW][KMAX_LEVELS];
-    MomRev<COMP> job{a, d, sm[threadIdx.x >> 5]};
+    __shared__ MomShared sm[AW];
+    MomShared &M = sm[threadIdx.x >> 5];
+    MomRev<COMP> job{a, d, M, M.rows};
     int IS, JS;
     sweep_dir_of(d.it, IS, JS);
     if (COMP == 1) { IS = -IS; JS = -JS; }   // model-1 V sweeps with (-IS, -JS)
@@ -450,14 +508,22 @@ __global__ void __launch_bounds__(AW * 32) k_adj_mom(KArgs a, AdjArgs d, SweepGe
 // not yet swept hold 0 (DPM is zeroed before the sweep), so only the two predecessors carry
 // cotangents; P and TERMP do not depend on the state.
 // ------------------------------------------------------------------------------------------------
+struct __align__(16) PresShared {
+    float4 rec[KMAX_LEVELS + 2 * RPAD];   // cotangent of Q (mu), carry cotangent, ATP*TERMP, TERMP
+    float2 sp[KMAX_LEVELS + 2 * RPAD];    // cotangent of DPM (relaxp * that of DPMNEW before the wait), P
+    float ldim[KMAX_LEVELS];              // cotangent of DIM
+};
+
 struct PresRev {
     const KArgs &a;
     const AdjArgs &d;
-    float (*S)[KMAX_LEVELS];     // rows: 0 cotangent of DPM (mu), 1 cotangent of DIM, 2 P, 3 TERMP
+    PresShared &M;
     ColCtx c;
     bool act;
     int dirx;                    // 0: IS = +1, 1: IS = -1
 
+    // before the wait: the state-independent level records, and the cotangent of DPMNEW, which no
+    // column of this sweep changes
     __device__ void pre(int i, int j, int IS, int) {
         const int lane = threadIdx.x & 31;
         c = make_col(a, i, j);
@@ -466,9 +532,12 @@ struct PresRev {
         if (!act) return;
         const size_t fsz = (size_t)a.ncols * a.ks;
         const float *P = d.ptab + (size_t)(2 * dirx) * fsz, *TM = d.ptab + (size_t)(2 * dirx + 1) * fsz;
+        const float *LN = d.lam[FDP];
         for (int k = lane; k <= c.VI + 1 && k < KMAX_LEVELS; k += 32) {
-            S[2][k] = P[cell(a, c.col, k)];
-            S[3][k] = TM[cell(a, c.col, k)];
+            const size_t e = cell(a, c.col, k);
+            const float tm = TM[e];
+            M.sp[RPAD + k] = make_float2(a.relaxp * __ldcg(LN + e), P[e]);
+            M.rec[RPAD + k] = make_float4(0.0f, 0.0f, a.atp[k] * tm, tm);
         }
         __syncwarp();
     }
@@ -476,42 +545,69 @@ struct PresRev {
     __device__ void critical(int IS, int JS) {
         if (!act) return;
         const int lane = threadIdx.x & 31;
-        float *LD = d.lam[L_DPM], *LN = d.lam[FDP], *LQ = d.lam[L_QC];
-        for (int k = lane; k < KMAX_LEVELS; k += 32) {
-            if (k <= c.KK || k > c.VI) continue;
+        float *LD = d.lam[L_DPM], *LQ = d.lam[L_QC];
+        float4 *rec = M.rec + RPAD;
+        float2 *sp = M.sp + RPAD;
+        const int K1 = c.KK + 1, VI = c.VI;
+        for (int k = K1 + lane; k <= VI; k += 32) {
             const size_t e = cell(a, c.col, k);
-            S[0][k] = __ldcg(LD + e) + a.relaxp * __ldcg(LN + e);
-            S[1][k] = __ldcg(LQ + e);   // carry cotangents left by readers later in the row
-            LQ[e] = 0.0f;
+            sp[k].x += __ldcg(LD + e);
+            rec[k].y = __ldcg(LQ + e);   // carry cotangents left by readers later in the row
         }
         __syncwarp();
         if (lane == 0) {
-            const int KK = c.KK, VI = c.VI;
-            // back-substitution reversed, top down: cotangent of Q_k
+            // back-substitution reversed, top down: mu_k = S0_k + P_{k+1}*mu_{k+1} (cotangent of Q_k)
             float next = 0.0f;
-            for (int k = VI; k > KK; --k) {
-                const float mu = S[0][k] + next;
-                S[0][k] = mu;
-                next = S[2][k] * mu;
+            float2 x0 = sp[VI], x1 = sp[VI - 1], x2 = sp[VI - 2], x3 = sp[VI - 3];
+            for (int k = VI; k >= K1; k -= 4) {
+                const float2 y0 = sp[k - 4], y1 = sp[k - 5], y2 = sp[k - 6], y3 = sp[k - 7];
+                float mu = x0.x + next;
+                next = x0.y * mu;
+                rec[k].x = mu;
+                mu = x1.x + next;
+                next = x1.y * mu;
+                if (k - 1 >= K1) rec[k - 1].x = mu;
+                mu = x2.x + next;
+                next = x2.y * mu;
+                if (k - 2 >= K1) rec[k - 2].x = mu;
+                mu = x3.x + next;
+                next = x3.y * mu;
+                if (k - 3 >= K1) rec[k - 3].x = mu;
+                x0 = y0; x1 = y1; x2 = y2; x3 = y3;
             }
-            // elimination reversed, bottom up: cotangent of DIM_k
-            float prev = 0.0f;
-            for (int k = KK + 1; k <= VI; ++k) {
-                const float lam = S[0][k] + S[1][k] + prev;
-                const float tm = S[3][k];
-                S[1][k] = lam * tm;
-                prev = a.atp[k] * tm * lam;
+            // elimination reversed, bottom up: lam_k = mu_k + S1_k + ATP_{k-1}*TERMP_{k-1}*lam_{k-1};
+            // the cotangent of DIM_k is lam_k*TERMP_k
+            float prev = 0.0f, topp = 0.0f;
+            float4 r0 = rec[K1], r1 = rec[K1 + 1], r2 = rec[K1 + 2], r3 = rec[K1 + 3];
+            for (int k = K1; k <= VI; k += 4) {
+                const float4 t0 = rec[k + 4], t1 = rec[k + 5], t2 = rec[k + 6], t3 = rec[k + 7];
+                float lam = r0.x + r0.y + prev;
+                M.ldim[k] = lam * r0.w;
+                prev = r0.z * lam;
+                if (k == VI) topp = prev;
+                lam = r1.x + r1.y + prev;
+                if (k + 1 <= VI) M.ldim[k + 1] = lam * r1.w;
+                prev = r1.z * lam;
+                if (k + 1 == VI) topp = prev;
+                lam = r2.x + r2.y + prev;
+                if (k + 2 <= VI) M.ldim[k + 2] = lam * r2.w;
+                prev = r2.z * lam;
+                if (k + 2 == VI) topp = prev;
+                lam = r3.x + r3.y + prev;
+                if (k + 3 <= VI) M.ldim[k + 3] = lam * r3.w;
+                prev = r3.z * lam;
+                if (k + 3 == VI) topp = prev;
+                r0 = t0; r1 = t1; r2 = t2; r3 = t3;
             }
             // the top level read Q_{VI+1} of the row carry: its writer runs after this column
             const short2 w = a.rcw[c.col];
             const int wi = dirx == 0 ? w.x : w.y;
-            if (wi >= 0 && prev != 0.0f) atomicAdd(LQ + cell(a, wi * a.nj2 + c.j, VI + 1), prev);
+            if (wi >= 0 && topp != 0.0f) atomicAdd(LQ + cell(a, wi * a.nj2 + c.j, VI + 1), topp);
         }
         __syncwarp();
         const long long d1 = -(long long)IS * a.nj2, d2 = -(long long)JS;
-        for (int k = lane; k < KMAX_LEVELS; k += 32) {
-            if (k <= c.KK || k > c.VI) continue;
-            const float lD = S[1][k];
+        for (int k = K1 + lane; k <= VI; k += 32) {
+            const float lD = M.ldim[k];
             if (lD == 0.0f) continue;
             const float dz = a.dzk[k];
             atomicAdd(LD + cell(a, (int)(c.col + d1), k), lD * (a.dyk * dz / a.dxk));
@@ -524,15 +620,17 @@ struct PresRev {
         if (!act) return;
         const int lane = threadIdx.x & 31;
         const float dt = a.sit[0].dtime;
-        for (int k = lane; k < KMAX_LEVELS; k += 32) {
-            if (k <= c.KK || k > c.VI) continue;
-            d.lam[L_DIV][cell(a, c.col, k)] = S[1][k] / dt;
+        float *LQ = d.lam[L_QC];
+        for (int k = c.KK + 1 + lane; k <= c.VI; k += 32) {
+            const size_t e = cell(a, c.col, k);
+            d.lam[L_DIV][e] = M.ldim[k] / dt;
+            LQ[e] = 0.0f;   // the carry cotangents were consumed
         }
     }
 };
 
 __global__ void __launch_bounds__(AW * 32) k_adj_pressure(KArgs a, AdjArgs d, SweepGeom g) {
-    __shared__ float sm[AW][4][KMAX_LEVELS];
+    __shared__ PresShared sm[AW];
     PresRev job{a, d, sm[threadIdx.x >> 5]};
     int IS, JS;
     sweep_dir_of(d.it, IS, JS);
