@@ -133,7 +133,10 @@ struct AdjArgs {
     const float *end[3];     // UK VK WK after the W sweep
     float *lam[NLAM];        // cotangents: FU..FVEG, then DPM, DIV, row-carry Q
     const float *ptab;       // [2][2][ncols][KS]: pressure P and TERMP per i-direction (IS = +1, -1)
-    int *flags;              // reverse-sweep flags per column
+    int *flags;              // reverse-sweep flags per column (pressure)
+    // momentum sweeps: per column and level, the cotangent sent by the successor in i (slot 0)
+    // and in j (slot 1), as 8-byte words (float bits, stamp): [2][ncols][KS]
+    unsigned long long *slot;
     unsigned int *ctr;       // task counter of the launch
     int stamp;               // flag value of the launch
     int it;                  // IterationLoops of the reversed iteration
@@ -149,6 +152,18 @@ __device__ __forceinline__ void sweep_dir_of(int it, int &IS, int &JS) {
     else if (m == 1) { IS = -1; JS = -1; }
     else if (m == 2) { IS = 1; JS = -1; }
     else { IS = 1; JS = 1; }
+}
+
+// 8-byte cotangent words: float bits in the low half, the launch stamp in the high half; one
+// aligned 8-byte access is single-copy atomic, so a word that shows the stamp carries its value
+__device__ __forceinline__ unsigned long long ld_word(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_word(unsigned long long *p, float v, int stamp) {
+    const unsigned long long w = ((unsigned long long)(unsigned)stamp << 32) | __float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
 
 // task t -> (i1, j1): diagonal-major, then position (one situation)
@@ -167,8 +182,10 @@ __device__ __forceinline__ void decode(unsigned t, const SweepGeom &g, int &i1, 
 
 // The reverse wavefront task loop: tasks in reverse diagonal order; a column waits for its two
 // sweep successors (i1+1, j1) and (i1, j1+1), runs job.critical, publishes its flag (a warp
-// barrier, then a gpu-scope release by lane 0), then runs job.after.  Successors are claimed
-// earlier, so no task waits on one that is not running or done.
+// barrier, then a gpu-scope release by lane 0), then runs job.after.  Jobs with kWords instead
+// receive their successors' cotangents as stamped words (job.receive) and send their
+// predecessors' the same way inside job.critical.  Successors are claimed earlier, so no task
+// waits on one that is not running or done.
 template <class Job>
 __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, const SweepGeom &g, int IS, int JS,
                                           Job &job) {
@@ -185,16 +202,23 @@ __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, cons
         const int i = (IS == 1) ? i1 : a.nii - i1 + 1;
         const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
         job.pre(i, j, IS, JS);
+        const bool s1 = i1 < g.ia + g.ni - 1, s2 = j1 < g.ja + g.nj - 1;   // successors in the sweep
         int ok = 1;
-        if (lane == 0)
-            ok = wait_stamps((i1 < g.ia + g.ni - 1) ? d.flags + (i + IS) * a.nj2 + j : nullptr,
-                             (j1 < g.ja + g.nj - 1) ? d.flags + i * a.nj2 + (j + JS) : nullptr, d.stamp, a.err,
-                             a.wait_limit_ns);
-        ok = __shfl_sync(0xffffffffu, ok, 0);
-        __syncwarp();
-        if (ok) job.critical(IS, JS);
-        __syncwarp();     // orders every lane's writes and atomics before lane 0's release
-        if (lane == 0) st_release(d.flags + i * a.nj2 + j, d.stamp);
+        if constexpr (Job::kWords) {
+            // the successors' cotangents arrive as stamped words: no flag, no fence on the chain
+            ok = job.receive(s1, s2);
+            __syncwarp();
+            if (ok) job.critical(IS, JS, i1 > g.ia, j1 > g.ja);
+        } else {
+            if (lane == 0)
+                ok = wait_stamps(s1 ? d.flags + (i + IS) * a.nj2 + j : nullptr,
+                                 s2 ? d.flags + i * a.nj2 + (j + JS) : nullptr, d.stamp, a.err, a.wait_limit_ns);
+            ok = __shfl_sync(0xffffffffu, ok, 0);
+            __syncwarp();
+            if (ok) job.critical(IS, JS);
+            __syncwarp();     // orders every lane's writes and atomics before lane 0's release
+            if (lane == 0) st_release(d.flags + i * a.nj2 + j, d.stamp);
+        }
         if (ok) job.after(IS, JS);
         __syncwarp();
     }
@@ -245,6 +269,7 @@ struct __align__(16) MomShared {
 
 template <int COMP>
 struct MomRev {
+    static constexpr bool kWords = true;
     const KArgs &a;
     const AdjArgs &d;
     MomShared &M;
@@ -329,35 +354,96 @@ struct MomRev {
         }
         __syncwarp();
         // the products the reversed recurrence needs, off its critical path
+        float *L = d.lam[COMP];
         for (int k = c.K0 + lane; k <= c.VI; k += 32) {
             const bool ch = k > c.KK + 1;
             const float B = S[R_B][k], C = S[R_C][k], D = S[R_D][k], T = S[R_T][k];
             const float Qp = ch ? S[R_Q][k - 1] : 0.0f;
             M.bect[RPAD + k] = make_float4(B, ch ? D + C * Qp : D, ch ? C * T : 0.0f, ch ? T * T * C : 0.0f);
-            M.lrp[RPAD + k].y = a.relax * S[R_P][k];
+            // an updated level's cotangent is handed over from its new to its old value: what the
+            // later phases left is taken now, the successors' parts arrive as words
+            float l0 = 0.0f;
+            if (kkm < k) {
+                const size_t e = cell(a, c.col, k);
+                l0 = __ldcg(L + e);
+                L[e] = 0.0f;
+            }
+            M.lrp[RPAD + k] = make_float2(l0, a.relax * S[R_P][k]);
             S[R_NT2][k] = -(T * T);
             S[R_QPT][k] = Qp * T;
             S[R_PP][k] = ch ? S[R_P][k - 1] : 0.0f;
         }
+        // the cleared cells are seen cleared before any word this column sends, hence before the
+        // predecessors add the cotangents of the old values to them
+        __threadfence();
         __syncwarp();
+    }
+
+    // the successors' words of this launch for every level: added to L0 at the updated levels,
+    // to the cotangent field everywhere else (levels outside the column's solve, inactive columns)
+    __device__ int receive(bool s1, bool s2) {
+        const int lane = threadIdx.x & 31;
+        const unsigned long long *w1 = d.slot + (size_t)c.col * a.ks;
+        const unsigned long long *w2 = d.slot + ((size_t)a.ncols + c.col) * a.ks;
+        const int stamp = d.stamp;
+        float v[2] = {0.0f, 0.0f};
+        bool need[2][2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            need[r][0] = s1 && k < a.ks;
+            need[r][1] = s2 && k < a.ks;
+        }
+        unsigned long long t0 = 0;
+        for (unsigned n = 0;; ++n) {
+#pragma unroll
+            for (int r = 0; r < 2; ++r) {
+                const int k = lane + 32 * r;
+                if (need[r][0]) {
+                    const unsigned long long x = ld_word(w1 + k);
+                    if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][0] = false; }
+                }
+                if (need[r][1]) {
+                    const unsigned long long x = ld_word(w2 + k);
+                    if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][1] = false; }
+                }
+            }
+            const bool pending = need[0][0] || need[0][1] || need[1][0] || need[1][1];
+            if (!__any_sync(0xffffffffu, pending)) break;
+            if (n == 0) t0 = globaltimer_ns();
+            if ((n & 15) == 15) {
+                int bad = *(volatile int *)a.err != ERR_NONE;
+                if (!bad && globaltimer_ns() - t0 > a.wait_limit_ns) {
+                    if (lane == 0) atomicCAS(a.err, ERR_NONE, ERR_TIMEOUT);
+                    bad = 1;
+                }
+                if (__any_sync(0xffffffffu, bad)) return 0;
+            }
+            if (n > 4) __nanosleep(32);
+        }
+        asm volatile("fence.acquire.gpu;" ::: "memory");
+        float *L = d.lam[COMP];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k >= a.ks || v[r] == 0.0f) continue;
+            if (act && k >= c.K0 && k <= c.VI && kkm < k) M.lrp[RPAD + k].x += v[r];
+            else atomicAdd(L + cell(a, c.col, k), v[r]);
+        }
+        return 1;
     }
 
     // after the wait: the cotangents of the column's new values are complete (later phases and
     // both successors have added theirs); reverse the back-substitution and the recurrence and
     // send the predecessors their cotangents
-    __device__ void critical(int IS, int JS) {
-        if (!act) return;
+    __device__ void critical(int IS, int JS, bool p1, bool p2) {
         const int lane = threadIdx.x & 31;
-        float *L = d.lam[COMP];
+        if (!act) {
+            send(IS, JS, p1, p2);
+            return;
+        }
         float2 *lrp = M.lrp + RPAD, *lpq = M.lpq + RPAD;
         const float4 *bect = M.bect + RPAD;
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int k = lane + 32 * r;
-            if (k < c.K0 || k > c.VI) continue;
-            // an updated level's cotangent is handed over from its new to its old value
-            lrp[k].x = (kkm < k) ? atomicExch(L + cell(a, c.col, k), 0.0f) : 0.0f;
-        }
         __syncwarp();
         const int K0 = c.K0, VI = c.VI;
         const float relax = a.relax, r1 = 1.0f - relax;
@@ -433,24 +519,41 @@ struct MomRev {
             }
         }
         __syncwarp();
-        // the cotangents of the row (A, B, C, D) on all lanes, and those of the predecessors' new
-        // values (they run after this column)
-        const long long dP1 = -(long long)IS * a.nj2, dP2 = -(long long)JS;
+        // the cotangents of the row (A, B, C, D) on all lanes
         for (int k = K0 + lane; k <= VI; k += 32) {
             const float2 pq = lpq[k];
             const float4 e = bect[k];
             const float lP = pq.x, lQ = pq.y, T = S[R_T][k];
             const float lT = fmaf(lP, e.x, lQ * e.y);
             const float lden = lT * S[R_NT2][k];
-            const float lD = lQ * T;
             S[R_A][k] = lden;
             S[R_B][k] = lP * T;
             S[R_C][k] = lQ * S[R_QPT][k] - lden * S[R_PP][k];
-            S[R_D][k] = lD;
-            if (lD == 0.0f) continue;
-            const float g1 = lD * S[R_C1][k], g2 = lD * S[R_C2][k];
-            if (g1 != 0.0f) atomicAdd(L + cell(a, (int)(c.col + dP1), k), g1);
-            if (g2 != 0.0f) atomicAdd(L + cell(a, (int)(c.col + dP2), k), g2);
+            S[R_D][k] = lQ * T;
+        }
+        __syncwarp();
+        send(IS, JS, p1, p2);
+    }
+
+    // the cotangents of the predecessors' new values (they run after this column), for every level
+    // (zero outside the column's solve): as words to a predecessor inside the sweep, added to the
+    // cotangent field of one outside it
+    __device__ void send(int IS, int JS, bool p1, bool p2) {
+        const int lane = threadIdx.x & 31;
+        const int c1 = c.col - IS * a.nj2, c2 = c.col - JS;
+        unsigned long long *w1 = d.slot + (size_t)c1 * a.ks;
+        unsigned long long *w2 = d.slot + ((size_t)a.ncols + c2) * a.ks;
+        float *L = d.lam[COMP];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k >= a.ks) continue;
+            const float lD = (act && k >= c.K0 && k <= c.VI) ? S[R_D][k] : 0.0f;
+            const float g1 = lD != 0.0f ? lD * S[R_C1][k] : 0.0f, g2 = lD != 0.0f ? lD * S[R_C2][k] : 0.0f;
+            if (p1) st_word(w1 + k, g1, d.stamp);
+            else if (g1 != 0.0f) atomicAdd(L + cell(a, c1, k), g1);
+            if (p2) st_word(w2 + k, g2, d.stamp);
+            else if (g2 != 0.0f) atomicAdd(L + cell(a, c2, k), g2);
         }
     }
 
@@ -515,6 +618,7 @@ struct __align__(16) PresShared {
 };
 
 struct PresRev {
+    static constexpr bool kWords = false;
     const KArgs &a;
     const AdjArgs &d;
     PresShared &M;
@@ -1275,10 +1379,12 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     CK(ctx->adj_lam.ensure((size_t)NLAM * fsz));
     CK(ctx->adj_stg.ensure(3 * ssz));
     CK(ctx->adj_flags.ensure(a.ncols));
+    CK(ctx->adj_slot.ensure(2 * (size_t)a.ncols * a.ks));
     CK(ctx->adj_ctr.ensure(4));
     CK(ctx->adj_bits.ensure((size_t)nbuf * K * nevk));
     CK(cudaMemsetAsync(ctx->adj_lam.p, 0, (size_t)NLAM * fsz * sizeof(float), st));
     CK(cudaMemsetAsync(ctx->adj_flags.p, 0, a.ncols * sizeof(int), st));
+    CK(cudaMemsetAsync(ctx->adj_slot.p, 0, 2 * (size_t)a.ncols * a.ks * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)nbuf * K * nevk, st));
     if (!ctx->adj_stream) CK(cudaStreamCreateWithFlags(&ctx->adj_stream, cudaStreamNonBlocking));
     cudaStream_t st2 = ctx->adj_stream;
@@ -1293,6 +1399,7 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     for (int q = 0; q < NLAM; ++q) d.lam[q] = ctx->adj_lam.p + (size_t)q * fsz;
     d.ptab = ctx->adj_ptab.p;
     d.flags = ctx->adj_flags.p;
+    d.slot = ctx->adj_slot.p;
     d.ctr = ctx->adj_ctr.p;
     d.nwe = ctx->adj_nwe;
     const int cb = col_blocks(a);

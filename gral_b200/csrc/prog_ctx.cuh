@@ -144,6 +144,7 @@ struct gral_ctx {
     DevBuf<SitDev> adj_cksit;
     DevBuf<int> adj_ckit, adj_flags;
     DevBuf<unsigned int> adj_ctr;
+    DevBuf<unsigned long long> adj_slot;   // stamped cotangent words of the momentum reverse sweeps
     DevBuf<uint8_t> adj_bits;
     cudaStream_t adj_stream = nullptr;   // recomputation of the next segment beside the reverse sweeps
 
@@ -159,7 +160,7 @@ struct gral_ctx {
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
         adj_ckpt.release(); adj_keep.release(); adj_lam.release(); adj_ptab.release(); adj_stg.release();
-        adj_cksit.release(); adj_ckit.release(); adj_flags.release(); adj_ctr.release(); adj_bits.release();
+        adj_cksit.release(); adj_ckit.release(); adj_flags.release(); adj_ctr.release(); adj_slot.release(); adj_bits.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
         if (adj_stream) cudaStreamDestroy(adj_stream);
         if (stream) cudaStreamDestroy(stream);
