@@ -14,11 +14,12 @@
 // the W sweep ("end") and the branch taken by every lateral boundary copy, then reverses the
 // segment's iterations one by one.  Reversing one iteration (PrognosticFlowfield.cs:584-1137):
 //
-//   W, V, U momentum sweeps   reverse Gauss-Seidel wavefronts: a column waits for its two sweep
-//                             successors, reverses the relaxed back-substitution and the Thomas
+//   W, V, U momentum sweeps   reverse Gauss-Seidel wavefronts: a column receives the cotangents
+//                             of its new values from its two sweep successors (stamped 8-byte
+//                             words), reverses the relaxed back-substitution and the Thomas
 //                             recurrence (U-prognostic-microscale_1.cs:485-524) on lane 0, sends
-//                             the cotangents of its two predecessors' new values, releases its
-//                             flag, and then adds the per-level vector-Jacobian products of the
+//                             its two predecessors the cotangents of their new values the same
+//                             way, and then adds the per-level vector-Jacobian products of the
 //                             coefficient assembly (adj_level.cuh) to every other input;
 //   staggered averages        gathers (PrognosticFlowfield.cs:958-1039);
 //   velocity correction       a gather into DPM (PrognosticFlowfield.cs:904-949);
@@ -133,12 +134,12 @@ struct AdjArgs {
     const float *end[3];     // UK VK WK after the W sweep
     float *lam[NLAM];        // cotangents: FU..FVEG, then DPM, DIV, row-carry Q
     const float *ptab;       // [2][2][ncols][KS]: pressure P and TERMP per i-direction (IS = +1, -1)
-    int *flags;              // reverse-sweep flags per column (pressure)
-    // momentum sweeps: per column and level, the cotangent sent by the successor in i (slot 0)
-    // and in j (slot 1), as 8-byte words (float bits, stamp): [2][ncols][KS]
+    // per column and level, the cotangent sent by the sweep successor in i (slot 0) and in j
+    // (slot 1), as 8-byte words (float bits, launch stamp): [2][ncols][KS]
     unsigned long long *slot;
+    const int *rcr;          // per column: bit 0 (IS = +1) / bit 1 (IS = -1) set where a column reads its row carry
     unsigned int *ctr;       // task counter of the launch
-    int stamp;               // flag value of the launch
+    int stamp;               // stamp of the launch's words
     int it;                  // IterationLoops of the reversed iteration
     const uint8_t *bits;     // boundary-copy branches of the iteration: [we events + sn events][KS]
     int nwe;                 // W/E events (the S/N events follow)
@@ -166,6 +167,53 @@ __device__ __forceinline__ void st_word(unsigned long long *p, float v, int stam
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
 
+// The words of this launch sent to column col by its successors in i (s1) and in j (s2), summed per
+// level k = lane + 32*r (v[r], zero above KS).  Bounded like every wait: 0 after the time limit
+// (the error word set) or on another warp's error.
+__device__ __forceinline__ int poll_words(const KArgs &a, const AdjArgs &d, int col, bool s1, bool s2, float v[2]) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long *w1 = d.slot + (size_t)col * a.ks;
+    const unsigned long long *w2 = d.slot + ((size_t)a.ncols + col) * a.ks;
+    const int stamp = d.stamp;
+    bool need[2][2];
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const int k = lane + 32 * r;
+        v[r] = 0.0f;
+        need[r][0] = s1 && k < a.ks;
+        need[r][1] = s2 && k < a.ks;
+    }
+    unsigned long long t0 = 0;
+    for (unsigned n = 0;; ++n) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (need[r][0]) {
+                const unsigned long long x = ld_word(w1 + k);
+                if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][0] = false; }
+            }
+            if (need[r][1]) {
+                const unsigned long long x = ld_word(w2 + k);
+                if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][1] = false; }
+            }
+        }
+        const bool pending = need[0][0] || need[0][1] || need[1][0] || need[1][1];
+        if (!__any_sync(0xffffffffu, pending)) break;
+        if (n == 0) t0 = globaltimer_ns();
+        if ((n & 15) == 15) {
+            int bad = *(volatile int *)a.err != ERR_NONE;
+            if (!bad && globaltimer_ns() - t0 > a.wait_limit_ns) {
+                if (lane == 0) atomicCAS(a.err, ERR_NONE, ERR_TIMEOUT);
+                bad = 1;
+            }
+            if (__any_sync(0xffffffffu, bad)) return 0;
+        }
+        if (n > 4) __nanosleep(32);
+    }
+    asm volatile("fence.acquire.gpu;" ::: "memory");
+    return 1;
+}
+
 // task t -> (i1, j1): diagonal-major, then position (one situation)
 __device__ __forceinline__ void decode(unsigned t, const SweepGeom &g, int &i1, int &j1) {
     int lo = 0, hi = g.ndiag;
@@ -180,12 +228,12 @@ __device__ __forceinline__ void decode(unsigned t, const SweepGeom &g, int &i1, 
     j1 = g.ja + d - ioff;
 }
 
-// The reverse wavefront task loop: tasks in reverse diagonal order; a column waits for its two
-// sweep successors (i1+1, j1) and (i1, j1+1), runs job.critical, publishes its flag (a warp
-// barrier, then a gpu-scope release by lane 0), then runs job.after.  Jobs with kWords instead
-// receive their successors' cotangents as stamped words (job.receive) and send their
-// predecessors' the same way inside job.critical.  Successors are claimed earlier, so no task
-// waits on one that is not running or done.
+// The reverse wavefront task loop: tasks in reverse diagonal order; a column receives the
+// cotangents its two sweep successors (i1+1, j1) and (i1, j1+1) send it as stamped words
+// (job.receive), runs job.critical, which sends its two predecessors theirs the same way, then
+// runs job.after.  A word carries its own value, so no flag, release or fence sits between a
+// column's recurrence and its predecessors'.  Successors are claimed earlier, so no task waits on
+// one that is not running or done.
 template <class Job>
 __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, const SweepGeom &g, int IS, int JS,
                                           Job &job) {
@@ -203,22 +251,10 @@ __device__ __forceinline__ void rev_tasks(const KArgs &a, const AdjArgs &d, cons
         const int j = (JS == 1) ? j1 : a.njj - j1 + 1;
         job.pre(i, j, IS, JS);
         const bool s1 = i1 < g.ia + g.ni - 1, s2 = j1 < g.ja + g.nj - 1;   // successors in the sweep
-        int ok = 1;
-        if constexpr (Job::kWords) {
-            // the successors' cotangents arrive as stamped words: no flag, no fence on the chain
-            ok = job.receive(s1, s2);
-            __syncwarp();
-            if (ok) job.critical(IS, JS, i1 > g.ia, j1 > g.ja);
-        } else {
-            if (lane == 0)
-                ok = wait_stamps(s1 ? d.flags + (i + IS) * a.nj2 + j : nullptr,
-                                 s2 ? d.flags + i * a.nj2 + (j + JS) : nullptr, d.stamp, a.err, a.wait_limit_ns);
-            ok = __shfl_sync(0xffffffffu, ok, 0);
-            __syncwarp();
-            if (ok) job.critical(IS, JS);
-            __syncwarp();     // orders every lane's writes and atomics before lane 0's release
-            if (lane == 0) st_release(d.flags + i * a.nj2 + j, d.stamp);
-        }
+        // the successors' cotangents arrive as stamped words: no flag, no fence on the chain
+        const int ok = job.receive(s1, s2);
+        __syncwarp();
+        if (ok) job.critical(IS, JS, i1 > g.ia, j1 > g.ja);
         if (ok) job.after(IS, JS);
         __syncwarp();
     }
@@ -269,7 +305,6 @@ struct __align__(16) MomShared {
 
 template <int COMP>
 struct MomRev {
-    static constexpr bool kWords = true;
     const KArgs &a;
     const AdjArgs &d;
     MomShared &M;
@@ -383,45 +418,8 @@ struct MomRev {
     // to the cotangent field everywhere else (levels outside the column's solve, inactive columns)
     __device__ int receive(bool s1, bool s2) {
         const int lane = threadIdx.x & 31;
-        const unsigned long long *w1 = d.slot + (size_t)c.col * a.ks;
-        const unsigned long long *w2 = d.slot + ((size_t)a.ncols + c.col) * a.ks;
-        const int stamp = d.stamp;
-        float v[2] = {0.0f, 0.0f};
-        bool need[2][2];
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-            const int k = lane + 32 * r;
-            need[r][0] = s1 && k < a.ks;
-            need[r][1] = s2 && k < a.ks;
-        }
-        unsigned long long t0 = 0;
-        for (unsigned n = 0;; ++n) {
-#pragma unroll
-            for (int r = 0; r < 2; ++r) {
-                const int k = lane + 32 * r;
-                if (need[r][0]) {
-                    const unsigned long long x = ld_word(w1 + k);
-                    if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][0] = false; }
-                }
-                if (need[r][1]) {
-                    const unsigned long long x = ld_word(w2 + k);
-                    if ((int)(x >> 32) >= stamp) { v[r] += __uint_as_float((unsigned)x); need[r][1] = false; }
-                }
-            }
-            const bool pending = need[0][0] || need[0][1] || need[1][0] || need[1][1];
-            if (!__any_sync(0xffffffffu, pending)) break;
-            if (n == 0) t0 = globaltimer_ns();
-            if ((n & 15) == 15) {
-                int bad = *(volatile int *)a.err != ERR_NONE;
-                if (!bad && globaltimer_ns() - t0 > a.wait_limit_ns) {
-                    if (lane == 0) atomicCAS(a.err, ERR_NONE, ERR_TIMEOUT);
-                    bad = 1;
-                }
-                if (__any_sync(0xffffffffu, bad)) return 0;
-            }
-            if (n > 4) __nanosleep(32);
-        }
-        asm volatile("fence.acquire.gpu;" ::: "memory");
+        float v[2];
+        if (!poll_words(a, d, c.col, s1, s2, v)) return 0;
         float *L = d.lam[COMP];
 #pragma unroll
         for (int r = 0; r < 2; ++r) {
@@ -578,7 +576,7 @@ struct MomRev {
                 constexpr InDesc e = InTab<COMP>::at(q.value);
                 const float v = g[q.value];
                 if constexpr (e.f == COMP) {
-                    // the predecessors' cotangents were sent before the flag
+                    // the predecessors' cotangents were sent as words
                     if ((e.di != 0 && e.dj == 0 && e.di == -IS) || (e.di == 0 && e.dj != 0 && e.dj == -JS)) return;
                 }
                 if constexpr (e.f == FVEG) {
@@ -618,46 +616,67 @@ struct __align__(16) PresShared {
 };
 
 struct PresRev {
-    static constexpr bool kWords = false;
     const KArgs &a;
     const AdjArgs &d;
     PresShared &M;
     ColCtx c;
     bool act;
+    bool reader;                 // some later column of the row read this column's row carry
     int dirx;                    // 0: IS = +1, 1: IS = -1
 
-    // before the wait: the state-independent level records, and the cotangent of DPMNEW, which no
-    // column of this sweep changes
+    // before the wait: the state-independent level records, and the cotangents of DPMNEW and of
+    // DPM as the later phases left them (the successors' parts arrive as words)
     __device__ void pre(int i, int j, int IS, int) {
         const int lane = threadIdx.x & 31;
         c = make_col(a, i, j);
         act = (c.fl & F_ADV) != 0;
         dirx = (IS == 1) ? 0 : 1;
+        reader = act && ((d.rcr[c.col] >> dirx) & 1);
         if (!act) return;
         const size_t fsz = (size_t)a.ncols * a.ks;
         const float *P = d.ptab + (size_t)(2 * dirx) * fsz, *TM = d.ptab + (size_t)(2 * dirx + 1) * fsz;
-        const float *LN = d.lam[FDP];
+        const float *LN = d.lam[FDP], *LD = d.lam[L_DPM];
         for (int k = lane; k <= c.VI + 1 && k < KMAX_LEVELS; k += 32) {
             const size_t e = cell(a, c.col, k);
             const float tm = TM[e];
-            M.sp[RPAD + k] = make_float2(a.relaxp * __ldcg(LN + e), P[e]);
+            const float ld = (k > c.KK && k <= c.VI) ? __ldcg(LD + e) : 0.0f;
+            M.sp[RPAD + k] = make_float2(ld + a.relaxp * __ldcg(LN + e), P[e]);
             M.rec[RPAD + k] = make_float4(0.0f, 0.0f, a.atp[k] * tm, tm);
         }
         __syncwarp();
     }
 
-    __device__ void critical(int IS, int JS) {
-        if (!act) return;
+    // the successors' words: added to the cotangent of DPM at the solved levels, to the field at
+    // every other level (and everywhere in an inactive column)
+    __device__ int receive(bool s1, bool s2) {
         const int lane = threadIdx.x & 31;
-        float *LD = d.lam[L_DPM], *LQ = d.lam[L_QC];
-        float4 *rec = M.rec + RPAD;
-        float2 *sp = M.sp + RPAD;
-        const int K1 = c.KK + 1, VI = c.VI;
-        for (int k = K1 + lane; k <= VI; k += 32) {
-            const size_t e = cell(a, c.col, k);
-            sp[k].x += __ldcg(LD + e);
-            rec[k].y = __ldcg(LQ + e);   // carry cotangents left by readers later in the row
+        float v[2];
+        if (!poll_words(a, d, c.col, s1, s2, v)) return 0;
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k >= a.ks || v[r] == 0.0f) continue;
+            if (act && k > c.KK && k <= c.VI) M.sp[RPAD + k].x += v[r];
+            else atomicAdd(d.lam[L_DPM] + cell(a, c.col, k), v[r]);
         }
+        return 1;
+    }
+
+    // after the wait: the two reversed recurrences on lane 0, then the predecessors' cotangents
+    __device__ void critical(int IS, int JS, bool p1, bool p2) {
+        const int lane = threadIdx.x & 31;
+        if (!act) {
+            send(IS, JS, p1, p2);
+            return;
+        }
+        float *LQ = d.lam[L_QC];
+        float4 *rec = M.rec + RPAD;
+        const float2 *sp = M.sp + RPAD;
+        const int K1 = c.KK + 1, VI = c.VI;
+        // carry cotangents left by the columns that read this one's row carry: every one of them
+        // fenced its add before the words that led here
+        if (reader)
+            for (int k = K1 + lane; k <= VI; k += 32) rec[k].y = __ldcg(LQ + cell(a, c.col, k));
         __syncwarp();
         if (lane == 0) {
             // back-substitution reversed, top down: mu_k = S0_k + P_{k+1}*mu_{k+1} (cotangent of Q_k)
@@ -703,20 +722,45 @@ struct PresRev {
                 if (k + 3 == VI) topp = prev;
                 r0 = t0; r1 = t1; r2 = t2; r3 = t3;
             }
-            // the top level read Q_{VI+1} of the row carry: its writer runs after this column
+            // the top level read Q_{VI+1} of the row carry: its writer runs after this column and
+            // reads the add once the words that follow have reached it, so the add is fenced first
             const short2 w = a.rcw[c.col];
             const int wi = dirx == 0 ? w.x : w.y;
-            if (wi >= 0 && topp != 0.0f) atomicAdd(LQ + cell(a, wi * a.nj2 + c.j, VI + 1), topp);
+            if (wi >= 0 && topp != 0.0f) {
+                atomicAdd(LQ + cell(a, wi * a.nj2 + c.j, VI + 1), topp);
+                __threadfence();
+            }
         }
         __syncwarp();
-        const long long d1 = -(long long)IS * a.nj2, d2 = -(long long)JS;
-        for (int k = K1 + lane; k <= VI; k += 32) {
-            const float lD = M.ldim[k];
-            if (lD == 0.0f) continue;
-            const float dz = a.dzk[k];
-            atomicAdd(LD + cell(a, (int)(c.col + d1), k), lD * (a.dyk * dz / a.dxk));
-            // DPM_jm enters with +, DPM_jp with - (the reference's sign, :853-854)
-            atomicAdd(LD + cell(a, (int)(c.col + d2), k), (JS == 1 ? 1.0f : -1.0f) * lD * (a.dxk * dz / a.dyk));
+        send(IS, JS, p1, p2);
+    }
+
+    // the cotangents of the predecessors' DPM for every level (zero outside the column's solve):
+    // as words to a predecessor inside the sweep, added to the field of one outside it
+    __device__ void send(int IS, int JS, bool p1, bool p2) {
+        const int lane = threadIdx.x & 31;
+        const int c1 = c.col - IS * a.nj2, c2 = c.col - JS;
+        unsigned long long *w1 = d.slot + (size_t)c1 * a.ks;
+        unsigned long long *w2 = d.slot + ((size_t)a.ncols + c2) * a.ks;
+        float *LD = d.lam[L_DPM];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const int k = lane + 32 * r;
+            if (k >= a.ks) continue;
+            float g1 = 0.0f, g2 = 0.0f;
+            if (act && k > c.KK && k <= c.VI) {
+                const float lD = M.ldim[k];
+                if (lD != 0.0f) {
+                    const float dz = a.dzk[k];
+                    g1 = lD * (a.dyk * dz / a.dxk);
+                    // DPM_jm enters with +, DPM_jp with - (the reference's sign, :853-854)
+                    g2 = (JS == 1 ? 1.0f : -1.0f) * lD * (a.dxk * dz / a.dyk);
+                }
+            }
+            if (p1) st_word(w1 + k, g1, d.stamp);
+            else if (g1 != 0.0f) atomicAdd(LD + cell(a, c1, k), g1);
+            if (p2) st_word(w2 + k, g2, d.stamp);
+            else if (g2 != 0.0f) atomicAdd(LD + cell(a, c2, k), g2);
         }
     }
 
@@ -728,7 +772,7 @@ struct PresRev {
         for (int k = c.KK + 1 + lane; k <= c.VI; k += 32) {
             const size_t e = cell(a, c.col, k);
             d.lam[L_DIV][e] = M.ldim[k] / dt;
-            LQ[e] = 0.0f;   // the carry cotangents were consumed
+            if (reader) LQ[e] = 0.0f;   // the carry cotangents were consumed
         }
     }
 };
@@ -739,6 +783,16 @@ __global__ void __launch_bounds__(AW * 32) k_adj_pressure(KArgs a, AdjArgs d, Sw
     int IS, JS;
     sweep_dir_of(d.it, IS, JS);
     rev_tasks(a, d, g, IS, JS, job);
+}
+
+// which columns' row carry some column reads (bit 0: IS = +1, bit 1: IS = -1); rcr zeroed before
+__global__ void k_adj_readers(KArgs a, int *rcr) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.ncols) return;
+    const short2 w = a.rcw[col];
+    const int j = col % a.nj2;
+    if (w.x >= 0) atomicOr(rcr + w.x * a.nj2 + j, 1);
+    if (w.y >= 0) atomicOr(rcr + w.y * a.nj2 + j, 2);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1378,12 +1432,11 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     CK(ctx->adj_keep.ensure((size_t)nbuf * K * NKEEP * fsz));
     CK(ctx->adj_lam.ensure((size_t)NLAM * fsz));
     CK(ctx->adj_stg.ensure(3 * ssz));
-    CK(ctx->adj_flags.ensure(a.ncols));
     CK(ctx->adj_slot.ensure(2 * (size_t)a.ncols * a.ks));
+    CK(ctx->adj_rcr.ensure(a.ncols));
     CK(ctx->adj_ctr.ensure(4));
     CK(ctx->adj_bits.ensure((size_t)nbuf * K * nevk));
     CK(cudaMemsetAsync(ctx->adj_lam.p, 0, (size_t)NLAM * fsz * sizeof(float), st));
-    CK(cudaMemsetAsync(ctx->adj_flags.p, 0, a.ncols * sizeof(int), st));
     CK(cudaMemsetAsync(ctx->adj_slot.p, 0, 2 * (size_t)a.ncols * a.ks * sizeof(unsigned long long), st));
     CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)nbuf * K * nevk, st));
     if (!ctx->adj_stream) CK(cudaStreamCreateWithFlags(&ctx->adj_stream, cudaStreamNonBlocking));
@@ -1398,8 +1451,10 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     AdjArgs d{};
     for (int q = 0; q < NLAM; ++q) d.lam[q] = ctx->adj_lam.p + (size_t)q * fsz;
     d.ptab = ctx->adj_ptab.p;
-    d.flags = ctx->adj_flags.p;
     d.slot = ctx->adj_slot.p;
+    d.rcr = ctx->adj_rcr.p;
+    CK(cudaMemsetAsync(ctx->adj_rcr.p, 0, a.ncols * sizeof(int), st));
+    k_adj_readers<<<(a.ncols + 255) / 256, 256, 0, st>>>(a, ctx->adj_rcr.p);
     d.ctr = ctx->adj_ctr.p;
     d.nwe = ctx->adj_nwe;
     const int cb = col_blocks(a);

@@ -136,15 +136,16 @@ struct gral_ctx {
     std::vector<SitDev> h_sit;
     std::vector<int> h_act;
     // discrete adjoint (gral_prog_vjp_forward / gral_prog_vjp): checkpoints of the forward state,
-    // the states kept for one checkpoint segment, cotangent fields, reverse-sweep flags
+    // the states kept for one checkpoint segment, cotangent fields, reverse-sweep words
     bool adj_ready = false;
     int adj_iters = 0, adj_every = 0, adj_nwe = 0, adj_nsn = 0;
     double adj_ms_forward = 0.0;
     DevBuf<float> adj_ckpt, adj_keep, adj_lam, adj_ptab, adj_stg;
     DevBuf<SitDev> adj_cksit;
-    DevBuf<int> adj_ckit, adj_flags;
+    DevBuf<int> adj_ckit;
     DevBuf<unsigned int> adj_ctr;
-    DevBuf<unsigned long long> adj_slot;   // stamped cotangent words of the momentum reverse sweeps
+    DevBuf<unsigned long long> adj_slot;   // stamped cotangent words of the reverse sweeps
+    DevBuf<int> adj_rcr;                   // per column: whose row carry some column reads
     DevBuf<uint8_t> adj_bits;
     cudaStream_t adj_stream = nullptr;   // recomputation of the next segment beside the reverse sweeps
 
@@ -160,7 +161,7 @@ struct gral_ctx {
         flags.release(); misc.release(); diag.release(); bcl.release(); counts.release();
         counters.release();
         adj_ckpt.release(); adj_keep.release(); adj_lam.release(); adj_ptab.release(); adj_stg.release();
-        adj_cksit.release(); adj_ckit.release(); adj_flags.release(); adj_ctr.release(); adj_slot.release(); adj_bits.release();
+        adj_cksit.release(); adj_ckit.release(); adj_ctr.release(); adj_slot.release(); adj_rcr.release(); adj_bits.release();
         for (auto &e : ev) if (e) cudaEventDestroy(e);
         if (adj_stream) cudaStreamDestroy(adj_stream);
         if (stream) cudaStreamDestroy(stream);
