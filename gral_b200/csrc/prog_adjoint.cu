@@ -155,18 +155,6 @@ __device__ __forceinline__ void sweep_dir_of(int it, int &IS, int &JS) {
     else { IS = 1; JS = 1; }
 }
 
-// 8-byte cotangent words: float bits in the low half, the launch stamp in the high half; one
-// aligned 8-byte access is single-copy atomic, so a word that shows the stamp carries its value
-__device__ __forceinline__ unsigned long long ld_word(const unsigned long long *p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_word(unsigned long long *p, float v, int stamp) {
-    const unsigned long long w = ((unsigned long long)(unsigned)stamp << 32) | __float_as_uint(v);
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
-}
-
 // The words of this launch sent to column col by its successors in i (s1) and in j (s2), summed per
 // level k = lane + 32*r (v[r], zero above KS).  Bounded like every wait: 0 after the time limit
 // (the error word set) or on another warp's error.

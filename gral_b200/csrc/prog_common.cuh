@@ -244,6 +244,19 @@ __device__ __forceinline__ int ld_relaxed(const int *p) {
     return v;
 }
 
+// 8-byte words of a value and a stamp: float bits in the low half, the stamp in the high half.
+// One aligned 8-byte access is single-copy atomic, so a word that shows the stamp carries its
+// value, with no flag, release or fence between the writer's store and the reader's use.
+__device__ __forceinline__ unsigned long long ld_word(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_word(unsigned long long *p, float v, int stamp) {
+    const unsigned long long w = ((unsigned long long)(unsigned)stamp << 32) | __float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+
 // Spin (one thread) until both predecessor flags hold at least `stamp` (a null flag has no
 // predecessor).  The two flags are polled with relaxed loads, so their round trips overlap, and
 // one fence.acquire follows: a strong read followed by an acquire fence is an acquire pattern, so
