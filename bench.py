@@ -777,7 +777,7 @@ def run_ours(args, rank, world):
         instm = instances_measure(args.instances, args.instances_iters, args.instances_concurrent)
     adjm = None
     if extras and not args.no_adjoint:
-        adjm = adjoint_measure()
+        adjm = adjoint_measure(args.adjoint_iters, args.adjoint_every)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -834,6 +834,8 @@ def main():
     ap.add_argument("--instances-iters", type=int, default=100, help="SIMPLE iterations per uneven-domain instance")
     ap.add_argument("--instances-concurrent", type=int, default=16, help="slots of the packed uneven-domain run")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the discrete-adjoint measurement")
+    ap.add_argument("--adjoint-iters", type=int, default=200, help="unrolled iterations of the adjoint measurement")
+    ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint spacing of the adjoint measurement")
     ap.add_argument("--no-to-stop", action="store_true", help="skip the weather set solved to its stop rule")
     ap.add_argument("--ref-iters", type=int, default=4, help="SIMPLE iterations per reference-arm step")
     args = ap.parse_args()
