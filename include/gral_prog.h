@@ -422,10 +422,12 @@ void gral_prog_destroy(gral_ctx *ctx);
  * GRAL_EINVAL; an error already pending in the CUDA runtime on entry returns GRAL_ECUDA and is
  * left pending for the caller.  The first call on a device looks up that array's device address
  * (with the device current) and keeps it for the life of the process, so do not call it on a
- * device after cudaDeviceReset of that device; make that first call before any stream capture.
- * All calls on a device share the array, so calls that overlap on the GPU (two host threads, or
- * two streams) race and may return wrong counts: serialise them.  The call synchronises `stream`
- * and returns after the counts are on the host. */
+ * device after cudaDeviceReset of that device.  Never call it while `stream` is capturing, nor
+ * while any stream is capturing in the global capture mode: every call copies the counts into
+ * pageable host memory and synchronises `stream`, which fails under capture (and in the global
+ * mode can invalidate another thread's capture).  All calls on a device share the array, so calls
+ * that overlap on the GPU (two host threads, or two streams) race and may return wrong counts:
+ * serialise them.  The call synchronises `stream` and returns after the counts are on the host. */
 #define GRAL_NOALLOC_MAX_ROWS 4096
 int gral_prog_check_speeds_noalloc(int32_t nii, int32_t njj, int32_t nkk, int32_t vert_cells_ff,
                                    double geschw_max, const float *uk, const float *vk,
