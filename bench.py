@@ -676,6 +676,18 @@ def adjoint_measure(iterations: int = 200, every: int = 20, n: int = 200):
         J, g = prep.misfit_and_cotangent(idx, tgt, f.uk, f.vk, f.wk, np.float32)
         d_veg, d_uk0, d_vk0, d_wk0, st = s.vjp(*g)
         d_veg, d_uk0, d_vk0, d_wk0, st = s.vjp(*g)   # second call timed (first one pays the allocations)
+        # every iteration's states kept on the device by the forward: nothing recomputed
+        fa = f0.copy()
+        s.vjp_forward(p, dom.static, fa, iterations, 0)
+        s.vjp(*g)
+        ga = s.vjp(*g)
+        sta = ga[4]
+        keep_all = {"forward_ms": round(sta["ms_forward"], 2), "vjp_ms": round(sta["ms_total"], 2),
+                    "reverse_ms": round(sta["ms_reverse"], 2),
+                    "cost_multiple_of_forward": round((sta["ms_forward"] + sta["ms_total"]) / sta["ms_forward"], 3),
+                    "cost_multiple_of_checkpointed_forward": round((sta["ms_forward"] + sta["ms_total"]) / st["ms_forward"], 3),
+                    "kept_bytes": int(iterations * 10 * (dom.nii + 2) * (dom.njj + 2) * ((dom.kadvmax + 9) // 8 * 8) * 4),
+                    "grad_rel_l2_vs_checkpointed": float(np.linalg.norm(ga[0] - d_veg) / max(np.linalg.norm(d_veg), 1e-30))}
     inflow = prep.inflow_gradient(dom, sit, d_uk0.astype(np.float64), d_vk0.astype(np.float64))
     fwd = st["ms_forward"]
     return {"workload": f"{n}x{n}x{dom.vert_cells_ff} at 2 m, {len(dom.buildings)} buildings, VEG over "
@@ -687,7 +699,7 @@ def adjoint_measure(iterations: int = 200, every: int = 20, n: int = 200):
             "reverse_ms": round(st["ms_reverse"], 2),
             "cost_multiple_of_forward": round((fwd + st["ms_total"]) / fwd, 3),
             "cost_multiple_of_plain_solve": round((fwd + st["ms_total"]) / plain_ms, 3),
-            "grad_norm_veg": float(np.linalg.norm(d_veg)), "dJ_dinflow": inflow,
+            "grad_norm_veg": float(np.linalg.norm(d_veg)), "dJ_dinflow": inflow, "keep_all": keep_all,
             "checks": "GPU gradients against FP64 central differences (20 directions, 32x32, 20 iterations) and "
                       "the FP64 tape gradient in tests/test_adjoint_gpu.py"}
 

@@ -1358,7 +1358,8 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
     if (!p || !s || !f) return fail(ctx, GRAL_EINVAL, "null argument");
     if (p->turbulence_model != 1 || p->simd_width != 8 || p->quantise != 0)
         return fail(ctx, GRAL_EINVAL, "the adjoint differentiates turbulence model 1, parity width 8, quantise 0");
-    if (iterations < 1 || checkpoint_every < 1) return fail(ctx, GRAL_EINVAL, "iterations and checkpoint_every must be >= 1");
+    if (iterations < 1 || checkpoint_every < 0)
+        return fail(ctx, GRAL_EINVAL, "iterations must be >= 1 and checkpoint_every >= 0");
     ctx->adj_ready = false;
     gral_params q = *p;
     q.iteration_steps_min = iterations;
@@ -1371,15 +1372,33 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
     CK_RC(plain_schedule_default(ctx));
     const KArgs &a = ctx->ka;
     const size_t fsz = (size_t)a.ncols * a.ks;
-    const int nck = (iterations + checkpoint_every - 1) / checkpoint_every;
-    CK(ctx->adj_ckpt.ensure((size_t)nck * NCKPT * fsz));
-    CK(ctx->adj_cksit.ensure(nck));
-    CK(ctx->adj_ckit.ensure(nck));
     cudaStream_t st = ctx->stream;
-    CK(cudaEventRecord(ctx->ev[0], st));
-    for (int it = 0; it < iterations; ++it) {
-        if (it % checkpoint_every == 0) CK_RC(save_checkpoint(ctx, it / checkpoint_every));
-        CK_RC(forward_iteration(ctx, nullptr, nullptr, st));
+    int nev[2] = {0, 0};
+    CK(cudaMemcpy(&nev[0], ctx->bc.we_ptr + a.nj2, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&nev[1], ctx->bc.sn_ptr + a.nii + 2, sizeof(int), cudaMemcpyDeviceToHost));
+    ctx->adj_nwe = nev[0];
+    ctx->adj_nsn = nev[1];
+    if (checkpoint_every == 0) {
+        // every iteration's kept states (and boundary branches) stay on the device: gral_prog_vjp
+        // reverses them without recomputing anything
+        const size_t nevk = (size_t)std::max(nev[0] + nev[1], 1) * a.ks;
+        CK(ctx->adj_keep.ensure((size_t)iterations * NKEEP * fsz));
+        CK(ctx->adj_bits.ensure((size_t)iterations * nevk));
+        CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)iterations * nevk, st));
+        CK(cudaEventRecord(ctx->ev[0], st));
+        for (int it = 0; it < iterations; ++it)
+            CK_RC(forward_iteration(ctx, ctx->adj_keep.p + (size_t)it * NKEEP * fsz, ctx->adj_bits.p + (size_t)it * nevk,
+                                    st));
+    } else {
+        const int nck = (iterations + checkpoint_every - 1) / checkpoint_every;
+        CK(ctx->adj_ckpt.ensure((size_t)nck * NCKPT * fsz));
+        CK(ctx->adj_cksit.ensure(nck));
+        CK(ctx->adj_ckit.ensure(nck));
+        CK(cudaEventRecord(ctx->ev[0], st));
+        for (int it = 0; it < iterations; ++it) {
+            if (it % checkpoint_every == 0) CK_RC(save_checkpoint(ctx, it / checkpoint_every));
+            CK_RC(forward_iteration(ctx, nullptr, nullptr, st));
+        }
     }
     CK(cudaEventRecord(ctx->ev[1], st));
     CK(cudaGetLastError());
@@ -1392,11 +1411,6 @@ int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static
     if (herr == ERR_TIMEOUT) return fail(ctx, GRAL_ETIMEDOUT, "a wavefront wait exceeded its time limit");
     ctx->it_host = iterations + 1;
     CK_RC(gral_prog_store(ctx, f, nullptr));
-    int nev[2] = {0, 0};
-    CK(cudaMemcpy(&nev[0], ctx->bc.we_ptr + a.nj2, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&nev[1], ctx->bc.sn_ptr + a.nii + 2, sizeof(int), cudaMemcpyDeviceToHost));
-    ctx->adj_nwe = nev[0];
-    ctx->adj_nsn = nev[1];
     CK_RC(pressure_tables(ctx));
     ctx->adj_iters = iterations;
     ctx->adj_every = checkpoint_every;
@@ -1411,11 +1425,14 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     CK(cudaSetDevice(ctx->device));
     KArgs &a = ctx->ka;
     cudaStream_t st = ctx->stream;
-    const int K = ctx->adj_every, N = ctx->adj_iters;
+    const int N = ctx->adj_iters;
+    const bool all = ctx->adj_every == 0;            // every iteration's states kept by the forward
+    const int K = all ? N : ctx->adj_every;
     const size_t fsz = (size_t)a.ncols * a.ks, ssz = (size_t)a.ncols * (a.nkk + 2);
     const int nev = ctx->adj_nwe + ctx->adj_nsn;
     const int nseg = (N + K - 1) / K;
     const int nbuf = nseg > 1 ? 2 : 1;     // the next segment is recomputed while this one is reversed
+    // (with all states kept there is one segment, and nothing to recompute)
     const size_t nevk = (size_t)std::max(nev, 1) * a.ks;
     CK(ctx->adj_keep.ensure((size_t)nbuf * K * NKEEP * fsz));
     CK(ctx->adj_lam.ensure((size_t)NLAM * fsz));
@@ -1426,7 +1443,7 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     CK(ctx->adj_bits.ensure((size_t)nbuf * K * nevk));
     CK(cudaMemsetAsync(ctx->adj_lam.p, 0, (size_t)NLAM * fsz * sizeof(float), st));
     CK(cudaMemsetAsync(ctx->adj_slot.p, 0, 2 * (size_t)a.ncols * a.ks * sizeof(unsigned long long), st));
-    CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)nbuf * K * nevk, st));
+    if (!all) CK(cudaMemsetAsync(ctx->adj_bits.p, 0, (size_t)nbuf * K * nevk, st));
     if (!ctx->adj_stream) CK(cudaStreamCreateWithFlags(&ctx->adj_stream, cudaStreamNonBlocking));
     cudaStream_t st2 = ctx->adj_stream;
     StageLam L{ctx->adj_stg.p, ctx->adj_stg.p + ssz, ctx->adj_stg.p + 2 * ssz};
@@ -1463,9 +1480,11 @@ int gral_prog_vjp(gral_ctx *ctx, const float *dj_duk, const float *dj_dvk, const
     auto recompute = [&](int sg) -> int {
         if (sg + nbuf < nseg) CK(cudaStreamWaitEvent(st2, E(sg + nbuf, 3), 0));   // that buffer's last reader
         CK(cudaEventRecord(E(sg, 0), st2));
-        CK_RC(restore_checkpoint(ctx, sg, st2));
-        const int n = std::min(K, N - sg * K);
-        for (int q = 0; q < n; ++q) CK_RC(forward_iteration(ctx, keep_of(sg, q), bits_of(sg, q), st2));
+        if (!all) {
+            CK_RC(restore_checkpoint(ctx, sg, st2));
+            const int n = std::min(K, N - sg * K);
+            for (int q = 0; q < n; ++q) CK_RC(forward_iteration(ctx, keep_of(sg, q), bits_of(sg, q), st2));
+        }
         CK(cudaEventRecord(E(sg, 1), st2));
         return GRAL_OK;
     };

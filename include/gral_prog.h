@@ -374,8 +374,13 @@ int gral_prog_prep_last_ms(gral_ctx *ctx, double *kernel_ms);
 /* Runs `iterations` SIMPLE iterations of one situation (p, s, f as for gral_prog_solve; p's
  * iteration limits are replaced by `iterations`, post_diagnostic is ignored), keeping the state
  * every `checkpoint_every` iterations on the device, and writes the final fields to f.  The
- * checkpoints stay for gral_prog_vjp until the next load of the context.  GRAL_EINVAL for another
- * model, parity width or rounding, or a batched layout. */
+ * checkpoints stay for gral_prog_vjp until the next load of the context; gral_prog_vjp recomputes
+ * each segment from its checkpoint.  checkpoint_every = 0 keeps instead every iteration's states
+ * (ten fields of (NII+2)*(NJJ+2)*KS floats per iteration, KS = KADVMAX+2 rounded up to a multiple
+ * of 8: 52 MB on a 200x200 grid with KS 32, plus the boundary-copy branches), and gral_prog_vjp
+ * recomputes nothing
+ * (GRAL_ENOMEM when they do not fit).  GRAL_EINVAL for another model, parity width or rounding, a
+ * batched layout, or a negative spacing. */
 int gral_prog_vjp_forward(gral_ctx *ctx, const gral_params *p, const gral_static *s, gral_fields *f,
                           int32_t iterations, int32_t checkpoint_every);
 

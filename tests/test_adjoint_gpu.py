@@ -99,10 +99,12 @@ def test_vjp_does_not_depend_on_the_checkpoint_spacing(gpu_required):
     O.solve(p, dom.static, fo)
     idx, tgt = prep.probe_misfit(dom, fo, n_probes=40, seed=6)
     _, g = prep.misfit_and_cotangent(idx, tgt, fo.uk, fo.vk, fo.wk)
-    outs = [gpu_vjp(dom, p, f, n, k, g)[1] for k in (1, 4, 9)]
+    # 0: every iteration's states kept by the forward, nothing recomputed
+    outs = [gpu_vjp(dom, p, f, n, k, g)[1] for k in (1, 4, 9, 0)]
     for o in outs[1:]:
         for a, b in zip(o[:4], outs[0][:4]):
             assert rel_l2(a, b) <= 1e-5
+    assert outs[3][4]["ms_recompute"] < outs[1][4]["ms_recompute"]
 
 
 def test_vjp_rejects_other_configurations_and_order(gpu_required):
@@ -119,3 +121,7 @@ def test_vjp_rejects_other_configurations_and_order(gpu_required):
             with pytest.raises(GralError) as e:
                 s.vjp_forward(p, dom.static, f.copy(), 3, 1)
             assert e.value.code == GRAL_EINVAL
+        p = dom.params(sit, iterations=3, model=1, quantise=0)
+        with pytest.raises(GralError) as e:   # a negative checkpoint spacing
+            s.vjp_forward(p, dom.static, f.copy(), 3, -1)
+        assert e.value.code == GRAL_EINVAL
