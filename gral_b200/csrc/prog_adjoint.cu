@@ -196,7 +196,6 @@ __device__ __forceinline__ int poll_words(const KArgs &a, const AdjArgs &d, int 
             }
             if (__any_sync(0xffffffffu, bad)) return 0;
         }
-        if (n > 4) __nanosleep(32);
     }
     asm volatile("fence.acquire.gpu;" ::: "memory");
     return 1;
